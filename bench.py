@@ -1,0 +1,338 @@
+"""Benchmark of the explicit Euler step on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1|0]
+
+Workload (default, --config 1): the plain single instance with two species (electron,
+photon) of 64 log p bins x 16 u bins = 1024 states each; FP32 gain tensor 1024 x 1,048,576
+per output species (8.6 GB, streamed from HBM every step, larger than L2), flux, loss and
+emission as in the config recipe (dtb/synth.py). A step is one Euler step. --config 0 is the
+FP64 N_s = 128 case (L2-resident, launch-bound).
+
+value: Euler steps/s over the timed steps, inputs resident in HBM, device-timed with CUDA
+events on the library's stream; N GPUs run independent replicas (weak scaling) and the
+whole-job value is the sum over ranks (total steps / max time over ranks).
+e2e: the same steps through the public API with host buffers: every step uploads f from
+pinned host memory, steps, and reads f back (dtb_set_f / dtb_step / dtb_get_f).
+roofline: the gain kernel (dominant), algorithmic bytes = every G element read once per
+step, duration from CUDA events around each gain launch in the timed region.
+cpu_baseline / --impl reference: the FP64 oracle port timed on the host cores with OpenMP on
+a bounded sample (a subset of gain rows scaled to the full row count, plus the full O(N^2)
+rest), reported in steps/s.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "diplodocustransport.jl_b200"))
+
+METRIC = "steps/s & p99 latency, batched BF16-split vs plain FP64, at ≤1e-5 rel err"
+
+
+def _env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic(name: str):
+    """dram bytes per launch recorded from an ncu capture in profiles/<name> (or None)."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+def _smi_id(local: int) -> str:
+    """nvidia-smi id of the torch device (UUID when torch exposes it, else the index)."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(local)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: str):
+        self.gpu = gpu
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p is not None:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            parts = [x.strip() for x in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(config: int, device: str, host_sample_rows=None):
+    from dtb import synth
+    if config == 1:
+        if host_sample_rows:
+            return synth.config1(seed=1, gain_on_device=False, gain_rows=host_sample_rows), "f32"
+        return synth.config1(seed=1, gain_on_device=True, device=device), "f32"
+    if config == 0:
+        return synth.config0(seed=0), "f64"
+    raise SystemExit(f"unknown --config {config}")
+
+
+def cpu_sample(w, dtype: str, budget_s: float = 15.0):
+    """Oracle port on the host cores: time a sample of gain rows (FP64) plus the O(N^2) rest,
+    scale the rows to the full count; returns (steps/s, cores, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    ps = w.ps
+    ns_list = ps.species_sizes
+    n_rows_total = sum(ns_list[g.out_sp] for g in w.binm.gains)
+    off = ps.momentum_species_offset
+    f0 = np.asarray(w.f0, dtype=np.float64)
+    # rows of the first gain block as FP64 host arrays
+    g0 = w.binm.gains[0]
+    n1, n2 = ns_list[g0.in1_sp], ns_list[g0.in2_sp]
+    row_bytes = n1 * n2 * 8
+    n_sample = int(max(1, min(np.asarray(g0.G).shape[0] if not hasattr(g0.G, "is_cuda") else ns_list[g0.out_sp],
+                              (2 << 30) // row_bytes)))
+    G = g0.G
+    if hasattr(G, "is_cuda"):
+        Gs = G[:n_sample].double().cpu().numpy()
+    else:
+        Gs = np.ascontiguousarray(np.asarray(G)[:n_sample], dtype=np.float64)
+    f1, f2 = f0[off[g0.in1_sp]:off[g0.in1_sp] + n1], f0[off[g0.in2_sp]:off[g0.in2_sp] + n2]
+    oracle.gain_rows(Gs, 0, 1, f1, f2)  # warm
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        oracle.gain_rows(Gs, 0, n_sample, f1, f2)
+        reps += 1
+        if time.perf_counter() - t0 > budget_s * 0.8 or reps >= 50:
+            break
+    t_rows = (time.perf_counter() - t0) / reps / n_sample
+    # the rest of a step (flux, emission, loss, update) with the gain rows removed
+    from dtb.structs import LossBlock  # noqa: F401
+    ops = oracle.BlockedOperands(ns_list, ps.n_space, [], w.binm.losses, w.emim.blocks, w.fluxm.F_Flux,
+                                 1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj)
+    t1 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t1 < budget_s * 0.2 and k < 200:
+        ops.step(f0, 1.0, 1)
+        k += 1
+    t_rest = (time.perf_counter() - t1) / k
+    t_step = t_rows * n_rows_total + t_rest
+    desc = (f"FP64 oracle (C, OpenMP): {n_sample} of {n_rows_total} gain rows x {reps} reps scaled to all rows, "
+            f"plus {k} full steps without gain")
+    return 1.0 / t_step, oracle.num_threads(), desc
+
+
+def run_reference(args):
+    rank, local, world = _env_rank()
+    if rank != 0:
+        return 0
+    # host-only workload: a sample of gain rows is all the timing needs
+    w, dtype = build_workload(args.config, "cpu", host_sample_rows=256)
+    v, cores, desc = cpu_sample(w, dtype, budget_s=20.0)
+    value = v
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config_dict(args.config, w),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def _config_dict(config: int, w):
+    sizes = w.ps.species_sizes
+    if config == 1:
+        return {"workload": "plain single instance (config 1): 2 species x 1024 states (64 log p x 16 u), "
+                            "FP32 gain 2 x 1024 x 1048576, 2000-step run shape",
+                "species_states": sizes, "precision": "FP32", "l2": "inputs larger than L2 (8.6 GB gain)"}
+    return {"workload": "plain single instance (config 0): 2 species x 128 states (16 log p x 8 u), FP64",
+            "species_states": sizes, "precision": "FP64",
+            "l2": "operators (34 MB) fit in L2; no flush between steps (launch/L2-bound case)"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from dtb import _lib
+    from dtb.stepping import ForwardEulerStruct
+    rank, local, world = _env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    w, dtype = build_workload(args.config, f"cuda:{local}")
+    stream = torch.cuda.Stream()
+    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm,
+                           Precision=np.float32 if dtype == "f32" else np.float64, device=local,
+                           stream=stream.cuda_stream)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_sample(w, dtype, budget_s=15.0)
+    # the library holds its own copy of G
+    w.binm.gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, None) for g in w.binm.gains]
+    torch.cuda.empty_cache()
+    L = m.L
+    K, W = args.steps, args.warmup
+    scales = np.ones(K)
+    # warm-up (also captures graphs)
+    m.run(np.ones(W))
+    lps = _lib.ctypes.c_int32()
+    L.dtb_launches_per_step(m.ctx, _lib.ctypes.byref(lps))
+    # ---- timed region: device resident, gain kernel timed per launch
+    use_profile = args.config == 1
+    L.dtb_set_profiling(m.ctx, 1 if use_profile else 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(_smi_id(local)) as cs:
+        e0.record(stream)
+        m.run(scales)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    avg_ms = _lib.ctypes.c_double()
+    bpl = _lib.ctypes.c_double()
+    L.dtb_gain_kernel_stats(m.ctx, _lib.ctypes.byref(avg_ms), _lib.ctypes.byref(bpl))
+    L.dtb_set_profiling(m.ctx, 0)
+    # ---- e2e: host buffers through the public API every step
+    n = w.ps.n_state
+    f_host = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    f_host[:] = m.f
+    K2 = K
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_wall0 = time.perf_counter()
+    e2.record(stream)
+    for _ in range(K2):
+        m.f = f_host
+        m(0.0, 1e30, m.dt0, 0)
+        f_host[:] = m.f
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    t_wall = time.perf_counter() - t_wall0
+    ms_e2e = max(ms_e2e, 0.0)
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    value = world * K / (ms / 1e3)
+    e2e_value = world * K2 / (ms_e2e / 1e3)
+    esz = 4 if dtype == "f32" else 8
+    peak, peak_kind = _peaks()
+    achieved = bpl.value / (avg_ms.value / 1e3) / 1e9 if avg_ms.value > 0 else None
+    traffic = _profile_traffic("gain_stream_f32_config1.md") if args.config == 1 else None
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": dtype, "data": "synthetic (seeded; no collision data files)",
+            "config": dict(_config_dict(args.config, w), parallelism=f"replicas x{world}"),
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": n * esz,
+                    "d2h_bytes_per_step": n * esz, "wall_s": t_wall},
+            "gpu_launches": int(lps.value) * K,
+            "roofline": {"bound": "hbm", "kernel": "gain_stream", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": bpl.value,
+                         "avg_launch_ms": avg_ms.value},
+            "clocks": cs.summary()}
+    if cpu is not None:
+        v, cores, desc = cpu
+        line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc}
+    m.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1153 @@
+// C ABI of libdtb.so: context, operator uploads and re-layout, stepping, Solve loop.
+//
+// The context plays the role of ForwardEulerStruct (SteppingStructs.jl:2-102) for the B200
+// backend: it owns the operators in device memory and the device state. The functor
+// (SteppingMethods.jl:12-107) is dtb_step; Solve (Solver.jl:1-64) is dtb_solve, which keeps
+// the reference's host-side dt logic and replays captured CUDA graphs between save points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "dtb_internal.h"
+
+namespace dtb {
+thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+}  // namespace dtb
+
+using namespace dtb;
+
+#define DTB_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" + \
+                      std::to_string(__LINE__) + ")");                                        \
+            return e_ == cudaErrorMemoryAllocation ? DTB_ENOMEM : DTB_ECUDA;                  \
+        }                                                                                     \
+    } while (0)
+
+#define DTB_CHECK(cond, code, msg) \
+    do {                           \
+        if (!(cond)) {             \
+            set_error(msg);        \
+            return (code);         \
+        }                          \
+    } while (0)
+
+namespace {
+
+constexpr int kProfRing = 256;
+constexpr int64_t kMaxScheduleSteps = 100000000;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+struct GainStage {
+    int out, in1, in2;
+    std::vector<double> host;  // [no][n1][n2], FP64 sum of all host uploads
+    std::vector<std::pair<const void*, int>> dev_src;  // device sources (pointer, dtype), added in order
+};
+
+struct EmiPiece {
+    int64_t row0, nrows, col0, ncols;
+    std::vector<double> data;  // row-major
+};
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+struct dtb_ctx {
+    dtb_dims dims{};
+    dtb_opts opts{};
+    int ns = 0;
+    int64_t sz[DTB_MAX_SPECIES]{};
+    int64_t off[DTB_MAX_SPECIES + 1]{};
+    int64_t offp[DTB_MAX_SPECIES + 1]{};
+    int64_t n_mom = 0, n_state = 0;
+    int n_space = 1;
+    int prec = DTB_F64;
+    size_t esz = 8;
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // host staging
+    std::map<std::tuple<int, int, int>, GainStage> gains;
+    std::map<std::pair<int, int>, std::vector<double>> losses;
+    std::vector<EmiPiece> emis;
+    std::vector<int64_t> flux_r, flux_c;
+    std::vector<double> flux_v;
+    std::vector<double> Ap, Vol, f_init, inj;
+    bool have_vectors = false;
+    bool committed = false;
+
+    // device memory
+    std::vector<void*> allocs;
+    size_t dev_bytes = 0;
+    void* G_all = nullptr;
+    double gain_bytes = 0;  // algorithmic gain bytes per step (one read of every G element)
+    GainUnit* units = nullptr;
+    int n_units = 0;
+    int gain_grid = 0;
+    int f_smem_len = 0;
+    int* unit_ptr = nullptr;
+    double* partial = nullptr;
+    void* f_buf[2] = {nullptr, nullptr};
+    void* f_init_dev = nullptr;
+    int cur = 0;
+    double* dt_arr = nullptr;
+    long long hist_cap = 65536;
+    unsigned long long* ctr = nullptr;
+    unsigned long long host_ctr = 0;
+    StepDiagDev* hist = nullptr;
+    double* blk_red = nullptr;
+    unsigned* ticket = nullptr;
+    int* err = nullptr;
+    int* sp_off_dev = nullptr;
+    double* mom_w = nullptr;
+    double* mom_out = nullptr;
+    int sp_off_host[2 * DTB_MAX_SPECIES + 2]{};
+    RowOps<double> ops_d{};
+    RowOps<float> ops_f{};
+    bool has_bin = false, has_emi = false;
+
+    // pinned staging
+    double* pin_dt = nullptr;
+    StepDiagDev* pin_hist = nullptr;
+    int* pin_err = nullptr;
+    float* pin_f32 = nullptr;  // FP32 state staging for dtb_get_f / dtb_set_f
+
+    // graphs
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 16;
+    int graph_verbose = -1;
+
+    // profiling
+    bool profiling = false;
+    double prof_ms = 0.0;
+    long long prof_n = 0;
+    int prof_pending = 0;
+    std::vector<cudaEvent_t> ev;
+
+    template <typename P>
+    int alloc(P** p, size_t bytes) {
+        void* q = nullptr;
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMalloc(&q, bytes);
+        if (e != cudaSuccess) {
+            set_error("cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+            return DTB_ENOMEM;
+        }
+        allocs.push_back(q);
+        dev_bytes += bytes;
+        *p = reinterpret_cast<P*>(q);
+        return DTB_OK;
+    }
+    void free_all() {
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        dev_bytes = 0;
+    }
+};
+
+#define DTB_TRY(expr)              \
+    do {                           \
+        int rc_ = (expr);          \
+        if (rc_ != DTB_OK) return rc_; \
+    } while (0)
+
+extern "C" {
+
+int32_t dtb_abi_version(void) { return DTB_ABI_VERSION; }
+
+const char* dtb_last_error(void) { return dtb::g_err.c_str(); }
+
+int32_t dtb_device_count(int32_t* n) {
+    DTB_CHECK(n, DTB_EINVAL, "dtb_device_count: null output");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        *n = 0;
+        set_error(std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+        return DTB_ENODEV;
+    }
+    *n = c;
+    return DTB_OK;
+}
+
+int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out) {
+    DTB_CHECK(dims && opts && out, DTB_EINVAL, "dtb_create: null argument");
+    *out = nullptr;
+    DTB_CHECK(dims->n_species >= 1 && dims->n_species <= DTB_MAX_SPECIES, DTB_EINVAL,
+              "dtb_create: n_species must be in [1, 16]");
+    DTB_CHECK(dims->n_space >= 1, DTB_EINVAL, "dtb_create: n_space must be >= 1");
+    DTB_CHECK(opts->precision == DTB_F64 || opts->precision == DTB_F32, DTB_EINVAL,
+              "dtb_create: precision must be DTB_F64 or DTB_F32 for the plain method");
+    DTB_CHECK(opts->index_base == 0 || opts->index_base == 1, DTB_EINVAL, "dtb_create: index_base must be 0 or 1");
+    DTB_CHECK(opts->batch <= 1, DTB_EINVAL, "dtb_create: the plain method takes batch 1");
+    DTB_CHECK(std::isfinite(opts->dt0) && opts->dt0 > 0, DTB_EINVAL, "dtb_create: dt0 must be finite and > 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("dtb_create: no CUDA device available");
+        return DTB_ENODEV;
+    }
+    DTB_CHECK(opts->device >= 0 && opts->device < ndev, DTB_EINVAL, "dtb_create: bad device ordinal");
+    std::unique_ptr<dtb_ctx> c(new dtb_ctx());
+    c->dims = *dims;
+    c->opts = *opts;
+    c->ns = dims->n_species;
+    c->n_space = dims->n_space;
+    c->prec = opts->precision;
+    c->esz = c->prec == DTB_F64 ? 8 : 4;
+    c->device = opts->device;
+    c->off[0] = 0;
+    c->offp[0] = 0;
+    for (int s = 0; s < c->ns; ++s) {
+        DTB_CHECK(dims->species_size[s] >= 1, DTB_EINVAL, "dtb_create: species_size must be >= 1");
+        c->sz[s] = dims->species_size[s];
+        c->off[s + 1] = c->off[s] + c->sz[s];
+        c->offp[s + 1] = c->offp[s] + round_up(c->sz[s], 8);
+    }
+    c->n_mom = c->off[c->ns];
+    c->n_state = c->n_mom * c->n_space;
+    DTB_CHECK(c->n_state < (int64_t)1 << 30, DTB_EINVAL, "dtb_create: state vector too long");
+    if (opts->graph_steps > 0) c->graph_steps = (opts->graph_steps + 1) / 2 * 2;
+    DeviceGuard g(c->device);
+    cudaDeviceProp prop;
+    DTB_CUDA(cudaGetDeviceProperties(&prop, c->device));
+    c->num_sms = prop.multiProcessorCount;
+    if (opts->stream) {
+        c->stream = reinterpret_cast<cudaStream_t>(opts->stream);
+    } else {
+        DTB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    *out = c.release();
+    return DTB_OK;
+}
+
+int32_t dtb_destroy(dtb_ctx* c) {
+    if (!c) return DTB_OK;
+    DeviceGuard g(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+    c->free_all();
+    if (c->pin_dt) cudaFreeHost(c->pin_dt);
+    if (c->pin_hist) cudaFreeHost(c->pin_hist);
+    if (c->pin_err) cudaFreeHost(c->pin_err);
+    if (c->pin_f32) cudaFreeHost(c->pin_f32);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DTB_OK;
+}
+
+static int species_of(const dtb_ctx* c, int64_t a) {
+    int s = 0;
+    while (s + 1 < c->ns && a >= c->off[s + 1]) ++s;
+    return s;
+}
+
+int32_t dtb_add_flux_csc(dtb_ctx* c, int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_add_flux_csc: null context");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_add_flux_csc: operators already committed");
+    DTB_CHECK(n == c->n_state, DTB_EINVAL, "dtb_add_flux_csc: n must equal the state length");
+    DTB_CHECK(colptr, DTB_EINVAL, "dtb_add_flux_csc: null colptr");
+    const int64_t base = c->opts.index_base;
+    const int64_t nnz = colptr[n] - colptr[0];
+    DTB_CHECK(colptr[0] == base && nnz >= 0, DTB_EINVAL, "dtb_add_flux_csc: colptr[0] must equal index_base");
+    DTB_CHECK(nnz == 0 || (rowval && nzval), DTB_EINVAL, "dtb_add_flux_csc: null rowval/nzval");
+    for (int64_t j = 0; j < n; ++j) {
+        DTB_CHECK(colptr[j + 1] >= colptr[j], DTB_EINVAL, "dtb_add_flux_csc: colptr not monotone");
+        for (int64_t p = colptr[j] - base; p < colptr[j + 1] - base; ++p) {
+            const int64_t r = rowval[p] - base;
+            DTB_CHECK(r >= 0 && r < n, DTB_EINVAL,
+                      "dtb_add_flux_csc: row index out of range at entry " + std::to_string(p));
+            c->flux_r.push_back(r);
+            c->flux_c.push_back(j);
+            c->flux_v.push_back(nzval[p]);
+        }
+    }
+    return DTB_OK;
+}
+
+static GainStage& gain_stage(dtb_ctx* c, int out, int in1, int in2) {
+    auto key = std::make_tuple(out, in1, in2);
+    auto it = c->gains.find(key);
+    if (it == c->gains.end()) {
+        GainStage g;
+        g.out = out;
+        g.in1 = in1;
+        g.in2 = in2;
+        it = c->gains.emplace(key, std::move(g)).first;
+    }
+    return it->second;
+}
+
+int32_t dtb_add_gain_block(dtb_ctx* c, int32_t out_sp, int32_t in1_sp, int32_t in2_sp, const void* G, int32_t dtype,
+                           int32_t on_device) {
+    DTB_CHECK(c && G, DTB_EINVAL, "dtb_add_gain_block: null argument");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_add_gain_block: operators already committed");
+    DTB_CHECK(out_sp >= 0 && out_sp < c->ns && in1_sp >= 0 && in1_sp < c->ns && in2_sp >= 0 && in2_sp < c->ns,
+              DTB_EINVAL, "dtb_add_gain_block: species index out of range");
+    DTB_CHECK(dtype == DTB_DTYPE_F64 || dtype == DTB_DTYPE_F32, DTB_EINVAL, "dtb_add_gain_block: bad dtype");
+    const int64_t no = c->sz[out_sp], n1 = c->sz[in1_sp], n2 = c->sz[in2_sp];
+    if (on_device) {
+        DTB_CHECK(in1_sp <= in2_sp, DTB_EINVAL, "dtb_add_gain_block: device blocks need in1_sp <= in2_sp");
+        GainStage& g = gain_stage(c, out_sp, in1_sp, in2_sp);
+        g.dev_src.emplace_back(G, dtype);
+        return DTB_OK;
+    }
+    // host: FP64 accumulation, transposed to in1 <= in2
+    const bool swap = in1_sp > in2_sp;
+    GainStage& g = swap ? gain_stage(c, out_sp, in2_sp, in1_sp) : gain_stage(c, out_sp, in1_sp, in2_sp);
+    if (g.host.empty()) g.host.assign((size_t)(no * n1 * n2), 0.0);
+    for (int64_t a = 0; a < no; ++a)
+        for (int64_t b = 0; b < n1; ++b)
+            for (int64_t cc = 0; cc < n2; ++cc) {
+                const size_t src = (size_t)((a * n1 + b) * n2 + cc);
+                const double v = dtype == DTB_DTYPE_F64 ? static_cast<const double*>(G)[src]
+                                                        : (double)static_cast<const float*>(G)[src];
+                const size_t dst = swap ? (size_t)((a * n2 + cc) * n1 + b) : src;
+                g.host[dst] += v;
+            }
+    return DTB_OK;
+}
+
+int32_t dtb_add_loss_block(dtb_ctx* c, int32_t sp, int32_t other_sp, const double* L) {
+    DTB_CHECK(c && L, DTB_EINVAL, "dtb_add_loss_block: null argument");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_add_loss_block: operators already committed");
+    DTB_CHECK(sp >= 0 && sp < c->ns && other_sp >= 0 && other_sp < c->ns, DTB_EINVAL,
+              "dtb_add_loss_block: species index out of range");
+    auto& v = c->losses[{sp, other_sp}];
+    const size_t n = (size_t)(c->sz[sp] * c->sz[other_sp]);
+    if (v.empty()) v.assign(n, 0.0);
+    for (size_t i = 0; i < n; ++i) v[i] += L[i];
+    return DTB_OK;
+}
+
+int32_t dtb_upload_mbin_ref(dtb_ctx* c, const double* M, int64_t n_mom) {
+    DTB_CHECK(c && M, DTB_EINVAL, "dtb_upload_mbin_ref: null argument");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_upload_mbin_ref: operators already committed");
+    DTB_CHECK(n_mom == c->n_mom, DTB_EINVAL, "dtb_upload_mbin_ref: M_Bin must be n_mom^2 x n_mom (SteppingMethods.jl:349)");
+    const int64_t N = n_mom;
+    const int64_t NN = N * N;
+    // T[a,j,k] = M[(j*N + a) + k*N^2]. Exact split: loss-form rows collect the entries with j == a
+    // or k == a (their contribution is f_a * sum_c L'[a,c] f_c); the rest is a gain tensor
+    // folded to in1 <= in2.
+    auto T = [&](int64_t a, int64_t j, int64_t k) { return M[(j * N + a) + k * NN]; };
+    for (int so = 0; so < c->ns; ++so)
+        for (int s1 = 0; s1 < c->ns; ++s1)
+            for (int s2 = s1; s2 < c->ns; ++s2) {
+                const int64_t no = c->sz[so], n1 = c->sz[s1], n2 = c->sz[s2];
+                std::vector<double> blk((size_t)(no * n1 * n2), 0.0);
+                bool nz = false;
+                for (int64_t al = 0; al < no; ++al) {
+                    const int64_t a = c->off[so] + al;
+                    for (int64_t bl = 0; bl < n1; ++bl) {
+                        const int64_t j = c->off[s1] + bl;
+                        if (j == a) continue;
+                        for (int64_t cl = 0; cl < n2; ++cl) {
+                            const int64_t k = c->off[s2] + cl;
+                            if (k == a) continue;
+                            double v = T(a, j, k);
+                            if (s1 != s2) v += T(a, k, j);
+                            if (v != 0.0) nz = true;
+                            blk[(size_t)((al * n1 + bl) * n2 + cl)] = v;
+                        }
+                    }
+                }
+                if (nz) {
+                    GainStage& g = gain_stage(c, so, s1, s2);
+                    if (g.host.empty()) g.host.assign(blk.size(), 0.0);
+                    for (size_t i = 0; i < blk.size(); ++i) g.host[i] += blk[i];
+                }
+            }
+    for (int sa = 0; sa < c->ns; ++sa)
+        for (int sc = 0; sc < c->ns; ++sc) {
+            const int64_t na = c->sz[sa], nc = c->sz[sc];
+            std::vector<double> L((size_t)(na * nc), 0.0);
+            bool nz = false;
+            for (int64_t al = 0; al < na; ++al) {
+                const int64_t a = c->off[sa] + al;
+                for (int64_t cl = 0; cl < nc; ++cl) {
+                    const int64_t k = c->off[sc] + cl;
+                    double v = T(a, a, k);
+                    if (k != a) v += T(a, k, a);
+                    if (v != 0.0) nz = true;
+                    L[(size_t)(al * nc + cl)] = -v;  // the kernel subtracts f_a * L f
+                }
+            }
+            if (nz) {
+                auto& v = c->losses[{sa, sc}];
+                if (v.empty()) v.assign(L.size(), 0.0);
+                for (size_t i = 0; i < L.size(); ++i) v[i] += L[i];
+            }
+        }
+    return DTB_OK;
+}
+
+int32_t dtb_add_emi_block(dtb_ctx* c, int64_t row0, int64_t nrows, int64_t col0, int64_t ncols, const double* E) {
+    DTB_CHECK(c && E, DTB_EINVAL, "dtb_add_emi_block: null argument");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_add_emi_block: operators already committed");
+    DTB_CHECK(row0 >= 0 && nrows > 0 && row0 + nrows <= c->n_state && col0 >= 0 && ncols > 0 &&
+                  col0 + ncols <= c->n_state,
+              DTB_EINVAL, "dtb_add_emi_block: piece outside the n x n matrix");
+    EmiPiece p{row0, nrows, col0, ncols, std::vector<double>(E, E + nrows * ncols)};
+    c->emis.push_back(std::move(p));
+    return DTB_OK;
+}
+
+int32_t dtb_upload_emi_ref(dtb_ctx* c, const double* M, int64_t n) {
+    DTB_CHECK(c && M, DTB_EINVAL, "dtb_upload_emi_ref: null argument");
+    DTB_CHECK(n == c->n_state, DTB_EINVAL, "dtb_upload_emi_ref: M_Emi must be n x n");
+    // nonzero (cell, species) x (cell, species) pieces
+    const int ng = c->n_space * c->ns;
+    for (int gr = 0; gr < ng; ++gr)
+        for (int gc = 0; gc < ng; ++gc) {
+            const int64_t r0 = (gr / c->ns) * c->n_mom + c->off[gr % c->ns], nr = c->sz[gr % c->ns];
+            const int64_t c0 = (gc / c->ns) * c->n_mom + c->off[gc % c->ns], nc = c->sz[gc % c->ns];
+            std::vector<double> d((size_t)(nr * nc));
+            bool nz = false;
+            for (int64_t r = 0; r < nr; ++r)
+                for (int64_t cc = 0; cc < nc; ++cc) {
+                    const double v = M[(r0 + r) + (c0 + cc) * n];
+                    d[(size_t)(r * nc + cc)] = v;
+                    if (v != 0.0) nz = true;
+                }
+            if (nz) DTB_TRY(dtb_add_emi_block(c, r0, nr, c0, nc, d.data()));
+        }
+    return DTB_OK;
+}
+
+int32_t dtb_upload_vectors(dtb_ctx* c, const double* Ap, const double* Vol, const double* f_init, const double* inj) {
+    DTB_CHECK(c && Ap && Vol && f_init && inj, DTB_EINVAL, "dtb_upload_vectors: null argument");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_upload_vectors: operators already committed");
+    c->Ap.assign(Ap, Ap + c->n_state);
+    c->Vol.assign(Vol, Vol + c->n_space);
+    c->f_init.assign(f_init, f_init + c->n_state);
+    c->inj.assign(inj, inj + c->n_state);
+    c->have_vectors = true;
+    return DTB_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ commit
+template <typename T>
+static int copy_host_vec(dtb_ctx* c, T** dst, const std::vector<double>& src) {
+    std::vector<T> tmp(src.size());
+    for (size_t i = 0; i < src.size(); ++i) tmp[i] = (T)src[i];
+    DTB_TRY(c->alloc(dst, sizeof(T) * std::max<size_t>(1, tmp.size())));
+    if (!tmp.empty()) DTB_CUDA(cudaMemcpy(*dst, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice));
+    return DTB_OK;
+}
+
+template <typename I>
+static int copy_host_ints(dtb_ctx* c, I** dst, const std::vector<I>& src) {
+    DTB_TRY(c->alloc(dst, sizeof(I) * std::max<size_t>(1, src.size())));
+    if (!src.empty()) DTB_CUDA(cudaMemcpy(*dst, src.data(), sizeof(I) * src.size(), cudaMemcpyHostToDevice));
+    return DTB_OK;
+}
+
+template <typename T>
+static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
+    const size_t esz = sizeof(T);
+    // ---------------- gain blocks
+    struct BlkInfo {
+        int out, in1, in2;
+        int64_t no, n1, n2, n2p;
+        int64_t elem_off;
+    };
+    std::vector<BlkInfo> blks;
+    int64_t total_elems = 0;
+    for (auto& kv : c->gains) {
+        GainStage& g = kv.second;
+        BlkInfo b{g.out, g.in1, g.in2, c->sz[g.out], c->sz[g.in1], c->sz[g.in2], round_up(c->sz[g.in2], 8), 0};
+        DTB_CHECK(b.n2p * (int64_t)esz <= kGainTileBytes, DTB_EINVAL,
+                  "gain block input-2 species has too many states for one staged b-row");
+        total_elems = round_up(total_elems, 256 / (int64_t)esz);
+        b.elem_off = total_elems;
+        total_elems += b.no * b.n1 * b.n2p;
+        blks.push_back(b);
+    }
+    c->has_bin = !c->gains.empty() || !c->losses.empty();
+    if (!blks.empty()) {
+        DTB_TRY(c->alloc(&c->G_all, esz * (size_t)total_elems));
+        DTB_CUDA(cudaMemset(c->G_all, 0, esz * (size_t)total_elems));
+        size_t bi = 0;
+        for (auto& kv : c->gains) {
+            GainStage& g = kv.second;
+            const BlkInfo& b = blks[bi++];
+            T* dst = reinterpret_cast<T*>(c->G_all) + b.elem_off;
+            const int64_t rows = b.no * b.n1;
+            if (!g.host.empty()) {
+                // host FP64 -> T, padded rows, through chunks
+                const int64_t chunk_rows = std::max<int64_t>(1, (64ll << 20) / (b.n2p * (int64_t)esz));
+                std::vector<T> tmp;
+                for (int64_t r0 = 0; r0 < rows; r0 += chunk_rows) {
+                    const int64_t nr = std::min(chunk_rows, rows - r0);
+                    tmp.assign((size_t)(nr * b.n2p), T(0));
+                    for (int64_t r = 0; r < nr; ++r)
+                        for (int64_t k = 0; k < b.n2; ++k)
+                            tmp[(size_t)(r * b.n2p + k)] = (T)g.host[(size_t)((r0 + r) * b.n2 + k)];
+                    DTB_CUDA(cudaMemcpy(dst + r0 * b.n2p, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice));
+                }
+            }
+            for (auto& src : g.dev_src) {
+                DTB_CHECK(g.host.empty() && g.dev_src.size() == 1, DTB_EINVAL,
+                          "a device-resident gain block cannot be summed with other uploads of the same block");
+                cudaError_t e;
+                if (src.second == DTB_DTYPE_F64)
+                    e = launch_pad_rows<double, T>(static_cast<const double*>(src.first), rows, (int)b.n2, dst,
+                                                   (int)b.n2p, c->stream);
+                else
+                    e = launch_pad_rows<float, T>(static_cast<const float*>(src.first), rows, (int)b.n2, dst,
+                                                  (int)b.n2p, c->stream);
+                DTB_CUDA(e);
+                DTB_CUDA(cudaStreamSynchronize(c->stream));
+            }
+            g.host.clear();
+            g.host.shrink_to_fit();
+        }
+    }
+    // work units, ordered by output row
+    c->f_smem_len = (int)c->offp[c->ns];
+    int bps = gain_stream_blocks_per_sm((int)esz, c->f_smem_len);
+    DTB_CHECK(bps >= 1 || blks.empty(), DTB_EINVAL, "gain kernel does not fit on an SM (state vector too long)");
+    if (bps < 1) bps = 1;
+    std::vector<GainUnit> units;
+    std::vector<int> unit_ptr((size_t)c->n_mom + 1, 0);
+    {
+        double tot_bytes = 0;
+        for (auto& b : blks) tot_bytes += (double)b.no * b.n1 * b.n2 * esz;
+        c->gain_bytes = tot_bytes;
+        const double target = std::min(256.0 * 1024, std::max((double)kGainTileBytes,
+                                                               tot_bytes / ((double)c->num_sms * bps * 8)));
+        for (int64_t a = 0; a < c->n_mom; ++a) {
+            unit_ptr[(size_t)a] = (int)units.size();
+            const int sa = species_of(c, a);
+            for (auto& b : blks) {
+                if (b.out != sa) continue;
+                const int64_t al = a - c->off[sa];
+                const int64_t row_b = b.n2p * (int64_t)esz;
+                const int tile_b = (int)std::max<int64_t>(1, std::min<int64_t>(b.n1, kGainTileBytes / row_b));
+                int64_t nb = std::max<int64_t>(tile_b, (int64_t)(target / row_b) / tile_b * tile_b);
+                for (int64_t b0 = 0; b0 < b.n1; b0 += nb) {
+                    GainUnit u;
+                    u.g_off = b.elem_off + (al * b.n1 + b0) * b.n2p;
+                    u.b_off = (int)(c->offp[b.in1] + b0);
+                    u.c_off = (int)c->offp[b.in2];
+                    u.nb = (int)std::min(nb, b.n1 - b0);
+                    u.n2p = (int)b.n2p;
+                    u.tile_b = tile_b;
+                    u.row = (int)a;
+                    units.push_back(u);
+                }
+            }
+        }
+        unit_ptr[(size_t)c->n_mom] = (int)units.size();
+    }
+    c->n_units = (int)units.size();
+    c->gain_grid = std::max(1, std::min(c->n_units, c->num_sms * bps));
+    DTB_TRY(copy_host_ints(c, &c->units, units));
+    DTB_TRY(copy_host_ints(c, &c->unit_ptr, unit_ptr));
+    DTB_TRY(c->alloc(&c->partial, sizeof(double) * (size_t)std::max(1, c->n_units) * c->n_space));
+    DTB_CUDA(cudaMemset(c->partial, 0, sizeof(double) * (size_t)std::max(1, c->n_units) * c->n_space));
+
+    // ---------------- loss blocks, grouped by row species
+    {
+        std::vector<long long> doff;
+        std::vector<int> ld, coff, ncols;
+        std::vector<double> data;
+        for (int s = 0; s < c->ns; ++s) {
+            ops.loss_ptr[s] = (int)doff.size();
+            for (auto& kv : c->losses) {
+                if (kv.first.first != s) continue;
+                const int oth = kv.first.second;
+                const int64_t nr = c->sz[s], nc = c->sz[oth], l = round_up(nc, 4);
+                doff.push_back((long long)data.size());
+                ld.push_back((int)l);
+                coff.push_back((int)c->off[oth]);
+                ncols.push_back((int)nc);
+                const size_t base = data.size();
+                data.resize(base + (size_t)(nr * l), 0.0);
+                for (int64_t r = 0; r < nr; ++r)
+                    for (int64_t k = 0; k < nc; ++k) data[base + (size_t)(r * l + k)] = kv.second[(size_t)(r * nc + k)];
+            }
+        }
+        ops.loss_ptr[c->ns] = (int)doff.size();
+        long long* d_doff;
+        int *d_ld, *d_coff, *d_nc;
+        T* d_data;
+        DTB_TRY(copy_host_ints(c, &d_doff, doff));
+        DTB_TRY(copy_host_ints(c, &d_ld, ld));
+        DTB_TRY(copy_host_ints(c, &d_coff, coff));
+        DTB_TRY(copy_host_ints(c, &d_nc, ncols));
+        DTB_TRY(copy_host_vec(c, &d_data, data));
+        ops.loss_data_off = d_doff;
+        ops.loss_ld = d_ld;
+        ops.loss_col_off = d_coff;
+        ops.loss_ncols = d_nc;
+        ops.loss_data = d_data;
+    }
+    // ---------------- emission pieces, per row lists
+    {
+        c->has_emi = !c->emis.empty();
+        std::vector<long long> doff;
+        std::vector<int> ld, r0v, c0v, ncv;
+        std::vector<double> data;
+        std::vector<std::vector<int>> rows((size_t)c->n_state);
+        for (size_t p = 0; p < c->emis.size(); ++p) {
+            const EmiPiece& e = c->emis[p];
+            const int64_t l = round_up(e.ncols, 4);
+            doff.push_back((long long)data.size());
+            ld.push_back((int)l);
+            r0v.push_back((int)e.row0);
+            c0v.push_back((int)e.col0);
+            ncv.push_back((int)e.ncols);
+            const size_t base = data.size();
+            data.resize(base + (size_t)(e.nrows * l), 0.0);
+            for (int64_t r = 0; r < e.nrows; ++r) {
+                for (int64_t k = 0; k < e.ncols; ++k) data[base + (size_t)(r * l + k)] = e.data[(size_t)(r * e.ncols + k)];
+                rows[(size_t)(e.row0 + r)].push_back((int)p);
+            }
+        }
+        std::vector<int> rptr((size_t)c->n_state + 1, 0), piece;
+        for (int64_t i = 0; i < c->n_state; ++i) {
+            rptr[(size_t)i] = (int)piece.size();
+            for (int p : rows[(size_t)i]) piece.push_back(p);
+        }
+        rptr[(size_t)c->n_state] = (int)piece.size();
+        int *d_rptr, *d_piece, *d_ld, *d_r0, *d_c0, *d_nc;
+        long long* d_doff;
+        T* d_data;
+        DTB_TRY(copy_host_ints(c, &d_rptr, rptr));
+        DTB_TRY(copy_host_ints(c, &d_piece, piece));
+        DTB_TRY(copy_host_ints(c, &d_doff, doff));
+        DTB_TRY(copy_host_ints(c, &d_ld, ld));
+        DTB_TRY(copy_host_ints(c, &d_r0, r0v));
+        DTB_TRY(copy_host_ints(c, &d_c0, c0v));
+        DTB_TRY(copy_host_ints(c, &d_nc, ncv));
+        DTB_TRY(copy_host_vec(c, &d_data, data));
+        ops.emi_rptr = d_rptr;
+        ops.emi_piece = d_piece;
+        ops.emi_data_off = d_doff;
+        ops.emi_ld = d_ld;
+        ops.emi_row0 = d_r0;
+        ops.emi_col0 = d_c0;
+        ops.emi_ncols = d_nc;
+        ops.emi_data = d_data;
+    }
+    // ---------------- flux: CSR with duplicates summed, then banded ELL
+    {
+        const int64_t n = c->n_state;
+        std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)n);
+        for (size_t p = 0; p < c->flux_r.size(); ++p) rows[(size_t)c->flux_r[p]].push_back({c->flux_c[p], c->flux_v[p]});
+        int w = 0;
+        for (auto& r : rows) {
+            std::stable_sort(r.begin(), r.end(), [](auto& x, auto& y) { return x.first < y.first; });
+            std::vector<std::pair<int64_t, double>> m;
+            for (auto& e : r) {
+                if (!m.empty() && m.back().first == e.first)
+                    m.back().second += e.second;
+                else
+                    m.push_back(e);
+            }
+            r.swap(m);
+            w = std::max<int>(w, (int)r.size());
+        }
+        w = (int)round_up(std::max(w, 1), 4);
+        std::vector<double> val((size_t)(n * w), 0.0);
+        std::vector<int> col((size_t)(n * w));
+        for (int64_t i = 0; i < n; ++i) {
+            for (int k = 0; k < w; ++k) {
+                if (k < (int)rows[(size_t)i].size()) {
+                    col[(size_t)(i * w + k)] = (int)rows[(size_t)i][(size_t)k].first;
+                    val[(size_t)(i * w + k)] = rows[(size_t)i][(size_t)k].second;
+                } else {
+                    col[(size_t)(i * w + k)] = -1;  // padding, skipped by the kernel
+                }
+            }
+        }
+        T* d_val;
+        int* d_col;
+        DTB_TRY(copy_host_vec(c, &d_val, val));
+        DTB_TRY(copy_host_ints(c, &d_col, col));
+        ops.ell_w = w;
+        ops.ell_val = d_val;
+        ops.ell_col = d_col;
+    }
+    // ---------------- vectors
+    {
+        std::vector<double> invAp(c->Ap.size());
+        for (size_t i = 0; i < invAp.size(); ++i) invAp[i] = (double)((T)1 / (T)c->Ap[i]);  // SteppingStructs.jl:55
+        T *d_inv, *d_inj, *d_vol;
+        DTB_TRY(copy_host_vec(c, &d_inv, invAp));
+        DTB_TRY(copy_host_vec(c, &d_inj, c->inj));
+        DTB_TRY(copy_host_vec(c, &d_vol, c->Vol));
+        ops.invAp = d_inv;
+        ops.inj = d_inj;
+        ops.vol = d_vol;
+        T* fi;
+        DTB_TRY(copy_host_vec(c, &fi, c->f_init));
+        c->f_init_dev = fi;
+        DTB_TRY(c->alloc(reinterpret_cast<T**>(&c->f_buf[0]), sizeof(T) * (size_t)c->n_state));
+        DTB_TRY(c->alloc(reinterpret_cast<T**>(&c->f_buf[1]), sizeof(T) * (size_t)c->n_state));
+        DTB_CUDA(cudaMemcpy(c->f_buf[0], fi, sizeof(T) * (size_t)c->n_state, cudaMemcpyDeviceToDevice));
+        c->cur = 0;
+    }
+    ops.n_mom = (int)c->n_mom;
+    ops.n_state = (int)c->n_state;
+    ops.n_space = c->n_space;
+    ops.n_species = c->ns;
+    for (int s = 0; s <= c->ns; ++s) {
+        ops.sp_off[s] = (int)c->off[s];
+        ops.sp_offp[s] = (int)c->offp[s];
+        c->sp_off_host[s] = (int)c->off[s];
+        c->sp_off_host[c->ns + 1 + s] = (int)c->offp[s];
+    }
+    ops.unit_ptr = c->unit_ptr;
+    ops.n_units = c->n_units;
+    ops.partial = c->partial;
+    ops.thr = c->prec == DTB_F64 ? (double)1e-10f : (double)(T)1e-10f;
+    ops.has_bin = c->has_bin;
+    ops.has_emi = c->has_emi;
+    return DTB_OK;
+}
+
+extern "C" int32_t dtb_commit(dtb_ctx* c) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_commit: null context");
+    if (c->committed) return DTB_OK;
+    DTB_CHECK(c->have_vectors, DTB_ESTATE, "dtb_commit: dtb_upload_vectors was not called");
+    DeviceGuard g(c->device);
+    int rc = c->prec == DTB_F64 ? commit_typed<double>(c, c->ops_d) : commit_typed<float>(c, c->ops_f);
+    if (rc != DTB_OK) {
+        c->free_all();
+        return rc;
+    }
+    DTB_TRY(c->alloc(&c->dt_arr, sizeof(double) * (size_t)c->hist_cap));
+    DTB_TRY(c->alloc(&c->ctr, sizeof(unsigned long long)));
+    DTB_TRY(c->alloc(&c->hist, sizeof(StepDiagDev) * (size_t)c->hist_cap));
+    const int rows_grid = (int)((c->n_state + kRowsWarps - 1) / kRowsWarps);
+    DTB_TRY(c->alloc(&c->blk_red, sizeof(double) * 7 * (size_t)rows_grid));
+    DTB_TRY(c->alloc(&c->ticket, sizeof(unsigned)));
+    DTB_TRY(c->alloc(&c->err, sizeof(int)));
+    std::vector<int> spo(c->off, c->off + c->ns + 1);
+    DTB_TRY(copy_host_ints(c, &c->sp_off_dev, spo));
+    DTB_TRY(c->alloc(&c->mom_w, sizeof(double) * (size_t)c->n_mom));
+    DTB_TRY(c->alloc(&c->mom_out, sizeof(double) * 2 * (size_t)c->ns * c->n_space));
+    DTB_CUDA(cudaMemset(c->ctr, 0, sizeof(unsigned long long)));
+    DTB_CUDA(cudaMemset(c->ticket, 0, sizeof(unsigned)));
+    DTB_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+    DTB_CUDA(cudaMallocHost(&c->pin_dt, sizeof(double) * (size_t)c->hist_cap));
+    DTB_CUDA(cudaMallocHost(&c->pin_hist, sizeof(StepDiagDev) * (size_t)c->hist_cap));
+    DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));
+    if (c->prec == DTB_F32) DTB_CUDA(cudaMallocHost(&c->pin_f32, sizeof(float) * (size_t)c->n_state));
+    DTB_CUDA(cudaDeviceSynchronize());
+    c->host_ctr = 0;
+    c->committed = true;
+    // staging no longer needed
+    c->gains.clear();
+    c->losses.clear();
+    c->emis.clear();
+    c->flux_r.clear();
+    c->flux_c.clear();
+    c->flux_v.clear();
+    return DTB_OK;
+}
+
+// ------------------------------------------------------------------ stepping internals
+static int flush_profile(dtb_ctx* c) {
+    if (c->prof_pending == 0) return DTB_OK;
+    DTB_CUDA(cudaEventSynchronize(c->ev[(size_t)(2 * (c->prof_pending - 1) + 1)]));
+    for (int k = 0; k < c->prof_pending; ++k) {
+        float ms = 0;
+        DTB_CUDA(cudaEventElapsedTime(&ms, c->ev[(size_t)(2 * k)], c->ev[(size_t)(2 * k + 1)]));
+        c->prof_ms += ms;
+    }
+    c->prof_pending = 0;
+    return DTB_OK;
+}
+
+template <typename T>
+static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, int verbose, bool profile) {
+    T* fin = reinterpret_cast<T*>(c->f_buf[c->cur]);
+    T* fout = reinterpret_cast<T*>(c->f_buf[c->cur ^ 1]);
+    if (c->n_units > 0) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (profile) {
+            const size_t k = (size_t)c->prof_pending * 2;
+            while (c->ev.size() < k + 2) {
+                cudaEvent_t e;
+                DTB_CUDA(cudaEventCreate(&e));
+                c->ev.push_back(e);
+            }
+            e0 = c->ev[k];
+            e1 = c->ev[k + 1];
+            DTB_CUDA(cudaEventRecord(e0, c->stream));
+        }
+        DTB_CUDA(launch_gain_stream<T>(reinterpret_cast<const T*>(c->G_all), c->units, c->n_units, fin, (int)c->n_mom,
+                                       c->sp_off_host, c->ns, c->f_smem_len, c->partial, c->n_space, c->gain_grid,
+                                       c->err, c->stream));
+        if (profile) {
+            DTB_CUDA(cudaEventRecord(e1, c->stream));
+            c->prof_n++;
+            if (++c->prof_pending == kProfRing) DTB_TRY(flush_profile(c));
+        }
+    }
+    DTB_CUDA(launch_euler_rows<T>(ops, fin, fout, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist, c->hist_cap,
+                                  verbose, c->blk_red, c->ticket, c->stream));
+    c->cur ^= 1;
+    c->host_ctr++;
+    return DTB_OK;
+}
+
+static int do_step(dtb_ctx* c, double dt_imm, bool use_arr, int verbose, bool profile) {
+    return c->prec == DTB_F64 ? launch_step<double>(c, c->ops_d, dt_imm, use_arr, verbose, profile)
+                              : launch_step<float>(c, c->ops_f, dt_imm, use_arr, verbose, profile);
+}
+
+static int check_kernel_err(dtb_ctx* c) {
+    DTB_CUDA(cudaMemcpyAsync(c->pin_err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    if (*c->pin_err) {
+        const int e = *c->pin_err;
+        cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
+        set_error("a bounded device wait gave up (kernel error flags " + std::to_string(e) + ")");
+        return DTB_ETIMEOUT;
+    }
+    return DTB_OK;
+}
+
+static int ensure_graph(dtb_ctx* c, int verbose) {
+    if (c->graph && c->graph_verbose == verbose) return DTB_OK;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    const int saved_cur = c->cur;
+    const unsigned long long saved_ctr = c->host_ctr;
+    c->cur = 0;
+    cudaGraph_t g;
+    DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = DTB_OK;
+    for (int k = 0; k < c->graph_steps && rc == DTB_OK; ++k) rc = do_step(c, 0.0, true, verbose, false);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->cur = saved_cur;
+    c->host_ctr = saved_ctr;
+    if (rc != DTB_OK) return rc;
+    DTB_CUDA(e);
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    DTB_CUDA(e);
+    c->graph_verbose = verbose;
+    return DTB_OK;
+}
+
+// Runs n steps whose dt/dt0 values are in pinned c->pin_dt[0..n) (n <= hist_cap); steps
+// read them through the device counter, which is reset to 0 first.
+static int run_chunk(dtb_ctx* c, int64_t n, int verbose, bool use_graph) {
+    DTB_CUDA(cudaMemcpyAsync(c->dt_arr, c->pin_dt, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaMemsetAsync(c->ctr, 0, sizeof(unsigned long long), c->stream));
+    c->host_ctr = 0;
+    int64_t done = 0;
+    if (use_graph && !c->profiling && n >= c->graph_steps) {
+        if (c->cur != 0) {
+            DTB_TRY(do_step(c, 0.0, true, verbose, false));
+            done++;
+        }
+        DTB_TRY(ensure_graph(c, verbose));
+        while (n - done >= c->graph_steps) {
+            DTB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+            done += c->graph_steps;
+            c->host_ctr += c->graph_steps;
+        }
+    }
+    for (; done < n; ++done) DTB_TRY(do_step(c, 0.0, true, verbose, c->profiling));
+    return DTB_OK;
+}
+
+static void print_cr(int verbose, const StepDiagDev& d, double t, double t_stop, double dt) {
+    if (verbose == 1 && d.cr[0] > 1.0)
+        std::printf("Cr = %.17g, t=%.17g, dt=%.17g, system may be unstable\n", d.cr[0], t, dt);
+    else if (verbose == 2)
+        std::printf("\rCr = %.17g, t=%.17g, dt=%.17g\n", d.cr[0], t, dt);
+    else if (verbose == 3)
+        std::printf("Cr = %.17g,Cr_Bin = %.17g, Cr_Emi = %.17g, Cr_Flux = %.17g, t=%.17g, t_save =%.17g, dt=%.17g\n",
+                    d.cr[0], d.cr[1], d.cr[2], d.cr[3], t, t_stop, dt);
+    if (!d.finite) std::printf("non-finite value in df calculation\n");
+}
+
+static double dt0_eff(const dtb_ctx* c) {
+    return c->prec == DTB_F32 ? (double)(float)c->opts.dt0 : c->opts.dt0;
+}
+
+extern "C" {
+
+int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t verbose, double* dt_out,
+                 int32_t* save_out, dtb_step_diag* diag_out) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_step: null context");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    // SteppingMethods.jl:18-27
+    int save = 0;
+    if (t_start + dt >= t_stop) {
+        dt = t_stop - t_start;
+        save = 1;
+    }
+    const double dt_scale = dt / dt0_eff(c);
+    if (c->host_ctr >= (unsigned long long)c->hist_cap) {
+        DTB_CUDA(cudaMemsetAsync(c->ctr, 0, sizeof(unsigned long long), c->stream));
+        c->host_ctr = 0;
+    }
+    const unsigned long long idx = c->host_ctr;
+    DTB_TRY(do_step(c, dt_scale, false, verbose, false));
+    if (dt_out) *dt_out = dt;
+    if (save_out) *save_out = save;
+    if (verbose == 1 || verbose == 2 || verbose == 3 || diag_out) {
+        DTB_CUDA(cudaMemcpyAsync(c->pin_hist, c->hist + idx, sizeof(StepDiagDev), cudaMemcpyDeviceToHost, c->stream));
+        DTB_TRY(check_kernel_err(c));
+        if (diag_out) std::memcpy(diag_out, c->pin_hist, sizeof(StepDiagDev));
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_run(dtb_ctx* c, const double* dt_scales, int64_t nsteps, int32_t verbose, dtb_step_diag* diag_hist) {
+    DTB_CHECK(c && (dt_scales || nsteps == 0), DTB_EINVAL, "dtb_run: null argument");
+    DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_run: nsteps < 0");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    for (int64_t s0 = 0; s0 < nsteps; s0 += c->hist_cap) {
+        const int64_t n = std::min<int64_t>(c->hist_cap, nsteps - s0);
+        DTB_CUDA(cudaStreamSynchronize(c->stream));  // pinned staging is reused
+        std::memcpy(c->pin_dt, dt_scales + s0, sizeof(double) * (size_t)n);
+        DTB_TRY(run_chunk(c, n, verbose, true));
+        if (diag_hist) {
+            DTB_CUDA(cudaMemcpyAsync(c->pin_hist, c->hist, sizeof(StepDiagDev) * (size_t)n, cudaMemcpyDeviceToHost,
+                                     c->stream));
+            DTB_TRY(check_kernel_err(c));
+            std::memcpy(diag_hist + s0, c->pin_hist, sizeof(StepDiagDev) * (size_t)n);
+        }
+    }
+    if (c->profiling) DTB_TRY(flush_profile(c));
+    if (!diag_hist) DTB_TRY(check_kernel_err(c));
+    return DTB_OK;
+}
+
+int32_t dtb_solve_schedule(double dt_initial, const double* t_save, int64_t n_save, double dt0, int32_t precision,
+                           int64_t* steps_per_interval, double* dt_scales, int64_t cap, int64_t* n_total_out) {
+    DTB_CHECK(t_save && n_save >= 1, DTB_EINVAL, "dtb_solve_schedule: need t_save");
+    DTB_CHECK(dt_initial > 0 && std::isfinite(dt_initial), DTB_EINVAL, "dtb_solve_schedule: dt must be > 0");
+    const double d0 = precision == DTB_F32 ? (double)(float)dt0 : dt0;
+    double dt = dt_initial;
+    int64_t total = 0;
+    for (int64_t i = 1; i < n_save; ++i) {
+        double t_start = t_save[i - 1];
+        const double t_stop = t_save[i];
+        int64_t k = 0;
+        bool save = false;
+        while (!save) {  // Solver.jl:34-37 with SteppingMethods.jl:18-23
+            if (t_start + dt >= t_stop) {
+                dt = t_stop - t_start;
+                save = true;
+            }
+            if (dt_scales && total < cap) dt_scales[total] = dt / d0;
+            ++total;
+            ++k;
+            t_start += dt;
+            DTB_CHECK(total <= kMaxScheduleSteps, DTB_EINVAL,
+                      "dtb_solve_schedule: more than 1e8 steps; the truncated dt of a save point is carried "
+                      "into later intervals (Solver.jl:35) and has become too small (dt = " +
+                          std::to_string(dt) + ")");
+        }
+        if (steps_per_interval) steps_per_interval[i - 1] = k;
+    }
+    if (n_total_out) *n_total_out = total;
+    return DTB_OK;
+}
+
+int32_t dtb_get_f(dtb_ctx* c, double* f) {
+    DTB_CHECK(c && f, DTB_EINVAL, "dtb_get_f: null argument");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    if (c->prec == DTB_F64) {
+        DTB_CUDA(cudaMemcpyAsync(f, c->f_buf[c->cur], sizeof(double) * (size_t)c->n_state, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+        DTB_CUDA(cudaMemcpyAsync(c->pin_f32, c->f_buf[c->cur], sizeof(float) * (size_t)c->n_state,
+                                 cudaMemcpyDeviceToHost, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+        for (int64_t i = 0; i < c->n_state; ++i) f[i] = c->pin_f32[i];
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_set_f(dtb_ctx* c, const double* f) {
+    DTB_CHECK(c && f, DTB_EINVAL, "dtb_set_f: null argument");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    if (c->prec == DTB_F64) {
+        DTB_CUDA(cudaMemcpyAsync(c->f_buf[c->cur], f, sizeof(double) * (size_t)c->n_state, cudaMemcpyHostToDevice,
+                                 c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+        DTB_CUDA(cudaStreamSynchronize(c->stream));  // the staging buffer may still feed a copy
+        for (int64_t i = 0; i < c->n_state; ++i) c->pin_f32[i] = (float)f[i];
+        DTB_CUDA(cudaMemcpyAsync(c->f_buf[c->cur], c->pin_f32, sizeof(float) * (size_t)c->n_state,
+                                 cudaMemcpyHostToDevice, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_reset(dtb_ctx* c) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_reset: null context");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    DTB_CUDA(cudaMemcpyAsync(c->f_buf[c->cur], c->f_init_dev, c->esz * (size_t)c->n_state, cudaMemcpyDeviceToDevice,
+                             c->stream));
+    return DTB_OK;
+}
+
+int32_t dtb_solve(dtb_ctx* c, double dt_initial, const double* t_save, int64_t n_save, int32_t verbose, double* f_out,
+                  int64_t* n_steps_out) {
+    DTB_CHECK(c && t_save && f_out && n_save >= 1, DTB_EINVAL, "dtb_solve: null argument");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    // Solver.jl:22 reset; :14 save the initial state
+    DTB_TRY(dtb_reset(c));
+    DTB_TRY(dtb_get_f(c, f_out));
+    double dt = dt_initial;
+    int64_t total = 0;
+    const double d0 = dt0_eff(c);
+    std::vector<double> t_of, dt_of;
+    for (int64_t i = 1; i < n_save; ++i) {
+        double t_start = t_save[i - 1];
+        const double t_stop = t_save[i];
+        bool save = false;
+        std::vector<double> scales;
+        t_of.clear();
+        dt_of.clear();
+        while (!save) {
+            if (t_start + dt >= t_stop) {
+                dt = t_stop - t_start;
+                save = true;
+            }
+            scales.push_back(dt / d0);
+            t_of.push_back(t_start);
+            dt_of.push_back(dt);
+            t_start += dt;
+            DTB_CHECK(total + (int64_t)scales.size() <= kMaxScheduleSteps, DTB_EINVAL,
+                      "dtb_solve: more than 1e8 steps; the truncated dt of a save point is carried into later "
+                      "intervals (Solver.jl:35) and has become too small");
+        }
+        const bool want_diag = verbose == 1 || verbose == 2 || verbose == 3;
+        std::vector<dtb_step_diag> hist(want_diag ? scales.size() : 0);
+        DTB_TRY(dtb_run(c, scales.data(), (int64_t)scales.size(), verbose, want_diag ? hist.data() : nullptr));
+        if (want_diag) {
+            for (size_t k = 0; k < hist.size(); ++k) {
+                StepDiagDev d;
+                std::memcpy(&d, &hist[k], sizeof(d));
+                print_cr(verbose, d, t_of[k], t_stop, dt_of[k]);
+            }
+        } else {
+            DTB_TRY(check_kernel_err(c));
+        }
+        total += (int64_t)scales.size();
+        DTB_TRY(dtb_get_f(c, f_out + (size_t)i * c->n_state));
+    }
+    if (n_steps_out) *n_steps_out = total;
+    return DTB_OK;
+}
+
+int32_t dtb_moments(dtb_ctx* c, const double* w, double* number, double* energy) {
+    DTB_CHECK(c && w && number && energy, DTB_EINVAL, "dtb_moments: null argument");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    DTB_CUDA(cudaMemcpyAsync(c->mom_w, w, sizeof(double) * (size_t)c->n_mom, cudaMemcpyHostToDevice, c->stream));
+    if (c->prec == DTB_F64)
+        DTB_CUDA(launch_moments_f64(reinterpret_cast<const double*>(c->f_buf[c->cur]), (int)c->n_mom, c->n_space,
+                                    c->sp_off_dev, c->ns, c->mom_w, c->mom_out, c->stream));
+    else
+        DTB_CUDA(launch_moments_f32(reinterpret_cast<const float*>(c->f_buf[c->cur]), (int)c->n_mom, c->n_space,
+                                    c->sp_off_dev, c->ns, c->mom_w, c->mom_out, c->stream));
+    std::vector<double> out((size_t)2 * c->ns * c->n_space);
+    DTB_CUDA(cudaMemcpyAsync(out.data(), c->mom_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < out.size() / 2; ++k) {
+        number[k] = out[2 * k];
+        energy[k] = out[2 * k + 1];
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_device_bytes(dtb_ctx* c, int64_t* bytes) {
+    DTB_CHECK(c && bytes, DTB_EINVAL, "dtb_device_bytes: null argument");
+    *bytes = (int64_t)c->dev_bytes;
+    return DTB_OK;
+}
+
+int32_t dtb_get_stream(dtb_ctx* c, void** stream) {
+    DTB_CHECK(c && stream, DTB_EINVAL, "dtb_get_stream: null argument");
+    *stream = c->stream;
+    return DTB_OK;
+}
+
+int32_t dtb_sync(dtb_ctx* c) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_sync: null context");
+    DeviceGuard g(c->device);
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->committed) DTB_TRY(check_kernel_err(c));
+    return DTB_OK;
+}
+
+int32_t dtb_launches_per_step(dtb_ctx* c, int32_t* n) {
+    DTB_CHECK(c && n, DTB_EINVAL, "dtb_launches_per_step: null argument");
+    DTB_TRY(dtb_commit(c));
+    *n = c->n_units > 0 ? 2 : 1;
+    return DTB_OK;
+}
+
+int32_t dtb_set_profiling(dtb_ctx* c, int32_t on) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_set_profiling: null context");
+    if (c->profiling && c->prof_pending) DTB_TRY(flush_profile(c));
+    c->profiling = on != 0;
+    c->prof_ms = 0.0;
+    c->prof_n = 0;
+    c->prof_pending = 0;
+    return DTB_OK;
+}
+
+int32_t dtb_gain_kernel_stats(dtb_ctx* c, double* avg_ms, double* bytes_per_launch) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_gain_kernel_stats: null context");
+    DTB_TRY(dtb_commit(c));
+    if (bytes_per_launch) *bytes_per_launch = c->gain_bytes * c->n_space;
+    if (avg_ms) *avg_ms = c->prof_n ? c->prof_ms / (double)c->prof_n : 0.0;
+    return DTB_OK;
+}
+
+}  // extern "C"

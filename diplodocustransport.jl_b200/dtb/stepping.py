@@ -1,0 +1,242 @@
+"""Python mirror of the reference's stepping API over libdtb.so.
+
+``ForwardEulerStruct(PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)`` follows
+SteppingStructs.jl:33-100: it uploads the operators once (M_Bin in the reference layout or
+as blocks, M_Emi dense or as pieces, F = X_Flux + P_Flux, invAp = 1 ./ Ap_Flux, Vol) and
+keeps f on the device. Calling it, ``method(t_start, t_stop, dt, Verbose) -> (dt, save)``,
+is the functor of SteppingMethods.jl:12-107. ``Solve`` follows Solver.jl:1-64.
+
+All compute runs in libdtb.so on a CUDA device; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, iptr
+from .structs import BinaryMatrices, EmissionMatrices, FluxMatrices, PhaseSpace
+
+THR_F64 = float(np.float32(1e-10))
+
+
+@dataclass
+class OutputStruct:
+    """StructsAndDictionaries.jl:362-377: saved states and their times."""
+
+    f: List[np.ndarray] = field(default_factory=list)
+    t: List[float] = field(default_factory=list)
+
+
+def _precision_code(Precision) -> int:
+    if Precision in (np.float64, float, "Float64", "f64"):
+        return _lib.DTB_F64
+    if Precision in (np.float32, "Float32", "f32"):
+        return _lib.DTB_F32
+    raise ValueError("Precision must be Float32 or Float64 (SteppingStructs.jl:38)")
+
+
+def _upload_csc(L, ctx, M) -> None:
+    if M is None or M.nnz == 0:
+        return
+    M = M.tocsc()
+    M.sort_indices()
+    colptr = np.ascontiguousarray(M.indptr, dtype=np.int64)
+    rowval = np.ascontiguousarray(M.indices, dtype=np.int64)
+    nzval = np.ascontiguousarray(M.data, dtype=np.float64)
+    check(L.dtb_add_flux_csc(ctx, M.shape[0], iptr(colptr), iptr(rowval), dptr(nzval)))
+
+
+def _upload_gain(L, ctx, g) -> None:
+    G = g.G
+    if hasattr(G, "is_cuda") and G.is_cuda:  # torch tensor already in device memory
+        import torch
+        G = G.contiguous()
+        dtype = _lib.DTB_DTYPE_F64 if G.dtype == torch.float64 else _lib.DTB_DTYPE_F32
+        if G.dtype not in (torch.float64, torch.float32):
+            raise TypeError("device gain blocks must be float32 or float64")
+        check(L.dtb_add_gain_block(ctx, g.out_sp, g.in1_sp, g.in2_sp, ctypes.c_void_p(G.data_ptr()), dtype, 1))
+        return
+    A = np.asarray(G)
+    if A.dtype == np.float32:
+        A = np.ascontiguousarray(A)
+        dtype = _lib.DTB_DTYPE_F32
+    else:
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        dtype = _lib.DTB_DTYPE_F64
+    check(L.dtb_add_gain_block(ctx, g.out_sp, g.in1_sp, g.in2_sp, ctypes.c_void_p(A.ctypes.data), dtype, 0))
+
+
+class ForwardEulerStruct:
+    """Explicit Euler method on a B200; SteppingStructs.jl:33-100 for the B200 backend."""
+
+    def __init__(self, PhaseSpace: PhaseSpace, Initial, Injection, BinM: BinaryMatrices,
+                 EmiM: EmissionMatrices, FluxM: FluxMatrices, *, Adaptive: bool = False,
+                 Precision=np.float64, device: int = 0, stream: Optional[int] = None,
+                 graph_steps: int = 16):
+        self.L = _lib.load()
+        self.PhaseSpace = PhaseSpace
+        self.Precision = Precision
+        self.Adaptive = Adaptive
+        self.Implicit = False
+        prec = _precision_code(Precision)
+        self.dt0 = float(np.float32(PhaseSpace.dt0)) if prec == _lib.DTB_F32 else float(PhaseSpace.dt0)
+        self.Binary_Interactions = BinM.has_interactions
+        self.Emission_Interactions = EmiM.has_interactions
+        self.f_init = np.array(Initial, dtype=np.float64, copy=True)
+        self.n = PhaseSpace.n_state
+        dims = _lib.Dims()
+        sizes = PhaseSpace.species_sizes
+        dims.n_species = len(sizes)
+        dims.n_space = PhaseSpace.n_space
+        for i, s in enumerate(sizes):
+            dims.species_size[i] = s
+        opts = _lib.Opts(precision=prec, device=device, stream=stream, index_base=0,
+                         graph_steps=graph_steps, dt0=float(PhaseSpace.dt0), batch=1, flags=0)
+        ctx = ctypes.c_void_p()
+        check(self.L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)))
+        self.ctx = ctx
+        try:
+            L = self.L
+            _upload_csc(L, ctx, FluxM.X_Flux)
+            _upload_csc(L, ctx, FluxM.P_Flux)
+            if BinM.M_Bin is not None:
+                M = np.asfortranarray(BinM.M_Bin, dtype=np.float64)
+                check(L.dtb_upload_mbin_ref(ctx, M.ctypes.data_as(_lib._dp), PhaseSpace.n_momentum))
+            for g in BinM.gains:
+                _upload_gain(L, ctx, g)
+            for l in BinM.losses:
+                A = np.ascontiguousarray(l.L, dtype=np.float64)
+                check(L.dtb_add_loss_block(ctx, l.sp, l.other_sp, dptr(A)))
+            if EmiM.M_Emi is not None:
+                M = np.asfortranarray(EmiM.M_Emi, dtype=np.float64)
+                check(L.dtb_upload_emi_ref(ctx, M.ctypes.data_as(_lib._dp), self.n))
+            for b in EmiM.blocks:
+                E = np.ascontiguousarray(b.E, dtype=np.float64)
+                check(L.dtb_add_emi_block(ctx, b.row0, E.shape[0], b.col0, E.shape[1], dptr(E)))
+            Ap = np.ascontiguousarray(FluxM.Ap_Flux, dtype=np.float64)
+            Vol = np.ascontiguousarray(FluxM.Vol, dtype=np.float64)
+            inj = np.ascontiguousarray(Injection, dtype=np.float64)
+            check(L.dtb_upload_vectors(ctx, dptr(Ap), dptr(Vol), dptr(self.f_init), dptr(inj)))
+            check(L.dtb_commit(ctx))
+        except Exception:
+            self.close()
+            raise
+        self.last_diag = _lib.StepDiag()
+
+    # ---- the functor (SteppingMethods.jl:12-107)
+    def __call__(self, t_start: float, t_stop: float, dt: float, Verbose: int = 1):
+        dt_out = ctypes.c_double()
+        save = ctypes.c_int32()
+        d = self.last_diag
+        check(self.L.dtb_step(self.ctx, float(t_start), float(t_stop), float(dt), int(Verbose),
+                              ctypes.byref(dt_out), ctypes.byref(save), ctypes.byref(d)))
+        if not d.finite:
+            print("non-finite value in df calculation")
+        if Verbose == 1 and d.cr > 1.0:
+            print(f"Cr = {d.cr}, t={t_start}, dt={dt_out.value}, system may be unstable")
+        elif Verbose == 2:
+            print(f"\rCr = {d.cr}, t={t_start}, dt={dt_out.value}")
+        elif Verbose == 3:
+            print(f"Cr = {d.cr},Cr_Bin = {d.cr_bin}, Cr_Emi = {d.cr_emi}, Cr_Flux = {d.cr_flux}, "
+                  f"t={t_start}, t_save ={t_stop}, dt={dt_out.value}")
+        return dt_out.value, bool(save.value)
+
+    # ---- state access
+    @property
+    def f(self) -> np.ndarray:
+        out = np.empty(self.n)
+        check(self.L.dtb_get_f(self.ctx, dptr(out)))
+        return out
+
+    @f.setter
+    def f(self, value) -> None:
+        v = np.ascontiguousarray(value, dtype=np.float64)
+        check(self.L.dtb_set_f(self.ctx, dptr(v)))
+
+    def reset(self) -> None:
+        check(self.L.dtb_reset(self.ctx))
+
+    def run(self, dt_scales: Sequence[float], Verbose: int = 0, diag: bool = False):
+        s = np.ascontiguousarray(dt_scales, dtype=np.float64)
+        hist = (_lib.StepDiag * len(s))() if diag else None
+        check(self.L.dtb_run(self.ctx, dptr(s), len(s), int(Verbose), hist))
+        return hist
+
+    def moments(self, weights) -> tuple:
+        """Per (cell, species) FP64 number and energy (DistributionMoments.jl:33,145,162)."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        ns = len(self.PhaseSpace.species_sizes)
+        num = np.zeros(self.PhaseSpace.n_space * ns)
+        en = np.zeros_like(num)
+        check(self.L.dtb_moments(self.ctx, dptr(w), dptr(num), dptr(en)))
+        return num.reshape(-1, ns), en.reshape(-1, ns)
+
+    def device_bytes(self) -> int:
+        v = ctypes.c_int64()
+        check(self.L.dtb_device_bytes(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def sync(self) -> None:
+        check(self.L.dtb_sync(self.ctx))
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.L.dtb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_schedule(dt_initial: float, t_save: Sequence[float], dt0: float, precision: int = _lib.DTB_F64):
+    """Host-side step schedule of Solve computed by the library (no device needed)."""
+    L = _lib.load()
+    t = np.ascontiguousarray(t_save, dtype=np.float64)
+    per = np.zeros(max(1, len(t) - 1), dtype=np.int64)
+    total = ctypes.c_int64()
+    check(L.dtb_solve_schedule(float(dt_initial), dptr(t), len(t), float(dt0), precision, iptr(per), None, 0,
+                               ctypes.byref(total)))
+    scales = np.zeros(max(1, total.value))
+    check(L.dtb_solve_schedule(float(dt_initial), dptr(t), len(t), float(dt0), precision, iptr(per), dptr(scales),
+                               total.value, ctypes.byref(total)))
+    return per[:len(t) - 1], scales[:total.value]
+
+
+def Solve(method: ForwardEulerStruct, dt_initial: float, t_save: Sequence[float], *, progress: bool = False,
+          fileName: Optional[str] = None, fileLocation: Optional[str] = None, Verbose: int = 1,
+          stepwise: bool = False) -> OutputStruct:
+    """Solver.jl:1-64. ``stepwise=True`` calls the functor once per step exactly like the
+    reference loop; the default runs each save interval as CUDA-graph replays (dtb_solve)."""
+    t_save = [float(t) for t in t_save]
+    n_save = len(t_save)
+    out = OutputStruct()
+    if stepwise:
+        method.reset()
+        out.f.append(method.f_init.copy())
+        out.t.append(t_save[0])
+        dt = float(dt_initial)
+        for i in range(1, n_save):
+            t_start, t_stop = t_save[i - 1], t_save[i]
+            save = False
+            while not save:
+                dt, save = method(t_start, t_stop, dt, Verbose)
+                t_start += dt
+            out.f.append(method.f)
+            out.t.append(t_stop)
+        return out
+    F = np.zeros((n_save, method.n))
+    nsteps = ctypes.c_int64()
+    t = np.ascontiguousarray(t_save, dtype=np.float64)
+    check(method.L.dtb_solve(method.ctx, float(dt_initial), dptr(t), n_save, int(Verbose), dptr(F),
+                             ctypes.byref(nsteps)))
+    out.f = [F[i].copy() for i in range(n_save)]
+    out.t = list(t_save)
+    out.n_steps = nsteps.value
+    return out

@@ -1,0 +1,181 @@
+/*
+ * dtb.h - C ABI of libdtb.so, a B200 (sm_100a) backend for the explicit Euler path of
+ * DiplodocusTransport.jl.
+ *
+ * The ABI is what a Julia `ccall` binds: plain pointers and sizes, 0 on success, an error
+ * code otherwise, never a C++ exception. Host arrays are owned by the caller and are only
+ * read or written during the call; the library copies everything it keeps into device
+ * memory it owns and frees in dtb_destroy. Calls on one context must be serialised by
+ * the caller; separate contexts may be used from separate threads.
+ *
+ * Each entry point names the reference interface it replaces (paths are relative to
+ * the DiplodocusTransport.jl project).
+ */
+#ifndef DTB_H
+#define DTB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTB_ABI_VERSION 1
+
+/* status codes */
+#define DTB_OK 0
+#define DTB_EINVAL 1   /* bad argument or inconsistent sizes */
+#define DTB_ENOMEM 2   /* device allocation failed or the HBM budget is exceeded */
+#define DTB_ECUDA 3    /* a CUDA runtime call failed (see dtb_last_error) */
+#define DTB_ETIMEOUT 4 /* a bounded device-side wait gave up; the context stays usable */
+#define DTB_ESTATE 5   /* call out of order (e.g. a step before any operator was uploaded) */
+#define DTB_ENODEV 6   /* no usable CUDA device */
+#define DTB_ENOTFOUND 7 /* unknown slot / request id */
+
+/* state precision (Main.Precision, SteppingStructs.jl:36-38) */
+#define DTB_F64 0       /* Float64 state and operators */
+#define DTB_F32 1       /* Float32 state and operators (the reference's CUDA precision, Backends.jl:12) */
+#define DTB_MIXED 2     /* batched: G and E as BF16 hi+lo with per-row FP32 scale, f in FP32,
+                           FP64 compensated update and moments */
+
+/* element type tags for uploads */
+#define DTB_DTYPE_F64 0
+#define DTB_DTYPE_F32 1
+
+#define DTB_MAX_SPECIES 16
+
+typedef struct dtb_ctx dtb_ctx;
+
+/* Grid description: the part of PhaseSpaceStruct (StructsAndDictionaries.jl:290) the step reads. */
+typedef struct dtb_dims {
+    int32_t n_species;                       /* length(name_list) */
+    int32_t n_space;                         /* x_num * y_num * z_num */
+    int64_t species_size[DTB_MAX_SPECIES];   /* px_num * py_num * pz_num per species */
+} dtb_dims;
+
+typedef struct dtb_opts {
+    int32_t precision;     /* DTB_F64, DTB_F32 or DTB_MIXED */
+    int32_t device;        /* CUDA device ordinal */
+    void* stream;          /* cudaStream_t to run on, or NULL for a library-owned stream */
+    int32_t index_base;    /* base of sparse indices the caller passes: 1 (Julia) or 0 */
+    int32_t graph_steps;   /* steps per captured CUDA graph in dtb_run (0: default 16) */
+    double dt0;            /* TimeStruct.dt0 (StructsAndDictionaries.jl:55) */
+    int32_t batch;         /* instances per context; 1 for the plain method */
+    int32_t flags;         /* reserved, 0 */
+} dtb_opts;
+
+/* Per-step diagnostics of the functor (SteppingMethods.jl:48-94). */
+typedef struct dtb_step_diag {
+    double cr;        /* Cr = -min(df ./ f), NaN mapped to Inf; 0 when sum(f) == 0 */
+    double cr_bin;    /* Verbose == 3 only: binary part */
+    double cr_emi;    /* Verbose == 3 only: emission part */
+    double cr_flux;   /* Verbose == 3 only: flux part */
+    double sum_df;    /* sum(df) after scaling (FP64 accumulation) */
+    double sum_f;     /* sum(f) before the update */
+    int32_t finite;   /* isfinite(sum(df)) */
+    int32_t pad;
+} dtb_step_diag;
+
+/* ---- version / device (host only) ---- */
+int32_t dtb_abi_version(void);
+const char* dtb_last_error(void);                 /* thread-local message of the last failure */
+int32_t dtb_device_count(int32_t* n);
+
+/* ---- construction: ForwardEulerStruct(PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)
+ *      (SteppingStructs.jl:33-100) ---- */
+int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out);
+int32_t dtb_destroy(dtb_ctx* ctx);
+
+/* F_Flux += M for a CSC matrix n x n (X_Flux + P_Flux, SteppingStructs.jl:60,68).
+ * colptr has n+1 entries; indices use opts.index_base. Call once per matrix to add. */
+int32_t dtb_add_flux_csc(dtb_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                         const double* nzval);
+
+/* Reference-layout M_Bin (n_mom^2 x n_mom, column-major, BuildBinaryMatrices.jl:54) replaces
+ * BinM.M_Bin (SteppingStructs.jl:58,66). It is decomposed on upload into gain blocks and
+ * loss rows, exactly (no thresholding). */
+int32_t dtb_upload_mbin_ref(dtb_ctx* ctx, const double* M_Bin, int64_t n_mom);
+
+/* Blocked gain: df[a] += Vol * sum_{b in in1, c in in2} G[a][b][c] f_b f_c.
+ * G is row-major [N_out][N_in1][N_in2] (c fastest); `on_device` != 0 means G is a device
+ * pointer (same dtype as the context precision, N_in2 a multiple of 8 and in1 <= in2).
+ * Calls for the same (out, in1, in2) add. This is the block GainMatrix_to_M_Bin!
+ * (BuildBinaryMatrices.jl:114-204) scatters into M_Bin. */
+int32_t dtb_add_gain_block(dtb_ctx* ctx, int32_t out_sp, int32_t in1_sp, int32_t in2_sp,
+                           const void* G, int32_t dtype, int32_t on_device);
+
+/* Blocked loss: df[a] -= Vol * f_a * sum_{c in other} L[a][c] f_c; L row-major [N_sp][N_other].
+ * The block LossMatrix_to_M_Bin! (BuildBinaryMatrices.jl:206-284) scatters into M_Bin. */
+int32_t dtb_add_loss_block(dtb_ctx* ctx, int32_t sp, int32_t other_sp, const double* L);
+
+/* Reference dense M_Emi (n x n column-major, EmissionMatricesStruct, SteppingStructs.jl:59,67);
+ * stored as its nonzero (cell, species) blocks. */
+int32_t dtb_upload_emi_ref(dtb_ctx* ctx, const double* M_Emi, int64_t n);
+
+/* A dense row-major piece of M_Emi at (row0, col0). Pieces add. */
+int32_t dtb_add_emi_block(dtb_ctx* ctx, int64_t row0, int64_t nrows, int64_t col0, int64_t ncols,
+                          const double* E);
+
+/* Ap_Flux (diagonal, n), Vol (n_space), Initial (n), Injection (n)
+ * (SteppingStructs.jl:53-55,61-64). invAp = 1 ./ Ap is formed in the state precision. */
+int32_t dtb_upload_vectors(dtb_ctx* ctx, const double* Ap, const double* Vol,
+                           const double* f_init, const double* inj);
+
+/* Builds the device layouts. Called implicitly by the first step; calling it early moves
+ * the upload cost out of the first step. */
+int32_t dtb_commit(dtb_ctx* ctx);
+
+/* ---- stepping ---- */
+
+/* The ForwardEuler functor (SteppingMethods.jl:12-107): truncates dt at t_stop, advances f
+ * by one step. Writes the (possibly truncated) dt and the save flag; when verbose is 1, 2 or
+ * 3 also writes the diagnostics (one device->host sync, like the reference's reductions). */
+int32_t dtb_step(dtb_ctx* ctx, double t_start, double t_stop, double dt, int32_t verbose,
+                 double* dt_out, int32_t* save_out, dtb_step_diag* diag_out);
+
+/* nsteps steps with the given dt/dt0 values, replayed from captured CUDA graphs.
+ * diag_hist (nullable) receives one dtb_step_diag per step. */
+int32_t dtb_run(dtb_ctx* ctx, const double* dt_scales, int64_t nsteps, int32_t verbose,
+                dtb_step_diag* diag_hist);
+
+/* Solve (Solver.jl:1-64): resets f to Initial, steps to every t_save[i] and writes f there
+ * (f_out: n_save x n, row i = state at t_save[i]). Steps whose Cr exceeds 1 are reported on
+ * stdout like the reference when verbose == 1. n_steps_out (nullable) gets the step count. */
+int32_t dtb_solve(dtb_ctx* ctx, double dt_initial, const double* t_save, int64_t n_save,
+                  int32_t verbose, double* f_out, int64_t* n_steps_out);
+
+/* Step schedule of Solve, host only: per save interval the number of steps, and the
+ * dt/dt0 of every step (capacity cap; n_total_out gets the total count). `precision`
+ * selects how dt0 is rounded (Float32(dt0) for DTB_F32, SteppingStructs.jl:44). */
+int32_t dtb_solve_schedule(double dt_initial, const double* t_save, int64_t n_save, double dt0,
+                           int32_t precision, int64_t* steps_per_interval, double* dt_scales,
+                           int64_t cap, int64_t* n_total_out);
+
+/* f (length n, as Float64) copy out / in; reset to Initial (Solver.jl:22). */
+int32_t dtb_get_f(dtb_ctx* ctx, double* f);
+int32_t dtb_set_f(dtb_ctx* ctx, const double* f);
+int32_t dtb_reset(dtb_ctx* ctx);
+
+/* Per (cell, species) number sum(f) and energy sum(f * w) in FP64 on the device
+ * (DistributionMoments.jl:33,145,162); w is the per-state energy weight of one cell
+ * (n_mom). Outputs are n_space x n_species, row-major. */
+int32_t dtb_moments(dtb_ctx* ctx, const double* w, double* number, double* energy);
+
+/* Device bytes held by the context; the stream it runs on; wait for its work. */
+int32_t dtb_device_bytes(dtb_ctx* ctx, int64_t* bytes);
+int32_t dtb_get_stream(dtb_ctx* ctx, void** stream);
+int32_t dtb_sync(dtb_ctx* ctx);
+
+/* Kernel launches issued per step by dtb_run (for launch accounting). */
+int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
+
+/* Dominant-kernel timing over the last dtb_run: average gain-kernel duration in ms measured
+ * with CUDA events on the context stream, and its algorithmic bytes per launch. */
+int32_t dtb_gain_kernel_stats(dtb_ctx* ctx, double* avg_ms, double* bytes_per_launch);
+int32_t dtb_set_profiling(dtb_ctx* ctx, int32_t on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DTB_H */

@@ -1,0 +1,224 @@
+"""Parity of the plain (single-instance) CUDA path with the oracle, through the C ABI.
+
+Tolerances: relative L-infinity (max|f - f_ref| / max|f_ref|) <= 1e-12 for the FP64 path;
+<= 2e-5 for the FP32 path against the FP64 oracle (FP32 operators and state).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle
+from dtb import _lib, synth
+from dtb.stepping import ForwardEulerStruct, Solve
+from dtb.structs import (BinaryMatrices, EmissionMatrices, FluxMatrices, PhaseSpace, blocked_to_ref,
+                         emission_to_dense, energy_weights)
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden_small.json")))
+
+
+def rel_linf(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / np.max(np.abs(np.asarray(b))))
+
+
+def make_method(w, precision=np.float64, ref_layout=False, **kw):
+    binm, emim = w.binm, w.emim
+    if ref_layout:
+        binm = BinaryMatrices(M_Bin=blocked_to_ref(w.ps, w.binm))
+        emim = EmissionMatrices(M_Emi=emission_to_dense(w.ps, w.emim))
+    return ForwardEulerStruct(w.ps, w.f0, w.inj, binm, emim, w.fluxm, Precision=precision, **kw)
+
+
+@pytest.mark.parametrize("p,u,seed,n_space,randv,emi", [
+    (4, 2, 0, 1, False, True), (4, 3, 1, 1, True, True), (6, 2, 2, 2, True, True),
+    (5, 3, 3, 1, True, False), (16, 8, 4, 1, False, True), (7, 5, 5, 3, True, True)])
+def test_f64_functor_matches_oracle(cuda, p, u, seed, n_space, randv, emi):
+    w = synth.small(p_num=p, u_num=u, seed=seed, n_space=n_space, with_emission=emi, randomize_vectors=randv)
+    m = make_method(w)
+    ops = oracle.blocked_from_workload(w)
+    f = w.f0.copy()
+    for k in range(25):
+        dt_scale = 0.9 if k % 5 else 0.6
+        _, _ = m(0.0, 1e9, dt_scale * m.dt0, 3)
+        f, diag, _ = ops.step(f, dt_scale, 3)
+        d = m.last_diag
+        assert bool(d.finite) == bool(diag[4])
+        for got, exp in zip((d.cr, d.cr_bin, d.cr_emi, d.cr_flux), diag[:4]):
+            assert got == pytest.approx(exp, rel=1e-10, abs=1e-300) or (math.isinf(exp) and got == exp)
+    assert rel_linf(m.f, f) <= TOL64
+    m.close()
+
+
+@pytest.mark.parametrize("ci", range(3))
+def test_golden_literal_cases(cuda, ci):
+    """Arbitrary reference-layout M_Bin (not gain/loss structured), dense M_Emi, random CSC flux."""
+    c = GOLD["cases"][ci]
+    sizes = c["sizes"]
+    N = sum(sizes)
+    n = N * c["n_space"]
+    ps = PhaseSpace(name_list=[f"s{i}" for i in range(len(sizes))], px_num_list=sizes,
+                    py_num_list=[1] * len(sizes), pz_num_list=[1] * len(sizes), x_num=c["n_space"])
+    F = sp.csc_matrix((c["nzval"], c["rowval"], c["colptr"]), shape=(n, n))
+    fluxm = FluxMatrices(Ap_Flux=1.0 / np.array(c["invAp"]), Am_Flux=np.zeros(n), X_Flux=sp.csc_matrix((n, n)),
+                         P_Flux=F, Vol=np.array(c["Vol"]))
+    binm = BinaryMatrices(M_Bin=np.array(c["M_Bin"]).reshape((N * N, N), order="F"))
+    emim = EmissionMatrices(M_Emi=np.array(c["M_Emi"]).reshape((n, n), order="F"))
+    m = ForwardEulerStruct(ps, c["f0"], c["inj"], binm, emim, fluxm)
+    for st in c["steps"]:
+        m(0.0, 1e9, c["dt_scale"], c["verbose"])
+        exp = np.array([float(x) for x in st["f"]])
+        assert rel_linf(m.f, exp) <= TOL64
+        d = st["diag"]
+        for got, key in zip((m.last_diag.cr, m.last_diag.cr_bin, m.last_diag.cr_emi, m.last_diag.cr_flux),
+                            ("Cr", "Cr_Bin", "Cr_Emi", "Cr_Flux")):
+            e = float(d[key])
+            assert (got == e) if math.isinf(e) else got == pytest.approx(e, rel=1e-9, abs=1e-300)
+    m.close()
+
+
+def test_reference_layout_upload_equals_blocked(cuda):
+    w = synth.small(p_num=6, u_num=3, seed=11, randomize_vectors=True)
+    a = make_method(w)
+    b = make_method(w, ref_layout=True)
+    sc = np.full(40, 0.8)
+    a.run(sc)
+    b.run(sc)
+    assert rel_linf(a.f, b.f) <= 1e-13
+    a.close()
+    b.close()
+
+
+def test_functor_run_and_solve_agree_bitwise(cuda):
+    w = synth.small(p_num=8, u_num=4, seed=12, randomize_vectors=True)
+    t_save = [0.0, 3.0, 7.5, 8.0]
+    m1 = make_method(w, graph_steps=4)
+    out_step = Solve(m1, 0.4, t_save, Verbose=0, stepwise=True)
+    out_graph = Solve(m1, 0.4, t_save, Verbose=0)
+    for a, b in zip(out_step.f, out_graph.f):
+        np.testing.assert_array_equal(a, b)
+    # oracle Solve on the same schedule
+    saved, _ = oracle.solve(oracle.blocked_from_workload(w), w.f0, 0.4, t_save, 1.0, verbose=0)
+    for a, b in zip(out_graph.f, saved):
+        assert rel_linf(a, b) <= TOL64
+    assert out_graph.n_steps == sum(len(s[1]) for s in oracle.solve_schedule(0.4, t_save, 1.0))
+    m1.close()
+
+
+def test_config0_full_run(cuda):
+    """Config 0: N_s = 128, two species, FP64, 1000 steps at fixed dt."""
+    w = synth.config0(0)
+    m = make_method(w)
+    n_steps = 1000
+    out = Solve(m, 1.0, [0.0, 500.0, 1000.0], Verbose=1)
+    ops = oracle.blocked_from_workload(w)
+    saved, crs = oracle.solve(ops, w.f0, 1.0, [0.0, 500.0, 1000.0], 1.0)
+    assert out.n_steps == n_steps
+    assert rel_linf(out.f[1], saved[1]) <= TOL64
+    assert rel_linf(out.f[2], saved[2]) <= TOL64
+    assert np.count_nonzero(out.f[2]) == np.count_nonzero(saved[2])  # same clamp decisions
+    m.close()
+
+
+def test_f32_path_against_f64_oracle(cuda):
+    w = synth.small(p_num=16, u_num=8, seed=13, randomize_vectors=True)
+    m = make_method(w, precision=np.float32)
+    ops = oracle.blocked_from_workload(w)
+    f = w.f0.copy()
+    sc = np.full(100, 0.95)
+    m.run(sc)
+    for s in sc:
+        f, _, _ = ops.step(f, s, 0)
+    assert rel_linf(m.f, f) <= TOL32
+    m.close()
+
+
+def test_clamp_semantics_on_device(cuda):
+    """Negative, tiny, NaN and Inf states go through SteppingMethods.jl:97-101 exactly."""
+    w = synth.small(p_num=4, u_num=2, seed=14, with_emission=False)
+    n = w.ps.n_state
+    f0 = w.f0.copy()
+    specials = [-1.0, 5e-11, float(np.float32(1e-10)), 1.1e-10, np.inf, 0.0, -0.0]
+    f0[:len(specials)] = specials
+    w.f0 = f0
+    w.binm = BinaryMatrices()
+    w.fluxm.P_Flux = sp.csc_matrix((n, n))
+    w.inj = np.zeros(n)
+    m = make_method(w)
+    m(0.0, 1e9, 1.0, 0)
+    got = m.f
+    exp, _, _ = oracle.ref_from_workload(w).step(f0, 1.0, 0)
+    np.testing.assert_array_equal(got, exp)
+    np.testing.assert_array_equal(np.signbit(got), np.signbit(exp))
+    m.close()
+
+
+def test_device_moments_match_oracle(cuda):
+    w = synth.small(p_num=16, u_num=8, seed=15)
+    m = make_method(w)
+    m.run(np.full(10, 1.0))
+    wts = energy_weights(w.ps)
+    num, en = m.moments(wts)
+    f = m.f
+    onum, oen = oracle.moments(w.ps.species_sizes, f, wts)
+    np.testing.assert_allclose(num[0], onum, rtol=1e-14)
+    np.testing.assert_allclose(en[0], oen, rtol=1e-14)
+    m.close()
+
+
+def test_config1_full_size_properties(cuda):
+    """Config 1 (N_s = 1024, FP32 G of 1024 x 1,048,576 per species) at full size:
+    (a) one step matches the FP64 oracle on a sample of rows (gain rows from the same G);
+    (b) with a number-conserving loss built from G, species numbers stay constant."""
+    import torch
+    w = synth.config1(seed=1, gain_on_device=True)
+    ns = w.ps.species_sizes[0]
+    m = make_method(w, precision=np.float32)
+    m(0.0, 1e9, 1.0, 0)
+    f1 = m.f
+    # FP64 oracle of the same step on sampled rows; all O(N^2) terms in numpy
+    f0 = w.f0.astype(np.float32).astype(np.float64)
+    F = w.fluxm.F_Flux.astype(np.float32).astype(np.float64)
+    flux = F @ f0
+    emi = np.zeros_like(f0)
+    for b in w.emim.blocks:
+        E = np.asarray(b.E, dtype=np.float32).astype(np.float64)
+        emi[b.row0:b.row0 + E.shape[0]] += E @ f0[b.col0:b.col0 + E.shape[1]]
+    loss = np.zeros_like(f0)
+    off = w.ps.momentum_species_offset
+    for l in w.binm.losses:
+        L = np.asarray(l.L, dtype=np.float32).astype(np.float64)
+        loss[off[l.sp]:off[l.sp] + ns] += L @ f0[off[l.other_sp]:off[l.other_sp] + ns]
+    rng = np.random.default_rng(0)
+    rows = np.sort(rng.choice(2 * ns, 48, replace=False))
+    for r in rows:
+        sp_out = r // ns
+        G = w.binm.gains[sp_out].G
+        Grow = G[r - off[sp_out]].double().cpu().numpy()[None]
+        gain = oracle.gain_rows(Grow, 0, 1, f0[:ns], f0[ns:])[0]
+        df = -flux[r] + emi[r] + (gain - f0[r] * loss[r])
+        exp = oracle.clamp(f0[r] + df)
+        assert abs(f1[r] - exp) <= TOL32 * np.max(np.abs(f1)), (r, f1[r], exp)
+    m.close()
+    # (b) conservation with L_e[b, c] = sum_a G_e[a, b, c], L_g[c, b] = sum_a G_g[a, b, c]
+    from dtb.structs import LossBlock
+    Le = w.binm.gains[0].G.double().sum(0).cpu().numpy()
+    Lg = w.binm.gains[1].G.double().sum(0).t().cpu().numpy()
+    w.binm.losses = [LossBlock(0, 1, Le), LossBlock(1, 0, Lg)]
+    w.emim.blocks = []
+    m = make_method(w, precision=np.float32)
+    n0 = m.f
+    m.run(np.full(50, 1.0))
+    n1 = m.f
+    for s in range(2):
+        sl = slice(s * ns, (s + 1) * ns)
+        assert abs(n1[sl].sum() - n0[sl].sum()) / n0[sl].sum() < 1e-5
+    m.close()
+    del w
+    torch.cuda.empty_cache()

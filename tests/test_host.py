@@ -1,0 +1,131 @@
+"""Host-side checks that need no GPU: the C ABI loads and exports every declared symbol,
+the library's Solve schedule equals the oracle's, and the synthetic workloads keep their
+recorded properties."""
+import ctypes
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from dtb import _lib, synth
+from dtb.stepping import solve_schedule
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = json.load(open(os.path.join(ROOT, "tests", "golden", "golden_small.json")))
+
+
+def _declared_symbols():
+    names = set()
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            names |= set(re.findall(r"^\s*(?:int32_t|const char\*|void)\s+(dtb_\w+)\s*\(", txt, re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    names = _declared_symbols()
+    assert len(names) >= 25
+    for n in sorted(names):
+        assert hasattr(L, n), n
+    # every declared symbol has a Python binding with a signature
+    assert names <= set(_lib.SIGNATURES), sorted(names - set(_lib.SIGNATURES))
+    assert L.dtb_abi_version() == 1
+
+
+def test_library_exports_match_nm():
+    """The shared object's dynamic symbol table holds exactly the dtb_ names the headers declare."""
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\sT\s(dtb_\w+)$", out, re.M))
+    assert exported == _declared_symbols()
+
+
+def test_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    L = _lib.load()
+    dims = _lib.Dims(n_species=1, n_space=1)
+    dims.species_size[0] = 4
+    opts = _lib.Opts(precision=0, device=0, index_base=0, dt0=1.0, batch=1)
+    ctx = ctypes.c_void_p()
+    rc = L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx))
+    assert rc == _lib.DTB_ENODEV
+    assert b"device" in L.dtb_last_error()
+
+
+def test_bad_arguments_are_rejected():
+    L = _lib.load()
+    dims = _lib.Dims(n_species=0, n_space=1)
+    opts = _lib.Opts(precision=0, device=0, index_base=0, dt0=1.0, batch=1)
+    ctx = ctypes.c_void_p()
+    assert L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)) == _lib.DTB_EINVAL
+    dims.n_species = 1
+    dims.species_size[0] = 4
+    opts.precision = 7
+    assert L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)) == _lib.DTB_EINVAL
+    assert L.dtb_create(None, None, None) == _lib.DTB_EINVAL
+
+
+@pytest.mark.parametrize("dt,t_save", [(0.4, [0.0, 1.0, 2.5, 2.6]), (0.3, [0.0, 1.0, 2.0, 3.0]),
+                                       (0.3, list(np.linspace(0, 7, 11))), (1.0, [0.0, 1000.0]), (0.25, [0.0, 1.0, 2.5, 3.0]),
+                                       (0.07, [0.0, 0.5, 0.51, 2.0])])
+@pytest.mark.parametrize("prec,dt0", [(_lib.DTB_F64, 1.0), (_lib.DTB_F64, 0.3), (_lib.DTB_F32, 0.1)])
+def test_solve_schedule_matches_oracle(dt, t_save, prec, dt0):
+    d0 = float(np.float32(dt0)) if prec == _lib.DTB_F32 else dt0
+    try:
+        ref = oracle.solve_schedule(dt, t_save, d0, max_steps=2_000_000)
+    except ValueError:  # carried dt collapsed: both sides must refuse
+        with pytest.raises(_lib.DtbError):
+            solve_schedule(dt, t_save, dt0, prec)
+        return
+    per, scales = solve_schedule(dt, t_save, dt0, prec)
+    assert list(per) == [len(s[1]) for s in ref]
+    assert list(scales) == [x for s in ref for x in s[1]]  # bit-exact
+
+
+def test_solve_schedule_carried_dt_explosion_is_reported():
+    """dt = 0.1 over [0, 1]: 0.1 * 10 falls 1.1e-16 short of 1, the last step is truncated to
+    1.1e-16 and Solve keeps that dt (Solver.jl:35), so the next interval would need ~1e16 steps.
+    The library refuses instead of spinning; the oracle does the same."""
+    with pytest.raises(_lib.DtbError) as e:
+        solve_schedule(0.1, [0.0, 1.0, 2.0], 1.0)
+    assert e.value.code == _lib.DTB_EINVAL and b"Solver.jl:35" in _lib.load().dtb_last_error()
+    with pytest.raises(ValueError):
+        oracle.solve_schedule(0.1, [0.0, 1.0, 2.0], 1.0)
+
+
+def test_solve_schedule_golden():
+    k = GOLD["kat_sched"]
+    per, scales = solve_schedule(k["dt_initial"], k["t_save"], k["dt0"])
+    assert list(per) == k["counts"]
+    assert list(scales) == [x for s in k["scales"] for x in s]
+    k = GOLD["kat_sched32"]
+    per, scales = solve_schedule(k["dt_initial"], k["t_save"], k["dt0"], _lib.DTB_F32)
+    assert list(scales) == k["scales"][0]
+
+
+def test_synthetic_flux_is_conserving_and_scaled():
+    w = synth.small(p_num=8, u_num=4, seed=2)
+    F = w.fluxm.F_Flux.toarray()
+    np.testing.assert_allclose(F.sum(axis=0), 0.0, atol=1e-14)  # number conserving columns
+    assert np.all(np.diag(F) >= 0)
+    rho = np.max(np.abs(np.linalg.eigvals(F)))
+    assert rho * w.dt == pytest.approx(synth.CFL_TARGET, rel=1e-9)
+    assert max(np.count_nonzero(F, axis=1)) <= 5
+
+
+def test_synthetic_config0_shapes():
+    w = synth.config0(0)
+    assert w.ps.species_sizes == [128, 128]
+    assert [g.G.shape for g in w.binm.gains] == [(128, 128, 128)] * 2
+    assert [l.L.shape for l in w.binm.losses] == [(128, 128)] * 2
+    assert w.emim.blocks[0].E.shape == (128, 128)
+    assert w.f0[:128].sum() == pytest.approx(1.0) and w.f0[128:].sum() == pytest.approx(1.0)
+    g = np.asarray(w.binm.gains[0].G) / w.meta["kappa_gain"]
+    assert g.min() >= 1e-6 and g.max() <= 1.0
