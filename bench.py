@@ -122,8 +122,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_workload(config: int, device: str, host_sample_rows=None):
+def build_workload(config: int, device: str, host_sample_rows=None, grid=None):
     from dtb import synth
+    if config == 1 and grid:  # same recipe on another grid, e.g. "32x16" (small profiling case)
+        p, u = (int(x) for x in grid.split("x"))
+        return synth.two_species(p, 1e-3, 1e3, u, seed=1, gain_on_device=True, device=device), "f32"
     if config == 1:
         if host_sample_rows:
             return synth.config1(seed=1, gain_on_device=False, gain_rows=host_sample_rows), "f32"
@@ -209,6 +212,9 @@ def _has_cuda():
 
 def _config_dict(config: int, w):
     sizes = w.ps.species_sizes
+    if config == 1 and sizes != [1024, 1024]:
+        return {"workload": f"config-1 recipe on a smaller grid: 2 species x {sizes[0]} states, FP32",
+                "species_states": sizes, "precision": "FP32"}
     if config == 1:
         return {"workload": "plain single instance (config 1): 2 species x 1024 states (64 log p x 16 u), "
                             "FP32 gain 2 x 1024 x 1048576, 2000-step run shape",
@@ -229,7 +235,7 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    w, dtype = build_workload(args.config, f"cuda:{local}")
+    w, dtype = build_workload(args.config, f"cuda:{local}", grid=args.grid)
     stream = torch.cuda.Stream()
     m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm,
                            Precision=np.float32 if dtype == "f32" else np.float64, device=local,
@@ -327,6 +333,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=None, help="p_bins x u_bins override of the config-1 grid, e.g. 32x16")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

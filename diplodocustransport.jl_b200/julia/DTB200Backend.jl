@@ -1,0 +1,160 @@
+# B200 backend for DiplodocusTransport.jl's explicit Euler path, over libdtb.so.
+#
+# Not exercised in this repository (no Julia toolchain here); it shows the exact `ccall`
+# bindings of include/dtb.h that the reference would add. Loaded after DiplodocusTransport:
+#
+#     using DiplodocusTransport
+#     include("DTB200Backend.jl"); using .DTB200Backend
+#     Backend = B200Backend()            # instead of CPUBackend() / CUDABackend()
+#     method = B200ForwardEulerStruct(PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)
+#     output = Solve(method, dt, t_save)  # the reference's Solve, unchanged
+#
+# B200ForwardEulerStruct takes the same arguments as ForwardEulerStruct and carries the
+# fields Solve reads; the reference's own types are left untouched.
+module DTB200Backend
+
+using DiplodocusTransport
+using SparseArrays
+
+import DiplodocusTransport: BackendType, PhaseSpaceStruct
+
+export B200Backend, B200ForwardEulerStruct, b200_solve
+
+const libdtb = get(ENV, "DTB_LIB", joinpath(@__DIR__, "..", "lib", "libdtb.so"))
+
+struct B200Backend <: BackendType end  # next to Backends.jl:3-4
+
+const DTB_F64 = Int32(0)
+const DTB_F32 = Int32(1)
+
+struct Dims
+    n_species::Int32
+    n_space::Int32
+    species_size::NTuple{16,Int64}
+end
+
+struct Opts
+    precision::Int32
+    device::Int32
+    stream::Ptr{Cvoid}
+    index_base::Int32
+    graph_steps::Int32
+    dt0::Float64
+    batch::Int32
+    flags::Int32
+end
+
+mutable struct StepDiag
+    cr::Float64
+    cr_bin::Float64
+    cr_emi::Float64
+    cr_flux::Float64
+    sum_df::Float64
+    sum_f::Float64
+    finite::Int32
+    pad::Int32
+end
+StepDiag() = StepDiag(0, 0, 0, 0, 0, 0, 1, 0)
+
+# Device-resident state: Solve's `@. method.f = method.f_init` (Solver.jl:22) uploads through
+# dtb_set_f and `copyto!(f, method.f)` (Solver.jl:40) downloads through dtb_get_f.
+mutable struct B200State <: AbstractVector{Float64}
+    ctx::Ptr{Cvoid}
+    n::Int
+end
+Base.size(v::B200State) = (v.n,)
+Base.getindex(v::B200State, i::Int) = Base.copyto!(Vector{Float64}(undef, v.n), v)[i]
+function Base.copyto!(dest::Vector{Float64}, src::B200State)
+    GC.@preserve dest check(ccall((:dtb_get_f, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}), src.ctx, dest))
+    return dest
+end
+function Base.copyto!(dest::B200State, bc::Base.Broadcast.Broadcasted)
+    v = Vector{Float64}(Base.materialize(bc))
+    GC.@preserve v check(ccall((:dtb_set_f, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}), dest.ctx, v))
+    return dest
+end
+Base.BroadcastStyle(::Type{B200State}) = Base.Broadcast.DefaultArrayStyle{1}()
+
+check(rc) = rc == 0 || error("libdtb: ", unsafe_string(ccall((:dtb_last_error, libdtb), Cstring, ())))
+
+function upload_csc!(ctx, A::SparseMatrixCSC)
+    nnz(A) == 0 && return
+    nz = Float64.(A.nzval)
+    GC.@preserve A nz check(ccall((:dtb_add_flux_csc, libdtb), Int32,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}),
+        ctx, size(A, 1), A.colptr, A.rowval, nz))
+end
+
+# The stepping struct of the B200 backend. Same constructor arguments as ForwardEulerStruct
+# (SteppingStructs.jl:33) and the fields Solve reads (PhaseSpace, f_init, f).
+mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
+    PhaseSpace::PhaseSpaceStruct
+    dt0::Float64
+    f_init::Vector{Float64}
+    f::B200State
+    ctx::Ptr{Cvoid}
+
+    function B200ForwardEulerStruct(PhaseSpace::PhaseSpaceStruct, Initial::Vector{Float64}, Injection::Vector{Float64},
+                                    BinM, EmiM, FluxM; Adaptive::Bool=false, device::Integer=0)
+        Precision = getfield(Main, :Precision)
+        Momentum = PhaseSpace.Momentum
+        sizes = Momentum.px_num_list .* Momentum.py_num_list .* Momentum.pz_num_list
+        ns = length(sizes)
+        n_space = PhaseSpace.Space.x_num * PhaseSpace.Space.y_num * PhaseSpace.Space.z_num
+        dims = Dims(ns, n_space, ntuple(i -> i <= ns ? Int64(sizes[i]) : Int64(0), 16))
+        opts = Opts(Precision == Float32 ? DTB_F32 : DTB_F64, device, C_NULL, 1, 16, PhaseSpace.Time.dt0, 1, 0)
+        ctx = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:dtb_create, libdtb), Int32, (Ref{Dims}, Ref{Opts}, Ref{Ptr{Cvoid}}), dims, opts, ctx))
+        upload_csc!(ctx[], FluxM.X_Flux)   # F = X + P (SteppingStructs.jl:60)
+        upload_csc!(ctx[], FluxM.P_Flux)
+        n_mom = sum(sizes)
+        if !isempty(BinM.Binary_list)
+            M = Matrix{Float64}(BinM.M_Bin)
+            GC.@preserve M check(ccall((:dtb_upload_mbin_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
+                                       ctx[], M, n_mom))
+        end
+        if !isempty(EmiM.Emission_list)
+            E = Matrix{Float64}(EmiM.M_Emi)
+            GC.@preserve E check(ccall((:dtb_upload_emi_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
+                                       ctx[], E, size(E, 1)))
+        end
+        Ap = Float64.(FluxM.Ap_Flux); Vol = Float64.(FluxM.Vol)
+        GC.@preserve Ap Vol Initial Injection check(ccall((:dtb_upload_vectors, libdtb), Int32,
+            (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), ctx[], Ap, Vol, Initial, Injection))
+        check(ccall((:dtb_commit, libdtb), Int32, (Ptr{Cvoid},), ctx[]))
+        self = new(PhaseSpace, PhaseSpace.Time.dt0, copy(Initial), B200State(ctx[], length(Initial)), ctx[])
+        finalizer(m -> ccall((:dtb_destroy, libdtb), Int32, (Ptr{Cvoid},), m.ctx), self)
+        return self
+    end
+end
+
+# The functor (SteppingMethods.jl:12-107): one ccall per step; dt truncation happens in the
+# library exactly as in :18-23 and the diagnostics are printed like :87-93.
+function (method::B200ForwardEulerStruct)(t_start, t_stop, dt, Verbose::Int64)
+    dt_out = Ref{Float64}(0.0); save = Ref{Int32}(0); d = Ref(StepDiag())
+    check(ccall((:dtb_step, libdtb), Int32,
+        (Ptr{Cvoid}, Float64, Float64, Float64, Int32, Ref{Float64}, Ref{Int32}, Ref{StepDiag}),
+        method.ctx, t_start, t_stop, dt, Verbose, dt_out, save, d))
+    d[].finite == 0 && println("non-finite value in df calculation")
+    if Verbose == 1 && d[].cr > 1.0
+        println("Cr = $(d[].cr), t=$t_start, dt=$(dt_out[]), system may be unstable")
+    elseif Verbose == 2
+        println("\rCr = $(d[].cr), t=$t_start, dt=$(dt_out[])")
+    elseif Verbose == 3
+        println("Cr = $(d[].cr),Cr_Bin = $(d[].cr_bin), Cr_Emi = $(d[].cr_emi), Cr_Flux = $(d[].cr_flux), t=$t_start, t_save =$t_stop, dt=$(dt_out[])")
+    end
+    return dt_out[], save[] != 0
+end
+
+# Solve (Solver.jl:1-64) with each save interval replayed from CUDA graphs on the device.
+function b200_solve(method::B200ForwardEulerStruct, dt_initial::Float64, t_save::Vector{Float64}; Verbose::Int64=1)
+    n = length(method.f_init)
+    F = Matrix{Float64}(undef, n, length(t_save))  # column i = state at t_save[i]
+    nsteps = Ref{Int64}(0)
+    check(ccall((:dtb_solve, libdtb), Int32,
+        (Ptr{Cvoid}, Float64, Ptr{Float64}, Int64, Int32, Ptr{Float64}, Ref{Int64}),
+        method.ctx, dt_initial, t_save, length(t_save), Verbose, F, nsteps))
+    return F, nsteps[]
+end
+
+end # module
