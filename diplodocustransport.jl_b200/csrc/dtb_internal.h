@@ -113,4 +113,16 @@ constexpr int kRowsWarps = 8;
 
 void set_error(const std::string& msg);
 
+// Kernel-level gain contraction of one block (gain_op.cu).
+cudaError_t launch_row_sums(const double* partial, int n_rows, int splits, double* out, cudaStream_t s);
+}  // namespace dtb
+#include <vector>
+namespace dtb {
+int gain_op_plan(int64_t n_out, int64_t n1, int64_t n2, int esz, int num_sms, int bps, std::vector<GainUnit>& units,
+                 int& splits);
+int gain_op_run(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2, const void* f1, const void* f2,
+                double* out, const std::vector<GainUnit>& units, int splits, unsigned char* scratch, int* err,
+                cudaStream_t s);
+size_t gain_op_scratch_bytes(int64_t n_units, int64_t n1, int64_t n2, int esz);
+
 }  // namespace dtb

@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
                                                                      long long hist_cap, int verbose,
                                                                      double* blk_red, unsigned* ticket) {
     __shared__ double s_red[kRowsWarps][kRedFields];
+    __shared__ double s_fin[6][kRowsWarps * 32];
     __shared__ int s_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
@@ -437,30 +438,44 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         s_last = (t == gridDim.x - 1);
     }
     __syncthreads();
-    if (s_last && threadIdx.x == 0) {
+    if (s_last) {
+        // last block: reduce the per-block records in parallel (fixed assignment and a fixed
+        // tree, so the result does not depend on block completion order)
         __threadfence();
-        double r[kRedFields];
-        for (int k = 0; k < kRedFields; ++k) r[k] = __ldcg(blk_red + k);
-        for (unsigned b = 1; b < gridDim.x; ++b) {
+        double r[6] = {CUDART_INF, CUDART_INF, CUDART_INF, CUDART_INF, 0.0, 0.0};
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
             const double* src = blk_red + (size_t)b * kRedFields;
             for (int k = 0; k < 4; ++k) r[k] = jl_min(r[k], __ldcg(src + k));
             r[4] += __ldcg(src + 4);
             r[5] += __ldcg(src + 5);
         }
-        StepDiagDev d;
-        const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && r[5] != 0.0;
-        d.cr[0] = on ? -r[0] : 0.0;
-        d.cr[1] = (on && verbose == 3 && ops.has_bin) ? -r[1] : 0.0;
-        d.cr[2] = (on && verbose == 3 && ops.has_emi) ? -r[2] : 0.0;
-        d.cr[3] = (on && verbose == 3) ? -r[3] : 0.0;
-        d.sum_df = r[4];
-        d.sum_f = r[5];
-        d.finite = isfinite(r[4]) ? 1 : 0;
-        d.pad = 0;
-        hist[step % (unsigned long long)hist_cap] = d;
-        *ticket = 0u;
-        __threadfence();
-        *reinterpret_cast<volatile unsigned long long*>(ctr) = step + 1ull;
+        for (int k = 0; k < 6; ++k) s_fin[k][threadIdx.x] = r[k];
+        __syncthreads();
+        for (int o = kRowsWarps * 16; o > 0; o >>= 1) {
+            if (threadIdx.x < o) {
+                for (int k = 0; k < 4; ++k) s_fin[k][threadIdx.x] = jl_min(s_fin[k][threadIdx.x], s_fin[k][threadIdx.x + o]);
+                s_fin[4][threadIdx.x] += s_fin[4][threadIdx.x + o];
+                s_fin[5][threadIdx.x] += s_fin[5][threadIdx.x + o];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < 6; ++k) r[k] = s_fin[k][0];
+            StepDiagDev d;
+            const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && r[5] != 0.0;
+            d.cr[0] = on ? -r[0] : 0.0;
+            d.cr[1] = (on && verbose == 3 && ops.has_bin) ? -r[1] : 0.0;
+            d.cr[2] = (on && verbose == 3 && ops.has_emi) ? -r[2] : 0.0;
+            d.cr[3] = (on && verbose == 3) ? -r[3] : 0.0;
+            d.sum_df = r[4];
+            d.sum_f = r[5];
+            d.finite = isfinite(r[4]) ? 1 : 0;
+            d.pad = 0;
+            hist[step % (unsigned long long)hist_cap] = d;
+            *ticket = 0u;
+            __threadfence();
+            *reinterpret_cast<volatile unsigned long long*>(ctr) = step + 1ull;
+        }
     }
 }
 

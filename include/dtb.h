@@ -174,6 +174,19 @@ int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
 int32_t dtb_gain_kernel_stats(dtb_ctx* ctx, double* avg_ms, double* bytes_per_launch);
 int32_t dtb_set_profiling(dtb_ctx* ctx, int32_t on);
 
+/* ---- kernel-level entry ---- */
+
+/* out[a] = sum_b f1[b] sum_c G[a][b][c] f2[c] for one dense gain block in the caller's device
+ * memory: the two products of update_Big_Bin! (SteppingMethods.jl:372-373) for one
+ * (output, input-1, input-2) species block. G is row-major [n_out][n1][n2] with n2 a
+ * multiple of 8 and 16-byte aligned; f1 (n1), f2 (n2) are device vectors of the same dtype;
+ * out (n_out doubles) is a device vector. Runs asynchronously on `stream` (NULL: the legacy
+ * default stream) on the current device. Its scratch (work table, per-unit partial sums and a
+ * copy of f1|f2) is allocated on the first call on a device, grown when a larger block needs
+ * more, and kept until the process exits. Calls on one device are serialised on the host. */
+int32_t dtb_gain_contract(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2,
+                          const void* f1, const void* f2, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
