@@ -82,6 +82,7 @@ SIGNATURES = {
     "dtb_gain_kernel_stats": (_i32, [_P, _dp, _dp]),
     "dtb_set_profiling": (_i32, [_P, _i32]),
     "dtb_gain_contract": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
+    "dtb_gain_contract_noalloc": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -187,6 +187,22 @@ int32_t dtb_set_profiling(dtb_ctx* ctx, int32_t on);
 int32_t dtb_gain_contract(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2,
                           const void* f1, const void* f2, double* out, void* stream);
 
+/* dtb_gain_contract for callers that cannot call cudaMalloc; it has no counterpart in the
+ * reference. A host application that gives all device memory to its own pool allocator (a
+ * Julia session whose CUDA.jl pool owns the device heap, a serving process that reserved its
+ * HBM budget up front) or a latency-critical loop that cannot afford an allocator call uses
+ * this entry point: it allocates nothing. Same arguments and result as dtb_gain_contract; the
+ * scratch is a static device array of about 1.4 MB in libdtb.so, held by every GPU that
+ * loads the library until the process exits. Limits: n1 + n2 <= 16384 and at most 32768 work
+ * units (e.g. n_out = 1024, n1 = n2 = 1024 in FP32 needs 16384); larger blocks return
+ * DTB_EINVAL with a message. The first call on a device looks up the array's device address
+ * (set-up, once per device, with that device current); make that first call before any
+ * stream capture. Every call on a device shares the one array and it keeps the last call's
+ * contents (each call clears what must start at zero), so calls that overlap on the GPU
+ * (different streams, no ordering between them) race; order them on one stream. */
+int32_t dtb_gain_contract_noalloc(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2,
+                                  const void* f1, const void* f2, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
