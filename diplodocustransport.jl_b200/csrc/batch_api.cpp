@@ -1,0 +1,681 @@
+// Batched mixed-precision contexts (precision DTB_MIXED): many independent instances of one
+// grid share the operators; each slot holds one instance with its own f, dt/dt0 and step count.
+//
+// Per batched step: for every gain group (gain blocks sharing an input pair) one tcgen05 GEMM
+// of the stacked G rows (BF16 hi+lo, per-row power-of-two scale) against the batch of
+// vec(f1 x f2), then one epilogue kernel over all (row, instance) pairs. Slots step while the
+// device step counter is below their stop step, so requests of different lengths share one
+// captured graph; a finished slot keeps its state until it is read and re-admitted.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "batch_internal.h"
+#include "ctx.h"
+
+namespace dtb {
+
+struct MixedGroup {
+    int in1 = 0, in2 = 0;
+    int M = 0, N1 = 0, n2 = 0, n2p = 0, n_cb = 0;
+    std::vector<std::pair<int, int>> members;  // (output species, first stacked row)
+    __nv_bfloat16* hi = nullptr;
+    __nv_bfloat16* lo = nullptr;
+    float* row_scale = nullptr;
+    CUtensorMap tm_hi{}, tm_lo{};
+    float* partial = nullptr;
+    int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256;
+    double flops = 0;  // 3 MMAs x 2 x M x K x Bcap
+    double bytes = 0;  // hi + lo bytes of G
+};
+
+struct MixedState {
+    int Bcap = 0;
+    std::vector<MixedGroup> groups;
+    float* F[2] = {nullptr, nullptr};
+    float* C[2] = {nullptr, nullptr};
+    int cur = 0;
+    float* sig = nullptr;   // [ns][Bcap]
+    float* isig = nullptr;  // [ns][Bcap]
+    double* dt_scale = nullptr;
+    long long* stop_step = nullptr;
+    unsigned long long* min_ratio = nullptr;
+    int* nonfinite = nullptr;
+    unsigned long long* gstep = nullptr;
+    unsigned* ticket = nullptr;
+    long long host_step = 0;
+    MixedRowOps ops{};
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 16;
+    std::vector<long long> h_stop, h_start;
+    float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation
+    bool profiling = false;
+    double prof_ms = 0;
+    long long prof_n = 0;
+    std::vector<cudaEvent_t> ev;
+    int prof_pending = 0;
+};
+
+}  // namespace dtb
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+int make_map(CUtensorMap* tm, void* base, int64_t K, int64_t M) {
+    auto fn = encode_fn();
+    DTB_CHECK(fn, DTB_ECUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)M};
+    cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kMmaK, (cuuint32_t)kMmaM};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    DTB_CHECK(r == CUDA_SUCCESS, DTB_ECUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return DTB_OK;
+}
+
+unsigned long long ord_enc_host(double x) {
+    unsigned long long u;
+    std::memcpy(&u, &x, 8);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+double ord_dec_host(unsigned long long e) {
+    unsigned long long u = (e >> 63) ? (e & 0x7FFFFFFFFFFFFFFFull) : ~e;
+    double x;
+    std::memcpy(&x, &u, 8);
+    return x;
+}
+
+}  // namespace
+
+// Builds the device layouts of a DTB_MIXED context.
+int commit_mixed(dtb_ctx* c) {
+    DTB_CHECK(c->n_space == 1, DTB_EINVAL, "batched contexts hold single-cell instances (n_space must be 1)");
+    DTB_CHECK(c->opts.batch >= 1, DTB_EINVAL, "batched context needs opts.batch >= 1");
+    auto* m = new MixedState();
+    c->mixed = m;
+    m->Bcap = c->opts.batch;
+    if (c->opts.graph_steps > 0) m->graph_steps = (c->opts.graph_steps + 1) / 2 * 2;
+    MixedRowOps& ops = m->ops;
+    const int B = m->Bcap;
+    const int n_mom = (int)c->n_mom;
+    cudaStream_t s = c->stream;
+
+    // ---------------- gain groups
+    std::map<std::pair<int, int>, int> gidx;
+    for (auto& kv : c->gains) {
+        GainStage& g = kv.second;
+        auto key = std::make_pair(g.in1, g.in2);
+        if (!gidx.count(key)) {
+            gidx[key] = (int)m->groups.size();
+            MixedGroup G;
+            G.in1 = g.in1;
+            G.in2 = g.in2;
+            G.N1 = (int)c->sz[g.in1];
+            G.n2 = (int)c->sz[g.in2];
+            G.n2p = (int)round_up(G.n2, kMmaK);
+            G.n_cb = G.n2p / kMmaK;
+            m->groups.push_back(G);
+        }
+        MixedGroup& G = m->groups[(size_t)gidx[key]];
+        G.members.push_back({g.out, G.M});
+        G.M += (int)c->sz[g.out];
+    }
+    DTB_CHECK(m->groups.size() <= 16, DTB_EINVAL, "at most 16 input pairs in a batched context");
+    c->has_bin = !c->gains.empty() || !c->losses.empty();
+    const int bn = B >= 192 ? 256 : (B > 64 ? 128 : 64);
+    for (auto& kv : c->gains) {
+        GainStage& g = kv.second;
+        MixedGroup& G = m->groups[(size_t)gidx[{g.in1, g.in2}]];
+        if (!G.hi) {
+            const size_t K = (size_t)G.N1 * G.n2p;
+            DTB_TRY(c->alloc(&G.hi, sizeof(__nv_bfloat16) * K * G.M));
+            DTB_TRY(c->alloc(&G.lo, sizeof(__nv_bfloat16) * K * G.M));
+            DTB_TRY(c->alloc(&G.row_scale, sizeof(float) * G.M));
+        }
+        int roff = 0;
+        for (auto& mb : G.members)
+            if (mb.first == g.out) roff = mb.second;
+        const int64_t no = c->sz[g.out];
+        const size_t elems = (size_t)(no * G.N1 * G.n2);
+        const size_t K = (size_t)G.N1 * G.n2p;
+        float* tmp = nullptr;
+        const float* srcf = nullptr;
+        if (!g.host.empty()) {
+            DTB_CHECK(g.dev_src.empty(), DTB_EINVAL, "a gain block cannot mix host and device uploads");
+            std::vector<float> h(elems);
+            for (size_t k = 0; k < elems; ++k) h[k] = (float)g.host[k];
+            DTB_CUDA(cudaMalloc(&tmp, sizeof(float) * elems));
+            DTB_CUDA(cudaMemcpy(tmp, h.data(), sizeof(float) * elems, cudaMemcpyHostToDevice));
+            srcf = tmp;
+        } else {
+            DTB_CHECK(g.dev_src.size() == 1, DTB_EINVAL, "a device-resident gain block must be uploaded once");
+            if (g.dev_src[0].second == DTB_DTYPE_F32) {
+                srcf = static_cast<const float*>(g.dev_src[0].first);
+            } else {
+                DTB_CUDA(cudaMalloc(&tmp, sizeof(float) * elems));
+                cudaError_t ce = launch_pad_rows<double, float>(static_cast<const double*>(g.dev_src[0].first),
+                                                                (long long)(no * G.N1), G.n2, tmp, G.n2, s);
+                DTB_CUDA(ce);
+                srcf = tmp;
+            }
+        }
+        DTB_CUDA(launch_split_rows(srcf, no, G.N1, G.n2, G.n2p, G.hi + (size_t)roff * K, G.lo + (size_t)roff * K,
+                                   G.row_scale + roff, nullptr, s));
+        DTB_CUDA(cudaStreamSynchronize(s));
+        if (tmp) cudaFree(tmp);
+        g.host.clear();
+        g.host.shrink_to_fit();
+    }
+    DTB_CUDA(prepare_gain_gemm(bn));
+    for (auto& G : m->groups) {
+        const int64_t K = (int64_t)G.N1 * G.n2p;
+        DTB_TRY(make_map(&G.tm_hi, G.hi, K, G.M));
+        DTB_TRY(make_map(&G.tm_lo, G.lo, K, G.M));
+        G.bn = bn;
+        G.n_tiles = (B + bn - 1) / bn;
+        G.Bpad = G.n_tiles * bn;
+        G.m_tiles = (G.M + kMmaM - 1) / kMmaM;
+        const int T = G.n_cb * G.N1;
+        int S = std::max(1, (int)std::lround((double)c->num_sms / (G.m_tiles * G.n_tiles)));
+        S = std::min(S, T);
+        G.tiles_per_split = (T + S - 1) / S;
+        G.n_splits = (T + G.tiles_per_split - 1) / G.tiles_per_split;
+        DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
+        G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * B;
+        G.bytes = 4.0 * G.M * (double)G.N1 * G.n2;
+    }
+    // ---------------- gain lookup per species
+    {
+        int e = 0;
+        for (int sp = 0; sp < c->ns; ++sp) {
+            ops.gain_ptr[sp] = e;
+            for (size_t gi = 0; gi < m->groups.size(); ++gi)
+                for (auto& mb : m->groups[gi].members)
+                    if (mb.first == sp) {
+                        DTB_CHECK(e < 64, DTB_EINVAL, "too many gain blocks per species");
+                        ops.gain_grp[e] = (int)gi;
+                        ops.gain_roff[e] = mb.second;
+                        ++e;
+                    }
+        }
+        ops.gain_ptr[c->ns] = e;
+    }
+    // ---------------- loss (FP32), grouped by row species
+    {
+        std::vector<long long> doff;
+        std::vector<int> ld, coff, ncols;
+        std::vector<double> data;
+        for (int sp = 0; sp < c->ns; ++sp) {
+            ops.loss_ptr[sp] = (int)doff.size();
+            for (auto& kv : c->losses) {
+                if (kv.first.first != sp) continue;
+                const int oth = kv.first.second;
+                const int64_t nr = c->sz[sp], nc = c->sz[oth];
+                doff.push_back((long long)data.size());
+                ld.push_back((int)nc);
+                coff.push_back((int)c->off[oth]);
+                ncols.push_back((int)nc);
+                data.insert(data.end(), kv.second.begin(), kv.second.begin() + nr * nc);
+            }
+        }
+        ops.loss_ptr[c->ns] = (int)doff.size();
+        long long* d_doff;
+        int *d_ld, *d_coff, *d_nc;
+        float* d_data;
+        DTB_TRY(copy_host_ints(c, &d_doff, doff));
+        DTB_TRY(copy_host_ints(c, &d_ld, ld));
+        DTB_TRY(copy_host_ints(c, &d_coff, coff));
+        DTB_TRY(copy_host_ints(c, &d_nc, ncols));
+        DTB_TRY(copy_host_vec(c, &d_data, data));
+        ops.loss_data_off = d_doff;
+        ops.loss_ld = d_ld;
+        ops.loss_col_off = d_coff;
+        ops.loss_ncols = d_nc;
+        ops.loss_data = d_data;
+    }
+    // ---------------- emission pieces: BF16 hi+lo with a power-of-two scale per piece row
+    {
+        c->has_emi = !c->emis.empty();
+        std::vector<long long> doff;
+        std::vector<int> ld, r0v, c0v, ncv, soff;
+        std::vector<std::vector<int>> rows((size_t)n_mom);
+        long long total = 0;
+        int srows = 0;
+        for (size_t p = 0; p < c->emis.size(); ++p) {
+            const EmiPiece& e = c->emis[p];
+            doff.push_back(total);
+            ld.push_back((int)e.ncols);
+            r0v.push_back((int)e.row0);
+            c0v.push_back((int)e.col0);
+            ncv.push_back((int)e.ncols);
+            soff.push_back(srows);
+            total += e.nrows * e.ncols;
+            srows += (int)e.nrows;
+            for (int64_t r = 0; r < e.nrows; ++r) rows[(size_t)(e.row0 + r)].push_back((int)p);
+        }
+        __nv_bfloat162* d_data = nullptr;
+        float* d_scale = nullptr;
+        DTB_TRY(c->alloc(&d_data, sizeof(__nv_bfloat162) * (size_t)std::max<long long>(1, total)));
+        DTB_TRY(c->alloc(&d_scale, sizeof(float) * (size_t)std::max(1, srows)));
+        for (size_t p = 0; p < c->emis.size(); ++p) {
+            const EmiPiece& e = c->emis[p];
+            std::vector<float> h(e.data.begin(), e.data.end());
+            float* tmp = nullptr;
+            DTB_CUDA(cudaMalloc(&tmp, sizeof(float) * h.size()));
+            DTB_CUDA(cudaMemcpy(tmp, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+            DTB_CUDA(launch_split_emi(tmp, (int)e.nrows, (int)e.ncols, (int)e.ncols, d_data + doff[p], d_scale + soff[p], s));
+            DTB_CUDA(cudaStreamSynchronize(s));
+            cudaFree(tmp);
+        }
+        std::vector<int> rptr((size_t)n_mom + 1, 0), piece;
+        for (int i = 0; i < n_mom; ++i) {
+            rptr[(size_t)i] = (int)piece.size();
+            for (int p : rows[(size_t)i]) piece.push_back(p);
+        }
+        rptr[(size_t)n_mom] = (int)piece.size();
+        int *d_rptr, *d_piece, *d_ld, *d_r0, *d_c0, *d_nc, *d_soff;
+        long long* d_doff;
+        DTB_TRY(copy_host_ints(c, &d_rptr, rptr));
+        DTB_TRY(copy_host_ints(c, &d_piece, piece));
+        DTB_TRY(copy_host_ints(c, &d_doff, doff));
+        DTB_TRY(copy_host_ints(c, &d_ld, ld));
+        DTB_TRY(copy_host_ints(c, &d_r0, r0v));
+        DTB_TRY(copy_host_ints(c, &d_c0, c0v));
+        DTB_TRY(copy_host_ints(c, &d_nc, ncv));
+        DTB_TRY(copy_host_ints(c, &d_soff, soff));
+        ops.emi_rptr = d_rptr;
+        ops.emi_piece = d_piece;
+        ops.emi_data_off = d_doff;
+        ops.emi_ld = d_ld;
+        ops.emi_row0 = d_r0;
+        ops.emi_col0 = d_c0;
+        ops.emi_ncols = d_nc;
+        ops.emi_data = d_data;
+        ops.emi_scale = d_scale;
+        ops.emi_scale_off = d_soff;
+    }
+    // ---------------- flux: CSR with duplicates summed, banded ELL (FP32), padding column -1
+    {
+        std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)n_mom);
+        for (size_t p = 0; p < c->flux_r.size(); ++p) rows[(size_t)c->flux_r[p]].push_back({c->flux_c[p], c->flux_v[p]});
+        int w = 0;
+        for (auto& r : rows) {
+            std::stable_sort(r.begin(), r.end(), [](auto& x, auto& y) { return x.first < y.first; });
+            std::vector<std::pair<int64_t, double>> mm;
+            for (auto& e : r) {
+                if (!mm.empty() && mm.back().first == e.first)
+                    mm.back().second += e.second;
+                else
+                    mm.push_back(e);
+            }
+            r.swap(mm);
+            w = std::max<int>(w, (int)r.size());
+        }
+        w = std::max(w, 1);
+        std::vector<double> val((size_t)n_mom * w, 0.0);
+        std::vector<int> col((size_t)n_mom * w, -1);
+        for (int i = 0; i < n_mom; ++i)
+            for (size_t k = 0; k < rows[(size_t)i].size(); ++k) {
+                col[(size_t)i * w + k] = (int)rows[(size_t)i][k].first;
+                val[(size_t)i * w + k] = rows[(size_t)i][k].second;
+            }
+        float* d_val;
+        int* d_col;
+        DTB_TRY(copy_host_vec(c, &d_val, val));
+        DTB_TRY(copy_host_ints(c, &d_col, col));
+        ops.ell_w = w;
+        ops.ell_val = d_val;
+        ops.ell_col = d_col;
+    }
+    // ---------------- vectors and state
+    {
+        std::vector<double> invAp(c->Ap.size());
+        for (size_t i = 0; i < invAp.size(); ++i) invAp[i] = (double)(1.0f / (float)c->Ap[i]);
+        float *d_inv, *d_inj;
+        DTB_TRY(copy_host_vec(c, &d_inv, invAp));
+        DTB_TRY(copy_host_vec(c, &d_inj, c->inj));
+        ops.invAp = d_inv;
+        ops.inj = d_inj;
+        ops.vol = (float)c->Vol[0];
+    }
+    const size_t nb = (size_t)n_mom * B;
+    for (int k = 0; k < 2; ++k) {
+        DTB_TRY(c->alloc(&m->F[k], sizeof(float) * nb));
+        DTB_TRY(c->alloc(&m->C[k], sizeof(float) * nb));
+        DTB_CUDA(cudaMemset(m->F[k], 0, sizeof(float) * nb));
+        DTB_CUDA(cudaMemset(m->C[k], 0, sizeof(float) * nb));
+    }
+    DTB_TRY(c->alloc(&m->sig, sizeof(float) * (size_t)c->ns * B));
+    DTB_TRY(c->alloc(&m->isig, sizeof(float) * (size_t)c->ns * B));
+    {
+        std::vector<float> ones((size_t)c->ns * B, 1.0f);
+        DTB_CUDA(cudaMemcpy(m->sig, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice));
+        DTB_CUDA(cudaMemcpy(m->isig, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice));
+    }
+    DTB_TRY(c->alloc(&m->dt_scale, sizeof(double) * B));
+    DTB_TRY(c->alloc(&m->stop_step, sizeof(long long) * B));
+    DTB_TRY(c->alloc(&m->min_ratio, sizeof(unsigned long long) * B));
+    DTB_TRY(c->alloc(&m->nonfinite, sizeof(int) * B));
+    DTB_TRY(c->alloc(&m->gstep, sizeof(unsigned long long)));
+    DTB_TRY(c->alloc(&m->ticket, sizeof(unsigned)));
+    DTB_TRY(c->alloc(&c->err, sizeof(int)));
+    DTB_CUDA(cudaMemset(m->dt_scale, 0, sizeof(double) * B));
+    DTB_CUDA(cudaMemset(m->stop_step, 0, sizeof(long long) * B));
+    DTB_CUDA(cudaMemset(m->nonfinite, 0, sizeof(int) * B));
+    DTB_CUDA(cudaMemset(m->gstep, 0, sizeof(unsigned long long)));
+    DTB_CUDA(cudaMemset(m->ticket, 0, sizeof(unsigned)));
+    DTB_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+    {
+        std::vector<unsigned long long> inf((size_t)B, ord_enc_host(INFINITY));
+        DTB_CUDA(cudaMemcpy(m->min_ratio, inf.data(), sizeof(unsigned long long) * B, cudaMemcpyHostToDevice));
+    }
+    DTB_CUDA(cudaMallocHost(&m->pin_col, sizeof(float) * 2 * (size_t)n_mom));
+    DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));
+    m->h_stop.assign((size_t)B, 0);
+    m->h_start.assign((size_t)B, 0);
+    ops.n_mom = n_mom;
+    ops.Bcap = B;
+    ops.n_species = c->ns;
+    for (int sp = 0; sp <= c->ns; ++sp) ops.sp_off[sp] = (int)c->off[sp];
+    for (size_t gi = 0; gi < m->groups.size(); ++gi) {
+        const MixedGroup& G = m->groups[gi];
+        ops.grp_partial[gi] = G.partial;
+        ops.grp_scale[gi] = G.row_scale;
+        ops.grp_sig1[gi] = m->sig + (size_t)G.in1 * B;
+        ops.grp_sig2[gi] = m->sig + (size_t)G.in2 * B;
+        ops.grp_M[gi] = G.M;
+        ops.grp_splits[gi] = G.n_splits;
+        ops.grp_Bpad[gi] = G.Bpad;
+    }
+    ops.thr = (double)1e-10f;
+    ops.has_bin = c->has_bin;
+    ops.has_emi = c->has_emi;
+    ops.dt_scale = m->dt_scale;
+    ops.stop_step = m->stop_step;
+    ops.min_ratio = m->min_ratio;
+    ops.nonfinite = m->nonfinite;
+    for (auto& G : m->groups) c->gain_bytes += G.bytes;
+    DTB_CUDA(cudaDeviceSynchronize());
+    return DTB_OK;
+}
+
+void destroy_mixed(dtb_ctx* c) {
+    MixedState* m = c->mixed;
+    if (!m) return;
+    if (m->graph) cudaGraphExecDestroy(m->graph);
+    for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
+    if (m->pin_col) cudaFreeHost(m->pin_col);
+    delete m;
+    c->mixed = nullptr;
+}
+
+namespace {
+
+int mixed_flush_profile(MixedState* m) {
+    if (m->prof_pending == 0) return DTB_OK;
+    DTB_CUDA(cudaEventSynchronize(m->ev[(size_t)(2 * (m->prof_pending - 1) + 1)]));
+    for (int k = 0; k < m->prof_pending; ++k) {
+        float ms = 0;
+        DTB_CUDA(cudaEventElapsedTime(&ms, m->ev[(size_t)(2 * k)], m->ev[(size_t)(2 * k + 1)]));
+        m->prof_ms += ms;
+    }
+    m->prof_pending = 0;
+    return DTB_OK;
+}
+
+int mixed_step(dtb_ctx* c, bool profile) {
+    MixedState* m = c->mixed;
+    const float* Fin = m->F[m->cur];
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (profile) {
+        const size_t k = (size_t)m->prof_pending * 2;
+        while (m->ev.size() < k + 2) {
+            cudaEvent_t e;
+            DTB_CUDA(cudaEventCreate(&e));
+            m->ev.push_back(e);
+        }
+        e0 = m->ev[k];
+        e1 = m->ev[k + 1];
+        DTB_CUDA(cudaEventRecord(e0, c->stream));
+    }
+    for (auto& G : m->groups) {
+        GemmArgs a;
+        a.M = G.M;
+        a.N1 = G.N1;
+        a.n2 = G.n2;
+        a.n_cb = G.n_cb;
+        a.off1 = (int)c->off[G.in1];
+        a.off2 = (int)c->off[G.in2];
+        a.tiles_per_split = G.tiles_per_split;
+        a.n_splits = G.n_splits;
+        a.m_tiles = G.m_tiles;
+        a.n_tiles = G.n_tiles;
+        a.Bcap = m->Bcap;
+        a.Bpad = G.Bpad;
+        a.F = Fin;
+        a.isig1 = m->isig + (size_t)G.in1 * m->Bcap;
+        a.isig2 = m->isig + (size_t)G.in2 * m->Bcap;
+        a.partial = G.partial;
+        a.err = c->err;
+        DTB_CUDA(launch_gain_gemm(G.bn, &G.tm_hi, &G.tm_lo, a, c->stream));
+    }
+    if (profile) {
+        DTB_CUDA(cudaEventRecord(e1, c->stream));
+        m->prof_n++;
+        if (++m->prof_pending == 256) DTB_TRY(mixed_flush_profile(m));
+    }
+    DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, m->ticket,
+                               c->stream));
+    m->cur ^= 1;
+    m->host_step++;
+    return DTB_OK;
+}
+
+int mixed_check_err(dtb_ctx* c) {
+    DTB_CUDA(cudaMemcpyAsync(c->pin_err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    if (*c->pin_err) {
+        const int e = *c->pin_err;
+        cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
+        set_error("a bounded device wait gave up in the batched step (kernel error flags " + std::to_string(e) + ")");
+        return DTB_ETIMEOUT;
+    }
+    return DTB_OK;
+}
+
+int mixed_ready(dtb_ctx* c) {
+    DTB_CHECK(c, DTB_EINVAL, "null context");
+    DTB_CHECK(c->prec == DTB_MIXED, DTB_ESTATE, "not a batched (DTB_MIXED) context");
+    DTB_TRY(dtb_commit(c));
+    return DTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_scale, int64_t n_steps) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_admit: slot out of range");
+    DTB_CHECK(f0, DTB_EINVAL, "dtb_batch_admit: null f0");
+    DTB_CHECK(n_steps >= 0 && std::isfinite(dt_scale), DTB_EINVAL, "dtb_batch_admit: bad dt_scale or step count");
+    DeviceGuard g(c->device);
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    const int n = (int)c->n_mom, B = m->Bcap;
+    for (int i = 0; i < n; ++i) {
+        m->pin_col[i] = (float)f0[i];
+        m->pin_col[n + i] = (float)(f0[i] - (double)(float)f0[i]);  // exact remainder as the compensation
+    }
+    float* Fd = m->F[m->cur] + slot;
+    float* Cd = m->C[m->cur] + slot;
+    DTB_CUDA(cudaMemcpy2DAsync(Fd, sizeof(float) * B, m->pin_col, sizeof(float), sizeof(float), n,
+                               cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaMemcpy2DAsync(Cd, sizeof(float) * B, m->pin_col + n, sizeof(float), sizeof(float), n,
+                               cudaMemcpyHostToDevice, c->stream));
+    // power-of-two species scales from the initial spectrum: X uses f * 2^-e
+    std::vector<float> sg((size_t)c->ns), isg((size_t)c->ns);
+    for (int sp = 0; sp < c->ns; ++sp) {
+        double mx = 0;
+        for (int64_t k = c->off[sp]; k < c->off[sp + 1]; ++k) mx = std::max(mx, std::fabs(f0[k]));
+        int ex = 0;
+        if (mx > 0 && std::isfinite(mx)) std::frexp(mx, &ex);
+        sg[(size_t)sp] = std::ldexp(1.0f, ex);
+        isg[(size_t)sp] = std::ldexp(1.0f, -ex);
+    }
+    for (int sp = 0; sp < c->ns; ++sp) {
+        DTB_CUDA(cudaMemcpyAsync(m->sig + (size_t)sp * B + slot, &sg[(size_t)sp], sizeof(float), cudaMemcpyHostToDevice,
+                                 c->stream));
+        DTB_CUDA(cudaMemcpyAsync(m->isig + (size_t)sp * B + slot, &isg[(size_t)sp], sizeof(float),
+                                 cudaMemcpyHostToDevice, c->stream));
+    }
+    const long long stop = m->host_step + n_steps;
+    const unsigned long long inf = ord_enc_host(INFINITY);
+    const int zero = 0;
+    DTB_CUDA(cudaMemcpyAsync(m->dt_scale + slot, &dt_scale, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(m->stop_step + slot, &stop, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(m->min_ratio + slot, &inf, sizeof(inf), cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(m->nonfinite + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    m->h_stop[(size_t)slot] = stop;
+    m->h_start[(size_t)slot] = m->host_step;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
+    DTB_TRY(mixed_ready(c));
+    DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_batch_run: nsteps < 0");
+    MixedState* m = c->mixed;
+    DeviceGuard g(c->device);
+    int64_t done = 0;
+    if (!m->profiling && nsteps >= m->graph_steps) {
+        if (m->cur != 0) {
+            DTB_TRY(mixed_step(c, false));
+            done++;
+        }
+        if (!m->graph) {
+            const long long hs = m->host_step;
+            cudaGraph_t gr;
+            DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = DTB_OK;
+            for (int k = 0; k < m->graph_steps && rc == DTB_OK; ++k) rc = mixed_step(c, false);
+            cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+            m->host_step = hs;
+            m->cur = 0;
+            if (rc != DTB_OK) return rc;
+            DTB_CUDA(e);
+            e = cudaGraphInstantiate(&m->graph, gr, 0);
+            cudaGraphDestroy(gr);
+            DTB_CUDA(e);
+        }
+        while (nsteps - done >= m->graph_steps) {
+            DTB_CUDA(cudaGraphLaunch(m->graph, c->stream));
+            done += m->graph_steps;
+            m->host_step += m->graph_steps;
+        }
+    }
+    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, m->profiling));
+    if (m->profiling) DTB_TRY(mixed_flush_profile(m));
+    return mixed_check_err(c);
+}
+
+int32_t dtb_batch_get_f(dtb_ctx* c, int32_t slot, double* f) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_get_f: slot out of range");
+    DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f: null output");
+    DeviceGuard g(c->device);
+    const int n = (int)c->n_mom, B = m->Bcap;
+    DTB_CUDA(cudaMemcpy2DAsync(m->pin_col, sizeof(float), m->F[m->cur] + slot, sizeof(float) * B, sizeof(float), n,
+                               cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaMemcpy2DAsync(m->pin_col + n, sizeof(float), m->C[m->cur] + slot, sizeof(float) * B, sizeof(float), n,
+                               cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < n; ++i) f[i] = (double)m->pin_col[i] + (double)m->pin_col[n + i];
+    return DTB_OK;
+}
+
+int32_t dtb_batch_slot_info(dtb_ctx* c, int32_t slot, int64_t* steps_done, int64_t* steps_left, double* cr_max,
+                            int32_t* finite) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_slot_info: slot out of range");
+    DeviceGuard g(c->device);
+    const long long stop = m->h_stop[(size_t)slot];
+    const long long now = std::min(m->host_step, stop);
+    if (steps_done) *steps_done = std::max(0LL, now - m->h_start[(size_t)slot]);
+    if (steps_left) *steps_left = std::max(0LL, stop - m->host_step);
+    if (cr_max || finite) {
+        unsigned long long e = 0;
+        int nf = 0;
+        DTB_CUDA(cudaMemcpyAsync(&e, m->min_ratio + slot, sizeof(e), cudaMemcpyDeviceToHost, c->stream));
+        DTB_CUDA(cudaMemcpyAsync(&nf, m->nonfinite + slot, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+        if (cr_max) *cr_max = -ord_dec_host(e);
+        if (finite) *finite = nf ? 0 : 1;
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_batch_release(dtb_ctx* c, int32_t slot) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_release: slot out of range");
+    DeviceGuard g(c->device);
+    const long long zero = 0;
+    DTB_CUDA(cudaMemcpyAsync(m->stop_step + slot, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    m->h_stop[(size_t)slot] = 0;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_capacity(dtb_ctx* c, int32_t* capacity, int64_t* step) {
+    DTB_TRY(mixed_ready(c));
+    if (capacity) *capacity = c->mixed->Bcap;
+    if (step) *step = c->mixed->host_step;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_set_profiling(dtb_ctx* c, int32_t on) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    if (m->profiling && m->prof_pending) DTB_TRY(mixed_flush_profile(m));
+    m->profiling = on != 0;
+    m->prof_ms = 0;
+    m->prof_n = 0;
+    m->prof_pending = 0;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_gemm_stats(dtb_ctx* c, double* avg_ms, double* flops_per_step, double* bytes_per_step,
+                             int32_t* launches_per_step) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    double fl = 0, by = 0;
+    for (auto& G : m->groups) {
+        fl += G.flops;
+        by += G.bytes;
+    }
+    if (avg_ms) *avg_ms = m->prof_n ? m->prof_ms / (double)m->prof_n : 0.0;
+    if (flops_per_step) *flops_per_step = fl;
+    if (bytes_per_step) *bytes_per_step = by;
+    if (launches_per_step) *launches_per_step = (int32_t)m->groups.size() + 1;
+    return DTB_OK;
+}
+
+}  // extern "C"

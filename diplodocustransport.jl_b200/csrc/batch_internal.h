@@ -1,0 +1,93 @@
+// Internal declarations of the batched mixed-precision path (kernels_batch.cu, batch_api.cpp).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dtb_internal.h"
+
+namespace dtb {
+
+constexpr int kMmaM = 128;  // rows of one UMMA tile (G rows)
+constexpr int kMmaK = 64;   // K per stage: one 128-byte swizzle row of BF16
+
+// Arguments of one gain-group GEMM: Y[i][r] = sum_k G[r][k] X[k][i] for the stacked output
+// rows r of all gain blocks that share the input pair (in1, in2), with
+// X[b * n2p + c][i] = (f_in1[b][i] * isig1[i]) * (f_in2[c][i] * isig2[i]).
+struct GemmArgs {
+    int M;          // stacked rows of the group
+    int N1;         // states of input species 1
+    int n2;         // states of input species 2 (unpadded)
+    int n_cb;       // 64-wide blocks of input species 2 (n2 padded to 64)
+    int off1, off2; // state offsets of the two input species
+    int tiles_per_split, n_splits, m_tiles, n_tiles;
+    int Bcap;       // instance stride of the state matrix F[n][Bcap]
+    int Bpad;       // n_tiles * BN, instance stride of the partial rows
+    const float* F;
+    const float* isig1;  // [Bcap] reciprocal power-of-two scale of species in1 per instance
+    const float* isig2;
+    float* partial;      // [n_splits][Bpad][M]
+    int* err;
+};
+
+cudaError_t launch_gain_gemm(int bn, const CUtensorMap* tm_hi, const CUtensorMap* tm_lo, const GemmArgs& a,
+                             cudaStream_t s);
+int gain_gemm_smem_bytes(int bn);
+cudaError_t prepare_gain_gemm(int bn);
+
+// Per-row operands of the batched Euler epilogue.
+struct MixedRowOps {
+    int n_mom, Bcap, n_species;
+    int sp_off[DTB_MAX_SPECIES + 1];
+    int ell_w;
+    const float* ell_val;
+    const int* ell_col;
+    const int* emi_rptr;
+    const int* emi_piece;
+    const long long* emi_data_off;
+    const int* emi_ld;
+    const int* emi_row0;
+    const int* emi_col0;
+    const int* emi_ncols;
+    const __nv_bfloat162* emi_data;  // (hi, lo) pairs of E / scale of the piece row
+    const float* emi_scale;          // per piece row
+    const int* emi_scale_off;        // per piece: index of its first row in emi_scale
+    int loss_ptr[DTB_MAX_SPECIES + 1];
+    const long long* loss_data_off;
+    const int* loss_ld;
+    const int* loss_col_off;
+    const int* loss_ncols;
+    const float* loss_data;
+    // gain: for a row of species s, entries [gain_ptr[s], gain_ptr[s+1]) give (group, row offset)
+    int gain_ptr[DTB_MAX_SPECIES + 1];
+    int gain_grp[64];
+    int gain_roff[64];
+    const float* grp_partial[16];
+    const float* grp_scale[16];   // per stacked row, the power-of-two scale of G
+    const float* grp_sig1[16];    // [Bcap] power-of-two scale of the input species
+    const float* grp_sig2[16];
+    int grp_M[16];
+    int grp_splits[16];
+    int grp_Bpad[16];
+    const float* invAp;
+    const float* inj;
+    float vol;
+    double thr;
+    int has_bin, has_emi;
+    const double* dt_scale;          // [Bcap]
+    const long long* stop_step;      // [Bcap]: the slot steps while gstep < stop_step
+    unsigned long long* min_ratio;   // [Bcap] ordered encoding of min(df / f) over the run
+    int* nonfinite;                  // [Bcap]
+};
+
+cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out,
+                              float* C_out, unsigned long long* gstep, unsigned* ticket, cudaStream_t s);
+
+cudaError_t launch_split_rows(const float* src, long long rows, int n1, int n2, int n2p, __nv_bfloat16* hi,
+                              __nv_bfloat16* lo, float* row_scale, int* err, cudaStream_t s);
+cudaError_t launch_split_emi(const float* src, int rows, int ncols, int ld, __nv_bfloat162* dst, float* row_scale,
+                             cudaStream_t s);
+
+}  // namespace dtb

@@ -16,7 +16,7 @@
 #include <tuple>
 #include <vector>
 
-#include "dtb_internal.h"
+#include "ctx.h"
 
 namespace dtb {
 thread_local std::string g_err;
@@ -25,157 +25,8 @@ void set_error(const std::string& msg) { g_err = msg; }
 
 using namespace dtb;
 
-#define DTB_CUDA(call)                                                                        \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess) {                                                              \
-            set_error(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" + \
-                      std::to_string(__LINE__) + ")");                                        \
-            return e_ == cudaErrorMemoryAllocation ? DTB_ENOMEM : DTB_ECUDA;                  \
-        }                                                                                     \
-    } while (0)
-
-#define DTB_CHECK(cond, code, msg) \
-    do {                           \
-        if (!(cond)) {             \
-            set_error(msg);        \
-            return (code);         \
-        }                          \
-    } while (0)
-
-namespace {
-
-constexpr int kProfRing = 256;
-constexpr int64_t kMaxScheduleSteps = 100000000;
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
-
-struct GainStage {
-    int out, in1, in2;
-    std::vector<double> host;  // [no][n1][n2], FP64 sum of all host uploads
-    std::vector<std::pair<const void*, int>> dev_src;  // device sources (pointer, dtype), added in order
-};
-
-struct EmiPiece {
-    int64_t row0, nrows, col0, ncols;
-    std::vector<double> data;  // row-major
-};
-
-inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
-
-}  // namespace
-
-struct dtb_ctx {
-    dtb_dims dims{};
-    dtb_opts opts{};
-    int ns = 0;
-    int64_t sz[DTB_MAX_SPECIES]{};
-    int64_t off[DTB_MAX_SPECIES + 1]{};
-    int64_t offp[DTB_MAX_SPECIES + 1]{};
-    int64_t n_mom = 0, n_state = 0;
-    int n_space = 1;
-    int prec = DTB_F64;
-    size_t esz = 8;
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-
-    // host staging
-    std::map<std::tuple<int, int, int>, GainStage> gains;
-    std::map<std::pair<int, int>, std::vector<double>> losses;
-    std::vector<EmiPiece> emis;
-    std::vector<int64_t> flux_r, flux_c;
-    std::vector<double> flux_v;
-    std::vector<double> Ap, Vol, f_init, inj;
-    bool have_vectors = false;
-    bool committed = false;
-
-    // device memory
-    std::vector<void*> allocs;
-    size_t dev_bytes = 0;
-    void* G_all = nullptr;
-    double gain_bytes = 0;  // algorithmic gain bytes per step (one read of every G element)
-    GainUnit* units = nullptr;
-    int n_units = 0;
-    int gain_grid = 0;
-    int f_smem_len = 0;
-    int* unit_ptr = nullptr;
-    double* partial = nullptr;
-    void* f_buf[2] = {nullptr, nullptr};
-    void* f_init_dev = nullptr;
-    int cur = 0;
-    double* dt_arr = nullptr;
-    long long hist_cap = 65536;
-    unsigned long long* ctr = nullptr;
-    unsigned long long host_ctr = 0;
-    StepDiagDev* hist = nullptr;
-    double* blk_red = nullptr;
-    unsigned* ticket = nullptr;
-    int* err = nullptr;
-    int* sp_off_dev = nullptr;
-    double* mom_w = nullptr;
-    double* mom_out = nullptr;
-    int sp_off_host[2 * DTB_MAX_SPECIES + 2]{};
-    RowOps<double> ops_d{};
-    RowOps<float> ops_f{};
-    bool has_bin = false, has_emi = false;
-
-    // pinned staging
-    double* pin_dt = nullptr;
-    StepDiagDev* pin_hist = nullptr;
-    int* pin_err = nullptr;
-    float* pin_f32 = nullptr;  // FP32 state staging for dtb_get_f / dtb_set_f
-
-    // graphs
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 16;
-    int graph_verbose = -1;
-
-    // profiling
-    bool profiling = false;
-    double prof_ms = 0.0;
-    long long prof_n = 0;
-    int prof_pending = 0;
-    std::vector<cudaEvent_t> ev;
-
-    template <typename P>
-    int alloc(P** p, size_t bytes) {
-        void* q = nullptr;
-        if (bytes == 0) bytes = 16;
-        cudaError_t e = cudaMalloc(&q, bytes);
-        if (e != cudaSuccess) {
-            set_error("cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
-            return DTB_ENOMEM;
-        }
-        allocs.push_back(q);
-        dev_bytes += bytes;
-        *p = reinterpret_cast<P*>(q);
-        return DTB_OK;
-    }
-    void free_all() {
-        for (void* p : allocs) cudaFree(p);
-        allocs.clear();
-        dev_bytes = 0;
-    }
-};
-
-#define DTB_TRY(expr)              \
-    do {                           \
-        int rc_ = (expr);          \
-        if (rc_ != DTB_OK) return rc_; \
-    } while (0)
+int commit_mixed(dtb_ctx* c);     // batch_api.cpp
+void destroy_mixed(dtb_ctx* c);   // batch_api.cpp
 
 extern "C" {
 
@@ -202,10 +53,13 @@ int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out) {
     DTB_CHECK(dims->n_species >= 1 && dims->n_species <= DTB_MAX_SPECIES, DTB_EINVAL,
               "dtb_create: n_species must be in [1, 16]");
     DTB_CHECK(dims->n_space >= 1, DTB_EINVAL, "dtb_create: n_space must be >= 1");
-    DTB_CHECK(opts->precision == DTB_F64 || opts->precision == DTB_F32, DTB_EINVAL,
-              "dtb_create: precision must be DTB_F64 or DTB_F32 for the plain method");
+    DTB_CHECK(opts->precision == DTB_F64 || opts->precision == DTB_F32 || opts->precision == DTB_MIXED, DTB_EINVAL,
+              "dtb_create: precision must be DTB_F64, DTB_F32 or DTB_MIXED");
     DTB_CHECK(opts->index_base == 0 || opts->index_base == 1, DTB_EINVAL, "dtb_create: index_base must be 0 or 1");
-    DTB_CHECK(opts->batch <= 1, DTB_EINVAL, "dtb_create: the plain method takes batch 1");
+    DTB_CHECK(opts->precision == DTB_MIXED || opts->batch <= 1, DTB_EINVAL,
+              "dtb_create: the plain method takes batch 1 (batched instances need DTB_MIXED)");
+    DTB_CHECK(opts->precision != DTB_MIXED || (opts->batch >= 1 && opts->batch <= 65536), DTB_EINVAL,
+              "dtb_create: a batched context needs 1 <= batch <= 65536");
     DTB_CHECK(std::isfinite(opts->dt0) && opts->dt0 > 0, DTB_EINVAL, "dtb_create: dt0 must be finite and > 0");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -219,7 +73,7 @@ int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out) {
     c->ns = dims->n_species;
     c->n_space = dims->n_space;
     c->prec = opts->precision;
-    c->esz = c->prec == DTB_F64 ? 8 : 4;
+    c->esz = c->prec == DTB_F64 ? 8 : 4;  // state element size (DTB_MIXED keeps f in FP32)
     c->device = opts->device;
     c->off[0] = 0;
     c->offp[0] = 0;
@@ -251,6 +105,7 @@ int32_t dtb_destroy(dtb_ctx* c) {
     if (!c) return DTB_OK;
     DeviceGuard g(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    destroy_mixed(c);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     c->free_all();
@@ -263,11 +118,6 @@ int32_t dtb_destroy(dtb_ctx* c) {
     return DTB_OK;
 }
 
-static int species_of(const dtb_ctx* c, int64_t a) {
-    int s = 0;
-    while (s + 1 < c->ns && a >= c->off[s + 1]) ++s;
-    return s;
-}
 
 int32_t dtb_add_flux_csc(dtb_ctx* c, int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval) {
     DTB_CHECK(c, DTB_EINVAL, "dtb_add_flux_csc: null context");
@@ -455,22 +305,6 @@ int32_t dtb_upload_vectors(dtb_ctx* c, const double* Ap, const double* Vol, cons
 }  // extern "C"
 
 // ------------------------------------------------------------------ commit
-template <typename T>
-static int copy_host_vec(dtb_ctx* c, T** dst, const std::vector<double>& src) {
-    std::vector<T> tmp(src.size());
-    for (size_t i = 0; i < src.size(); ++i) tmp[i] = (T)src[i];
-    DTB_TRY(c->alloc(dst, sizeof(T) * std::max<size_t>(1, tmp.size())));
-    if (!tmp.empty()) DTB_CUDA(cudaMemcpy(*dst, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice));
-    return DTB_OK;
-}
-
-template <typename I>
-static int copy_host_ints(dtb_ctx* c, I** dst, const std::vector<I>& src) {
-    DTB_TRY(c->alloc(dst, sizeof(I) * std::max<size_t>(1, src.size())));
-    if (!src.empty()) DTB_CUDA(cudaMemcpy(*dst, src.data(), sizeof(I) * src.size(), cudaMemcpyHostToDevice));
-    return DTB_OK;
-}
-
 template <typename T>
 static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     const size_t esz = sizeof(T);
@@ -742,6 +576,22 @@ extern "C" int32_t dtb_commit(dtb_ctx* c) {
     if (c->committed) return DTB_OK;
     DTB_CHECK(c->have_vectors, DTB_ESTATE, "dtb_commit: dtb_upload_vectors was not called");
     DeviceGuard g(c->device);
+    if (c->prec == DTB_MIXED) {
+        int rc = commit_mixed(c);
+        if (rc != DTB_OK) {
+            destroy_mixed(c);
+            c->free_all();
+            return rc;
+        }
+        c->committed = true;
+        c->gains.clear();
+        c->losses.clear();
+        c->emis.clear();
+        c->flux_r.clear();
+        c->flux_c.clear();
+        c->flux_v.clear();
+        return DTB_OK;
+    }
     int rc = c->prec == DTB_F64 ? commit_typed<double>(c, c->ops_d) : commit_typed<float>(c, c->ops_f);
     if (rc != DTB_OK) {
         c->free_all();
@@ -910,6 +760,7 @@ extern "C" {
 int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t verbose, double* dt_out,
                  int32_t* save_out, dtb_step_diag* diag_out) {
     DTB_CHECK(c, DTB_EINVAL, "dtb_step: null context");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_step: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     // SteppingMethods.jl:18-27
@@ -938,6 +789,7 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
 int32_t dtb_run(dtb_ctx* c, const double* dt_scales, int64_t nsteps, int32_t verbose, dtb_step_diag* diag_hist) {
     DTB_CHECK(c && (dt_scales || nsteps == 0), DTB_EINVAL, "dtb_run: null argument");
     DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_run: nsteps < 0");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_run: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     for (int64_t s0 = 0; s0 < nsteps; s0 += c->hist_cap) {
@@ -991,6 +843,7 @@ int32_t dtb_solve_schedule(double dt_initial, const double* t_save, int64_t n_sa
 
 int32_t dtb_get_f(dtb_ctx* c, double* f) {
     DTB_CHECK(c && f, DTB_EINVAL, "dtb_get_f: null argument");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_get_f: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     if (c->prec == DTB_F64) {
@@ -1008,6 +861,7 @@ int32_t dtb_get_f(dtb_ctx* c, double* f) {
 
 int32_t dtb_set_f(dtb_ctx* c, const double* f) {
     DTB_CHECK(c && f, DTB_EINVAL, "dtb_set_f: null argument");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_set_f: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     if (c->prec == DTB_F64) {
@@ -1026,6 +880,7 @@ int32_t dtb_set_f(dtb_ctx* c, const double* f) {
 
 int32_t dtb_reset(dtb_ctx* c) {
     DTB_CHECK(c, DTB_EINVAL, "dtb_reset: null context");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_reset: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     DTB_CUDA(cudaMemcpyAsync(c->f_buf[c->cur], c->f_init_dev, c->esz * (size_t)c->n_state, cudaMemcpyDeviceToDevice,
@@ -1036,6 +891,7 @@ int32_t dtb_reset(dtb_ctx* c) {
 int32_t dtb_solve(dtb_ctx* c, double dt_initial, const double* t_save, int64_t n_save, int32_t verbose, double* f_out,
                   int64_t* n_steps_out) {
     DTB_CHECK(c && t_save && f_out && n_save >= 1, DTB_EINVAL, "dtb_solve: null argument");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_solve: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     // Solver.jl:22 reset; :14 save the initial state
@@ -1086,6 +942,7 @@ int32_t dtb_solve(dtb_ctx* c, double dt_initial, const double* t_save, int64_t n
 
 int32_t dtb_moments(dtb_ctx* c, const double* w, double* number, double* energy) {
     DTB_CHECK(c && w && number && energy, DTB_EINVAL, "dtb_moments: null argument");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_moments: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
     DTB_CUDA(cudaMemcpyAsync(c->mom_w, w, sizeof(double) * (size_t)c->n_mom, cudaMemcpyHostToDevice, c->stream));

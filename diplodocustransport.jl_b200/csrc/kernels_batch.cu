@@ -1,0 +1,583 @@
+// Kernels of the batched mixed-precision Euler step.
+//
+// gain_gemm<BN>: the gain contraction of many instances as a GEMM on the 5th-generation
+// tensor cores. A = G rows (BF16 hi and lo halves, K-major, 128-byte swizzle) staged by TMA;
+// B = X = f1 (x) f2 for BN instances, formed on the fly by producer warps in shared memory as
+// BF16 hi and lo halves in the same swizzled K-major layout; D (FP32) lives in tensor memory.
+// Per 16-wide K step three MMAs accumulate hi*hi + hi*lo + lo*hi. One elected thread issues
+// the MMAs and commits them to mbarriers; every wait is bounded.
+//
+// mixed_rows: one (32 rows x 32 instances) tile per block: split-K partial sums of the gain
+// (transposed through shared memory), banded flux, emission (BF16 hi+lo), loss, then the
+// update of SteppingMethods.jl:46-101 with an FP64 compensated (Kahan) accumulation of f.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "batch_internal.h"
+
+namespace dtb {
+
+namespace {
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mb_init(uint32_t bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mb_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mb_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mb_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mb_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    if (mb_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (true) {
+        if (mb_try(bar, parity)) return true;
+        if (abort_flag && *abort_flag) return false;
+        if (gtimer() - t0 > kWaitLimitNs) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+// K-major operand tile in the canonical 128-byte swizzle layout: rows of 128 bytes, 8-row
+// groups 1024 bytes apart (stride byte offset 64 x 16 B), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) | ((uint64_t)1 << 46) |
+           ((uint64_t)2 << 61);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo_elem, hi_elem);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+template <int BN>
+struct GemmCfg {
+    static constexpr int NPW = BN / 32 < 4 ? 4 : BN / 32;  // producer / epilogue warps
+    static constexpr int THREADS = (NPW + 2) * 32;
+    static constexpr int A_BYTES = kMmaM * 128;             // one half (hi or lo) of an A stage
+    static constexpr int B_BYTES = BN * 128;                // one half of a B stage
+    static constexpr int SB = 2;
+    static constexpr int SA = BN == 256 ? 3 : (BN == 128 ? 4 : 6);
+    static constexpr int DATA = SA * 2 * A_BYTES + SB * 2 * B_BYTES;
+    static constexpr int BARS = (2 * SA + 2 * SB + 2) * 8;
+    static constexpr int SMEM = 1024 + DATA + BARS + 16;   // 1024: alignment slack
+};
+
+template <int BN>
+__global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
+    gain_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, GemmArgs a) {
+    using C = GemmCfg<BN>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* a_base = smem;                                // [SA][hi, lo][128 rows x 128 B]
+    unsigned char* b_base = smem + C::SA * 2 * C::A_BYTES;       // [SB][hi, lo][BN rows x 128 B]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + C::DATA);
+    uint64_t* full_a = bars;
+    uint64_t* empty_a = full_a + C::SA;
+    uint64_t* full_b = empty_a + C::SA;
+    uint64_t* empty_b = full_b + C::SB;
+    uint64_t* acc_bar = empty_b + C::SB;
+    uint64_t* drain_bar = acc_bar + 1;
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain_bar + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int task = blockIdx.x;
+    const int n_tile = task % a.n_tiles;
+    const int m_tile = (task / a.n_tiles) % a.m_tiles;
+    const int split = task / (a.n_tiles * a.m_tiles);
+    const int T = a.n_cb * a.N1;
+    const int t0 = split * a.tiles_per_split;
+    const int t1 = min(T, t0 + a.tiles_per_split);
+    const int nt = t1 > t0 ? t1 - t0 : 0;
+    const int m0 = m_tile * kMmaM, n0 = n_tile * BN;
+    const int n2p = a.n_cb * kMmaK;
+
+    if (tid == 0) {
+        for (int s = 0; s < C::SA; ++s) {
+            mb_init(smem_addr(&full_a[s]), 1);
+            mb_init(smem_addr(&empty_a[s]), 1);
+        }
+        for (int s = 0; s < C::SB; ++s) {
+            mb_init(smem_addr(&full_b[s]), BN);
+            mb_init(smem_addr(&empty_b[s]), 1);
+        }
+        mb_init(smem_addr(acc_bar), 1);
+        mb_init(smem_addr(drain_bar), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == C::NPW + 1) {  // TMEM: BN fp32 columns x 128 lanes
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_holder)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp == C::NPW) {
+        // ---------------- TMA producer of the G tiles
+        if (lane == 0 && nt > 0) {
+            int j = 0;
+            for (; j < nt; ++j) {
+                const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
+                const int sa = j % C::SA;
+                const uint32_t ph = (j / C::SA) & 1u;
+                if (!mb_wait(smem_addr(&empty_a[sa]), ph ^ 1u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_EMPTY);
+                    *abort_flag = 1;
+                    break;
+                }
+                mb_expect_tx(smem_addr(&full_a[sa]), 2 * C::A_BYTES);
+                const int x = b * n2p + cb * kMmaK;
+                tma_load_2d(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), &tm_hi, x, m0, smem_addr(&full_a[sa]));
+                tma_load_2d(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), &tm_lo, x, m0, smem_addr(&full_a[sa]));
+            }
+            // drain: this block's own copies must land before it may exit
+            for (int k = j > C::SA ? j - C::SA : 0; k < j; ++k) {
+                if (!mb_wait(smem_addr(&full_a[k % C::SA]), (k / C::SA) & 1u, nullptr)) atomicOr(a.err, KERR_TIMEOUT_DRAIN);
+            }
+        }
+    } else if (warp == C::NPW + 1) {
+        // ---------------- MMA issuer
+        if (lane == 0 && nt > 0) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)(kMmaM >> 4) << 24);
+            int issued = 0;
+            for (int j = 0; j < nt; ++j) {
+                const int sa = j % C::SA, sb = j % C::SB;
+                if (!mb_wait(smem_addr(&full_a[sa]), (j / C::SA) & 1u, abort_flag) ||
+                    !mb_wait(smem_addr(&full_b[sb]), (j / C::SB) & 1u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ahi = smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES);
+                const uint32_t alo = smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES);
+                const uint32_t bhi = smem_addr(b_base + (size_t)(sb * 2) * C::B_BYTES);
+                const uint32_t blo = smem_addr(b_base + (size_t)(sb * 2 + 1) * C::B_BYTES);
+                const uint64_t dahi = umma_desc_sw128(ahi), dalo = umma_desc_sw128(alo);
+                const uint64_t dbhi = umma_desc_sw128(bhi), dblo = umma_desc_sw128(blo);
+#pragma unroll
+                for (int kk = 0; kk < kMmaK / 16; ++kk) {
+                    const uint64_t o = (uint64_t)(kk * 2);  // 16 BF16 = 32 bytes = 2 x 16 B
+                    umma_bf16(tmem, dahi + o, dbhi + o, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+                    umma_bf16(tmem, dahi + o, dblo + o, idesc, 1u);
+                    umma_bf16(tmem, dalo + o, dbhi + o, idesc, 1u);
+                }
+                umma_commit(smem_addr(&empty_a[sa]));
+                umma_commit(smem_addr(&empty_b[sb]));
+                ++issued;
+            }
+            if (*abort_flag) {
+                if (issued > 0) {  // let the MMAs already issued finish before tensor memory is freed
+                    umma_commit(smem_addr(drain_bar));
+                    if (!mb_wait(smem_addr(drain_bar), 0u, nullptr)) atomicOr(a.err, KERR_TIMEOUT_DRAIN);
+                }
+            } else {
+                umma_commit(smem_addr(acc_bar));
+            }
+        }
+    } else {
+        // ---------------- X producers (one instance row per thread), then the epilogue
+        const int p = tid;  // row of the B tile
+        if (p < BN && nt > 0) {
+            const int inst = n0 + p;
+            const bool valid = inst < a.Bcap;
+            const float s1 = valid ? a.isig1[inst] : 0.f;
+            const float s2 = valid ? a.isig2[inst] : 0.f;
+            float f2r[kMmaK];
+            int cur_cb = -1;
+            for (int j = 0; j < nt; ++j) {
+                const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
+                const int sb = j % C::SB;
+                if (!mb_wait(smem_addr(&empty_b[sb]), ((j / C::SB) & 1u) ^ 1u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_EMPTY);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (cb != cur_cb) {
+#pragma unroll
+                    for (int c = 0; c < kMmaK; ++c) {
+                        const int cc = cb * kMmaK + c;
+                        f2r[c] = (valid && cc < a.n2) ? a.F[(size_t)(a.off2 + cc) * a.Bcap + inst] * s2 : 0.f;
+                    }
+                    cur_cb = cb;
+                }
+                const float x1 = valid ? a.F[(size_t)(a.off1 + b) * a.Bcap + inst] * s1 : 0.f;
+                unsigned char* rhi = b_base + (size_t)(sb * 2) * C::B_BYTES + (size_t)p * 128;
+                unsigned char* rlo = b_base + (size_t)(sb * 2 + 1) * C::B_BYTES + (size_t)p * 128;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    uint32_t h[4], l[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float v0 = x1 * f2r[8 * q + 2 * e];
+                        const float v1 = x1 * f2r[8 * q + 2 * e + 1];
+                        const __nv_bfloat162 hh = __floats2bfloat162_rn(v0, v1);
+                        const float2 hf = __bfloat1622float2(hh);
+                        h[e] = *reinterpret_cast<const uint32_t*>(&hh);
+                        l[e] = pack_bf16x2(v0 - hf.x, v1 - hf.y);
+                    }
+                    const int phys = ((q ^ (p & 7)) << 4);
+                    *reinterpret_cast<uint4*>(rhi + phys) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(rlo + phys) = make_uint4(l[0], l[1], l[2], l[3]);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mb_arrive(smem_addr(&full_b[sb]));
+            }
+        }
+        // epilogue: TMEM lanes 32*(warp%4).. hold rows m0 + 32*(warp%4) + lane
+        const int lg = warp & 3;
+        const int ncol = BN / (C::NPW / 4);
+        const int c0 = (warp >> 2) * ncol;
+        const int row = m0 + lg * 32 + lane;
+        bool ok = true;
+        if (nt > 0) {
+            ok = mb_wait(smem_addr(acc_bar), 0u, abort_flag);
+            if (!ok && !*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+            tc_fence_after();
+        }
+        if (ok && !*abort_flag) {
+            float* dst = a.partial + (size_t)split * a.Bpad * a.M;
+            for (int cc = 0; cc < ncol; cc += 16) {
+                float v[16];
+                if (nt > 0) {
+                    tmem_ld16(tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc), v);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) v[k] = 0.f;
+                }
+                if (row < a.M) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = v[k];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == C::NPW + 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    }
+}
+
+}  // namespace
+
+int gain_gemm_smem_bytes(int bn) {
+    switch (bn) {
+        case 64: return GemmCfg<64>::SMEM;
+        case 128: return GemmCfg<128>::SMEM;
+        default: return GemmCfg<256>::SMEM;
+    }
+}
+
+cudaError_t prepare_gain_gemm(int bn) {
+    switch (bn) {
+        case 64:
+            return cudaFuncSetAttribute(gain_gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<64>::SMEM);
+        case 128:
+            return cudaFuncSetAttribute(gain_gemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        GemmCfg<128>::SMEM);
+        case 256:
+            return cudaFuncSetAttribute(gain_gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        GemmCfg<256>::SMEM);
+        default:
+            return cudaErrorInvalidValue;
+    }
+}
+
+// The dynamic shared-memory limit is raised once per device by prepare_gain_gemm (commit time),
+// so launches stay legal inside a stream capture.
+template <int BN>
+static cudaError_t launch_gemm_bn(const CUtensorMap* hi, const CUtensorMap* lo, const GemmArgs& a, cudaStream_t s) {
+    using C = GemmCfg<BN>;
+    const int grid = a.m_tiles * a.n_tiles * a.n_splits;
+    gain_gemm_kernel<BN><<<grid, C::THREADS, C::SMEM, s>>>(*hi, *lo, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gain_gemm(int bn, const CUtensorMap* tm_hi, const CUtensorMap* tm_lo, const GemmArgs& a,
+                             cudaStream_t s) {
+    switch (bn) {
+        case 64: return launch_gemm_bn<64>(tm_hi, tm_lo, a, s);
+        case 128: return launch_gemm_bn<128>(tm_hi, tm_lo, a, s);
+        case 256: return launch_gemm_bn<256>(tm_hi, tm_lo, a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ------------------------------------------------------------------ operand preparation
+// One block per row: scale = 2^floor(log2(max |g|)) (1 for an all-zero row), then
+// hi = bf16(g / scale), lo = bf16(g / scale - hi), written into K-padded rows.
+__global__ void split_rows_kernel(const float* __restrict__ src, int n1, int n2, int n2p, __nv_bfloat16* hi,
+                                  __nv_bfloat16* lo, float* row_scale) {
+    __shared__ float s_max[256];
+    const long long r = blockIdx.x;
+    const float* g = src + (size_t)r * n1 * n2;
+    float m = 0.f;
+    for (long long k = threadIdx.x; k < (long long)n1 * n2; k += blockDim.x) m = fmaxf(m, fabsf(g[k]));
+    s_max[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s_max[threadIdx.x] = fmaxf(s_max[threadIdx.x], s_max[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const float mx = s_max[0];
+    int ex = 0;
+    if (mx > 0.f && isfinite(mx)) frexpf(mx, &ex);  // mx = f * 2^ex, f in [0.5, 1)
+    const float scale = ldexpf(1.f, ex - 1);         // mx / scale in [1, 2)
+    const float inv = ldexpf(1.f, 1 - ex);
+    if (threadIdx.x == 0) row_scale[r] = scale;
+    __nv_bfloat16* dh = hi + (size_t)r * n1 * n2p;
+    __nv_bfloat16* dl = lo + (size_t)r * n1 * n2p;
+    for (long long k = threadIdx.x; k < (long long)n1 * n2p; k += blockDim.x) {
+        const long long b = k / n2p;
+        const int c = (int)(k - b * n2p);
+        const float v = c < n2 ? g[b * n2 + c] * inv : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        dh[k] = h;
+        dl[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+cudaError_t launch_split_rows(const float* src, long long rows, int n1, int n2, int n2p, __nv_bfloat16* hi,
+                              __nv_bfloat16* lo, float* row_scale, int* err, cudaStream_t s) {
+    (void)err;
+    split_rows_kernel<<<(unsigned)rows, 256, 0, s>>>(src, n1, n2, n2p, hi, lo, row_scale);
+    return cudaGetLastError();
+}
+
+// Emission rows: (hi, lo) pairs of E / scale[row] with the same power-of-two row scale.
+__global__ void split_emi_kernel(const float* __restrict__ src, int ncols, int ld, __nv_bfloat162* dst, float* row_scale) {
+    __shared__ float s_max[128];
+    const int r = blockIdx.x;
+    float m = 0.f;
+    for (int k = threadIdx.x; k < ncols; k += blockDim.x) m = fmaxf(m, fabsf(src[(size_t)r * ncols + k]));
+    s_max[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s_max[threadIdx.x] = fmaxf(s_max[threadIdx.x], s_max[threadIdx.x + o]);
+        __syncthreads();
+    }
+    int ex = 0;
+    if (s_max[0] > 0.f && isfinite(s_max[0])) frexpf(s_max[0], &ex);
+    const float inv = ldexpf(1.f, 1 - ex);
+    if (threadIdx.x == 0) row_scale[r] = ldexpf(1.f, ex - 1);
+    for (int k = threadIdx.x; k < ld; k += blockDim.x) {
+        const float v = k < ncols ? src[(size_t)r * ncols + k] * inv : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        dst[(size_t)r * ld + k] = __halves2bfloat162(h, __float2bfloat16_rn(v - __bfloat162float(h)));
+    }
+}
+
+cudaError_t launch_split_emi(const float* src, int rows, int ncols, int ld, __nv_bfloat162* dst, float* row_scale,
+                             cudaStream_t s) {
+    split_emi_kernel<<<rows, 128, 0, s>>>(src, ncols, ld, dst, row_scale);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ batched Euler epilogue
+namespace {
+
+// Order-preserving map of doubles to unsigned integers (NaN is mapped to +Inf before):
+// x < y (with -0.0 < +0.0) <=> enc(x) < enc(y).
+__device__ __forceinline__ unsigned long long ord_enc(double x) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+constexpr int kTR = 32;  // rows per tile
+constexpr int kTI = 32;  // instances per tile
+
+__global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
+                                                         const float* __restrict__ Cc, float* __restrict__ Fo,
+                                                         float* __restrict__ Co, unsigned long long* gstep,
+                                                         unsigned* ticket) {
+    __shared__ float s_gain[kTR][kTI + 1];
+    __shared__ int s_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int a0 = blockIdx.x * kTR, i0 = blockIdx.y * kTI;
+    const long long step = (long long)*reinterpret_cast<volatile unsigned long long*>(gstep);
+    const int B = ops.Bcap;
+
+    // phase 1: gain of the tile, lanes along rows (coalesced partial reads), 4 instances per warp
+    {
+        const int a = a0 + lane;
+        int s = 0;
+        if (a < ops.n_mom)
+            while (s + 1 < ops.n_species && a >= ops.sp_off[s + 1]) ++s;
+#pragma unroll
+        for (int q = 0; q < kTI / 8; ++q) {
+            const int il = warp * (kTI / 8) + q;
+            const int i = i0 + il;
+            float g = 0.f;
+            if (a < ops.n_mom && i < B && ops.has_bin) {
+                for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
+                    const int gi = ops.gain_grp[e];
+                    const int r = ops.gain_roff[e] + (a - ops.sp_off[s]);
+                    const float* P = ops.grp_partial[gi];
+                    const int M = ops.grp_M[gi], Bp = ops.grp_Bpad[gi];
+                    float acc = 0.f;
+                    for (int sp = 0; sp < ops.grp_splits[gi]; ++sp) acc += P[((size_t)sp * Bp + i) * M + r];
+                    g += acc * ops.grp_scale[gi][r] * ops.grp_sig1[gi][i] * ops.grp_sig2[gi][i];
+                }
+            }
+            s_gain[lane][il] = g;
+        }
+    }
+    __syncthreads();
+
+    // phase 2: lanes along instances, 4 rows per warp
+    const int i = i0 + lane;
+    const bool inst_ok = i < B;
+    const bool active = inst_ok && step < ops.stop_step[i];
+    const double dts = inst_ok ? ops.dt_scale[i] : 0.0;
+    double rmin = CUDART_INF;
+    int nonfin = 0;
+    for (int rr = 0; rr < kTR / 8; ++rr) {
+        const int al = warp * (kTR / 8) + rr;
+        const int a = a0 + al;
+        if (a >= ops.n_mom || !inst_ok) continue;
+        const size_t idx = (size_t)a * B + i;
+        const float fa = F[idx];
+        const float ca = Cc[idx];
+        if (!active) {
+            Fo[idx] = fa;
+            Co[idx] = ca;
+            continue;
+        }
+        int s = 0;
+        while (s + 1 < ops.n_species && a >= ops.sp_off[s + 1]) ++s;
+        float flux = 0.f;
+        for (int k = 0; k < ops.ell_w; ++k) {
+            const int c = ops.ell_col[(size_t)a * ops.ell_w + k];
+            if (c >= 0) flux += ops.ell_val[(size_t)a * ops.ell_w + k] * F[(size_t)c * B + i];
+        }
+        float emi = 0.f;
+        if (ops.has_emi) {
+            for (int p = ops.emi_rptr[a]; p < ops.emi_rptr[a + 1]; ++p) {
+                const int pc = ops.emi_piece[p];
+                const __nv_bfloat162* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
+                const int col0 = ops.emi_col0[pc], nc = ops.emi_ncols[pc];
+                float acc = 0.f;
+                for (int c = 0; c < nc; ++c) {
+                    const float2 e2 = __bfloat1622float2(row[c]);
+                    acc += (e2.x + e2.y) * F[(size_t)(col0 + c) * B + i];
+                }
+                emi += acc * ops.emi_scale[ops.emi_scale_off[pc] + (a - ops.emi_row0[pc])];
+            }
+        }
+        float loss = 0.f;
+        if (ops.has_bin) {
+            const int la = a - ops.sp_off[s];
+            for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
+                const float* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
+                const int co = ops.loss_col_off[b], nc = ops.loss_ncols[b];
+                for (int c = 0; c < nc; ++c) loss += row[c] * F[(size_t)(co + c) * B + i];
+            }
+        }
+        const float gain = s_gain[al][lane];
+        // SteppingMethods.jl:31-46 in FP32, scale in FP64
+        float df = -flux;
+        if (ops.has_emi) df += emi;
+        if (ops.has_bin) df += ops.vol * (gain - fa * loss);
+        const double dfs = (double)df * ((double)ops.invAp[a] * dts);
+        // :97-101 with an FP64 compensated sum: the state is fa + ca
+        double t = ((double)fa + (double)ca) + (dfs + (double)ops.inj[a] * dts);
+        t = (t >= ops.thr) ? t : copysign(0.0, t);
+        t = (t != CUDART_INF) ? t : copysign(0.0, t);
+        const float fn = (float)t;
+        Fo[idx] = fn;
+        Co[idx] = (float)(t - (double)fn);
+        double ratio = dfs / (double)fa;
+        if (isnan(ratio)) ratio = CUDART_INF;
+        if (ratio < rmin || (ratio == rmin && signbit(ratio))) rmin = ratio;
+        if (!isfinite(dfs)) nonfin = 1;
+    }
+    if (active) {
+        atomicMin(&ops.min_ratio[i], ord_enc(rmin));
+        if (nonfin) atomicOr(&ops.nonfinite[i], 1);
+    }
+    // the last block to finish advances the global step counter
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned total = gridDim.x * gridDim.y;
+        const unsigned t = atomicAdd(ticket, 1u);
+        s_last = (t == total - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        *ticket = 0u;
+        __threadfence();
+        *reinterpret_cast<volatile unsigned long long*>(gstep) = (unsigned long long)(step + 1);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
+                              unsigned long long* gstep, unsigned* ticket, cudaStream_t s) {
+    dim3 grid((ops.n_mom + kTR - 1) / kTR, (ops.Bcap + kTI - 1) / kTI);
+    mixed_rows_kernel<<<grid, 256, 0, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
+    return cudaGetLastError();
+}
+
+}  // namespace dtb

@@ -82,6 +82,14 @@ SIGNATURES = {
     "dtb_gain_kernel_stats": (_i32, [_P, _dp, _dp]),
     "dtb_set_profiling": (_i32, [_P, _i32]),
     "dtb_gain_contract": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
+    "dtb_batch_admit": (_i32, [_P, _i32, _dp, _d, _i64]),
+    "dtb_batch_run": (_i32, [_P, _i64]),
+    "dtb_batch_get_f": (_i32, [_P, _i32, _dp]),
+    "dtb_batch_slot_info": (_i32, [_P, _i32, _ip, _ip, _dp, _i32p]),
+    "dtb_batch_release": (_i32, [_P, _i32]),
+    "dtb_batch_capacity": (_i32, [_P, _i32p, _ip]),
+    "dtb_batch_set_profiling": (_i32, [_P, _i32]),
+    "dtb_batch_gemm_stats": (_i32, [_P, _dp, _dp, _dp, _i32p]),
     "dtb_gain_contract_noalloc": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
 }
 

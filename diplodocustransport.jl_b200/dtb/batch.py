@@ -1,0 +1,129 @@
+"""Batched independent solves on one grid (mixed precision) over libdtb.so.
+
+``BatchedEuler(PhaseSpace, Injection, BinM, EmiM, FluxM, capacity)`` uploads the shared
+operators once (as ``ForwardEulerStruct`` does for a single solve, SteppingStructs.jl:33-100)
+and holds ``capacity`` slots. Each admitted slot runs the explicit Euler step of
+SteppingMethods.jl:12-107 with its own initial f, dt and step count; ``run(k)`` advances every
+slot with steps left by k batched steps. The gain contraction of all slots is a tensor-core
+GEMM with G in BF16 hi + lo (three MMAs, FP32 accumulation) and f is updated with an FP64
+compensated sum.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr
+from .stepping import _upload_csc, _upload_gain
+from .structs import BinaryMatrices, EmissionMatrices, FluxMatrices, PhaseSpace
+
+
+class BatchedEuler:
+    def __init__(self, PhaseSpace: PhaseSpace, Injection, BinM: BinaryMatrices, EmiM: EmissionMatrices,
+                 FluxM: FluxMatrices, capacity: int, *, device: int = 0, stream: Optional[int] = None,
+                 graph_steps: int = 16):
+        if PhaseSpace.n_space != 1:
+            raise ValueError("batched instances are single-cell")
+        self.L = _lib.load()
+        self.PhaseSpace = PhaseSpace
+        self.capacity = int(capacity)
+        self.dt0 = float(PhaseSpace.dt0)
+        self.n = PhaseSpace.n_momentum
+        dims = _lib.Dims()
+        sizes = PhaseSpace.species_sizes
+        dims.n_species = len(sizes)
+        dims.n_space = 1
+        for i, s in enumerate(sizes):
+            dims.species_size[i] = s
+        opts = _lib.Opts(precision=_lib.DTB_MIXED, device=device, stream=stream, index_base=0,
+                         graph_steps=graph_steps, dt0=self.dt0, batch=self.capacity, flags=0)
+        ctx = ctypes.c_void_p()
+        check(self.L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)))
+        self.ctx = ctx
+        try:
+            L = self.L
+            _upload_csc(L, ctx, FluxM.X_Flux)
+            _upload_csc(L, ctx, FluxM.P_Flux)
+            if BinM.M_Bin is not None:
+                M = np.asfortranarray(BinM.M_Bin, dtype=np.float64)
+                check(L.dtb_upload_mbin_ref(ctx, M.ctypes.data_as(_lib._dp), self.n))
+            for g in BinM.gains:
+                _upload_gain(L, ctx, g)
+            for l in BinM.losses:
+                A = np.ascontiguousarray(l.L, dtype=np.float64)
+                check(L.dtb_add_loss_block(ctx, l.sp, l.other_sp, dptr(A)))
+            if EmiM.M_Emi is not None:
+                M = np.asfortranarray(EmiM.M_Emi, dtype=np.float64)
+                check(L.dtb_upload_emi_ref(ctx, M.ctypes.data_as(_lib._dp), self.n))
+            for b in EmiM.blocks:
+                E = np.ascontiguousarray(b.E, dtype=np.float64)
+                check(L.dtb_add_emi_block(ctx, b.row0, E.shape[0], b.col0, E.shape[1], dptr(E)))
+            Ap = np.ascontiguousarray(FluxM.Ap_Flux, dtype=np.float64)
+            Vol = np.ascontiguousarray(FluxM.Vol, dtype=np.float64)
+            inj = np.ascontiguousarray(Injection, dtype=np.float64)
+            zeros = np.zeros(self.n)
+            check(L.dtb_upload_vectors(ctx, dptr(Ap), dptr(Vol), dptr(zeros), dptr(inj)))
+            check(L.dtb_commit(ctx))
+        except Exception:
+            self.close()
+            raise
+
+    def admit(self, slot: int, f0, dt: float, n_steps: int) -> None:
+        """Start a solve in `slot` with initial state f0, step dt (dt/dt0 is applied) and n_steps steps."""
+        f = np.ascontiguousarray(f0, dtype=np.float64)
+        check(self.L.dtb_batch_admit(self.ctx, int(slot), dptr(f), float(dt) / self.dt0, int(n_steps)))
+
+    def run(self, nsteps: int) -> None:
+        check(self.L.dtb_batch_run(self.ctx, int(nsteps)))
+
+    def get_f(self, slot: int) -> np.ndarray:
+        out = np.empty(self.n)
+        check(self.L.dtb_batch_get_f(self.ctx, int(slot), dptr(out)))
+        return out
+
+    def info(self, slot: int) -> dict:
+        done, left = ctypes.c_int64(), ctypes.c_int64()
+        cr = ctypes.c_double()
+        fin = ctypes.c_int32()
+        check(self.L.dtb_batch_slot_info(self.ctx, int(slot), ctypes.byref(done), ctypes.byref(left),
+                                         ctypes.byref(cr), ctypes.byref(fin)))
+        return {"steps_done": done.value, "steps_left": left.value, "cr_max": cr.value, "finite": bool(fin.value)}
+
+    def release(self, slot: int) -> None:
+        check(self.L.dtb_batch_release(self.ctx, int(slot)))
+
+    @property
+    def step(self) -> int:
+        cap, st = ctypes.c_int32(), ctypes.c_int64()
+        check(self.L.dtb_batch_capacity(self.ctx, ctypes.byref(cap), ctypes.byref(st)))
+        return st.value
+
+    def set_profiling(self, on: bool) -> None:
+        check(self.L.dtb_batch_set_profiling(self.ctx, 1 if on else 0))
+
+    def gemm_stats(self) -> dict:
+        ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        lps = ctypes.c_int32()
+        check(self.L.dtb_batch_gemm_stats(self.ctx, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(by),
+                                          ctypes.byref(lps)))
+        return {"avg_ms": ms.value, "flops_per_step": fl.value, "bytes_per_step": by.value,
+                "launches_per_step": lps.value}
+
+    def device_bytes(self) -> int:
+        v = ctypes.c_int64()
+        check(self.L.dtb_device_bytes(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.L.dtb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

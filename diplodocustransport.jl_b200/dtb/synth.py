@@ -224,3 +224,81 @@ def small(p_num: int = 4, u_num: int = 2, seed: int = 0, dt: float = 1.0, n_spac
         w.inj = rng.uniform(0.0, 1e-4, n)
     w.n_steps = 20
     return w
+
+
+def batched_two_species(p_num: int, p_lo: float, p_hi: float, u_num: int, batch: int, seed: int,
+                        dt_max: float = 1.0, g_range=(-6.0, 0.0), gain_on_device: bool = False,
+                        device: str = "cuda", with_emission: bool = True) -> Workload:
+    """Shared e + gamma operators and `batch` instances: f0 log-normal in p with mean log p drawn
+    from U[-1, 1] per instance, dt drawn from U[0.5, 1] * dt_max per instance."""
+    w = two_species(p_num, p_lo, p_hi, u_num, seed, dt=dt_max, g_range=g_range, gain_on_device=gain_on_device,
+                    device=device, with_emission=with_emission)
+    rng = np.random.default_rng(seed + 7)
+    mus = rng.uniform(-1.0, 1.0, size=batch)
+    w.f0 = np.stack([lognormal_f0(w.ps, [mu, mu], 1.0) for mu in mus])
+    w.dt = rng.uniform(0.5, 1.0, size=batch) * dt_max
+    w.meta["mu"] = mus
+    return w
+
+
+def config2(seed: int = 2, gain_on_device: bool = True, device: str = "cuda") -> Workload:
+    """Batching: 256 instances on 32 log p bins over 1e-2..1e2 x 8 u bins (256 states per
+    species), one shared G (2 x 256 x 65,536), 10,000 steps."""
+    w = batched_two_species(32, 1e-2, 1e2, 8, 256, seed, gain_on_device=gain_on_device, device=device)
+    w.n_steps = 10000
+    return w
+
+
+def synchrotron_like(ps: PhaseSpace, emitter: int, photon: int, B: float, kappa: float) -> np.ndarray:
+    """Photon rows x emitter columns: kappa * B^2 * x^(1/3) exp(-x), x = eps_gamma / eps_c,
+    eps_c = 1.5 B gamma^2 (gamma from the emitter's p-bin mean, mass 1), isotropic in u."""
+    pe = np.sqrt(ps.pxr_list[emitter][:-1] * ps.pxr_list[emitter][1:])
+    pg = np.sqrt(ps.pxr_list[photon][:-1] * ps.pxr_list[photon][1:])
+    gam = np.sqrt(1.0 + pe * pe)
+    x = pg[:, None] / (1.5 * B * gam[None, :] ** 2)
+    k = kappa * B * B * np.cbrt(x) * np.exp(-np.minimum(x, 700.0))  # (p_gamma, p_e)
+    ug, ue = ps.py_num_list[photon], ps.py_num_list[emitter]
+    E = np.zeros((ps.species_sizes[photon], ps.species_sizes[emitter]))
+    pn_g, pn_e = ps.px_num_list[photon], ps.px_num_list[emitter]
+    for jg in range(ug):
+        for je in range(ue):
+            E[jg * pn_g:(jg + 1) * pn_g, je * pn_e:(je + 1) * pn_e] = k / ug
+    return E
+
+
+def config3(seed: int = 3, batch: int = 64, gain_on_device: bool = True, device: str = "cuda") -> Workload:
+    """Mixed precision, three interactions: electrons, positrons, photons on 48 log p bins over
+    1e-3..1e3 x 12 u bins (576 states per species); e- + gamma and e+ + gamma Compton-like
+    gain/loss and gamma + gamma -> e+ e- pair gain/loss, each gain tensor 576 x 331,776 with
+    values log-uniform over 1e-8..1; synchrotron-like emission of e-/e+ into photons from a
+    uniform B of seeded magnitude; `batch` instances, 5000 steps."""
+    ps = phase_space(["Ele", "Pos", "Pho"], 48, 1e-3, 1e3, 12, [1.0, 1.0, 0.0])
+    rng = np.random.default_rng(seed)
+    fluxm = upwind_flux(ps, rng, 1.0)
+    ns = ps.species_sizes[0]
+    lo, hi = -8.0, 0.0
+    kg = gain_kappa(lo, hi, ns, 1.0)
+    blocks = [(0, 0, 2), (2, 0, 2), (1, 1, 2), (2, 1, 2), (0, 2, 2), (1, 2, 2)]
+    gains = []
+    for k, (o, a, b) in enumerate(blocks):
+        if gain_on_device:
+            G = device_log_uniform((ns, ns, ns), lo, hi, kg, seed * 1000 + 31 + k, None, device)
+        else:
+            G = _log_uniform(rng, (ns, ns, ns), lo, hi) * kg
+        gains.append(GainBlock(o, a, b, G))
+    kl = loss_kappa(lo, hi, 1.0)
+    losses = [LossBlock(s, o, _log_uniform(rng, (ns, ns), lo, hi) * kl)
+              for s, o in ((0, 2), (2, 0), (1, 2), (2, 1), (2, 2))]
+    Bmag = float(10.0 ** rng.uniform(-1.0, 1.0))
+    emim = EmissionMatrices()
+    for em in (0, 1):
+        E = synchrotron_like(ps, em, 2, Bmag, 1.0)
+        E *= RATE_EMI / max(E.sum(axis=0).max(), 1e-300)  # largest column moves 0.5% per step
+        emim.blocks.append(EmiBlock(row0=ps.momentum_species_offset[2], col0=ps.momentum_species_offset[em], E=E))
+    rng2 = np.random.default_rng(seed + 7)
+    mus = rng2.uniform(-1.0, 1.0, size=batch)
+    f0 = np.stack([lognormal_f0(ps, [mu, mu, mu], 1.0) for mu in mus])
+    dts = rng2.uniform(0.5, 1.0, size=batch)
+    return Workload(ps=ps, binm=BinaryMatrices(gains=gains, losses=losses), emim=emim, fluxm=fluxm, f0=f0,
+                    inj=np.zeros(ps.n_state), dt=dts, n_steps=5000,
+                    meta=dict(seed=seed, kappa_gain=kg, kappa_loss=kl, B=Bmag, mu=mus))

@@ -174,6 +174,44 @@ int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
 int32_t dtb_gain_kernel_stats(dtb_ctx* ctx, double* avg_ms, double* bytes_per_launch);
 int32_t dtb_set_profiling(dtb_ctx* ctx, int32_t on);
 
+/* ---- batched instances (precision DTB_MIXED, opts.batch = number of slots) ----
+ * Many independent solves of one grid share the operators uploaded with the calls above;
+ * each slot holds one instance (its own f, dt/dt0 and step count). The gain contraction of
+ * all slots is one tensor-core GEMM per input pair with G stored as BF16 hi + lo with a
+ * power-of-two scale per row (three MMAs: hi*hi + hi*lo + lo*hi, FP32 accumulation), f in
+ * FP32 with a power-of-two scale per (slot, species) inside the GEMM operand, and the update
+ * f += df of SteppingMethods.jl:97-101 accumulated in FP64 with a compensation term. */
+
+/* Starts a solve in `slot`: f = f0 (n_mom values), dt_scale = dt/dt0, n_steps steps from the
+ * current batched step. A slot that finished (or was never admitted) does not step. */
+int32_t dtb_batch_admit(dtb_ctx* ctx, int32_t slot, const double* f0, double dt_scale, int64_t n_steps);
+
+/* nsteps batched steps of every slot that still has steps left, replayed from a captured
+ * CUDA graph. */
+int32_t dtb_batch_run(dtb_ctx* ctx, int64_t nsteps);
+
+/* The slot's current f (FP32 state plus its compensation term, as Float64). */
+int32_t dtb_batch_get_f(dtb_ctx* ctx, int32_t slot, double* f);
+
+/* Steps taken and left, the largest Cr = -min(df ./ f) seen over the slot's steps, and
+ * whether every df was finite (SteppingMethods.jl:48-94 reduced over the run). */
+int32_t dtb_batch_slot_info(dtb_ctx* ctx, int32_t slot, int64_t* steps_done, int64_t* steps_left,
+                            double* cr_max, int32_t* finite);
+
+/* Stops a slot (it no longer steps). */
+int32_t dtb_batch_release(dtb_ctx* ctx, int32_t slot);
+
+/* Number of slots and the batched steps taken so far. */
+int32_t dtb_batch_capacity(dtb_ctx* ctx, int32_t* capacity, int64_t* step);
+
+/* Times the gain GEMM launches of each step with CUDA events while on (direct launches). */
+int32_t dtb_batch_set_profiling(dtb_ctx* ctx, int32_t on);
+
+/* Average gain-GEMM time per step over the profiled steps, its algorithmic FLOPs (three MMAs)
+ * and operator bytes per step, and the kernel launches per batched step. */
+int32_t dtb_batch_gemm_stats(dtb_ctx* ctx, double* avg_ms, double* flops_per_step, double* bytes_per_step,
+                             int32_t* launches_per_step);
+
 /* ---- kernel-level entry ---- */
 
 /* out[a] = sum_b f1[b] sum_c G[a][b][c] f2[c] for one dense gain block in the caller's device

@@ -1,0 +1,130 @@
+"""Batched mixed-precision path (tcgen05 gain GEMM, BF16 hi+lo operands) against the FP64 oracle.
+
+Tolerances: the gain term alone within 2e-5 (normwise relative) of the FP64 contraction; whole
+runs within relative L-infinity 1e-5 of the FP64 oracle run with the same dt per instance.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle
+from dtb import synth
+from dtb.batch import BatchedEuler
+from dtb.structs import BinaryMatrices, EmissionMatrices, LossBlock
+
+pytestmark = pytest.mark.gpu
+
+TOL_GAIN = 2e-5
+TOL_RUN = 1e-5
+
+
+def rel_linf(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / np.max(np.abs(np.asarray(b))))
+
+
+def _gain_only(w):
+    n = w.ps.n_state
+    w.binm = BinaryMatrices(gains=w.binm.gains)
+    w.emim = EmissionMatrices()
+    w.fluxm.P_Flux = sp.csc_matrix((n, n))
+    w.fluxm.X_Flux = sp.csc_matrix((n, n))
+    w.inj = np.zeros(n)
+    return w
+
+
+@pytest.mark.parametrize("p,u,batch", [(8, 4, 8), (16, 8, 100), (8, 8, 300), (12, 6, 40)])
+def test_batched_gain_term_matches_fp64(cuda, p, u, batch):
+    """One step with only the gain term: f1 - f0 = gain; covers BN = 64, 128, 256, several N
+    tiles, n2 padded to 64 (p*u = 32, 72) and more than one M tile."""
+    w = _gain_only(synth.batched_two_species(p, 1e-2, 1e2, u, batch, seed=p * 100 + u))
+    for g in w.binm.gains:  # make the gain dominate the step
+        g.G = np.asarray(g.G) * 50.0
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, batch)
+    for i in range(batch):
+        m.admit(i, w.f0[i], 1.0, 1)
+    m.run(1)
+    ns = w.ps.species_sizes[0]
+    Ge = np.asarray(w.binm.gains[0].G)
+    Gg = np.asarray(w.binm.gains[1].G)
+    for i in list(range(min(batch, 6))) + [batch - 1]:
+        f0 = w.f0[i]
+        gain = np.concatenate([oracle.gain_rows(Ge, 0, ns, f0[:ns], f0[ns:]),
+                               oracle.gain_rows(Gg, 0, ns, f0[:ns], f0[ns:])])
+        got = m.get_f(i) - f0
+        assert rel_linf(got, gain) <= TOL_GAIN, i
+    m.close()
+
+
+def test_batched_run_matches_oracle(cuda):
+    """All operators, per-instance dt, 60 steps."""
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, 12, seed=5)
+    rng = np.random.default_rng(1)
+    w.inj = rng.uniform(0, 1e-4, w.ps.n_state)
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 12)
+    for i in range(12):
+        m.admit(i, w.f0[i], w.dt[i], 60)
+    m.run(60)
+    ops = oracle.blocked_from_workload(w)
+    for i in range(12):
+        f = w.f0[i].copy()
+        for _ in range(60):
+            f, _, _ = ops.step(f, w.dt[i], 0)
+        assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
+        info = m.info(i)
+        assert info["steps_done"] == 60 and info["steps_left"] == 0 and info["finite"]
+    m.close()
+
+
+def test_slot_alone_equals_slot_in_mix(cuda):
+    """A solve gives the same result alone in the batch and among other running solves."""
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, 16, seed=6)
+    a = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 16)
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 16)
+    a.admit(3, w.f0[3], w.dt[3], 40)
+    for i in range(16):
+        b.admit(i, w.f0[i], w.dt[i], 40 + 7 * i)
+    a.run(40)
+    b.run(40)
+    np.testing.assert_array_equal(a.get_f(3), b.get_f(3))
+    a.close()
+    b.close()
+
+
+def test_stop_and_readmit(cuda):
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, 4, seed=7)
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 4)
+    m.admit(0, w.f0[0], w.dt[0], 10)
+    m.admit(1, w.f0[1], w.dt[1], 25)
+    m.run(20)
+    f10 = m.get_f(0)
+    m.run(10)
+    np.testing.assert_array_equal(m.get_f(0), f10)  # finished slots do not step
+    assert m.info(0)["steps_done"] == 10 and m.info(1)["steps_done"] == 25
+    # re-admit slot 0 mid-run: it restarts from its new initial state
+    m.admit(0, w.f0[2], w.dt[2], 5)
+    m.run(5)
+    ops = oracle.blocked_from_workload(w)
+    f = w.f0[2].copy()
+    for _ in range(5):
+        f, _, _ = ops.step(f, w.dt[2], 0)
+    assert rel_linf(m.get_f(0), f) <= TOL_RUN
+    m.close()
+
+
+def test_config2_sampled_instances(cuda):
+    """Config 2 (256 instances, N_s = 256, shared G 2 x 256 x 65,536): 24 steps, 3 instances
+    checked against the FP64 oracle."""
+    w = synth.config2(seed=2, gain_on_device=True)
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 256)
+    for i in range(256):
+        m.admit(i, w.f0[i], w.dt[i], 24)
+    m.run(24)
+    gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, g.G.double().cpu().numpy()) for g in w.binm.gains]
+    ops = oracle.BlockedOperands(w.ps.species_sizes, 1, gains, w.binm.losses, w.emim.blocks, w.fluxm.F_Flux,
+                                 1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj)
+    for i in (0, 101, 255):
+        f = w.f0[i].copy()
+        for _ in range(24):
+            f, _, _ = ops.step(f, w.dt[i], 0)
+        assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
+    m.close()
