@@ -159,7 +159,9 @@ int commit_mixed(dtb_ctx* c) {
             std::vector<float> h(elems);
             for (size_t k = 0; k < elems; ++k) h[k] = (float)g.host[k];
             DTB_CUDA(cudaMalloc(&tmp, sizeof(float) * elems));
-            DTB_CUDA(cudaMemcpy(tmp, h.data(), sizeof(float) * elems, cudaMemcpyHostToDevice));
+            // stream-ordered with the conversion kernel below: a plain cudaMemcpy from pageable
+            // memory may return before its DMA lands, unordered with this non-blocking stream
+            DTB_CUDA(cudaMemcpyAsync(tmp, h.data(), sizeof(float) * elems, cudaMemcpyHostToDevice, s));
             srcf = tmp;
         } else {
             DTB_CHECK(g.dev_src.size() == 1, DTB_EINVAL, "a device-resident gain block must be uploaded once");
@@ -276,7 +278,7 @@ int commit_mixed(dtb_ctx* c) {
             std::vector<float> h(e.data.begin(), e.data.end());
             float* tmp = nullptr;
             DTB_CUDA(cudaMalloc(&tmp, sizeof(float) * h.size()));
-            DTB_CUDA(cudaMemcpy(tmp, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+            DTB_CUDA(cudaMemcpyAsync(tmp, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, s));
             DTB_CUDA(launch_split_emi(tmp, (int)e.nrows, (int)e.ncols, (int)e.ncols, d_data + doff[p], d_scale + soff[p], s));
             DTB_CUDA(cudaStreamSynchronize(s));
             cudaFree(tmp);
@@ -356,15 +358,16 @@ int commit_mixed(dtb_ctx* c) {
     for (int k = 0; k < 2; ++k) {
         DTB_TRY(c->alloc(&m->F[k], sizeof(float) * nb));
         DTB_TRY(c->alloc(&m->C[k], sizeof(float) * nb));
-        DTB_CUDA(cudaMemset(m->F[k], 0, sizeof(float) * nb));
-        DTB_CUDA(cudaMemset(m->C[k], 0, sizeof(float) * nb));
+        DTB_CUDA(cudaMemsetAsync(m->F[k], 0, sizeof(float) * nb, s));
+        DTB_CUDA(cudaMemsetAsync(m->C[k], 0, sizeof(float) * nb, s));
     }
     DTB_TRY(c->alloc(&m->sig, sizeof(float) * (size_t)c->ns * B));
     DTB_TRY(c->alloc(&m->isig, sizeof(float) * (size_t)c->ns * B));
     {
         std::vector<float> ones((size_t)c->ns * B, 1.0f);
-        DTB_CUDA(cudaMemcpy(m->sig, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice));
-        DTB_CUDA(cudaMemcpy(m->isig, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice));
+        DTB_CUDA(cudaMemcpyAsync(m->sig, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice, s));
+        DTB_CUDA(cudaMemcpyAsync(m->isig, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice, s));
+        DTB_CUDA(cudaStreamSynchronize(s));
     }
     DTB_TRY(c->alloc(&m->dt_scale, sizeof(double) * B));
     DTB_TRY(c->alloc(&m->stop_step, sizeof(long long) * B));
@@ -373,15 +376,16 @@ int commit_mixed(dtb_ctx* c) {
     DTB_TRY(c->alloc(&m->gstep, sizeof(unsigned long long)));
     DTB_TRY(c->alloc(&m->ticket, sizeof(unsigned)));
     DTB_TRY(c->alloc(&c->err, sizeof(int)));
-    DTB_CUDA(cudaMemset(m->dt_scale, 0, sizeof(double) * B));
-    DTB_CUDA(cudaMemset(m->stop_step, 0, sizeof(long long) * B));
-    DTB_CUDA(cudaMemset(m->nonfinite, 0, sizeof(int) * B));
-    DTB_CUDA(cudaMemset(m->gstep, 0, sizeof(unsigned long long)));
-    DTB_CUDA(cudaMemset(m->ticket, 0, sizeof(unsigned)));
-    DTB_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+    DTB_CUDA(cudaMemsetAsync(m->dt_scale, 0, sizeof(double) * B, s));
+    DTB_CUDA(cudaMemsetAsync(m->stop_step, 0, sizeof(long long) * B, s));
+    DTB_CUDA(cudaMemsetAsync(m->nonfinite, 0, sizeof(int) * B, s));
+    DTB_CUDA(cudaMemsetAsync(m->gstep, 0, sizeof(unsigned long long), s));
+    DTB_CUDA(cudaMemsetAsync(m->ticket, 0, sizeof(unsigned), s));
+    DTB_CUDA(cudaMemsetAsync(c->err, 0, sizeof(int), s));
     {
         std::vector<unsigned long long> inf((size_t)B, ord_enc_host(INFINITY));
-        DTB_CUDA(cudaMemcpy(m->min_ratio, inf.data(), sizeof(unsigned long long) * B, cudaMemcpyHostToDevice));
+        DTB_CUDA(cudaMemcpyAsync(m->min_ratio, inf.data(), sizeof(unsigned long long) * B, cudaMemcpyHostToDevice, s));
+        DTB_CUDA(cudaStreamSynchronize(s));
     }
     DTB_CUDA(cudaMallocHost(&m->pin_col, sizeof(float) * 2 * (size_t)n_mom));
     DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));

@@ -176,14 +176,20 @@ inline int copy_host_vec(dtb_ctx* c, T** dst, const std::vector<double>& src) {
     std::vector<T> tmp(src.size());
     for (size_t i = 0; i < src.size(); ++i) tmp[i] = (T)src[i];
     DTB_TRY(c->alloc(dst, sizeof(T) * std::max<size_t>(1, tmp.size())));
-    if (!tmp.empty()) DTB_CUDA(cudaMemcpy(*dst, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice));
+    if (!tmp.empty()) {
+        DTB_CUDA(cudaMemcpyAsync(*dst, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+    }
     return DTB_OK;
 }
 
 template <typename I>
 inline int copy_host_ints(dtb_ctx* c, I** dst, const std::vector<I>& src) {
     DTB_TRY(c->alloc(dst, sizeof(I) * std::max<size_t>(1, src.size())));
-    if (!src.empty()) DTB_CUDA(cudaMemcpy(*dst, src.data(), sizeof(I) * src.size(), cudaMemcpyHostToDevice));
+    if (!src.empty()) {
+        DTB_CUDA(cudaMemcpyAsync(*dst, src.data(), sizeof(I) * src.size(), cudaMemcpyHostToDevice, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+    }
     return DTB_OK;
 }
 

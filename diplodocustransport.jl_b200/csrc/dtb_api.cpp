@@ -329,7 +329,7 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     c->has_bin = !c->gains.empty() || !c->losses.empty();
     if (!blks.empty()) {
         DTB_TRY(c->alloc(&c->G_all, esz * (size_t)total_elems));
-        DTB_CUDA(cudaMemset(c->G_all, 0, esz * (size_t)total_elems));
+        DTB_CUDA(cudaMemsetAsync(c->G_all, 0, esz * (size_t)total_elems, c->stream));
         size_t bi = 0;
         for (auto& kv : c->gains) {
             GainStage& g = kv.second;
@@ -346,7 +346,9 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
                     for (int64_t r = 0; r < nr; ++r)
                         for (int64_t k = 0; k < b.n2; ++k)
                             tmp[(size_t)(r * b.n2p + k)] = (T)g.host[(size_t)((r0 + r) * b.n2 + k)];
-                    DTB_CUDA(cudaMemcpy(dst + r0 * b.n2p, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice));
+                    DTB_CUDA(cudaMemcpyAsync(dst + r0 * b.n2p, tmp.data(), sizeof(T) * tmp.size(),
+                                             cudaMemcpyHostToDevice, c->stream));
+                    DTB_CUDA(cudaStreamSynchronize(c->stream));
                 }
             }
             for (auto& src : g.dev_src) {
@@ -408,7 +410,8 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     DTB_TRY(copy_host_ints(c, &c->units, units));
     DTB_TRY(copy_host_ints(c, &c->unit_ptr, unit_ptr));
     DTB_TRY(c->alloc(&c->partial, sizeof(double) * (size_t)std::max(1, c->n_units) * c->n_space));
-    DTB_CUDA(cudaMemset(c->partial, 0, sizeof(double) * (size_t)std::max(1, c->n_units) * c->n_space));
+    DTB_CUDA(cudaMemsetAsync(c->partial, 0, sizeof(double) * (size_t)std::max(1, c->n_units) * c->n_space,
+                             c->stream));
 
     // ---------------- loss blocks, grouped by row species
     {
@@ -549,7 +552,8 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
         c->f_init_dev = fi;
         DTB_TRY(c->alloc(reinterpret_cast<T**>(&c->f_buf[0]), sizeof(T) * (size_t)c->n_state));
         DTB_TRY(c->alloc(reinterpret_cast<T**>(&c->f_buf[1]), sizeof(T) * (size_t)c->n_state));
-        DTB_CUDA(cudaMemcpy(c->f_buf[0], fi, sizeof(T) * (size_t)c->n_state, cudaMemcpyDeviceToDevice));
+        DTB_CUDA(cudaMemcpyAsync(c->f_buf[0], fi, sizeof(T) * (size_t)c->n_state, cudaMemcpyDeviceToDevice,
+                                 c->stream));
         c->cur = 0;
     }
     ops.n_mom = (int)c->n_mom;
@@ -608,9 +612,9 @@ extern "C" int32_t dtb_commit(dtb_ctx* c) {
     DTB_TRY(copy_host_ints(c, &c->sp_off_dev, spo));
     DTB_TRY(c->alloc(&c->mom_w, sizeof(double) * (size_t)c->n_mom));
     DTB_TRY(c->alloc(&c->mom_out, sizeof(double) * 2 * (size_t)c->ns * c->n_space));
-    DTB_CUDA(cudaMemset(c->ctr, 0, sizeof(unsigned long long)));
-    DTB_CUDA(cudaMemset(c->ticket, 0, sizeof(unsigned)));
-    DTB_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+    DTB_CUDA(cudaMemsetAsync(c->ctr, 0, sizeof(unsigned long long), c->stream));
+    DTB_CUDA(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), c->stream));
+    DTB_CUDA(cudaMemsetAsync(c->err, 0, sizeof(int), c->stream));
     DTB_CUDA(cudaMallocHost(&c->pin_dt, sizeof(double) * (size_t)c->hist_cap));
     DTB_CUDA(cudaMallocHost(&c->pin_hist, sizeof(StepDiagDev) * (size_t)c->hist_cap));
     DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));

@@ -168,7 +168,7 @@ extern "C" int32_t dtb_gain_contract(int32_t dtype, const void* G, int64_t n_out
         sc.bytes = need;
     }
     if (!sc.err) {
-        if (cudaMalloc(&sc.err, sizeof(int)) != cudaSuccess || cudaMemset(sc.err, 0, sizeof(int)) != cudaSuccess) {
+        if (cudaMalloc(&sc.err, sizeof(int)) != cudaSuccess || cudaMemsetAsync(sc.err, 0, sizeof(int), s) != cudaSuccess) {
             set_error("dtb_gain_contract: error-flag allocation failed");
             return DTB_ENOMEM;
         }
