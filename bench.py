@@ -184,9 +184,53 @@ def cpu_sample(w, dtype: str, budget_s: float = 15.0):
     return 1.0 / t_step, oracle.num_threads(), desc
 
 
+def build_batched(config: int, device: str, host: bool = False):
+    from dtb import synth
+    if config == 2:
+        return synth.config2(seed=2, gain_on_device=not host, device=device)
+    if config == 3:
+        return synth.config3(seed=3, batch=64, gain_on_device=not host, device=device)
+    raise SystemExit(f"unknown batched config {config}")
+
+
+def cpu_sample_batched(w, budget_s: float = 15.0):
+    """FP64 oracle port of one instance on the host cores (OpenMP), a few steps; instance-steps/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp,
+                     g.G.double().cpu().numpy() if hasattr(g.G, "is_cuda") else np.asarray(g.G, dtype=np.float64))
+             for g in w.binm.gains]
+    ops = oracle.BlockedOperands(w.ps.species_sizes, 1, gains, w.binm.losses, w.emim.blocks, w.fluxm.F_Flux,
+                                 1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj)
+    f = np.array(w.f0[0])
+    ops.step(f, float(w.dt[0]), 1)
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < budget_s and k < 200:
+        f, _, _ = ops.step(f, float(w.dt[0]), 1)
+        k += 1
+    dt = (time.perf_counter() - t0) / k
+    return 1.0 / dt, oracle.num_threads(), f"FP64 oracle (C, OpenMP), one instance, {k} full steps"
+
+
 def run_reference(args):
     rank, local, world = _env_rank()
     if rank != 0:
+        return 0
+    if args.config in (2, 3):
+        w = build_batched(args.config, "cpu", host=True)
+        v, cores, desc = cpu_sample_batched(w, budget_s=20.0)
+        value = v
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "instance-steps/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": _config_dict(args.config, w),
+                "cpu_baseline": {"value": value, "unit": "instance-steps/s", "cores": cores, "kind": "port",
+                                 "sample": desc},
+                "e2e": {"value": value, "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return 0
     # host-only workload: a sample of gain rows is all the timing needs
     w, dtype = build_workload(args.config, "cpu", host_sample_rows=256)
@@ -212,6 +256,16 @@ def _has_cuda():
 
 def _config_dict(config: int, w):
     sizes = w.ps.species_sizes
+    if config == 2:
+        return {"workload": "batching (config 2): 256 independent instances, 2 species x 256 states "
+                            "(32 log p x 8 u), shared G 2 x 256 x 65536 as BF16 hi+lo, per-instance f0 and dt",
+                "species_states": sizes, "batch": 256, "precision": "BF16x3 gain GEMM, FP32 f, FP64 update",
+                "l2": "G hi+lo 134 MB per step, larger than L2"}
+    if config == 3:
+        return {"workload": "mixed precision (config 3): 64 instances, e-, e+, gamma x 576 states "
+                            "(48 log p x 12 u), 6 gain tensors 576 x 331776 as BF16 hi+lo, synchrotron-like emission",
+                "species_states": sizes, "batch": 64, "precision": "BF16x3 gain GEMM, FP32 f, FP64 update",
+                "l2": "G hi+lo 4.6 GB per step, larger than L2"}
     if config == 1 and sizes != [1024, 1024]:
         return {"workload": f"config-1 recipe on a smaller grid: 2 species x {sizes[0]} states, FP32",
                 "species_states": sizes, "precision": "FP32"}
@@ -325,19 +379,164 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from dtb.batch import BatchedEuler
+    from dtb.stepping import ForwardEulerStruct
+    rank, local, world = _env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = f"cuda:{local}"
+    w = build_batched(args.config, dev)
+    B = w.f0.shape[0]
+    n = w.ps.n_state
+    K, W = args.steps, args.warmup
+    stream = torch.cuda.Stream()
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B, device=local, stream=stream.cuda_stream)
+    for i in range(B):
+        m.admit(i, w.f0[i], float(w.dt[i]), 1 << 40)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_sample_batched(w, budget_s=15.0)
+    # accuracy against the FP64 oracle: W warm-up steps of two instances
+    acc = None
+    if rank == 0 and not args.no_check:
+        import oracle
+        gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, g.G.double().cpu().numpy()) for g in w.binm.gains]
+        ops = oracle.BlockedOperands(w.ps.species_sizes, 1, gains, w.binm.losses, w.emim.blocks, w.fluxm.F_Flux,
+                                     1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj)
+    # plain FP64 path on the same grid (one instance), for the batched-vs-plain comparison
+    gains64 = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, g.G.double()) for g in w.binm.gains]
+    from dtb.structs import BinaryMatrices
+    binm64 = BinaryMatrices(gains=gains64, losses=w.binm.losses)
+    plain = ForwardEulerStruct(w.ps, w.f0[0], w.inj, binm64, w.emim, w.fluxm, Precision=np.float64, device=local,
+                               stream=stream.cuda_stream)
+    del gains64, binm64
+    w.binm.gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, None) for g in w.binm.gains]
+    torch.cuda.empty_cache()
+    m.run(W)  # warm-up (captures the graph)
+    if rank == 0 and not args.no_check:
+        errs = []
+        for i in (0, B - 1):
+            f = np.array(w.f0[i])
+            for _ in range(W):
+                f, _, _ = ops.step(f, float(w.dt[i]), 0)
+            g = m.get_f(i)
+            errs.append(float(np.max(np.abs(g - f)) / np.max(np.abs(f))))
+        acc = {"rel_linf_vs_fp64_oracle": max(errs), "steps": W, "instances": [0, B - 1]}
+        del ops
+    # ---- timed region: graph replay, device resident
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(_smi_id(local)) as cs:
+        e0.record(stream)
+        m.run(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    # ---- the same K steps with CUDA events around every gain-GEMM launch (direct launches)
+    m.set_profiling(True)
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e4.record(stream)
+    m.run(K)
+    e5.record(stream)
+    torch.cuda.synchronize()
+    ms_prof = e4.elapsed_time(e5)
+    st = m.gemm_stats()
+    m.set_profiling(False)
+    # ---- e2e: the whole batch state from pinned host memory in and out every step
+    Fh = torch.empty((B, n), dtype=torch.float64).pin_memory().numpy()
+    m.get_f_all(Fh)
+    K2 = max(1, K // 4)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(K2):
+        m.set_f_all(Fh)
+        m.run(1)
+        m.get_f_all(Fh)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    # ---- plain FP64 single instance on the same grid
+    K3 = max(16, K // 4)
+    plain.run(np.ones(4))
+    e6, e7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e6.record(stream)
+    plain.run(np.full(K3, float(w.dt[0])))
+    e7.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e6.elapsed_time(e7)
+    plain.close()
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e, ms_plain], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e, ms_plain = float(t[0]), float(t[1]), float(t[2])
+    value = world * B * K / (ms / 1e3)
+    plain_sps = world * K3 / (ms_plain / 1e3)
+    pj = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(pj.get("bf16_tflops", 1590.0))
+    peak_s = float(pj.get("bf16_tflops_sustained", 1400.0))
+    achieved = st["flops_per_step"] / (st["avg_ms"] / 1e3) / 1e12 if st["avg_ms"] > 0 else None
+    traffic = _profile_traffic(f"gain_gemm_config{args.config}.md")
+    line = {"metric": METRIC, "value": value, "unit": "instance-steps/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 (gain GEMM), f32 state, f64 update", "data": "synthetic (seeded; no collision data files)",
+            "config": dict(_config_dict(args.config, w), parallelism=f"batch replicas x{world}"),
+            "e2e": {"value": world * B * K2 / (ms_e2e / 1e3), "unit": "instance-steps/s",
+                    "h2d_bytes_per_step": B * n * 8, "d2h_bytes_per_step": B * n * 8},
+            "gpu_launches": int(st["launches_per_step"]) * K,
+            "roofline": {"bound": "tensor", "kernel": "gain_gemm (tcgen05, BF16 hi+lo x3)", "achieved": achieved,
+                         "peak": peak, "peak_kind": "measured burst" if pj else "fallback", "unit": "TFLOP/s",
+                         "frac": achieved / peak if achieved else None,
+                         "frac_of_sustained": achieved / peak_s if achieved else None,
+                         "traffic": traffic, "algorithmic_flops_per_step": st["flops_per_step"],
+                         "operator_bytes_per_step": st["bytes_per_step"], "avg_gemm_ms_per_step": st["avg_ms"],
+                         "profiled_ms_per_step": ms_prof / K},
+            "plain_fp64": {"value": plain_sps, "unit": "steps/s", "workload": "same grid, one instance, FP64"},
+            "speedup_vs_plain_fp64": value / plain_sps,
+            "clocks": cs.summary()}
+    if acc is not None:
+        line["accuracy"] = acc
+    if cpu is not None:
+        v, cores, desc = cpu
+        line["cpu_baseline"] = {"value": v, "unit": "instance-steps/s", "cores": cores, "kind": "port",
+                                "sample": desc}
+    m.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="p_bins x u_bins override of the config-1 grid, e.g. 32x16")
+    ap.add_argument("--no-check", action="store_true", help="skip the FP64 accuracy check of the batched run")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.config in (2, 3):
+        return run_batched(args)
     return run_ours(args)
 
 

@@ -51,6 +51,7 @@ struct MixedState {
     int graph_steps = 16;
     std::vector<long long> h_stop, h_start;
     float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation
+    float* pin_all = nullptr;  // [2][n_mom][Bcap] staging of the whole batch
     bool profiling = false;
     double prof_ms = 0;
     long long prof_n = 0;
@@ -423,6 +424,7 @@ void destroy_mixed(dtb_ctx* c) {
     if (m->graph) cudaGraphExecDestroy(m->graph);
     for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
     if (m->pin_col) cudaFreeHost(m->pin_col);
+    if (m->pin_all) cudaFreeHost(m->pin_all);
     delete m;
     c->mixed = nullptr;
 }
@@ -645,6 +647,46 @@ int32_t dtb_batch_release(dtb_ctx* c, int32_t slot) {
     DTB_CUDA(cudaMemcpyAsync(m->stop_step + slot, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
     m->h_stop[(size_t)slot] = 0;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_set_f_all(dtb_ctx* c, const double* f) {
+    DTB_TRY(mixed_ready(c));
+    DTB_CHECK(f, DTB_EINVAL, "dtb_batch_set_f_all: null input");
+    MixedState* m = c->mixed;
+    DeviceGuard g(c->device);
+    const int n = (int)c->n_mom, B = m->Bcap;
+    if (!m->pin_all) DTB_CUDA(cudaMallocHost(&m->pin_all, sizeof(float) * 2 * (size_t)n * B));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    float* hf = m->pin_all;
+    float* hc = m->pin_all + (size_t)n * B;
+    for (int i = 0; i < B; ++i)
+        for (int a = 0; a < n; ++a) {
+            const double v = f[(size_t)i * n + a];
+            const float fv = (float)v;
+            hf[(size_t)a * B + i] = fv;
+            hc[(size_t)a * B + i] = (float)(v - (double)fv);
+        }
+    DTB_CUDA(cudaMemcpyAsync(m->F[m->cur], hf, sizeof(float) * (size_t)n * B, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(m->C[m->cur], hc, sizeof(float) * (size_t)n * B, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    return DTB_OK;
+}
+
+int32_t dtb_batch_get_f_all(dtb_ctx* c, double* f) {
+    DTB_TRY(mixed_ready(c));
+    DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f_all: null output");
+    MixedState* m = c->mixed;
+    DeviceGuard g(c->device);
+    const int n = (int)c->n_mom, B = m->Bcap;
+    if (!m->pin_all) DTB_CUDA(cudaMallocHost(&m->pin_all, sizeof(float) * 2 * (size_t)n * B));
+    float* hf = m->pin_all;
+    float* hc = m->pin_all + (size_t)n * B;
+    DTB_CUDA(cudaMemcpyAsync(hf, m->F[m->cur], sizeof(float) * (size_t)n * B, cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(hc, m->C[m->cur], sizeof(float) * (size_t)n * B, cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    for (int a = 0; a < n; ++a)
+        for (int i = 0; i < B; ++i) f[(size_t)i * n + a] = (double)hf[(size_t)a * B + i] + (double)hc[(size_t)a * B + i];
     return DTB_OK;
 }
 

@@ -87,6 +87,8 @@ SIGNATURES = {
     "dtb_batch_get_f": (_i32, [_P, _i32, _dp]),
     "dtb_batch_slot_info": (_i32, [_P, _i32, _ip, _ip, _dp, _i32p]),
     "dtb_batch_release": (_i32, [_P, _i32]),
+    "dtb_batch_set_f_all": (_i32, [_P, _dp]),
+    "dtb_batch_get_f_all": (_i32, [_P, _dp]),
     "dtb_batch_capacity": (_i32, [_P, _i32p, _ip]),
     "dtb_batch_set_profiling": (_i32, [_P, _i32]),
     "dtb_batch_gemm_stats": (_i32, [_P, _dp, _dp, _dp, _i32p]),

@@ -84,6 +84,18 @@ class BatchedEuler:
         check(self.L.dtb_batch_get_f(self.ctx, int(slot), dptr(out)))
         return out
 
+    def set_f_all(self, F) -> None:
+        """Every slot's f from a (capacity, n) array."""
+        A = np.ascontiguousarray(F, dtype=np.float64)
+        check(self.L.dtb_batch_set_f_all(self.ctx, dptr(A)))
+
+    def get_f_all(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Every slot's f as a (capacity, n) array."""
+        if out is None:
+            out = np.empty((self.capacity, self.n))
+        check(self.L.dtb_batch_get_f_all(self.ctx, dptr(out)))
+        return out
+
     def info(self, slot: int) -> dict:
         done, left = ctypes.c_int64(), ctypes.c_int64()
         cr = ctypes.c_double()

@@ -198,6 +198,11 @@ int32_t dtb_batch_get_f(dtb_ctx* ctx, int32_t slot, double* f);
 int32_t dtb_batch_slot_info(dtb_ctx* ctx, int32_t slot, int64_t* steps_done, int64_t* steps_left,
                             double* cr_max, int32_t* finite);
 
+/* The whole batch's state in or out: f is [batch][n_mom] Float64 (slot-major). set_f_all
+ * replaces every slot's f (steps left and dt are kept); get_f_all reads every slot's f. */
+int32_t dtb_batch_set_f_all(dtb_ctx* ctx, const double* f);
+int32_t dtb_batch_get_f_all(dtb_ctx* ctx, double* f);
+
 /* Stops a slot (it no longer steps). */
 int32_t dtb_batch_release(dtb_ctx* ctx, int32_t slot);
 
