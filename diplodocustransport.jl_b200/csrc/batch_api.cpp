@@ -26,13 +26,15 @@ struct MixedGroup {
     float* row_scale = nullptr;
     CUtensorMap tm_hi{}, tm_lo{};
     float* partial = nullptr;
+    float* gsum = nullptr;  // [Bcap][M]
     int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256;
     double flops = 0;  // 3 MMAs x 2 x M x K x Bcap
     double bytes = 0;  // hi + lo bytes of G
 };
 
 struct MixedState {
-    int Bcap = 0;
+    int Bcap = 0;   // slots in the state matrix: the requested capacity rounded up to 4 (row stride)
+    int Buser = 0;  // slots the caller may use
     std::vector<MixedGroup> groups;
     float* F[2] = {nullptr, nullptr};
     float* C[2] = {nullptr, nullptr};
@@ -52,6 +54,9 @@ struct MixedState {
     std::vector<long long> h_stop, h_start;
     float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation
     float* pin_all = nullptr;  // [2][n_mom][Bcap] staging of the whole batch
+    int* sp_off = nullptr;     // device species offsets
+    double* mom_w = nullptr;   // device energy weights (n_mom)
+    double* mom_out = nullptr; // device moments [Bcap][ns][2]
     bool profiling = false;
     double prof_ms = 0;
     long long prof_n = 0;
@@ -108,7 +113,8 @@ int commit_mixed(dtb_ctx* c) {
     DTB_CHECK(c->opts.batch >= 1, DTB_EINVAL, "batched context needs opts.batch >= 1");
     auto* m = new MixedState();
     c->mixed = m;
-    m->Bcap = c->opts.batch;
+    m->Buser = c->opts.batch;
+    m->Bcap = (int)round_up(c->opts.batch, 4);
     if (c->opts.graph_steps > 0) m->graph_steps = (c->opts.graph_steps + 1) / 2 * 2;
     MixedRowOps& ops = m->ops;
     const int B = m->Bcap;
@@ -198,7 +204,8 @@ int commit_mixed(dtb_ctx* c) {
         G.tiles_per_split = (T + S - 1) / S;
         G.n_splits = (T + G.tiles_per_split - 1) / G.tiles_per_split;
         DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
-        G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * B;
+        DTB_TRY(c->alloc(&G.gsum, sizeof(float) * (size_t)B * G.M));
+        G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * m->Buser;
         G.bytes = 4.0 * G.M * (double)G.N1 * G.n2;
     }
     // ---------------- gain lookup per species
@@ -388,6 +395,12 @@ int commit_mixed(dtb_ctx* c) {
         DTB_CUDA(cudaMemcpyAsync(m->min_ratio, inf.data(), sizeof(unsigned long long) * B, cudaMemcpyHostToDevice, s));
         DTB_CUDA(cudaStreamSynchronize(s));
     }
+    {
+        std::vector<int> spo(c->off, c->off + c->ns + 1);
+        DTB_TRY(copy_host_ints(c, &m->sp_off, spo));
+        DTB_TRY(c->alloc(&m->mom_w, sizeof(double) * (size_t)n_mom));
+        DTB_TRY(c->alloc(&m->mom_out, sizeof(double) * 2 * (size_t)c->ns * B));
+    }
     DTB_CUDA(cudaMallocHost(&m->pin_col, sizeof(float) * 2 * (size_t)n_mom));
     DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));
     m->h_stop.assign((size_t)B, 0);
@@ -398,13 +411,27 @@ int commit_mixed(dtb_ctx* c) {
     for (int sp = 0; sp <= c->ns; ++sp) ops.sp_off[sp] = (int)c->off[sp];
     for (size_t gi = 0; gi < m->groups.size(); ++gi) {
         const MixedGroup& G = m->groups[gi];
-        ops.grp_partial[gi] = G.partial;
-        ops.grp_scale[gi] = G.row_scale;
-        ops.grp_sig1[gi] = m->sig + (size_t)G.in1 * B;
-        ops.grp_sig2[gi] = m->sig + (size_t)G.in2 * B;
+        ops.grp_gsum[gi] = G.gsum;
         ops.grp_M[gi] = G.M;
-        ops.grp_splits[gi] = G.n_splits;
-        ops.grp_Bpad[gi] = G.Bpad;
+    }
+    // tiles whose rows share one species and one list of emission pieces that cover all of
+    // them take the shared-memory tile products
+    {
+        const int tr = mixed_rows_tile_rows();
+        const int n_tiles_r = (n_mom + tr - 1) / tr;
+        std::vector<std::vector<int>> emi_rows((size_t)n_mom);
+        for (size_t p = 0; p < c->emis.size(); ++p)
+            for (int64_t r = 0; r < c->emis[p].nrows; ++r) emi_rows[(size_t)(c->emis[p].row0 + r)].push_back((int)p);
+        std::vector<unsigned char> fast((size_t)n_tiles_r, 1);
+        for (int t = 0; t < n_tiles_r; ++t) {
+            const int a0 = t * tr, a1 = std::min(n_mom, a0 + tr);
+            const int s0 = species_of(c, a0);
+            for (int a = a0; a < a1; ++a)
+                if (species_of(c, a) != s0 || emi_rows[(size_t)a] != emi_rows[(size_t)a0]) fast[(size_t)t] = 0;
+        }
+        unsigned char* d_fast;
+        DTB_TRY(copy_host_ints(c, &d_fast, fast));
+        ops.tile_fast = d_fast;
     }
     ops.thr = (double)1e-10f;
     ops.has_bin = c->has_bin;
@@ -484,10 +511,33 @@ int mixed_step(dtb_ctx* c, bool profile) {
         m->prof_n++;
         if (++m->prof_pending == 256) DTB_TRY(mixed_flush_profile(m));
     }
+    for (auto& G : m->groups)
+        DTB_CUDA(launch_split_reduce(G.partial, G.n_splits, G.Bpad, G.M, m->Bcap, G.row_scale,
+                                     m->sig + (size_t)G.in1 * m->Bcap, m->sig + (size_t)G.in2 * m->Bcap, G.gsum,
+                                     c->stream));
     DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, m->ticket,
                                c->stream));
     m->cur ^= 1;
     m->host_step++;
+    return DTB_OK;
+}
+
+int ensure_mixed_graph(dtb_ctx* c) {
+    MixedState* m = c->mixed;
+    if (m->graph) return DTB_OK;
+    const long long hs = m->host_step;
+    cudaGraph_t gr;
+    DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = DTB_OK;
+    for (int k = 0; k < m->graph_steps && rc == DTB_OK; ++k) rc = mixed_step(c, false);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+    m->host_step = hs;
+    m->cur = 0;
+    if (rc != DTB_OK) return rc;
+    DTB_CUDA(e);
+    e = cudaGraphInstantiate(&m->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    DTB_CUDA(e);
     return DTB_OK;
 }
 
@@ -513,12 +563,42 @@ int mixed_ready(dtb_ctx* c) {
 
 }  // namespace
 
+// Launch / finish halves of dtb_batch_run for the serving loop (contexts of different grids
+// run their chunks concurrently on their own streams).
+int batch_launch(dtb_ctx* c, int64_t nsteps) {
+    MixedState* m = c->mixed;
+    DeviceGuard g(c->device);
+    int64_t done = 0;
+    if (nsteps >= m->graph_steps) {
+        if (m->cur != 0) {
+            DTB_TRY(mixed_step(c, false));
+            done++;
+        }
+        DTB_TRY(ensure_mixed_graph(c));
+        while (nsteps - done >= m->graph_steps) {
+            DTB_CUDA(cudaGraphLaunch(m->graph, c->stream));
+            done += m->graph_steps;
+            m->host_step += m->graph_steps;
+        }
+    }
+    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, false));
+    return DTB_OK;
+}
+
+int batch_finish(dtb_ctx* c) {
+    DeviceGuard g(c->device);
+    return mixed_check_err(c);
+}
+
+int batch_capacity(dtb_ctx* c) { return c->mixed ? c->mixed->Buser : 0; }
+long long batch_step(dtb_ctx* c) { return c->mixed ? c->mixed->host_step : 0; }
+
 extern "C" {
 
 int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_scale, int64_t n_steps) {
     DTB_TRY(mixed_ready(c));
     MixedState* m = c->mixed;
-    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_admit: slot out of range");
+    DTB_CHECK(slot >= 0 && slot < m->Buser, DTB_ENOTFOUND, "dtb_batch_admit: slot out of range");
     DTB_CHECK(f0, DTB_EINVAL, "dtb_batch_admit: null f0");
     DTB_CHECK(n_steps >= 0 && std::isfinite(dt_scale), DTB_EINVAL, "dtb_batch_admit: bad dt_scale or step count");
     DeviceGuard g(c->device);
@@ -574,21 +654,7 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
             DTB_TRY(mixed_step(c, false));
             done++;
         }
-        if (!m->graph) {
-            const long long hs = m->host_step;
-            cudaGraph_t gr;
-            DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            int rc = DTB_OK;
-            for (int k = 0; k < m->graph_steps && rc == DTB_OK; ++k) rc = mixed_step(c, false);
-            cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
-            m->host_step = hs;
-            m->cur = 0;
-            if (rc != DTB_OK) return rc;
-            DTB_CUDA(e);
-            e = cudaGraphInstantiate(&m->graph, gr, 0);
-            cudaGraphDestroy(gr);
-            DTB_CUDA(e);
-        }
+        DTB_TRY(ensure_mixed_graph(c));
         while (nsteps - done >= m->graph_steps) {
             DTB_CUDA(cudaGraphLaunch(m->graph, c->stream));
             done += m->graph_steps;
@@ -603,7 +669,7 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
 int32_t dtb_batch_get_f(dtb_ctx* c, int32_t slot, double* f) {
     DTB_TRY(mixed_ready(c));
     MixedState* m = c->mixed;
-    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_get_f: slot out of range");
+    DTB_CHECK(slot >= 0 && slot < m->Buser, DTB_ENOTFOUND, "dtb_batch_get_f: slot out of range");
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f: null output");
     DeviceGuard g(c->device);
     const int n = (int)c->n_mom, B = m->Bcap;
@@ -620,7 +686,7 @@ int32_t dtb_batch_slot_info(dtb_ctx* c, int32_t slot, int64_t* steps_done, int64
                             int32_t* finite) {
     DTB_TRY(mixed_ready(c));
     MixedState* m = c->mixed;
-    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_slot_info: slot out of range");
+    DTB_CHECK(slot >= 0 && slot < m->Buser, DTB_ENOTFOUND, "dtb_batch_slot_info: slot out of range");
     DeviceGuard g(c->device);
     const long long stop = m->h_stop[(size_t)slot];
     const long long now = std::min(m->host_step, stop);
@@ -641,7 +707,7 @@ int32_t dtb_batch_slot_info(dtb_ctx* c, int32_t slot, int64_t* steps_done, int64
 int32_t dtb_batch_release(dtb_ctx* c, int32_t slot) {
     DTB_TRY(mixed_ready(c));
     MixedState* m = c->mixed;
-    DTB_CHECK(slot >= 0 && slot < m->Bcap, DTB_ENOTFOUND, "dtb_batch_release: slot out of range");
+    DTB_CHECK(slot >= 0 && slot < m->Buser, DTB_ENOTFOUND, "dtb_batch_release: slot out of range");
     DeviceGuard g(c->device);
     const long long zero = 0;
     DTB_CUDA(cudaMemcpyAsync(m->stop_step + slot, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream));
@@ -660,7 +726,8 @@ int32_t dtb_batch_set_f_all(dtb_ctx* c, const double* f) {
     DTB_CUDA(cudaStreamSynchronize(c->stream));
     float* hf = m->pin_all;
     float* hc = m->pin_all + (size_t)n * B;
-    for (int i = 0; i < B; ++i)
+    if (m->Buser < B) std::memset(m->pin_all, 0, sizeof(float) * 2 * (size_t)n * B);
+    for (int i = 0; i < m->Buser; ++i)
         for (int a = 0; a < n; ++a) {
             const double v = f[(size_t)i * n + a];
             const float fv = (float)v;
@@ -686,13 +753,32 @@ int32_t dtb_batch_get_f_all(dtb_ctx* c, double* f) {
     DTB_CUDA(cudaMemcpyAsync(hc, m->C[m->cur], sizeof(float) * (size_t)n * B, cudaMemcpyDeviceToHost, c->stream));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
     for (int a = 0; a < n; ++a)
-        for (int i = 0; i < B; ++i) f[(size_t)i * n + a] = (double)hf[(size_t)a * B + i] + (double)hc[(size_t)a * B + i];
+        for (int i = 0; i < m->Buser; ++i)
+            f[(size_t)i * n + a] = (double)hf[(size_t)a * B + i] + (double)hc[(size_t)a * B + i];
+    return DTB_OK;
+}
+
+int32_t dtb_batch_moments(dtb_ctx* c, const double* w, double* number, double* energy) {
+    DTB_TRY(mixed_ready(c));
+    DTB_CHECK(w && number && energy, DTB_EINVAL, "dtb_batch_moments: null argument");
+    MixedState* m = c->mixed;
+    DeviceGuard g(c->device);
+    const int B = m->Bcap, ns = c->ns;
+    DTB_CUDA(cudaMemcpyAsync(m->mom_w, w, sizeof(double) * (size_t)c->n_mom, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(launch_batch_moments(m->F[m->cur], m->C[m->cur], B, m->sp_off, ns, m->mom_w, m->mom_out, c->stream));
+    std::vector<double> out((size_t)2 * ns * B);
+    DTB_CUDA(cudaMemcpyAsync(out.data(), m->mom_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < (size_t)m->Buser * ns; ++k) {
+        number[k] = out[2 * k];
+        energy[k] = out[2 * k + 1];
+    }
     return DTB_OK;
 }
 
 int32_t dtb_batch_capacity(dtb_ctx* c, int32_t* capacity, int64_t* step) {
     DTB_TRY(mixed_ready(c));
-    if (capacity) *capacity = c->mixed->Bcap;
+    if (capacity) *capacity = c->mixed->Buser;
     if (step) *step = c->mixed->host_step;
     return DTB_OK;
 }
@@ -720,7 +806,7 @@ int32_t dtb_batch_gemm_stats(dtb_ctx* c, double* avg_ms, double* flops_per_step,
     if (avg_ms) *avg_ms = m->prof_n ? m->prof_ms / (double)m->prof_n : 0.0;
     if (flops_per_step) *flops_per_step = fl;
     if (bytes_per_step) *bytes_per_step = by;
-    if (launches_per_step) *launches_per_step = (int32_t)m->groups.size() + 1;
+    if (launches_per_step) *launches_per_step = 2 * (int32_t)m->groups.size() + 1;
     return DTB_OK;
 }
 

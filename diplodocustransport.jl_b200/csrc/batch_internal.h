@@ -39,7 +39,7 @@ cudaError_t prepare_gain_gemm(int bn);
 
 // Per-row operands of the batched Euler epilogue.
 struct MixedRowOps {
-    int n_mom, Bcap, n_species;
+    int n_mom, Bcap, n_species;  // Bcap: slots in the state matrix (a multiple of 4), its row stride
     int sp_off[DTB_MAX_SPECIES + 1];
     int ell_w;
     const float* ell_val;
@@ -64,13 +64,9 @@ struct MixedRowOps {
     int gain_ptr[DTB_MAX_SPECIES + 1];
     int gain_grp[64];
     int gain_roff[64];
-    const float* grp_partial[16];
-    const float* grp_scale[16];   // per stacked row, the power-of-two scale of G
-    const float* grp_sig1[16];    // [Bcap] power-of-two scale of the input species
-    const float* grp_sig2[16];
+    const float* grp_gsum[16];    // [Bcap][M] reduced, rescaled gain sums of the group
     int grp_M[16];
-    int grp_splits[16];
-    int grp_Bpad[16];
+    const unsigned char* tile_fast;  // per 64-row tile: loss/emission as shared-memory tile products
     const float* invAp;
     const float* inj;
     float vol;
@@ -84,6 +80,12 @@ struct MixedRowOps {
 
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out,
                               float* C_out, unsigned long long* gstep, unsigned* ticket, cudaStream_t s);
+cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
+                                const float* sig1, const float* sig2, float* gsum, cudaStream_t s);
+int mixed_rows_tile_rows();
+
+cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
+                                 const double* w, double* out, cudaStream_t s);
 
 cudaError_t launch_split_rows(const float* src, long long rows, int n1, int n2, int n2p, __nv_bfloat16* hi,
                               __nv_bfloat16* lo, float* row_scale, int* err, cudaStream_t s);

@@ -443,128 +443,261 @@ __device__ __forceinline__ unsigned long long ord_enc(double x) {
     return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
 
-constexpr int kTR = 32;  // rows per tile
-constexpr int kTI = 32;  // instances per tile
+constexpr int kRT = 64;  // rows per tile
+constexpr int kIT = 64;  // instances per tile
+constexpr int kCK = 32;  // K chunk of the loss / emission tile products
 
+// Sum of the split-K partial tiles of one gain group, scaled back to G and f units:
+// gsum[i][r] = row_scale[r] * sig1[i] * sig2[i] * sum_s partial[s][i][r]. Fixed summation order.
+__global__ void split_reduce_kernel(const float* __restrict__ partial, int n_splits, int Bpad, int M, int Bcap,
+                                    const float* __restrict__ row_scale, const float* __restrict__ sig1,
+                                    const float* __restrict__ sig2, float* __restrict__ gsum) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (r >= M || i >= Bcap) return;
+    const float* p = partial + (size_t)i * M + r;
+    const size_t stride = (size_t)Bpad * M;
+    float acc = 0.f;
+    int sp = 0;
+    for (; sp + 4 <= n_splits; sp += 4) {
+        const float v0 = p[(size_t)sp * stride], v1 = p[(size_t)(sp + 1) * stride];
+        const float v2 = p[(size_t)(sp + 2) * stride], v3 = p[(size_t)(sp + 3) * stride];
+        acc += v0;
+        acc += v1;
+        acc += v2;
+        acc += v3;
+    }
+    for (; sp < n_splits; ++sp) acc += p[(size_t)sp * stride];
+    gsum[(size_t)i * M + r] = acc * row_scale[r] * sig1[i] * sig2[i];
+}
+
+__device__ __forceinline__ int species_of_row(const MixedRowOps& ops, int a) {
+    int s = 0;
+    while (s + 1 < ops.n_species && a >= ops.sp_off[s + 1]) ++s;
+    return s;
+}
+
+// Loss and emission of one (row, instance) pair with direct loads (tiles the fast path cannot take).
+__device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict__ F, int a, int s, int i,
+                                 float& loss, float& emi) {
+    const int B = ops.Bcap;
+    loss = 0.f;
+    emi = 0.f;
+    if (ops.has_bin) {
+        const int la = a - ops.sp_off[s];
+        for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
+            const float* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
+            const int co = ops.loss_col_off[b], nc = ops.loss_ncols[b];
+            for (int c = 0; c < nc; ++c) loss += row[c] * F[(size_t)(co + c) * B + i];
+        }
+    }
+    if (ops.has_emi) {
+        for (int p = ops.emi_rptr[a]; p < ops.emi_rptr[a + 1]; ++p) {
+            const int pc = ops.emi_piece[p];
+            const __nv_bfloat162* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
+            const int col0 = ops.emi_col0[pc], nc = ops.emi_ncols[pc];
+            float acc = 0.f;
+            for (int c = 0; c < nc; ++c) {
+                const float2 e2 = __bfloat1622float2(row[c]);
+                acc += (e2.x + e2.y) * F[(size_t)(col0 + c) * B + i];
+            }
+            emi += acc * ops.emi_scale[ops.emi_scale_off[pc] + (a - ops.emi_row0[pc])];
+        }
+    }
+}
+
+// One 64-row x 64-instance tile per block, 256 threads, a 4 x 4 (row x instance) micro-tile
+// per thread. Loss and emission are tile products through shared memory when the tile's rows
+// belong to one species and every emission piece touching them covers them all (tile_fast).
 __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
                                                          const float* __restrict__ Cc, float* __restrict__ Fo,
                                                          float* __restrict__ Co, unsigned long long* gstep,
                                                          unsigned* ticket) {
-    __shared__ float s_gain[kTR][kTI + 1];
+    __shared__ float s_gain[kRT][kIT + 1];
+    __shared__ float s_L[kRT][kCK + 1];
+    __shared__ __align__(16) float s_F[kCK][kIT];
+    __shared__ double s_min[16][kIT];
+    __shared__ int s_nonfin[kIT];
     __shared__ int s_last;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int a0 = blockIdx.x * kTR, i0 = blockIdx.y * kTI;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int a0 = blockIdx.x * kRT, i0 = blockIdx.y * kIT;
+    const int n = ops.n_mom, B = ops.Bcap;
     const long long step = (long long)*reinterpret_cast<volatile unsigned long long*>(gstep);
-    const int B = ops.Bcap;
 
-    // phase 1: gain of the tile, lanes along rows (coalesced partial reads), 4 instances per warp
-    {
-        const int a = a0 + lane;
-        int s = 0;
-        if (a < ops.n_mom)
-            while (s + 1 < ops.n_species && a >= ops.sp_off[s + 1]) ++s;
-#pragma unroll
-        for (int q = 0; q < kTI / 8; ++q) {
-            const int il = warp * (kTI / 8) + q;
+    // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
+    if (ops.has_bin) {
+        const int r = tid & 63;
+        const int a = a0 + r;
+        const int s = a < n ? species_of_row(ops, a) : 0;
+        for (int q = 0; q < kIT / 4; ++q) {
+            const int il = (tid >> 6) + 4 * q;
             const int i = i0 + il;
             float g = 0.f;
-            if (a < ops.n_mom && i < B && ops.has_bin) {
+            if (a < n && i < B) {
                 for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
                     const int gi = ops.gain_grp[e];
-                    const int r = ops.gain_roff[e] + (a - ops.sp_off[s]);
-                    const float* P = ops.grp_partial[gi];
-                    const int M = ops.grp_M[gi], Bp = ops.grp_Bpad[gi];
-                    float acc = 0.f;
-                    for (int sp = 0; sp < ops.grp_splits[gi]; ++sp) acc += P[((size_t)sp * Bp + i) * M + r];
-                    g += acc * ops.grp_scale[gi][r] * ops.grp_sig1[gi][i] * ops.grp_sig2[gi][i];
+                    g += ops.grp_gsum[gi][(size_t)i * ops.grp_M[gi] + ops.gain_roff[e] + (a - ops.sp_off[s])];
                 }
             }
-            s_gain[lane][il] = g;
+            s_gain[r][il] = g;
+        }
+    }
+    if (tid < kIT) s_nonfin[tid] = 0;
+
+    float acc_l[4][4], acc_e[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc_l[k][j] = acc_e[k][j] = 0.f;
+
+    const bool fast = ops.tile_fast[blockIdx.x] != 0;
+    if (fast) {
+        const int s = species_of_row(ops, a0);
+        // tile product: acc[r][i] += sum_c T[a0 + r][c] * F[col0 + c][i0 + i]
+        auto tile_product = [&](auto load_T, int col0, int nc, float(&acc)[4][4]) {
+            for (int c0 = 0; c0 < nc; c0 += kCK) {
+                __syncthreads();
+                for (int q = 0; q < (kRT * kCK) / 256; ++q) {
+                    const int cc = tid & (kCK - 1), rr = (tid >> 5) + 8 * q;
+                    const int a = a0 + rr, c = c0 + cc;
+                    s_L[rr][cc] = (a < n && c < nc) ? load_T(a, c) : 0.f;
+                }
+                for (int q = 0; q < (kCK * kIT) / 256; ++q) {
+                    const int ii = tid & (kIT - 1), cc = (tid >> 6) + 4 * q;
+                    const int i = i0 + ii, c = c0 + cc;
+                    s_F[cc][ii] = (c < nc && i < B) ? F[(size_t)(col0 + c) * B + i] : 0.f;
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int cc = 0; cc < kCK; ++cc) {
+                    const float4 fv = *reinterpret_cast<const float4*>(&s_F[cc][tx * 4]);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float l = s_L[ty * 4 + k][cc];
+                        acc[k][0] += l * fv.x;
+                        acc[k][1] += l * fv.y;
+                        acc[k][2] += l * fv.z;
+                        acc[k][3] += l * fv.w;
+                    }
+                }
+            }
+        };
+        if (ops.has_bin) {
+            for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
+                const float* base = ops.loss_data + ops.loss_data_off[b];
+                const int ld = ops.loss_ld[b], off = ops.sp_off[s];
+                tile_product([&](int a, int c) { return base[(size_t)(a - off) * ld + c]; }, ops.loss_col_off[b],
+                             ops.loss_ncols[b], acc_l);
+            }
+        }
+        if (ops.has_emi && a0 < n) {
+            for (int p = ops.emi_rptr[a0]; p < ops.emi_rptr[a0 + 1]; ++p) {
+                const int pc = ops.emi_piece[p];
+                const __nv_bfloat162* base = ops.emi_data + ops.emi_data_off[pc];
+                const int ld = ops.emi_ld[pc], r0 = ops.emi_row0[pc];
+                const float* sc = ops.emi_scale + ops.emi_scale_off[pc];
+                tile_product(
+                    [&](int a, int c) {
+                        const float2 e2 = __bfloat1622float2(base[(size_t)(a - r0) * ld + c]);
+                        return (e2.x + e2.y) * sc[a - r0];
+                    },
+                    ops.emi_col0[pc], ops.emi_ncols[pc], acc_e);
+            }
         }
     }
     __syncthreads();
 
-    // phase 2: lanes along instances, 4 rows per warp
-    const int i = i0 + lane;
-    const bool inst_ok = i < B;
-    const bool active = inst_ok && step < ops.stop_step[i];
-    const double dts = inst_ok ? ops.dt_scale[i] : 0.0;
-    double rmin = CUDART_INF;
-    int nonfin = 0;
-    for (int rr = 0; rr < kTR / 8; ++rr) {
-        const int al = warp * (kTR / 8) + rr;
-        const int a = a0 + al;
-        if (a >= ops.n_mom || !inst_ok) continue;
-        const size_t idx = (size_t)a * B + i;
-        const float fa = F[idx];
-        const float ca = Cc[idx];
-        if (!active) {
-            Fo[idx] = fa;
-            Co[idx] = ca;
-            continue;
-        }
-        int s = 0;
-        while (s + 1 < ops.n_species && a >= ops.sp_off[s + 1]) ++s;
-        float flux = 0.f;
-        for (int k = 0; k < ops.ell_w; ++k) {
-            const int c = ops.ell_col[(size_t)a * ops.ell_w + k];
-            if (c >= 0) flux += ops.ell_val[(size_t)a * ops.ell_w + k] * F[(size_t)c * B + i];
-        }
-        float emi = 0.f;
-        if (ops.has_emi) {
-            for (int p = ops.emi_rptr[a]; p < ops.emi_rptr[a + 1]; ++p) {
-                const int pc = ops.emi_piece[p];
-                const __nv_bfloat162* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
-                const int col0 = ops.emi_col0[pc], nc = ops.emi_ncols[pc];
-                float acc = 0.f;
-                for (int c = 0; c < nc; ++c) {
-                    const float2 e2 = __bfloat1622float2(row[c]);
-                    acc += (e2.x + e2.y) * F[(size_t)(col0 + c) * B + i];
-                }
-                emi += acc * ops.emi_scale[ops.emi_scale_off[pc] + (a - ops.emi_row0[pc])];
-            }
-        }
-        float loss = 0.f;
-        if (ops.has_bin) {
-            const int la = a - ops.sp_off[s];
-            for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
-                const float* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
-                const int co = ops.loss_col_off[b], nc = ops.loss_ncols[b];
-                for (int c = 0; c < nc; ++c) loss += row[c] * F[(size_t)(co + c) * B + i];
-            }
-        }
-        const float gain = s_gain[al][lane];
-        // SteppingMethods.jl:31-46 in FP32, scale in FP64
-        float df = -flux;
-        if (ops.has_emi) df += emi;
-        if (ops.has_bin) df += ops.vol * (gain - fa * loss);
-        const double dfs = (double)df * ((double)ops.invAp[a] * dts);
-        // :97-101 with an FP64 compensated sum: the state is fa + ca
-        double t = ((double)fa + (double)ca) + (dfs + (double)ops.inj[a] * dts);
-        t = (t >= ops.thr) ? t : copysign(0.0, t);
-        t = (t != CUDART_INF) ? t : copysign(0.0, t);
-        const float fn = (float)t;
-        Fo[idx] = fn;
-        Co[idx] = (float)(t - (double)fn);
-        double ratio = dfs / (double)fa;
-        if (isnan(ratio)) ratio = CUDART_INF;
-        if (ratio < rmin || (ratio == rmin && signbit(ratio))) rmin = ratio;
-        if (!isfinite(dfs)) nonfin = 1;
+    // ---- update of the thread's 4 x 4 (row, instance) pairs
+    double rmin[4] = {CUDART_INF, CUDART_INF, CUDART_INF, CUDART_INF};
+    int nonfin[4] = {0, 0, 0, 0};
+    const int ib = i0 + tx * 4;
+    bool act[4];
+    double dts[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int i = ib + j;
+        act[j] = i < B && step < ops.stop_step[i];
+        dts[j] = i < B ? ops.dt_scale[i] : 0.0;
     }
-    if (active) {
-        atomicMin(&ops.min_ratio[i], ord_enc(rmin));
-        if (nonfin) atomicOr(&ops.nonfinite[i], 1);
+    for (int k = 0; k < 4; ++k) {
+        const int a = a0 + ty * 4 + k;
+        if (a >= n || ib >= B) continue;
+        const size_t idx = (size_t)a * B + ib;  // B and ib are multiples of 4
+        const float4 fa4 = *reinterpret_cast<const float4*>(F + idx);
+        const float4 ca4 = *reinterpret_cast<const float4*>(Cc + idx);
+        float flux[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int e = 0; e < ops.ell_w; ++e) {
+            const int col = ops.ell_col[(size_t)a * ops.ell_w + e];
+            if (col < 0) continue;
+            const float v = ops.ell_val[(size_t)a * ops.ell_w + e];
+            const float4 f4 = *reinterpret_cast<const float4*>(F + (size_t)col * B + ib);
+            flux[0] += v * f4.x;
+            flux[1] += v * f4.y;
+            flux[2] += v * f4.z;
+            flux[3] += v * f4.w;
+        }
+        const int s = species_of_row(ops, a);
+        const float fa[4] = {fa4.x, fa4.y, fa4.z, fa4.w};
+        const float ca[4] = {ca4.x, ca4.y, ca4.z, ca4.w};
+        float fo[4], co[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!act[j]) {
+                fo[j] = fa[j];
+                co[j] = ca[j];
+                continue;
+            }
+            float loss = acc_l[k][j], emi = acc_e[k][j];
+            if (!fast) row_terms_direct(ops, F, a, s, ib + j, loss, emi);
+            const float gain = ops.has_bin ? s_gain[ty * 4 + k][tx * 4 + j] : 0.f;
+            // SteppingMethods.jl:31-46 in FP32, the scaling in FP64
+            float df = -flux[j];
+            if (ops.has_emi) df += emi;
+            if (ops.has_bin) df += ops.vol * (gain - fa[j] * loss);
+            const double dfs = (double)df * ((double)ops.invAp[a] * dts[j]);
+            // :97-101 with an FP64 compensated sum: the state is fa + ca
+            double t = ((double)fa[j] + (double)ca[j]) + (dfs + (double)ops.inj[a] * dts[j]);
+            t = (t >= ops.thr) ? t : copysign(0.0, t);
+            t = (t != CUDART_INF) ? t : copysign(0.0, t);
+            fo[j] = (float)t;
+            co[j] = (float)(t - (double)fo[j]);
+            double ratio = dfs / (double)fa[j];
+            if (isnan(ratio)) ratio = CUDART_INF;
+            if (ratio < rmin[j] || (ratio == rmin[j] && signbit(ratio))) rmin[j] = ratio;
+            if (!isfinite(dfs)) nonfin[j] = 1;
+        }
+        *reinterpret_cast<float4*>(Fo + idx) = make_float4(fo[0], fo[1], fo[2], fo[3]);
+        *reinterpret_cast<float4*>(Co + idx) = make_float4(co[0], co[1], co[2], co[3]);
+    }
+    // ---- per-instance diagnostics over the tile's rows, then one atomic per instance
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        s_min[ty][tx * 4 + j] = rmin[j];
+        if (nonfin[j]) atomicOr(&s_nonfin[tx * 4 + j], 1);
+    }
+    __syncthreads();
+    if (tid < kIT) {
+        double m = CUDART_INF;
+        for (int y = 0; y < 16; ++y) {
+            const double v = s_min[y][tid];
+            if (v < m || (v == m && signbit(v))) m = v;
+        }
+        const int i = i0 + tid;
+        if (i < B && step < ops.stop_step[i]) {
+            atomicMin(&ops.min_ratio[i], ord_enc(m));
+            if (s_nonfin[tid]) atomicOr(&ops.nonfinite[i], 1);
+        }
     }
     // the last block to finish advances the global step counter
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         __threadfence();
         const unsigned total = gridDim.x * gridDim.y;
         const unsigned t = atomicAdd(ticket, 1u);
         s_last = (t == total - 1);
     }
     __syncthreads();
-    if (s_last && threadIdx.x == 0) {
+    if (s_last && tid == 0) {
         *ticket = 0u;
         __threadfence();
         *reinterpret_cast<volatile unsigned long long*>(gstep) = (unsigned long long)(step + 1);
@@ -573,11 +706,55 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
 
 }  // namespace
 
+// Per (slot, species) FP64 number sum(f) and energy sum(f * w) of the compensated state F + C
+// (DistributionMoments.jl:33,145,162); out[(slot * n_species + s) * 2 + {0, 1}].
+__global__ void batch_moments_kernel(const float* __restrict__ F, const float* __restrict__ C, int Bcap,
+                                     const int* __restrict__ sp_off, int n_species, const double* __restrict__ w,
+                                     double* __restrict__ out) {
+    __shared__ double s_n[128], s_e[128];
+    const int sp = blockIdx.x, slot = blockIdx.y;
+    double a = 0.0, e = 0.0;
+    for (int k = sp_off[sp] + threadIdx.x; k < sp_off[sp + 1]; k += blockDim.x) {
+        const double v = (double)F[(size_t)k * Bcap + slot] + (double)C[(size_t)k * Bcap + slot];
+        a += v;
+        e += v * w[k];
+    }
+    s_n[threadIdx.x] = a;
+    s_e[threadIdx.x] = e;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s_n[threadIdx.x] += s_n[threadIdx.x + o];
+            s_e[threadIdx.x] += s_e[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[((size_t)slot * n_species + sp) * 2 + 0] = s_n[0];
+        out[((size_t)slot * n_species + sp) * 2 + 1] = s_e[0];
+    }
+}
+
+cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
+                                 const double* w, double* out, cudaStream_t s) {
+    batch_moments_kernel<<<dim3(n_species, Bcap), 128, 0, s>>>(F, C, Bcap, sp_off, n_species, w, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
                               unsigned long long* gstep, unsigned* ticket, cudaStream_t s) {
-    dim3 grid((ops.n_mom + kTR - 1) / kTR, (ops.Bcap + kTI - 1) / kTI);
+    dim3 grid((ops.n_mom + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
     mixed_rows_kernel<<<grid, 256, 0, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
     return cudaGetLastError();
 }
+
+cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
+                                const float* sig1, const float* sig2, float* gsum, cudaStream_t s) {
+    dim3 grid((M + 255) / 256, Bcap);
+    split_reduce_kernel<<<grid, 256, 0, s>>>(partial, n_splits, Bpad, M, Bcap, row_scale, sig1, sig2, gsum);
+    return cudaGetLastError();
+}
+
+int mixed_rows_tile_rows() { return kRT; }
 
 }  // namespace dtb

@@ -1,0 +1,327 @@
+// Serving loop: continuous batching of solve requests over batched (DTB_MIXED) contexts.
+//
+// Each registered grid is one batched context with its own stream. A library-owned host
+// thread repeatedly (1) admits queued requests into free slots of their grid, (2) launches a
+// chunk of batched steps on every grid that has running slots (the chunks of different grids
+// run concurrently on their streams), (3) waits for the chunks, reads back the f of every slot
+// whose steps are done and frees the slot. Requests that arrive meanwhile join at the next
+// admission point, so work of different requests and grids overlaps on the device. Device
+// memory of all grids is checked against an HBM budget when a grid is registered.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "ctx.h"
+
+// batch_api.cpp internals
+int batch_launch(dtb_ctx* c, int64_t nsteps);
+int batch_finish(dtb_ctx* c);
+int batch_capacity(dtb_ctx* c);
+long long batch_step(dtb_ctx* c);
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+struct Request {
+    int64_t id = 0;
+    int grid = 0;
+    std::vector<double> f;  // f0 on submission, the result when done
+    double dt_scale = 1.0;
+    int64_t n_steps = 0;
+    int state = 0;          // 0 queued, 1 running, 2 done, 3 failed
+    int slot = -1;
+    long long stop = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    double cr_max = 0;
+    int finite = 1;
+};
+
+struct Grid {
+    dtb_ctx* ctx = nullptr;
+    int capacity = 0;
+    std::vector<int64_t> slot_req;  // request id per slot, -1 when free
+    std::deque<int64_t> queue;
+    double ema_step_ms = 0.1;
+    int n_running = 0;
+};
+
+}  // namespace
+
+struct dtb_server {
+    dtb_serve_opts opts{};
+    std::vector<Grid> grids;
+    std::map<int64_t, Request> req;
+    int64_t next_id = 1;
+    int64_t bytes = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread th;
+    bool running = false, stop = false;
+    int error = DTB_OK;
+    std::string error_msg;
+    clk::time_point t0 = clk::now();
+    // statistics
+    int64_t steps_done = 0;      // instance-steps completed
+    int64_t batched_steps = 0;   // batched steps launched, summed over grids
+    int64_t completed = 0;
+    double busy_s = 0;
+
+    double now() const { return std::chrono::duration<double>(clk::now() - t0).count(); }
+};
+
+namespace {
+
+void fail(dtb_server* s, int rc) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->error = rc;
+    s->error_msg = dtb_last_error();
+    s->stop = true;
+    for (auto& kv : s->req)
+        if (kv.second.state < 2) kv.second.state = 3;
+    s->cv_done.notify_all();
+}
+
+void loop(dtb_server* s) {
+    const int max_chunk = s->opts.max_chunk_steps > 0 ? s->opts.max_chunk_steps : 256;
+    const double target_ms = s->opts.chunk_ms > 0 ? s->opts.chunk_ms : 20.0;
+    while (true) {
+        std::vector<std::pair<int, std::vector<std::pair<int, Request*>>>> admits;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            bool any = false;
+            for (auto& g : s->grids) any = any || g.n_running > 0 || !g.queue.empty();
+            if (!any && !s->stop) s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            if (s->stop) return;
+            // (1) admission: queued requests into free slots
+            for (size_t gi = 0; gi < s->grids.size(); ++gi) {
+                Grid& g = s->grids[gi];
+                std::vector<std::pair<int, Request*>> a;
+                for (int sl = 0; sl < g.capacity && !g.queue.empty(); ++sl) {
+                    if (g.slot_req[(size_t)sl] >= 0) continue;
+                    const int64_t id = g.queue.front();
+                    g.queue.pop_front();
+                    Request& r = s->req[id];
+                    r.slot = sl;
+                    r.state = 1;
+                    g.slot_req[(size_t)sl] = id;
+                    g.n_running++;
+                    a.push_back({sl, &r});
+                }
+                if (!a.empty()) admits.push_back({(int)gi, std::move(a)});
+            }
+        }
+        // admission uploads outside the lock (requests stay valid: the map only grows, entries
+        // are erased by nobody while the server runs)
+        for (auto& ga : admits) {
+            Grid& g = s->grids[(size_t)ga.first];
+            for (auto& sr : ga.second) {
+                Request& r = *sr.second;
+                int rc = dtb_batch_admit(g.ctx, sr.first, r.f.data(), r.dt_scale, r.n_steps);
+                if (rc != DTB_OK) return fail(s, rc);
+                r.t_admit = s->now();
+                r.stop = batch_step(g.ctx) + r.n_steps;
+            }
+        }
+        // (2) a chunk of batched steps on every grid with running slots
+        std::vector<int> launched;
+        std::vector<int64_t> chunks;
+        const double t_start = s->now();
+        for (size_t gi = 0; gi < s->grids.size(); ++gi) {
+            Grid& g = s->grids[gi];
+            if (g.n_running == 0) continue;
+            long long left = (long long)1 << 60;
+            const long long st = batch_step(g.ctx);
+            for (int sl = 0; sl < g.capacity; ++sl) {
+                const int64_t id = g.slot_req[(size_t)sl];
+                if (id >= 0) left = std::min(left, s->req[id].stop - st);
+            }
+            const int cap = std::max(1, std::min(max_chunk, (int)(target_ms / std::max(1e-3, g.ema_step_ms))));
+            const int64_t chunk = std::max<long long>(1, std::min<long long>(left, cap));
+            int rc = batch_launch(g.ctx, chunk);
+            if (rc != DTB_OK) return fail(s, rc);
+            launched.push_back((int)gi);
+            chunks.push_back(chunk);
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->batched_steps += chunk;
+        }
+        // (3) completions
+        for (size_t li = 0; li < launched.size(); ++li) {
+            Grid& g = s->grids[(size_t)launched[li]];
+            int rc = batch_finish(g.ctx);
+            if (rc != DTB_OK) return fail(s, rc);
+            const double t_end = s->now();
+            // device time per batched step of this grid (an upper bound while grids overlap)
+            g.ema_step_ms = 0.7 * g.ema_step_ms + 0.3 * (1e3 * (t_end - t_start) / (double)chunks[li]);
+            const long long st = batch_step(g.ctx);
+            for (int sl = 0; sl < g.capacity; ++sl) {
+                const int64_t id = g.slot_req[(size_t)sl];
+                if (id < 0) continue;
+                Request* r;
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    r = &s->req[id];
+                }
+                if (st < r->stop) continue;
+                int64_t done = 0, left = 0;
+                double cr = 0;
+                int32_t fin = 1;
+                rc = dtb_batch_get_f(g.ctx, sl, r->f.data());
+                if (rc == DTB_OK) rc = dtb_batch_slot_info(g.ctx, sl, &done, &left, &cr, &fin);
+                if (rc == DTB_OK) rc = dtb_batch_release(g.ctx, sl);
+                if (rc != DTB_OK) return fail(s, rc);
+                std::lock_guard<std::mutex> lk(s->mu);
+                r->cr_max = cr;
+                r->finite = fin;
+                r->t_done = s->now();
+                r->state = 2;
+                g.slot_req[(size_t)sl] = -1;
+                g.n_running--;
+                s->steps_done += r->n_steps;
+                s->completed++;
+                (void)t_end;
+            }
+            s->cv_done.notify_all();
+        }
+        if (!launched.empty()) {
+            const double dt = s->now() - t_start;
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->busy_s += dt;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t dtb_serve_create(const dtb_serve_opts* opts, dtb_server** out) {
+    DTB_CHECK(out, DTB_EINVAL, "dtb_serve_create: null output");
+    auto* s = new dtb_server();
+    if (opts) s->opts = *opts;
+    *out = s;
+    return DTB_OK;
+}
+
+int32_t dtb_serve_add_grid(dtb_server* s, dtb_ctx* ctx, int32_t* grid_id) {
+    DTB_CHECK(s && ctx && grid_id, DTB_EINVAL, "dtb_serve_add_grid: null argument");
+    DTB_CHECK(!s->running, DTB_ESTATE, "dtb_serve_add_grid: register grids before dtb_serve_start");
+    DTB_CHECK(ctx->prec == DTB_MIXED, DTB_EINVAL, "dtb_serve_add_grid: the context must be batched (DTB_MIXED)");
+    DTB_TRY(dtb_commit(ctx));
+    int64_t b = 0;
+    DTB_TRY(dtb_device_bytes(ctx, &b));
+    if (s->opts.hbm_budget_bytes > 0 && s->bytes + b > s->opts.hbm_budget_bytes) {
+        set_error("dtb_serve_add_grid: the grid needs " + std::to_string(b) + " device bytes; " +
+                  std::to_string(s->opts.hbm_budget_bytes - s->bytes) + " of the HBM budget are left");
+        return DTB_ENOMEM;
+    }
+    s->bytes += b;
+    Grid g;
+    g.ctx = ctx;
+    g.capacity = batch_capacity(ctx);
+    g.slot_req.assign((size_t)g.capacity, -1);
+    s->grids.push_back(std::move(g));
+    *grid_id = (int32_t)s->grids.size() - 1;
+    return DTB_OK;
+}
+
+int32_t dtb_serve_start(dtb_server* s) {
+    DTB_CHECK(s, DTB_EINVAL, "dtb_serve_start: null server");
+    DTB_CHECK(!s->running, DTB_ESTATE, "dtb_serve_start: already running");
+    DTB_CHECK(!s->grids.empty(), DTB_ESTATE, "dtb_serve_start: no grid registered");
+    s->t0 = clk::now();
+    s->running = true;
+    s->th = std::thread(loop, s);
+    return DTB_OK;
+}
+
+int32_t dtb_serve_submit(dtb_server* s, int32_t grid_id, const double* f0, double dt_scale, int64_t n_steps,
+                         int64_t* request_id) {
+    DTB_CHECK(s && f0 && request_id, DTB_EINVAL, "dtb_serve_submit: null argument");
+    DTB_CHECK(grid_id >= 0 && grid_id < (int32_t)s->grids.size(), DTB_ENOTFOUND, "dtb_serve_submit: unknown grid");
+    DTB_CHECK(n_steps >= 1 && std::isfinite(dt_scale), DTB_EINVAL, "dtb_serve_submit: bad step count or dt");
+    Grid& g = s->grids[(size_t)grid_id];
+    const int64_t n = g.ctx->n_mom;
+    std::lock_guard<std::mutex> lk(s->mu);
+    DTB_CHECK(s->error == DTB_OK, s->error, "dtb_serve_submit: the server stopped after an error: " + s->error_msg);
+    Request r;
+    r.id = s->next_id++;
+    r.grid = grid_id;
+    r.f.assign(f0, f0 + n);
+    r.dt_scale = dt_scale;
+    r.n_steps = n_steps;
+    r.t_submit = s->now();
+    *request_id = r.id;
+    g.queue.push_back(r.id);
+    s->req.emplace(r.id, std::move(r));
+    s->cv_work.notify_all();
+    return DTB_OK;
+}
+
+int32_t dtb_serve_wait(dtb_server* s, int64_t request_id, double timeout_s, double* f_out, dtb_request_stats* st) {
+    DTB_CHECK(s, DTB_EINVAL, "dtb_serve_wait: null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->req.find(request_id);
+    DTB_CHECK(it != s->req.end(), DTB_ENOTFOUND, "dtb_serve_wait: unknown request");
+    const auto deadline = clk::now() + std::chrono::duration<double>(timeout_s > 0 ? timeout_s : 1e9);
+    while (it->second.state < 2) {
+        if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && it->second.state < 2) {
+            set_error("dtb_serve_wait: request " + std::to_string(request_id) + " not done within the timeout");
+            return DTB_ETIMEOUT;
+        }
+    }
+    Request& r = it->second;
+    if (r.state == 3) {
+        set_error("dtb_serve_wait: the server stopped after an error: " + s->error_msg);
+        return s->error != DTB_OK ? s->error : DTB_ECUDA;
+    }
+    if (f_out) std::copy(r.f.begin(), r.f.end(), f_out);
+    if (st) {
+        st->t_submit = r.t_submit;
+        st->t_admit = r.t_admit;
+        st->t_done = r.t_done;
+        st->steps = r.n_steps;
+        st->cr_max = r.cr_max;
+        st->finite = r.finite;
+        st->grid = r.grid;
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_serve_get_stats(dtb_server* s, dtb_serve_stats* st) {
+    DTB_CHECK(s && st, DTB_EINVAL, "dtb_serve_get_stats: null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    st->completed = s->completed;
+    st->instance_steps = s->steps_done;
+    st->batched_steps = s->batched_steps;
+    st->busy_s = s->busy_s;
+    st->elapsed_s = s->now();
+    int64_t q = 0, r = 0;
+    for (auto& g : s->grids) {
+        q += (int64_t)g.queue.size();
+        r += g.n_running;
+    }
+    st->queued = q;
+    st->running = r;
+    st->device_bytes = s->bytes;
+    return s->error;
+}
+
+int32_t dtb_serve_destroy(dtb_server* s) {
+    if (!s) return DTB_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->th.joinable()) s->th.join();
+    delete s;
+    return DTB_OK;
+}
+
+}  // extern "C"

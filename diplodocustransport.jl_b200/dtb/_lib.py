@@ -38,6 +38,23 @@ class Opts(ctypes.Structure):
                 ("batch", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
+class ServeOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("max_chunk_steps", ctypes.c_int32), ("flags", ctypes.c_int32),
+                ("chunk_ms", ctypes.c_double)]
+
+
+class RequestStats(ctypes.Structure):
+    _fields_ = [("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("steps", ctypes.c_int64), ("cr_max", ctypes.c_double), ("finite", ctypes.c_int32),
+                ("grid", ctypes.c_int32)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("instance_steps", ctypes.c_int64), ("batched_steps", ctypes.c_int64),
+                ("queued", ctypes.c_int64), ("running", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+                ("busy_s", ctypes.c_double), ("elapsed_s", ctypes.c_double)]
+
+
 class StepDiag(ctypes.Structure):
     _fields_ = [("cr", ctypes.c_double), ("cr_bin", ctypes.c_double), ("cr_emi", ctypes.c_double),
                 ("cr_flux", ctypes.c_double), ("sum_df", ctypes.c_double), ("sum_f", ctypes.c_double),
@@ -89,6 +106,14 @@ SIGNATURES = {
     "dtb_batch_release": (_i32, [_P, _i32]),
     "dtb_batch_set_f_all": (_i32, [_P, _dp]),
     "dtb_batch_get_f_all": (_i32, [_P, _dp]),
+    "dtb_batch_moments": (_i32, [_P, _dp, _dp, _dp]),
+    "dtb_serve_create": (_i32, [ctypes.POINTER(ServeOpts), ctypes.POINTER(_P)]),
+    "dtb_serve_add_grid": (_i32, [_P, _P, _i32p]),
+    "dtb_serve_start": (_i32, [_P]),
+    "dtb_serve_submit": (_i32, [_P, _i32, _dp, _d, _i64, _ip]),
+    "dtb_serve_wait": (_i32, [_P, _i64, _d, _dp, ctypes.POINTER(RequestStats)]),
+    "dtb_serve_get_stats": (_i32, [_P, ctypes.POINTER(ServeStats)]),
+    "dtb_serve_destroy": (_i32, [_P]),
     "dtb_batch_capacity": (_i32, [_P, _i32p, _ip]),
     "dtb_batch_set_profiling": (_i32, [_P, _i32]),
     "dtb_batch_gemm_stats": (_i32, [_P, _dp, _dp, _dp, _i32p]),

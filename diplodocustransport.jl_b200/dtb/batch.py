@@ -96,6 +96,15 @@ class BatchedEuler:
         check(self.L.dtb_batch_get_f_all(self.ctx, dptr(out)))
         return out
 
+    def moments(self, weights) -> tuple:
+        """FP64 number and energy per (slot, species) on the device."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        ns = len(self.PhaseSpace.species_sizes)
+        num = np.zeros((self.capacity, ns))
+        en = np.zeros_like(num)
+        check(self.L.dtb_batch_moments(self.ctx, dptr(w), dptr(num), dptr(en)))
+        return num, en
+
     def info(self, slot: int) -> dict:
         done, left = ctypes.c_int64(), ctypes.c_int64()
         cr = ctypes.c_double()

@@ -266,17 +266,16 @@ def synchrotron_like(ps: PhaseSpace, emitter: int, photon: int, B: float, kappa:
     return E
 
 
-def config3(seed: int = 3, batch: int = 64, gain_on_device: bool = True, device: str = "cuda") -> Workload:
-    """Mixed precision, three interactions: electrons, positrons, photons on 48 log p bins over
-    1e-3..1e3 x 12 u bins (576 states per species); e- + gamma and e+ + gamma Compton-like
-    gain/loss and gamma + gamma -> e+ e- pair gain/loss, each gain tensor 576 x 331,776 with
-    values log-uniform over 1e-8..1; synchrotron-like emission of e-/e+ into photons from a
-    uniform B of seeded magnitude; `batch` instances, 5000 steps."""
-    ps = phase_space(["Ele", "Pos", "Pho"], 48, 1e-3, 1e3, 12, [1.0, 1.0, 0.0])
+def three_species(p_num: int, p_lo: float, p_hi: float, u_num: int, batch: int, seed: int,
+                  gain_on_device: bool = False, device: str = "cuda", g_range=(-8.0, 0.0)) -> Workload:
+    """Electrons, positrons, photons with e- + gamma and e+ + gamma Compton-like gain/loss and
+    gamma + gamma -> e+ e- pair gain/loss; synchrotron-like emission of e-/e+ into photons from a
+    uniform B of seeded magnitude; `batch` instances with log-normal f0 and dt in [0.5, 1]."""
+    ps = phase_space(["Ele", "Pos", "Pho"], p_num, p_lo, p_hi, u_num, [1.0, 1.0, 0.0])
     rng = np.random.default_rng(seed)
     fluxm = upwind_flux(ps, rng, 1.0)
     ns = ps.species_sizes[0]
-    lo, hi = -8.0, 0.0
+    lo, hi = g_range
     kg = gain_kappa(lo, hi, ns, 1.0)
     blocks = [(0, 0, 2), (2, 0, 2), (1, 1, 2), (2, 1, 2), (0, 2, 2), (1, 2, 2)]
     gains = []
@@ -287,8 +286,8 @@ def config3(seed: int = 3, batch: int = 64, gain_on_device: bool = True, device:
             G = _log_uniform(rng, (ns, ns, ns), lo, hi) * kg
         gains.append(GainBlock(o, a, b, G))
     kl = loss_kappa(lo, hi, 1.0)
-    losses = [LossBlock(s, o, _log_uniform(rng, (ns, ns), lo, hi) * kl)
-              for s, o in ((0, 2), (2, 0), (1, 2), (2, 1), (2, 2))]
+    losses = [LossBlock(s_, o, _log_uniform(rng, (ns, ns), lo, hi) * kl)
+              for s_, o in ((0, 2), (2, 0), (1, 2), (2, 1), (2, 2))]
     Bmag = float(10.0 ** rng.uniform(-1.0, 1.0))
     emim = EmissionMatrices()
     for em in (0, 1):
@@ -300,5 +299,14 @@ def config3(seed: int = 3, batch: int = 64, gain_on_device: bool = True, device:
     f0 = np.stack([lognormal_f0(ps, [mu, mu, mu], 1.0) for mu in mus])
     dts = rng2.uniform(0.5, 1.0, size=batch)
     return Workload(ps=ps, binm=BinaryMatrices(gains=gains, losses=losses), emim=emim, fluxm=fluxm, f0=f0,
-                    inj=np.zeros(ps.n_state), dt=dts, n_steps=5000,
+                    inj=np.zeros(ps.n_state), dt=dts, n_steps=0,
                     meta=dict(seed=seed, kappa_gain=kg, kappa_loss=kl, B=Bmag, mu=mus))
+
+
+def config3(seed: int = 3, batch: int = 64, gain_on_device: bool = True, device: str = "cuda") -> Workload:
+    """Mixed precision, three interactions: electrons, positrons, photons on 48 log p bins over
+    1e-3..1e3 x 12 u bins (576 states per species), each gain tensor 576 x 331,776 with values
+    log-uniform over 1e-8..1; 64 instances, 5000 steps."""
+    w = three_species(48, 1e-3, 1e3, 12, batch, seed, gain_on_device=gain_on_device, device=device)
+    w.n_steps = 5000
+    return w

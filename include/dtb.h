@@ -203,6 +203,11 @@ int32_t dtb_batch_slot_info(dtb_ctx* ctx, int32_t slot, int64_t* steps_done, int
 int32_t dtb_batch_set_f_all(dtb_ctx* ctx, const double* f);
 int32_t dtb_batch_get_f_all(dtb_ctx* ctx, double* f);
 
+/* FP64 number sum(f) and energy sum(f * w) of every slot and species, on the device
+ * (DistributionMoments.jl:33,145,162); w is the per-state energy weight (n_mom). Outputs are
+ * batch x n_species, slot-major. */
+int32_t dtb_batch_moments(dtb_ctx* ctx, const double* w, double* number, double* energy);
+
 /* Stops a slot (it no longer steps). */
 int32_t dtb_batch_release(dtb_ctx* ctx, int32_t slot);
 
@@ -216,6 +221,51 @@ int32_t dtb_batch_set_profiling(dtb_ctx* ctx, int32_t on);
  * and operator bytes per step, and the kernel launches per batched step. */
 int32_t dtb_batch_gemm_stats(dtb_ctx* ctx, double* avg_ms, double* flops_per_step, double* bytes_per_step,
                              int32_t* launches_per_step);
+
+/* ---- serving: continuous batching of solve requests ----
+ * A server owns a host thread that admits queued requests into free slots of their grid's
+ * batched context, launches chunks of batched steps on every grid with running requests (the
+ * grids' chunks overlap on the device, each on its context's stream), reads back finished
+ * requests and frees their slots. Requests of one grid share the operators; requests that
+ * arrive while others run join at the next admission point. */
+typedef struct dtb_server dtb_server;
+
+typedef struct dtb_serve_opts {
+    int64_t hbm_budget_bytes;  /* device bytes all registered grids may hold (0: no limit) */
+    int32_t max_chunk_steps;   /* most batched steps between admission points (0: 256) */
+    int32_t flags;             /* reserved, 0 */
+    double chunk_ms;           /* target device time of one chunk of a grid (0: 20 ms) */
+} dtb_serve_opts;
+
+typedef struct dtb_request_stats {
+    double t_submit, t_admit, t_done;  /* seconds since dtb_serve_start */
+    int64_t steps;
+    double cr_max;                     /* largest Cr seen over the request's steps */
+    int32_t finite;                    /* every df was finite */
+    int32_t grid;
+} dtb_request_stats;
+
+typedef struct dtb_serve_stats {
+    int64_t completed, instance_steps, batched_steps, queued, running, device_bytes;
+    double busy_s, elapsed_s;
+} dtb_serve_stats;
+
+int32_t dtb_serve_create(const dtb_serve_opts* opts, dtb_server** out);
+/* Registers a committed batched context as a grid (its device bytes count against the HBM
+ * budget: DTB_ENOMEM when they do not fit). The server drives the context from its thread; the
+ * caller must not use it directly until dtb_serve_destroy, and destroys it afterwards. */
+int32_t dtb_serve_add_grid(dtb_server* srv, dtb_ctx* batched_ctx, int32_t* grid_id);
+int32_t dtb_serve_start(dtb_server* srv);
+/* Queues a solve (f0 copied; dt_scale = dt/dt0; n_steps steps). Thread-safe. */
+int32_t dtb_serve_submit(dtb_server* srv, int32_t grid_id, const double* f0, double dt_scale, int64_t n_steps,
+                         int64_t* request_id);
+/* Waits for a request (timeout in seconds, <= 0: no limit; DTB_ETIMEOUT when it runs out) and
+ * copies its final f and timings. */
+int32_t dtb_serve_wait(dtb_server* srv, int64_t request_id, double timeout_s, double* f_out,
+                       dtb_request_stats* stats);
+int32_t dtb_serve_get_stats(dtb_server* srv, dtb_serve_stats* stats);
+/* Stops the loop thread (running requests are abandoned) and frees the server. */
+int32_t dtb_serve_destroy(dtb_server* srv);
 
 /* ---- kernel-level entry ---- */
 

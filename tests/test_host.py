@@ -129,3 +129,19 @@ def test_synthetic_config0_shapes():
     assert w.f0[:128].sum() == pytest.approx(1.0) and w.f0[128:].sum() == pytest.approx(1.0)
     g = np.asarray(w.binm.gains[0].G) / w.meta["kappa_gain"]
     assert g.min() >= 1e-6 and g.max() <= 1.0
+
+
+def test_server_host_errors_without_a_device():
+    """Server errors that need no GPU: starting without grids, unknown grids and requests."""
+    import ctypes
+    L = _lib.load()
+    srv = ctypes.c_void_p()
+    opts = _lib.ServeOpts(hbm_budget_bytes=0, max_chunk_steps=0, flags=0, chunk_ms=0.0)
+    assert L.dtb_serve_create(ctypes.byref(opts), ctypes.byref(srv)) == _lib.DTB_OK
+    assert L.dtb_serve_start(srv) == _lib.DTB_ESTATE
+    f = np.zeros(4)
+    rid = ctypes.c_int64()
+    assert L.dtb_serve_submit(srv, 0, _lib.dptr(f), 1.0, 10, ctypes.byref(rid)) == _lib.DTB_ENOTFOUND
+    st = _lib.RequestStats()
+    assert L.dtb_serve_wait(srv, 7, 0.01, None, ctypes.byref(st)) == _lib.DTB_ENOTFOUND
+    assert L.dtb_serve_destroy(srv) == _lib.DTB_OK
