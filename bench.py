@@ -521,6 +521,109 @@ def run_batched(args):
     return 0
 
 
+SERVE_GRIDS = [(16, 8), (32, 8), (32, 16), (64, 16)]
+
+
+def run_serving(args):
+    """Config 4: a Poisson stream of solve requests over four grids, served with continuous
+    batching; p50/p99 time-to-solution and aggregate instance-steps/s, beside the same stream
+    one at a time on the plain FP64 path (FIFO single server with per-grid FP64 step times
+    measured here)."""
+    import numpy as np
+    import torch
+    from dtb import synth
+    from dtb.batch import BatchedEuler
+    from dtb.serve import Server
+    from dtb.stepping import ForwardEulerStruct
+    from dtb.structs import BinaryMatrices
+    rank, local, world = _env_rank()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(44)
+    n_req = args.requests
+    rate = args.rate
+    grids, batched, step_ms_fp64 = [], [], []
+    srv = Server(hbm_budget_bytes=150 * 10**9)
+    gids = []
+    for g, (p, u) in enumerate(SERVE_GRIDS):
+        w = synth.two_species(p, 1e-2, 1e2, u, seed=100 + g, gain_on_device=True, device=f"cuda:{local}")
+        b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, args.capacity, device=local)
+        gids.append(srv.add_grid(b))
+        # plain FP64 step time of this grid (one instance), for the one-at-a-time comparison
+        gains64 = [type(x)(x.out_sp, x.in1_sp, x.in2_sp, x.G.double()) for x in w.binm.gains]
+        ps_stream = torch.cuda.Stream()
+        pl = ForwardEulerStruct(w.ps, w.f0, w.inj, BinaryMatrices(gains=gains64, losses=w.binm.losses), w.emim,
+                                w.fluxm, Precision=np.float64, device=local, stream=ps_stream.cuda_stream)
+        del gains64
+        pl.run(np.ones(8))
+        K = 200 if p * u <= 256 else 50
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(ps_stream)
+        pl.run(np.ones(K))
+        t1.record(ps_stream)
+        torch.cuda.synchronize()
+        step_ms_fp64.append(t0.elapsed_time(t1) / K)
+        pl.close()
+        w.binm.gains = []
+        torch.cuda.empty_cache()
+        grids.append(w)
+        batched.append(b)
+    # the request stream
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    gsel = rng.integers(0, len(SERVE_GRIDS), size=n_req)
+    steps = rng.integers(500, 20001, size=n_req)
+    mus = rng.uniform(-1, 1, size=n_req)
+    dts = rng.uniform(0.5, 1.0, size=n_req)
+    f0s = [synth.lognormal_f0(grids[g].ps, [mu, mu], 1.0) for g, mu in zip(gsel, mus)]
+    srv.start()
+    t_start = time.perf_counter()
+    rids = []
+    for k in range(n_req):
+        delay = arrivals[k] - (time.perf_counter() - t_start)
+        if delay > 0:
+            time.sleep(delay)
+        rids.append(srv.submit(gids[gsel[k]], f0s[k], float(dts[k]), int(steps[k])))
+    infos = [srv.wait(r, timeout_s=3600, with_f=False)[1] for r in rids]
+    st = srv.stats()
+    srv.close()
+    for b in batched:
+        b.close()
+    tts = np.array([i["t_done"] - i["t_submit"] for i in infos])
+    t_first = min(i["t_submit"] for i in infos)
+    t_last = max(i["t_done"] for i in infos)
+    total = int(steps.sum())
+    agg = total / (t_last - t_first)
+    # one at a time on the plain FP64 path: FIFO single server over the same arrivals
+    svc = np.array([steps[k] * step_ms_fp64[gsel[k]] / 1e3 for k in range(n_req)])
+    free_at, tts_plain, done_plain = 0.0, [], []
+    for k in range(n_req):
+        start = max(free_at, arrivals[k])
+        free_at = start + svc[k]
+        tts_plain.append(free_at - arrivals[k])
+    agg_plain = total / (free_at - arrivals[0])
+    line = {"metric": METRIC, "value": agg, "unit": "instance-steps/s", "n_gpus": 1, "steps": total,
+            "warmup": 0, "ms_per_step": 1e3 / agg, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3 (gain GEMM), f32 state, f64 update",
+            "data": "synthetic (seeded Poisson stream, seeded operators and spectra)",
+            "config": {"workload": f"serving (config 4): {n_req} requests, Poisson rate {rate}/s, grids "
+                                   "p16xu8, p32xu8, p32xu16, p64xu16 (2 species), 500-20000 steps each",
+                       "capacity_per_grid": args.capacity, "hbm_budget_bytes": 150 * 10**9,
+                       "device_bytes": st["device_bytes"]},
+            "tts_p50_s": float(np.percentile(tts, 50)), "tts_p99_s": float(np.percentile(tts, 99)),
+            "plain_fp64_one_at_a_time": {"value": agg_plain, "unit": "instance-steps/s",
+                                         "tts_p50_s": float(np.percentile(tts_plain, 50)),
+                                         "tts_p99_s": float(np.percentile(tts_plain, 99)),
+                                         "step_ms_per_grid": step_ms_fp64,
+                                         "method": "FIFO single server over the same arrivals, service time = "
+                                                   "steps x FP64 step time measured per grid"},
+            "speedup_vs_plain_fp64": agg / agg_plain,
+            "serve_stats": st}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -531,12 +634,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="p_bins x u_bins override of the config-1 grid, e.g. 32x16")
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 accuracy check of the batched run")
+    ap.add_argument("--requests", type=int, default=2000, help="serving stream length (--config 4)")
+    ap.add_argument("--rate", type=float, default=20.0, help="mean request arrival rate per second (--config 4)")
+    ap.add_argument("--capacity", type=int, default=256, help="slots per grid (--config 4)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
     if args.config in (2, 3):
         return run_batched(args)
+    if args.config == 4:
+        return run_serving(args)
     return run_ours(args)
 
 

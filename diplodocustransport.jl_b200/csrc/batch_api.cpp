@@ -497,7 +497,8 @@ int mixed_step(dtb_ctx* c, bool profile) {
         a.n_splits = G.n_splits;
         a.m_tiles = G.m_tiles;
         a.n_tiles = G.n_tiles;
-        a.Bcap = m->Bcap;
+        a.Bcap = m->Buser;
+        a.Bst = m->Bcap;
         a.Bpad = G.Bpad;
         a.F = Fin;
         a.isig1 = m->isig + (size_t)G.in1 * m->Bcap;

@@ -23,10 +23,11 @@ struct GemmArgs {
     int n_cb;       // 64-wide blocks of input species 2 (n2 padded to 64)
     int off1, off2; // state offsets of the two input species
     int tiles_per_split, n_splits, m_tiles, n_tiles;
-    int Bcap;       // instance stride of the state matrix F[n][Bcap]
+    int Bcap;       // instances that exist (columns >= Bcap are zero in X)
+    int Bst;        // row stride of the state matrix F[n][Bst]
     int Bpad;       // n_tiles * BN, instance stride of the partial rows
     const float* F;
-    const float* isig1;  // [Bcap] reciprocal power-of-two scale of species in1 per instance
+    const float* isig1;  // [Bst] reciprocal power-of-two scale of species in1 per instance
     const float* isig2;
     float* partial;      // [n_splits][Bpad][M]
     int* err;

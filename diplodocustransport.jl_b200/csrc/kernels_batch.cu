@@ -243,9 +243,22 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             const float s2 = valid ? a.isig2[inst] : 0.f;
             float f2r[kMmaK];
             int cur_cb = -1;
+            // f1[b] of the next tile is loaded one tile ahead so its latency hides behind the
+            // current tile's conversion
+            float x1_next = 0.f;
+            if (valid) {
+                const int b0 = t0 - (t0 / a.N1) * a.N1;
+                x1_next = __ldg(a.F + (size_t)(a.off1 + b0) * a.Bst + inst);
+            }
             for (int j = 0; j < nt; ++j) {
                 const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
                 const int sb = j % C::SB;
+                const float x1 = x1_next * s1;
+                if (valid && j + 1 < nt) {
+                    const int tn = t + 1, bn = tn - (tn / a.N1) * a.N1;
+                    x1_next = __ldg(a.F + (size_t)(a.off1 + bn) * a.Bst + inst);
+                }
+                (void)b;
                 if (!mb_wait(smem_addr(&empty_b[sb]), ((j / C::SB) & 1u) ^ 1u, abort_flag)) {
                     if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_EMPTY);
                     *abort_flag = 1;
@@ -255,11 +268,10 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
 #pragma unroll
                     for (int c = 0; c < kMmaK; ++c) {
                         const int cc = cb * kMmaK + c;
-                        f2r[c] = (valid && cc < a.n2) ? a.F[(size_t)(a.off2 + cc) * a.Bcap + inst] * s2 : 0.f;
+                        f2r[c] = (valid && cc < a.n2) ? __ldg(a.F + (size_t)(a.off2 + cc) * a.Bst + inst) * s2 : 0.f;
                     }
                     cur_cb = cb;
                 }
-                const float x1 = valid ? a.F[(size_t)(a.off1 + b) * a.Bcap + inst] * s1 : 0.f;
                 unsigned char* rhi = b_base + (size_t)(sb * 2) * C::B_BYTES + (size_t)p * 128;
                 unsigned char* rlo = b_base + (size_t)(sb * 2 + 1) * C::B_BYTES + (size_t)p * 128;
 #pragma unroll
@@ -443,8 +455,8 @@ __device__ __forceinline__ unsigned long long ord_enc(double x) {
     return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
 
-constexpr int kRT = 64;  // rows per tile
-constexpr int kIT = 64;  // instances per tile
+constexpr int kRT = 32;  // rows per tile
+constexpr int kIT = 32;  // instances per tile
 constexpr int kCK = 32;  // K chunk of the loss / emission tile products
 
 // Sum of the split-K partial tiles of one gain group, scaled back to G and f units:
@@ -506,16 +518,17 @@ __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict
     }
 }
 
-// One 64-row x 64-instance tile per block, 256 threads, a 4 x 4 (row x instance) micro-tile
-// per thread. Loss and emission are tile products through shared memory when the tile's rows
-// belong to one species and every emission piece touching them covers them all (tile_fast).
+// One 32-row x 32-instance tile per block, 256 threads, a 2 x 2 (row x instance) micro-tile per
+// thread. Loss and emission are tile products through double-buffered shared memory when the
+// tile's rows belong to one species and every emission piece touching them covers them all
+// (tile_fast); other tiles take direct loads.
 __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
                                                          const float* __restrict__ Cc, float* __restrict__ Fo,
                                                          float* __restrict__ Co, unsigned long long* gstep,
                                                          unsigned* ticket) {
     __shared__ float s_gain[kRT][kIT + 1];
-    __shared__ float s_L[kRT][kCK + 1];
-    __shared__ __align__(16) float s_F[kCK][kIT];
+    __shared__ float s_L[2][kRT][kCK + 1];
+    __shared__ __align__(16) float s_F[2][kCK][kIT];
     __shared__ double s_min[16][kIT];
     __shared__ int s_nonfin[kIT];
     __shared__ int s_last;
@@ -526,11 +539,11 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
 
     // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
     if (ops.has_bin) {
-        const int r = tid & 63;
+        const int r = tid & (kRT - 1);
         const int a = a0 + r;
         const int s = a < n ? species_of_row(ops, a) : 0;
-        for (int q = 0; q < kIT / 4; ++q) {
-            const int il = (tid >> 6) + 4 * q;
+        for (int q = 0; q < kIT / 8; ++q) {
+            const int il = (tid >> 5) + 8 * q;
             const int i = i0 + il;
             float g = 0.f;
             if (a < n && i < B) {
@@ -544,49 +557,63 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
     }
     if (tid < kIT) s_nonfin[tid] = 0;
 
-    float acc_l[4][4], acc_e[4][4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc_l[k][j] = acc_e[k][j] = 0.f;
-
+    float acc_l[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    float acc_e[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
     const bool fast = ops.tile_fast[blockIdx.x] != 0;
     if (fast) {
         const int s = species_of_row(ops, a0);
-        // tile product: acc[r][i] += sum_c T[a0 + r][c] * F[col0 + c][i0 + i]
-        auto tile_product = [&](auto load_T, int col0, int nc, float(&acc)[4][4]) {
-            for (int c0 = 0; c0 < nc; c0 += kCK) {
-                __syncthreads();
-                for (int q = 0; q < (kRT * kCK) / 256; ++q) {
-                    const int cc = tid & (kCK - 1), rr = (tid >> 5) + 8 * q;
+        // acc[r][i] += sum_c T[a0 + r][c] * F[col0 + c][i0 + i], chunks of kCK columns; the next
+        // chunk is loaded into registers while the current one is multiplied
+        auto tile_product = [&](auto load_T, int col0, int nc, float(&acc)[2][2]) {
+            constexpr int PER = (kRT * kCK) / 256;  // elements of each operand per thread and chunk
+            float rl[PER], rf[PER];
+            auto fetch = [&](int c0) {
+#pragma unroll
+                for (int q = 0; q < PER; ++q) {
+                    const int e = tid + 256 * q;
+                    const int cc = e & (kCK - 1), rr = e / kCK;
                     const int a = a0 + rr, c = c0 + cc;
-                    s_L[rr][cc] = (a < n && c < nc) ? load_T(a, c) : 0.f;
+                    rl[q] = (a < n && c < nc) ? load_T(a, c) : 0.f;
+                    const int ii = e & (kIT - 1), cf = e / kIT;
+                    const int i = i0 + ii, c2 = c0 + cf;
+                    rf[q] = (c2 < nc && i < B) ? F[(size_t)(col0 + c2) * B + i] : 0.f;
                 }
-                for (int q = 0; q < (kCK * kIT) / 256; ++q) {
-                    const int ii = tid & (kIT - 1), cc = (tid >> 6) + 4 * q;
-                    const int i = i0 + ii, c = c0 + cc;
-                    s_F[cc][ii] = (c < nc && i < B) ? F[(size_t)(col0 + c) * B + i] : 0.f;
+            };
+            auto stash = [&](int buf) {
+#pragma unroll
+                for (int q = 0; q < PER; ++q) {
+                    const int e = tid + 256 * q;
+                    s_L[buf][e / kCK][e & (kCK - 1)] = rl[q];
+                    s_F[buf][e / kIT][e & (kIT - 1)] = rf[q];
                 }
-                __syncthreads();
+            };
+            const int nch = (nc + kCK - 1) / kCK;
+            if (nch == 0) return;
+            fetch(0);
+            __syncthreads();  // the previous product's last reads of both buffers are done
+            stash(0);
+            __syncthreads();
+            for (int k = 0; k < nch; ++k) {
+                const int buf = k & 1;
+                if (k + 1 < nch) fetch((k + 1) * kCK);
 #pragma unroll 8
                 for (int cc = 0; cc < kCK; ++cc) {
-                    const float4 fv = *reinterpret_cast<const float4*>(&s_F[cc][tx * 4]);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const float l = s_L[ty * 4 + k][cc];
-                        acc[k][0] += l * fv.x;
-                        acc[k][1] += l * fv.y;
-                        acc[k][2] += l * fv.z;
-                        acc[k][3] += l * fv.w;
-                    }
+                    const float2 fv = *reinterpret_cast<const float2*>(&s_F[buf][cc][tx * 2]);
+                    const float l0 = s_L[buf][ty * 2][cc], l1 = s_L[buf][ty * 2 + 1][cc];
+                    acc[0][0] += l0 * fv.x;
+                    acc[0][1] += l0 * fv.y;
+                    acc[1][0] += l1 * fv.x;
+                    acc[1][1] += l1 * fv.y;
                 }
+                if (k + 1 < nch) stash(buf ^ 1);
+                __syncthreads();
             }
         };
         if (ops.has_bin) {
             for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
                 const float* base = ops.loss_data + ops.loss_data_off[b];
                 const int ld = ops.loss_ld[b], off = ops.sp_off[s];
-                tile_product([&](int a, int c) { return base[(size_t)(a - off) * ld + c]; }, ops.loss_col_off[b],
+                tile_product([&](int a, int c) { return __ldg(base + (size_t)(a - off) * ld + c); }, ops.loss_col_off[b],
                              ops.loss_ncols[b], acc_l);
             }
         }
@@ -607,41 +634,39 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
     }
     __syncthreads();
 
-    // ---- update of the thread's 4 x 4 (row, instance) pairs
-    double rmin[4] = {CUDART_INF, CUDART_INF, CUDART_INF, CUDART_INF};
-    int nonfin[4] = {0, 0, 0, 0};
-    const int ib = i0 + tx * 4;
-    bool act[4];
-    double dts[4];
+    // ---- update of the thread's 2 x 2 (row, instance) pairs
+    double rmin[2] = {CUDART_INF, CUDART_INF};
+    int nonfin[2] = {0, 0};
+    const int ib = i0 + tx * 2;
+    bool act[2];
+    double dts[2];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < 2; ++j) {
         const int i = ib + j;
         act[j] = i < B && step < ops.stop_step[i];
         dts[j] = i < B ? ops.dt_scale[i] : 0.0;
     }
-    for (int k = 0; k < 4; ++k) {
-        const int a = a0 + ty * 4 + k;
+    for (int k = 0; k < 2; ++k) {
+        const int a = a0 + ty * 2 + k;
         if (a >= n || ib >= B) continue;
-        const size_t idx = (size_t)a * B + ib;  // B and ib are multiples of 4
-        const float4 fa4 = *reinterpret_cast<const float4*>(F + idx);
-        const float4 ca4 = *reinterpret_cast<const float4*>(Cc + idx);
-        float flux[4] = {0.f, 0.f, 0.f, 0.f};
+        const size_t idx = (size_t)a * B + ib;  // B and ib are even
+        const float2 fa2 = *reinterpret_cast<const float2*>(F + idx);
+        const float2 ca2 = *reinterpret_cast<const float2*>(Cc + idx);
+        float flux[2] = {0.f, 0.f};
         for (int e = 0; e < ops.ell_w; ++e) {
-            const int col = ops.ell_col[(size_t)a * ops.ell_w + e];
+            const int col = __ldg(ops.ell_col + (size_t)a * ops.ell_w + e);
             if (col < 0) continue;
-            const float v = ops.ell_val[(size_t)a * ops.ell_w + e];
-            const float4 f4 = *reinterpret_cast<const float4*>(F + (size_t)col * B + ib);
-            flux[0] += v * f4.x;
-            flux[1] += v * f4.y;
-            flux[2] += v * f4.z;
-            flux[3] += v * f4.w;
+            const float v = __ldg(ops.ell_val + (size_t)a * ops.ell_w + e);
+            const float2 f2 = *reinterpret_cast<const float2*>(F + (size_t)col * B + ib);
+            flux[0] += v * f2.x;
+            flux[1] += v * f2.y;
         }
         const int s = species_of_row(ops, a);
-        const float fa[4] = {fa4.x, fa4.y, fa4.z, fa4.w};
-        const float ca[4] = {ca4.x, ca4.y, ca4.z, ca4.w};
-        float fo[4], co[4];
+        const float fa[2] = {fa2.x, fa2.y};
+        const float ca[2] = {ca2.x, ca2.y};
+        float fo[2], co[2];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 2; ++j) {
             if (!act[j]) {
                 fo[j] = fa[j];
                 co[j] = ca[j];
@@ -649,7 +674,7 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
             }
             float loss = acc_l[k][j], emi = acc_e[k][j];
             if (!fast) row_terms_direct(ops, F, a, s, ib + j, loss, emi);
-            const float gain = ops.has_bin ? s_gain[ty * 4 + k][tx * 4 + j] : 0.f;
+            const float gain = ops.has_bin ? s_gain[ty * 2 + k][tx * 2 + j] : 0.f;
             // SteppingMethods.jl:31-46 in FP32, the scaling in FP64
             float df = -flux[j];
             if (ops.has_emi) df += emi;
@@ -666,14 +691,14 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
             if (ratio < rmin[j] || (ratio == rmin[j] && signbit(ratio))) rmin[j] = ratio;
             if (!isfinite(dfs)) nonfin[j] = 1;
         }
-        *reinterpret_cast<float4*>(Fo + idx) = make_float4(fo[0], fo[1], fo[2], fo[3]);
-        *reinterpret_cast<float4*>(Co + idx) = make_float4(co[0], co[1], co[2], co[3]);
+        *reinterpret_cast<float2*>(Fo + idx) = make_float2(fo[0], fo[1]);
+        *reinterpret_cast<float2*>(Co + idx) = make_float2(co[0], co[1]);
     }
     // ---- per-instance diagnostics over the tile's rows, then one atomic per instance
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        s_min[ty][tx * 4 + j] = rmin[j];
-        if (nonfin[j]) atomicOr(&s_nonfin[tx * 4 + j], 1);
+    for (int j = 0; j < 2; ++j) {
+        s_min[ty][tx * 2 + j] = rmin[j];
+        if (nonfin[j]) atomicOr(&s_nonfin[tx * 2 + j], 1);
     }
     __syncthreads();
     if (tid < kIT) {
