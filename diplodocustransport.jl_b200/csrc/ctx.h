@@ -90,6 +90,11 @@ struct dtb_ctx {
     std::vector<EmiPiece> emis;
     std::vector<int64_t> flux_r, flux_c;
     std::vector<double> flux_v;
+    bool symplectic = false;             // ForwardSymplecticEuler: X kept apart from P
+    std::vector<int64_t> xflux_r, xflux_c;
+    std::vector<double> xflux_v;
+    void* fm_buf = nullptr;              // f_Momentum of the symplectic step
+    void* dfm_buf = nullptr;             // df_Momentum of the symplectic step
     std::vector<double> Ap, Vol, f_init, inj;
     bool have_vectors = false;
     bool committed = false;

@@ -75,6 +75,9 @@ int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out) {
     c->prec = opts->precision;
     c->esz = c->prec == DTB_F64 ? 8 : 4;  // state element size (DTB_MIXED keeps f in FP32)
     c->device = opts->device;
+    c->symplectic = (opts->flags & DTB_FLAG_SYMPLECTIC) != 0;
+    DTB_CHECK(!c->symplectic || c->prec != DTB_MIXED, DTB_EINVAL,
+              "dtb_create: the symplectic method is available for DTB_F64 / DTB_F32 contexts");
     c->off[0] = 0;
     c->offp[0] = 0;
     for (int s = 0; s < c->ns; ++s) {
@@ -119,8 +122,8 @@ int32_t dtb_destroy(dtb_ctx* c) {
 }
 
 
-int32_t dtb_add_flux_csc(dtb_ctx* c, int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval) {
-    DTB_CHECK(c, DTB_EINVAL, "dtb_add_flux_csc: null context");
+static int add_csc(dtb_ctx* c, std::vector<int64_t>& R, std::vector<int64_t>& Cv, std::vector<double>& V, int64_t n,
+                   const int64_t* colptr, const int64_t* rowval, const double* nzval) {
     DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_add_flux_csc: operators already committed");
     DTB_CHECK(n == c->n_state, DTB_EINVAL, "dtb_add_flux_csc: n must equal the state length");
     DTB_CHECK(colptr, DTB_EINVAL, "dtb_add_flux_csc: null colptr");
@@ -134,12 +137,27 @@ int32_t dtb_add_flux_csc(dtb_ctx* c, int64_t n, const int64_t* colptr, const int
             const int64_t r = rowval[p] - base;
             DTB_CHECK(r >= 0 && r < n, DTB_EINVAL,
                       "dtb_add_flux_csc: row index out of range at entry " + std::to_string(p));
-            c->flux_r.push_back(r);
-            c->flux_c.push_back(j);
-            c->flux_v.push_back(nzval[p]);
+            R.push_back(r);
+            Cv.push_back(j);
+            V.push_back(nzval[p]);
         }
     }
     return DTB_OK;
+}
+
+int32_t dtb_add_flux_csc(dtb_ctx* c, int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_add_flux_csc: null context");
+    DTB_CHECK(!c->symplectic, DTB_EINVAL,
+              "dtb_add_flux_csc: the symplectic method keeps X and P apart; use dtb_add_flux_csc_part");
+    return add_csc(c, c->flux_r, c->flux_c, c->flux_v, n, colptr, rowval, nzval);
+}
+
+int32_t dtb_add_flux_csc_part(dtb_ctx* c, int32_t part, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                              const double* nzval) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_add_flux_csc_part: null context");
+    DTB_CHECK(part == DTB_FLUX_X || part == DTB_FLUX_P, DTB_EINVAL, "dtb_add_flux_csc_part: part must be X or P");
+    if (c->symplectic && part == DTB_FLUX_X) return add_csc(c, c->xflux_r, c->xflux_c, c->xflux_v, n, colptr, rowval, nzval);
+    return add_csc(c, c->flux_r, c->flux_c, c->flux_v, n, colptr, rowval, nzval);
 }
 
 static GainStage& gain_stage(dtb_ctx* c, int out, int in1, int in2) {
@@ -305,6 +323,45 @@ int32_t dtb_upload_vectors(dtb_ctx* c, const double* Ap, const double* Vol, cons
 }  // extern "C"
 
 // ------------------------------------------------------------------ commit
+// CSR with duplicates summed, then a banded ELL of width w (max row length rounded to 4);
+// padding slots have column -1.
+template <typename T>
+static int build_ell(dtb_ctx* c, const std::vector<int64_t>& fr, const std::vector<int64_t>& fc,
+                     const std::vector<double>& fv, int& w_out, const T*& val_out, const int*& col_out) {
+    const int64_t n = c->n_state;
+    std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)n);
+    for (size_t p = 0; p < fr.size(); ++p) rows[(size_t)fr[p]].push_back({fc[p], fv[p]});
+    int w = 0;
+    for (auto& r : rows) {
+        std::stable_sort(r.begin(), r.end(), [](auto& x, auto& y) { return x.first < y.first; });
+        std::vector<std::pair<int64_t, double>> m;
+        for (auto& e : r) {
+            if (!m.empty() && m.back().first == e.first)
+                m.back().second += e.second;
+            else
+                m.push_back(e);
+        }
+        r.swap(m);
+        w = std::max<int>(w, (int)r.size());
+    }
+    w = (int)round_up(std::max(w, 1), 4);
+    std::vector<double> val((size_t)(n * w), 0.0);
+    std::vector<int> col((size_t)(n * w), -1);
+    for (int64_t i = 0; i < n; ++i)
+        for (size_t k = 0; k < rows[(size_t)i].size(); ++k) {
+            col[(size_t)i * w + k] = (int)rows[(size_t)i][k].first;
+            val[(size_t)i * w + k] = rows[(size_t)i][k].second;
+        }
+    T* d_val;
+    int* d_col;
+    DTB_TRY(copy_host_vec(c, &d_val, val));
+    DTB_TRY(copy_host_ints(c, &d_col, col));
+    w_out = w;
+    val_out = d_val;
+    col_out = d_col;
+    return DTB_OK;
+}
+
 template <typename T>
 static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     const size_t esz = sizeof(T);
@@ -497,45 +554,21 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
         ops.emi_ncols = d_nc;
         ops.emi_data = d_data;
     }
-    // ---------------- flux: CSR with duplicates summed, then banded ELL
-    {
-        const int64_t n = c->n_state;
-        std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)n);
-        for (size_t p = 0; p < c->flux_r.size(); ++p) rows[(size_t)c->flux_r[p]].push_back({c->flux_c[p], c->flux_v[p]});
-        int w = 0;
-        for (auto& r : rows) {
-            std::stable_sort(r.begin(), r.end(), [](auto& x, auto& y) { return x.first < y.first; });
-            std::vector<std::pair<int64_t, double>> m;
-            for (auto& e : r) {
-                if (!m.empty() && m.back().first == e.first)
-                    m.back().second += e.second;
-                else
-                    m.push_back(e);
-            }
-            r.swap(m);
-            w = std::max<int>(w, (int)r.size());
-        }
-        w = (int)round_up(std::max(w, 1), 4);
-        std::vector<double> val((size_t)(n * w), 0.0);
-        std::vector<int> col((size_t)(n * w));
-        for (int64_t i = 0; i < n; ++i) {
-            for (int k = 0; k < w; ++k) {
-                if (k < (int)rows[(size_t)i].size()) {
-                    col[(size_t)(i * w + k)] = (int)rows[(size_t)i][(size_t)k].first;
-                    val[(size_t)(i * w + k)] = rows[(size_t)i][(size_t)k].second;
-                } else {
-                    col[(size_t)(i * w + k)] = -1;  // padding, skipped by the kernel
-                }
-            }
-        }
-        T* d_val;
-        int* d_col;
-        DTB_TRY(copy_host_vec(c, &d_val, val));
-        DTB_TRY(copy_host_ints(c, &d_col, col));
-        ops.ell_w = w;
-        ops.ell_val = d_val;
-        ops.ell_col = d_col;
+    // ---------------- flux: CSR with duplicates summed, then banded ELL (X + P, or P and X
+    // separately for the symplectic method)
+    DTB_TRY(build_ell<T>(c, c->flux_r, c->flux_c, c->flux_v, ops.ell_w, ops.ell_val, ops.ell_col));
+    if (c->symplectic) {
+        DTB_TRY(build_ell<T>(c, c->xflux_r, c->xflux_c, c->xflux_v, ops.x_ell_w, ops.x_ell_val, ops.x_ell_col));
+        T *fm, *dfm;
+        DTB_TRY(c->alloc(&fm, sizeof(T) * (size_t)c->n_state));
+        DTB_TRY(c->alloc(&dfm, sizeof(T) * (size_t)c->n_state));
+        c->fm_buf = fm;
+        c->dfm_buf = dfm;
+        ops.dfm_out = dfm;
     }
+    ops.mode = 0;
+    ops.thr_mom = c->prec == DTB_F64 ? (double)1e-10f : (double)(T)1e-10f;
+    ops.thr_space = c->prec == DTB_F64 ? (double)1e-20f : (double)(T)1e-20f;
     // ---------------- vectors
     {
         std::vector<double> invAp(c->Ap.size());
@@ -671,8 +704,19 @@ static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, 
             if (++c->prof_pending == kProfRing) DTB_TRY(flush_profile(c));
         }
     }
-    DTB_CUDA(launch_euler_rows<T>(ops, fin, fout, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist, c->hist_cap,
-                                  verbose, c->blk_red, c->ticket, c->stream));
+    if (c->symplectic) {
+        RowOps<T> mom = ops;
+        mom.mode = 1;
+        T* fm = reinterpret_cast<T*>(c->fm_buf);
+        T* dfm = reinterpret_cast<T*>(c->dfm_buf);
+        DTB_CUDA(launch_euler_rows<T>(mom, fin, fm, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist,
+                                      c->hist_cap, verbose, c->blk_red, c->ticket, c->stream));
+        DTB_CUDA(launch_sympl_space<T>(ops, fin, fm, dfm, fout, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist,
+                                       c->hist_cap, verbose, c->blk_red, c->ticket, c->stream));
+    } else {
+        DTB_CUDA(launch_euler_rows<T>(ops, fin, fout, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist,
+                                      c->hist_cap, verbose, c->blk_red, c->ticket, c->stream));
+    }
     c->cur ^= 1;
     c->host_ctr++;
     return DTB_OK;
@@ -989,7 +1033,7 @@ int32_t dtb_sync(dtb_ctx* c) {
 int32_t dtb_launches_per_step(dtb_ctx* c, int32_t* n) {
     DTB_CHECK(c && n, DTB_EINVAL, "dtb_launches_per_step: null argument");
     DTB_TRY(dtb_commit(c));
-    *n = c->n_units > 0 ? 2 : 1;
+    *n = (c->n_units > 0 ? 2 : 1) + (c->symplectic ? 1 : 0);
     return DTB_OK;
 }
 
@@ -1001,6 +1045,26 @@ int32_t dtb_set_profiling(dtb_ctx* c, int32_t on) {
     c->prof_n = 0;
     c->prof_pending = 0;
     return DTB_OK;
+}
+
+int32_t dtb_selftest_bounded_wait(dtb_ctx* c, double limit_s) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_selftest_bounded_wait: null context");
+    DTB_CHECK(limit_s > 0 && limit_s <= 2.0, DTB_EINVAL, "dtb_selftest_bounded_wait: limit must be in (0, 2] s");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    DTB_CUDA(launch_bounded_wait_selftest((unsigned long long)(limit_s * 1e9), c->err, c->stream));
+    if (c->prec == DTB_MIXED) {
+        DTB_CUDA(cudaMemcpyAsync(c->pin_err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+        if (*c->pin_err) {
+            cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+            cudaStreamSynchronize(c->stream);
+            set_error("a bounded device wait gave up (self-test)");
+            return DTB_ETIMEOUT;
+        }
+        return DTB_OK;
+    }
+    return check_kernel_err(c);
 }
 
 int32_t dtb_gain_kernel_stats(dtb_ctx* c, double* avg_ms, double* bytes_per_launch) {

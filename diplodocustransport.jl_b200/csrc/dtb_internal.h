@@ -82,6 +82,14 @@ struct RowOps {
     const T* vol;
     double thr;                            // clamp threshold in the state precision
     int has_bin, has_emi;
+    // ForwardSymplecticEuler (SteppingMethods.jl:120-243): mode 1 is its momentum pass, which
+    // writes f_Momentum (clamped at thr_mom) and df_Momentum; the space pass uses the X flux
+    int mode;
+    T* dfm_out;
+    double thr_mom, thr_space;
+    int x_ell_w;
+    const T* x_ell_val;
+    const int* x_ell_col;
 };
 
 // Launch helpers (kernels_plain.cu).
@@ -96,6 +104,11 @@ cudaError_t launch_euler_rows(const RowOps<T>& ops, const T* f_in, T* f_out, dou
                               long long hist_cap, int verbose, double* blk_red, unsigned* ticket,
                               cudaStream_t s);
 
+template <typename T>
+cudaError_t launch_sympl_space(const RowOps<T>& ops, const T* f_old, const T* fm, const T* dfm, T* f_out,
+                               double dt_imm, const double* dt_arr, unsigned long long* ctr, StepDiagDev* hist,
+                               long long hist_cap, int verbose, double* blk_red, unsigned* ticket, cudaStream_t s);
+
 template <typename Tin, typename Tout>
 cudaError_t launch_pad_rows(const Tin* src, long long rows, int n, Tout* dst, int np, cudaStream_t s);
 
@@ -103,6 +116,8 @@ cudaError_t launch_moments_f64(const double* f, int n_mom, int n_space, const in
                                int n_species, const double* w, double* out, cudaStream_t s);
 cudaError_t launch_moments_f32(const float* f, int n_mom, int n_space, const int* sp_off,
                                int n_species, const double* w, double* out, cudaStream_t s);
+
+cudaError_t launch_bounded_wait_selftest(unsigned long long limit_ns, int* err, cudaStream_t s);
 
 int gain_stream_smem_bytes(int elem_size, int f_smem_len);
 int gain_stream_blocks_per_sm(int elem_size, int f_smem_len);

@@ -385,7 +385,19 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         loss = warp_sum(loss);
         gain = warp_sum(gain);
 
-        if (lane == 0) {
+        if (lane == 0 && ops.mode == 1) {
+            // ForwardSymplecticEuler momentum pass (SteppingMethods.jl:140-160)
+            const T fa = fc[a];
+            T df = -(T)flux;
+            if (ops.has_emi) df = df + (T)emi;
+            if (ops.has_bin) df = df + (T)((double)ops.vol[cell] * (gain - (double)fa * loss));
+            df = (T)((double)df * ((double)ops.invAp[i] * dt_scale));
+            T fm = fa + df;
+            fm = jl_mul_bool(fm, fm >= (T)ops.thr_mom);
+            f_out[i] = fm;
+            ops.dfm_out[i] = df;
+        }
+        if (lane == 0 && ops.mode == 0) {
             const T fa = fc[a];
             const T dflux = (T)flux;
             const T demi = (T)emi;
@@ -413,6 +425,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
             s_f = fd;
         }
     }
+    if (ops.mode == 1) return;  // the space pass reduces the step's diagnostics
     if (lane == 0) {
         s_red[warp][0] = m_cr;
         s_red[warp][1] = m_bin;
@@ -495,6 +508,144 @@ template cudaError_t launch_euler_rows<double>(const RowOps<double>&, const doub
 template cudaError_t launch_euler_rows<float>(const RowOps<float>&, const float*, float*, double, const double*,
                                               unsigned long long*, StepDiagDev*, long long, int, double*,
                                               unsigned*, cudaStream_t);
+
+// ------------------------------------------------------------------ sympl_space
+// ForwardSymplecticEuler space pass (SteppingMethods.jl:165-237): one warp per row,
+// df_Space = -(X f_Momentum) invAp dt/dt0, f_Space = clamp(f_Momentum + df_Space, 1f-20), then
+// f = f_Space + inj dt/dt0 clamped with the sign factor of :235 and the Inf fix of :237.
+// Cr = -min((df_Space + df_Momentum) ./ f_old) (:217-218), reduced by the last block.
+template <typename T>
+__global__ void __launch_bounds__(kRowsWarps * 32) sympl_space_kernel(RowOps<T> ops, const T* __restrict__ f_old,
+                                                                      const T* __restrict__ fm,
+                                                                      const T* __restrict__ dfm, T* __restrict__ f_out,
+                                                                      double dt_imm, const double* __restrict__ dt_arr,
+                                                                      unsigned long long* ctr, StepDiagDev* hist,
+                                                                      long long hist_cap, int verbose, double* blk_red,
+                                                                      unsigned* ticket) {
+    __shared__ double s_red[kRowsWarps][2];
+    __shared__ double s_fin[2][kRowsWarps * 32];
+    __shared__ int s_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
+    const double dt_scale = dt_arr ? dt_arr[step] : dt_imm;
+    const int i = blockIdx.x * kRowsWarps + warp;
+    double m_cr = CUDART_INF, s_f = 0.0;
+    if (i < ops.n_state) {
+        double xf = 0.0;
+        for (int k = lane; k < ops.x_ell_w; k += 32) {
+            const int c = ops.x_ell_col[(size_t)i * ops.x_ell_w + k];
+            if (c >= 0) xf += (double)ops.x_ell_val[(size_t)i * ops.x_ell_w + k] * (double)fm[c];
+        }
+        xf = warp_sum(xf);
+        if (lane == 0) {
+            const T dsp = (T)((double)(-(T)xf * ops.invAp[i]) * dt_scale);
+            T fs = fm[i] + dsp;
+            fs = jl_mul_bool(fs, fs >= (T)ops.thr_space);
+            T v = (T)((double)fs + (double)ops.inj[i] * dt_scale);
+            const T sg = isnan(v) ? v : (v > T(0) ? T(1) : (v < T(0) ? T(-1) : v));
+            v = jl_mul_bool(v, v >= (T)ops.thr_space) * sg;
+            v = jl_mul_bool(v, v != (T)CUDART_INF);
+            f_out[i] = v;
+            const double fo = (double)f_old[i];
+            m_cr = nan_to_inf((double)(dsp + dfm[i]) / fo);
+            s_f = fo;
+        }
+    }
+    if (lane == 0) {
+        s_red[warp][0] = m_cr;
+        s_red[warp][1] = s_f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r0 = s_red[0][0], r1 = s_red[0][1];
+        for (int w = 1; w < kRowsWarps; ++w) {
+            r0 = jl_min(r0, s_red[w][0]);
+            r1 += s_red[w][1];
+        }
+        blk_red[(size_t)blockIdx.x * 2] = r0;
+        blk_red[(size_t)blockIdx.x * 2 + 1] = r1;
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double r0 = CUDART_INF, r1 = 0.0;
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            r0 = jl_min(r0, __ldcg(blk_red + (size_t)b * 2));
+            r1 += __ldcg(blk_red + (size_t)b * 2 + 1);
+        }
+        s_fin[0][threadIdx.x] = r0;
+        s_fin[1][threadIdx.x] = r1;
+        __syncthreads();
+        for (int o = kRowsWarps * 16; o > 0; o >>= 1) {
+            if (threadIdx.x < o) {
+                s_fin[0][threadIdx.x] = jl_min(s_fin[0][threadIdx.x], s_fin[0][threadIdx.x + o]);
+                s_fin[1][threadIdx.x] += s_fin[1][threadIdx.x + o];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            StepDiagDev d;
+            const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && s_fin[1][0] != 0.0;
+            d.cr[0] = on ? -s_fin[0][0] : 0.0;
+            d.cr[1] = d.cr[2] = d.cr[3] = 0.0;
+            d.sum_df = 0.0;
+            d.sum_f = s_fin[1][0];
+            d.finite = 1;  // the symplectic method has no finite check (SteppingMethods.jl:120-243)
+            d.pad = 0;
+            hist[step % (unsigned long long)hist_cap] = d;
+            *ticket = 0u;
+            __threadfence();
+            *reinterpret_cast<volatile unsigned long long*>(ctr) = step + 1ull;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t launch_sympl_space(const RowOps<T>& ops, const T* f_old, const T* fm, const T* dfm, T* f_out,
+                               double dt_imm, const double* dt_arr, unsigned long long* ctr, StepDiagDev* hist,
+                               long long hist_cap, int verbose, double* blk_red, unsigned* ticket, cudaStream_t s) {
+    const int grid = (ops.n_state + kRowsWarps - 1) / kRowsWarps;
+    sympl_space_kernel<T><<<grid, kRowsWarps * 32, 0, s>>>(ops, f_old, fm, dfm, f_out, dt_imm, dt_arr, ctr, hist,
+                                                           hist_cap, verbose, blk_red, ticket);
+    return cudaGetLastError();
+}
+template cudaError_t launch_sympl_space<double>(const RowOps<double>&, const double*, const double*, const double*,
+                                                double*, double, const double*, unsigned long long*, StepDiagDev*,
+                                                long long, int, double*, unsigned*, cudaStream_t);
+template cudaError_t launch_sympl_space<float>(const RowOps<float>&, const float*, const float*, const float*, float*,
+                                               double, const double*, unsigned long long*, StepDiagDev*, long long,
+                                               int, double*, unsigned*, cudaStream_t);
+
+// ------------------------------------------------------------------ bounded-wait self-test
+// One block waits on an mbarrier phase that nothing completes, with a limit of limit_ns, and
+// reports the timeout through err: the same give-up path every pipeline wait in this library
+// takes, exercised without a fault.
+__global__ void bounded_wait_selftest_kernel(unsigned long long limit_ns, int* err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long t0 = globaltimer();
+        bool done = false;
+        while (!done) {
+            done = mbar_try_wait(smem_u32(&bar), 0u);
+            if (!done && globaltimer() - t0 > limit_ns) break;
+        }
+        if (!done) atomicOr(err, KERR_TIMEOUT_FULL);
+        mbar_arrive(smem_u32(&bar));  // complete the phase so the barrier is left consistent
+    }
+}
+
+cudaError_t launch_bounded_wait_selftest(unsigned long long limit_ns, int* err, cudaStream_t s) {
+    bounded_wait_selftest_kernel<<<1, 32, 0, s>>>(limit_ns, err);
+    return cudaGetLastError();
+}
 
 // ------------------------------------------------------------------ helpers
 template <typename Tin, typename Tout>

@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(PKG, "lib", "libdtb.so")
 DTB_OK, DTB_EINVAL, DTB_ENOMEM, DTB_ECUDA, DTB_ETIMEOUT, DTB_ESTATE, DTB_ENODEV, DTB_ENOTFOUND = range(8)
 DTB_F64, DTB_F32, DTB_MIXED = 0, 1, 2
 DTB_DTYPE_F64, DTB_DTYPE_F32 = 0, 1
+DTB_FLAG_SYMPLECTIC = 1
+DTB_FLUX_X, DTB_FLUX_P = 0, 1
 MAX_SPECIES = 16
 
 ERROR_NAMES = {1: "DTB_EINVAL", 2: "DTB_ENOMEM", 3: "DTB_ECUDA", 4: "DTB_ETIMEOUT", 5: "DTB_ESTATE",
@@ -77,6 +79,7 @@ SIGNATURES = {
     "dtb_create": (_i32, [ctypes.POINTER(Dims), ctypes.POINTER(Opts), ctypes.POINTER(_P)]),
     "dtb_destroy": (_i32, [_P]),
     "dtb_add_flux_csc": (_i32, [_P, _i64, _ip, _ip, _dp]),
+    "dtb_add_flux_csc_part": (_i32, [_P, _i32, _i64, _ip, _ip, _dp]),
     "dtb_upload_mbin_ref": (_i32, [_P, _dp, _i64]),
     "dtb_add_gain_block": (_i32, [_P, _i32, _i32, _i32, _P, _i32, _i32]),
     "dtb_add_loss_block": (_i32, [_P, _i32, _i32, _dp]),
@@ -98,6 +101,7 @@ SIGNATURES = {
     "dtb_launches_per_step": (_i32, [_P, _i32p]),
     "dtb_gain_kernel_stats": (_i32, [_P, _dp, _dp]),
     "dtb_set_profiling": (_i32, [_P, _i32]),
+    "dtb_selftest_bounded_wait": (_i32, [_P, _d]),
     "dtb_gain_contract": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
     "dtb_batch_admit": (_i32, [_P, _i32, _dp, _d, _i64]),
     "dtb_batch_run": (_i32, [_P, _i64]),

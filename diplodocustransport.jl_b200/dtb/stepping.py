@@ -70,8 +70,21 @@ def _upload_gain(L, ctx, g) -> None:
     check(L.dtb_add_gain_block(ctx, g.out_sp, g.in1_sp, g.in2_sp, ctypes.c_void_p(A.ctypes.data), dtype, 0))
 
 
+def _upload_csc_part(L, ctx, M, part) -> None:
+    if M is None or M.nnz == 0:
+        return
+    M = M.tocsc()
+    M.sort_indices()
+    colptr = np.ascontiguousarray(M.indptr, dtype=np.int64)
+    rowval = np.ascontiguousarray(M.indices, dtype=np.int64)
+    nzval = np.ascontiguousarray(M.data, dtype=np.float64)
+    check(L.dtb_add_flux_csc_part(ctx, part, M.shape[0], iptr(colptr), iptr(rowval), dptr(nzval)))
+
+
 class ForwardEulerStruct:
     """Explicit Euler method on a B200; SteppingStructs.jl:33-100 for the B200 backend."""
+
+    _flags = 0
 
     def __init__(self, PhaseSpace: PhaseSpace, Initial, Injection, BinM: BinaryMatrices,
                  EmiM: EmissionMatrices, FluxM: FluxMatrices, *, Adaptive: bool = False,
@@ -95,14 +108,14 @@ class ForwardEulerStruct:
         for i, s in enumerate(sizes):
             dims.species_size[i] = s
         opts = _lib.Opts(precision=prec, device=device, stream=stream, index_base=0,
-                         graph_steps=graph_steps, dt0=float(PhaseSpace.dt0), batch=1, flags=0)
+                         graph_steps=graph_steps, dt0=float(PhaseSpace.dt0), batch=1, flags=self._flags)
         ctx = ctypes.c_void_p()
         check(self.L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)))
         self.ctx = ctx
         try:
             L = self.L
-            _upload_csc(L, ctx, FluxM.X_Flux)
-            _upload_csc(L, ctx, FluxM.P_Flux)
+            _upload_csc_part(L, ctx, FluxM.X_Flux, _lib.DTB_FLUX_X)
+            _upload_csc_part(L, ctx, FluxM.P_Flux, _lib.DTB_FLUX_P)
             if BinM.M_Bin is not None:
                 M = np.asfortranarray(BinM.M_Bin, dtype=np.float64)
                 check(L.dtb_upload_mbin_ref(ctx, M.ctypes.data_as(_lib._dp), PhaseSpace.n_momentum))
@@ -193,6 +206,16 @@ class ForwardEulerStruct:
             self.close()
         except Exception:
             pass
+
+
+class ForwardSymplecticEulerStruct(ForwardEulerStruct):
+    """Forward symplectic (semi-implicit) Euler on a B200: SteppingStructs.jl:104-229 for the B200
+    backend, stepping as SteppingMethods.jl:120-243 (momentum fluxes, emission and binary terms
+    first, clamped at 1f-10; then the space fluxes on the updated f, clamped at 1f-20). The
+    diagnostics report the whole-step Cr (:217-218); the per-term Crs of Verbose == 3 are not
+    reduced on the device."""
+
+    _flags = _lib.DTB_FLAG_SYMPLECTIC
 
 
 def solve_schedule(dt_initial: float, t_save: Sequence[float], dt0: float, precision: int = _lib.DTB_F64):

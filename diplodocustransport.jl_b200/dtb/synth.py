@@ -107,6 +107,32 @@ def upwind_flux(ps: PhaseSpace, rng: np.random.Generator, dt: float,
                         Vol=np.ones(ps.n_space))
 
 
+def space_flux(ps: PhaseSpace, rng: np.random.Generator, dt: float, cfl: float = 0.2):
+    """Upwind flux of every momentum state between neighbouring space cells (closed ends): a
+    seeded velocity U[-1, 1] per (face, state); columns sum to zero. Scaled so that
+    dt * spectral_radius = cfl."""
+    n, nm = ps.n_state, ps.n_momentum
+    rows, cols, vals = [], [], []
+    for cell in range(ps.n_space - 1):
+        v = rng.uniform(-1.0, 1.0, size=nm)
+        for m in range(nm):
+            lo, hi = cell * nm + m, (cell + 1) * nm + m
+            src, dst = (lo, hi) if v[m] > 0 else (hi, lo)
+            aw = abs(v[m])
+            rows += [src, dst]
+            cols += [src, src]
+            vals += [aw, -aw]
+    X = sp.csc_matrix((vals, (rows, cols)), shape=(n, n))
+    X.sum_duplicates()
+    if X.nnz:
+        rho = float(np.max(np.abs(np.linalg.eigvals(X.toarray())))) if n <= 512 else abs(
+            spla.eigs(X, k=1, which="LM", return_eigenvectors=False)[0])
+        X = X * (cfl / (dt * rho))
+    X = X.tocsc()
+    X.sort_indices()
+    return X
+
+
 def lognormal_f0(ps: PhaseSpace, mu: List[float], sigma: float = 1.0) -> np.ndarray:
     """Cell-integrated log-normal p spectrum, isotropic in u, unit number per species."""
     f = np.zeros(ps.n_state)

@@ -38,6 +38,14 @@ extern "C" {
 #define DTB_MIXED 2     /* batched: G and E as BF16 hi+lo with per-row FP32 scale, f in FP32,
                            FP64 compensated update and moments */
 
+/* dtb_opts.flags */
+#define DTB_FLAG_SYMPLECTIC 1  /* ForwardSymplecticEulerStruct (SteppingStructs.jl:104-229):
+                                  momentum update, then space update (SteppingMethods.jl:120-243) */
+
+/* flux parts (FluxMatricesStruct.X_Flux / P_Flux, StructsAndDictionaries.jl:346-347) */
+#define DTB_FLUX_X 0
+#define DTB_FLUX_P 1
+
 /* element type tags for uploads */
 #define DTB_DTYPE_F64 0
 #define DTB_DTYPE_F32 1
@@ -90,6 +98,12 @@ int32_t dtb_destroy(dtb_ctx* ctx);
  * colptr has n+1 entries; indices use opts.index_base. Call once per matrix to add. */
 int32_t dtb_add_flux_csc(dtb_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
                          const double* nzval);
+
+/* Adds X_Flux (part DTB_FLUX_X) or P_Flux (DTB_FLUX_P). The explicit Euler method sums both
+ * into F; the symplectic method (DTB_FLAG_SYMPLECTIC) keeps X apart for its space update
+ * (SteppingStructs.jl:170-171,188-189). */
+int32_t dtb_add_flux_csc_part(dtb_ctx* ctx, int32_t part, int64_t n, const int64_t* colptr,
+                              const int64_t* rowval, const double* nzval);
 
 /* Reference-layout M_Bin (n_mom^2 x n_mom, column-major, BuildBinaryMatrices.jl:54) replaces
  * BinM.M_Bin (SteppingStructs.jl:58,66). It is decomposed on upload into gain blocks and
@@ -168,6 +182,11 @@ int32_t dtb_sync(dtb_ctx* ctx);
 
 /* Kernel launches issued per step by dtb_run (for launch accounting). */
 int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
+
+/* Failure-detection self-test: launches one block that waits, with a limit of limit_s
+ * seconds (at most 2), on an mbarrier phase nothing completes, i.e. the give-up path of every
+ * pipeline wait of the library. Returns DTB_ETIMEOUT and leaves the context usable. */
+int32_t dtb_selftest_bounded_wait(dtb_ctx* ctx, double limit_s);
 
 /* Dominant-kernel timing over the last dtb_run: average gain-kernel duration in ms measured
  * with CUDA events on the context stream, and its algorithmic bytes per launch. */

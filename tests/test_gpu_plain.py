@@ -222,3 +222,46 @@ def test_config1_full_size_properties(cuda):
     m.close()
     del w
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("precision,tol", [(np.float64, TOL64), (np.float32, TOL32)])
+def test_symplectic_euler_matches_oracle(cuda, precision, tol):
+    """ForwardSymplecticEuler (SteppingMethods.jl:120-243) on 3 space cells with a space flux X
+    and the momentum flux P kept apart; 30 steps against the FP64 oracle restatement."""
+    from dtb.stepping import ForwardSymplecticEulerStruct
+    w = synth.small(p_num=6, u_num=3, seed=17, n_space=3, randomize_vectors=True)
+    w.fluxm.X_Flux = synth.space_flux(w.ps, np.random.default_rng(5), 1.0)
+    m = ForwardSymplecticEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, Precision=precision)
+    r = oracle.ref_from_workload(w)
+    L = oracle.lib()
+    X, P = (oracle._csc_arrays(M) for M in (w.fluxm.X_Flux, w.fluxm.P_Flux))
+    f = w.f0.copy()
+    d = np.zeros(8)
+    thr_m = float(np.float32(1e-10))
+    thr_s = float(np.float32(1e-20))
+    for k in range(30):
+        dt = 0.9 if k % 3 else 0.7
+        m(0.0, 1e9, dt, 1)
+        rc = L.orc_step_symplectic_ref(r.n_mom, r.n_space, oracle._d(r.M_Bin), oracle._d(r.M_Emi),
+                                       oracle._i(X[0]), oracle._i(X[1]), oracle._d(X[2]),
+                                       oracle._i(P[0]), oracle._i(P[1]), oracle._d(P[2]), 0,
+                                       oracle._d(r.invAp), oracle._d(r.Vol), oracle._d(r.inj), dt,
+                                       thr_m, thr_s, 1, oracle._d(f), oracle._d(d))
+        assert rc == 0
+        assert m.last_diag.cr == pytest.approx(d[0], rel=1e-6 if precision == np.float32 else 1e-10)
+    assert rel_linf(m.f, f) <= tol
+    m.close()
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
+    """A device wait on a barrier nothing completes gives up after its limit and reports
+    DTB_ETIMEOUT; the same context then steps normally (no fault, no hang)."""
+    w = synth.small(p_num=4, u_num=2, seed=31)
+    m = make_method(w)
+    rc = m.L.dtb_selftest_bounded_wait(m.ctx, 0.2)
+    assert rc == _lib.DTB_ETIMEOUT
+    assert b"self-test" in m.L.dtb_last_error()
+    m(0.0, 1e9, 1.0, 0)
+    f, _, _ = oracle.blocked_from_workload(w).step(w.f0, 1.0, 0)
+    assert rel_linf(m.f, f) <= TOL64
+    m.close()
