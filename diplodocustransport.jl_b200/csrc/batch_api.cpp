@@ -47,6 +47,8 @@ struct MixedState {
     int* nonfinite = nullptr;
     unsigned long long* gstep = nullptr;
     unsigned* ticket = nullptr;
+    int* active_hi = nullptr;  // device: 1 + the highest slot that still steps
+    int last_active_hi = -1;
     long long host_step = 0;
     MixedRowOps ops{};
     cudaGraphExec_t graph = nullptr;
@@ -190,6 +192,7 @@ int commit_mixed(dtb_ctx* c) {
         g.host.shrink_to_fit();
     }
     DTB_CUDA(prepare_gain_gemm(bn));
+    DTB_CUDA(prepare_mixed_rows());
     for (auto& G : m->groups) {
         const int64_t K = (int64_t)G.N1 * G.n2p;
         DTB_TRY(make_map(&G.tm_hi, G.hi, K, G.M));
@@ -381,6 +384,9 @@ int commit_mixed(dtb_ctx* c) {
     DTB_TRY(c->alloc(&m->stop_step, sizeof(long long) * B));
     DTB_TRY(c->alloc(&m->min_ratio, sizeof(unsigned long long) * B));
     DTB_TRY(c->alloc(&m->nonfinite, sizeof(int) * B));
+    DTB_TRY(c->alloc(&m->active_hi, sizeof(int)));
+    DTB_CUDA(cudaMemsetAsync(m->active_hi, 0, sizeof(int), s));
+    m->last_active_hi = 0;
     DTB_TRY(c->alloc(&m->gstep, sizeof(unsigned long long)));
     DTB_TRY(c->alloc(&m->ticket, sizeof(unsigned)));
     DTB_TRY(c->alloc(&c->err, sizeof(int)));
@@ -505,6 +511,7 @@ int mixed_step(dtb_ctx* c, bool profile) {
         a.isig2 = m->isig + (size_t)G.in2 * m->Bcap;
         a.partial = G.partial;
         a.err = c->err;
+        a.active_hi = m->active_hi;
         DTB_CUDA(launch_gain_gemm(G.bn, &G.tm_hi, &G.tm_lo, a, c->stream));
     }
     if (profile) {
@@ -515,7 +522,7 @@ int mixed_step(dtb_ctx* c, bool profile) {
     for (auto& G : m->groups)
         DTB_CUDA(launch_split_reduce(G.partial, G.n_splits, G.Bpad, G.M, m->Bcap, G.row_scale,
                                      m->sig + (size_t)G.in1 * m->Bcap, m->sig + (size_t)G.in2 * m->Bcap, G.gsum,
-                                     c->stream));
+                                     m->active_hi, c->stream));
     DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, m->ticket,
                                c->stream));
     m->cur ^= 1;
@@ -539,6 +546,24 @@ int ensure_mixed_graph(dtb_ctx* c) {
     e = cudaGraphInstantiate(&m->graph, gr, 0);
     cudaGraphDestroy(gr);
     DTB_CUDA(e);
+    return DTB_OK;
+}
+
+// Columns the gain GEMM computes: up to the highest slot that still steps (slots are admitted
+// into the lowest free slots, so this tracks the number of running solves).
+int refresh_active_hi(dtb_ctx* c) {
+    MixedState* m = c->mixed;
+    int hi = 0;
+    for (int sl = m->Buser - 1; sl >= 0; --sl)
+        if (m->h_stop[(size_t)sl] > m->host_step) {
+            hi = sl + 1;
+            break;
+        }
+    if (hi != m->last_active_hi) {
+        const int v = hi;  // pageable source: staged before the call returns
+        DTB_CUDA(cudaMemcpyAsync(m->active_hi, &v, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        m->last_active_hi = hi;
+    }
     return DTB_OK;
 }
 
@@ -569,6 +594,7 @@ int mixed_ready(dtb_ctx* c) {
 int batch_launch(dtb_ctx* c, int64_t nsteps) {
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
+    DTB_TRY(refresh_active_hi(c));
     int64_t done = 0;
     if (nsteps >= m->graph_steps) {
         if (m->cur != 0) {
@@ -649,6 +675,7 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
     DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_batch_run: nsteps < 0");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
+    DTB_TRY(refresh_active_hi(c));
     int64_t done = 0;
     if (!m->profiling && nsteps >= m->graph_steps) {
         if (m->cur != 0) {

@@ -31,6 +31,7 @@ struct GemmArgs {
     const float* isig2;
     float* partial;      // [n_splits][Bpad][M]
     int* err;
+    const int* active_hi;  // device: 1 + the highest slot that still steps (columns past it are skipped)
 };
 
 cudaError_t launch_gain_gemm(int bn, const CUtensorMap* tm_hi, const CUtensorMap* tm_lo, const GemmArgs& a,
@@ -82,8 +83,10 @@ struct MixedRowOps {
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out,
                               float* C_out, unsigned long long* gstep, unsigned* ticket, cudaStream_t s);
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
-                                const float* sig1, const float* sig2, float* gsum, cudaStream_t s);
+                                const float* sig1, const float* sig2, float* gsum, const int* active_hi,
+                                cudaStream_t s);
 int mixed_rows_tile_rows();
+cudaError_t prepare_mixed_rows();
 
 cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
                                  const double* w, double* out, cudaStream_t s);

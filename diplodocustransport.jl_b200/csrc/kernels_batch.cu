@@ -139,9 +139,12 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     const int T = a.n_cb * a.N1;
     const int t0 = split * a.tiles_per_split;
     const int t1 = min(T, t0 + a.tiles_per_split);
-    const int nt = t1 > t0 ? t1 - t0 : 0;
     const int m0 = m_tile * kMmaM, n0 = n_tile * BN;
     const int n2p = a.n_cb * kMmaK;
+    // columns of this tile that belong to slots still stepping, rounded up to the MMA's N granule
+    const int hi_cols = *reinterpret_cast<const volatile int*>(a.active_hi);
+    const int n_eff = max(0, min(BN, (hi_cols - n0 + 15) / 16 * 16));
+    const int nt = (n_eff > 0 && t1 > t0) ? t1 - t0 : 0;
 
     if (tid == 0) {
         for (int s = 0; s < C::SA; ++s) {
@@ -149,7 +152,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             mb_init(smem_addr(&empty_a[s]), 1);
         }
         for (int s = 0; s < C::SB; ++s) {
-            mb_init(smem_addr(&full_b[s]), BN);
+            mb_init(smem_addr(&full_b[s]), BN / 32);  // one arrive per producing warp
             mb_init(smem_addr(&empty_b[s]), 1);
         }
         mb_init(smem_addr(acc_bar), 1);
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     } else if (warp == C::NPW + 1) {
         // ---------------- MMA issuer
         if (lane == 0 && nt > 0) {
-            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_eff >> 3) << 17) |
                                    ((uint32_t)(kMmaM >> 4) << 24);
             int issued = 0;
             for (int j = 0; j < nt; ++j) {
@@ -238,7 +241,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
         const int p = tid;  // row of the B tile
         if (p < BN && nt > 0) {
             const int inst = n0 + p;
-            const bool valid = inst < a.Bcap;
+            const bool valid = inst < a.Bcap && p < n_eff;
             const float s1 = valid ? a.isig1[inst] : 0.f;
             const float s2 = valid ? a.isig2[inst] : 0.f;
             float f2r[kMmaK];
@@ -290,8 +293,11 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                     *reinterpret_cast<uint4*>(rhi + phys) = make_uint4(h[0], h[1], h[2], h[3]);
                     *reinterpret_cast<uint4*>(rlo + phys) = make_uint4(l[0], l[1], l[2], l[3]);
                 }
+                // make this thread's generic-proxy stores visible to the tensor core, then one
+                // arrive per warp once every lane has fenced
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mb_arrive(smem_addr(&full_b[sb]));
+                __syncwarp();
+                if (lane == 0) mb_arrive(smem_addr(&full_b[sb]));
             }
         }
         // epilogue: TMEM lanes 32*(warp%4).. hold rows m0 + 32*(warp%4) + lane
@@ -309,7 +315,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             float* dst = a.partial + (size_t)split * a.Bpad * a.M;
             for (int cc = 0; cc < ncol; cc += 16) {
                 float v[16];
-                if (nt > 0) {
+                if (nt > 0 && c0 + cc < n_eff) {
                     tmem_ld16(tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc), v);
                 } else {
 #pragma unroll
@@ -455,18 +461,20 @@ __device__ __forceinline__ unsigned long long ord_enc(double x) {
     return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
 
-constexpr int kRT = 32;  // rows per tile
-constexpr int kIT = 32;  // instances per tile
-constexpr int kCK = 32;  // K chunk of the loss / emission tile products
+constexpr int kRT = 32;   // rows per tile
+constexpr int kIT = 32;   // instances per tile
+constexpr int kCK = 128;  // K chunk of the loss / emission tile products
+constexpr int kRowsSmem = (2 * kRT * (kCK + 1) + 2 * kCK * kIT) * 4;  // dynamic: two L and two F chunks
 
 // Sum of the split-K partial tiles of one gain group, scaled back to G and f units:
 // gsum[i][r] = row_scale[r] * sig1[i] * sig2[i] * sum_s partial[s][i][r]. Fixed summation order.
 __global__ void split_reduce_kernel(const float* __restrict__ partial, int n_splits, int Bpad, int M, int Bcap,
                                     const float* __restrict__ row_scale, const float* __restrict__ sig1,
-                                    const float* __restrict__ sig2, float* __restrict__ gsum) {
+                                    const float* __restrict__ sig2, float* __restrict__ gsum,
+                                    const int* __restrict__ active_hi) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
-    if (r >= M || i >= Bcap) return;
+    if (r >= M || i >= Bcap || i >= *active_hi) return;
     const float* p = partial + (size_t)i * M + r;
     const size_t stride = (size_t)Bpad * M;
     float acc = 0.f;
@@ -527,8 +535,9 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
                                                          float* __restrict__ Co, unsigned long long* gstep,
                                                          unsigned* ticket) {
     __shared__ float s_gain[kRT][kIT + 1];
-    __shared__ float s_L[2][kRT][kCK + 1];
-    __shared__ __align__(16) float s_F[2][kCK][kIT];
+    extern __shared__ __align__(16) float rows_dyn[];
+    float(*s_F)[kCK][kIT] = reinterpret_cast<float(*)[kCK][kIT]>(rows_dyn);
+    float(*s_L)[kRT][kCK + 1] = reinterpret_cast<float(*)[kRT][kCK + 1]>(rows_dyn + 2 * kCK * kIT);
     __shared__ double s_min[16][kIT];
     __shared__ int s_nonfin[kIT];
     __shared__ int s_last;
@@ -769,17 +778,23 @@ cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
                               unsigned long long* gstep, unsigned* ticket, cudaStream_t s) {
     dim3 grid((ops.n_mom + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
-    mixed_rows_kernel<<<grid, 256, 0, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
+    mixed_rows_kernel<<<grid, 256, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
     return cudaGetLastError();
 }
 
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
-                                const float* sig1, const float* sig2, float* gsum, cudaStream_t s) {
+                                const float* sig1, const float* sig2, float* gsum, const int* active_hi,
+                                cudaStream_t s) {
     dim3 grid((M + 255) / 256, Bcap);
-    split_reduce_kernel<<<grid, 256, 0, s>>>(partial, n_splits, Bpad, M, Bcap, row_scale, sig1, sig2, gsum);
+    split_reduce_kernel<<<grid, 256, 0, s>>>(partial, n_splits, Bpad, M, Bcap, row_scale, sig1, sig2, gsum,
+                                             active_hi);
     return cudaGetLastError();
 }
 
 int mixed_rows_tile_rows() { return kRT; }
+
+cudaError_t prepare_mixed_rows() {
+    return cudaFuncSetAttribute(mixed_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowsSmem);
+}
 
 }  // namespace dtb
