@@ -55,7 +55,7 @@ struct MixedState {
     int graph_steps = 16;
     std::vector<long long> h_stop, h_start;
     float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation
-    float* pin_all = nullptr;  // [2][n_mom][Bcap] staging of the whole batch
+    double* io_all = nullptr;  // device staging of the whole batch, f64 [Buser][n_mom]
     int* sp_off = nullptr;     // device species offsets
     double* mom_w = nullptr;   // device energy weights (n_mom)
     double* mom_out = nullptr; // device moments [Bcap][ns][2]
@@ -457,7 +457,6 @@ void destroy_mixed(dtb_ctx* c) {
     if (m->graph) cudaGraphExecDestroy(m->graph);
     for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
     if (m->pin_col) cudaFreeHost(m->pin_col);
-    if (m->pin_all) cudaFreeHost(m->pin_all);
     delete m;
     c->mixed = nullptr;
 }
@@ -749,22 +748,12 @@ int32_t dtb_batch_set_f_all(dtb_ctx* c, const double* f) {
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_set_f_all: null input");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
-    const int n = (int)c->n_mom, B = m->Bcap;
-    if (!m->pin_all) DTB_CUDA(cudaMallocHost(&m->pin_all, sizeof(float) * 2 * (size_t)n * B));
-    DTB_CUDA(cudaStreamSynchronize(c->stream));
-    float* hf = m->pin_all;
-    float* hc = m->pin_all + (size_t)n * B;
-    if (m->Buser < B) std::memset(m->pin_all, 0, sizeof(float) * 2 * (size_t)n * B);
-    for (int i = 0; i < m->Buser; ++i)
-        for (int a = 0; a < n; ++a) {
-            const double v = f[(size_t)i * n + a];
-            const float fv = (float)v;
-            hf[(size_t)a * B + i] = fv;
-            hc[(size_t)a * B + i] = (float)(v - (double)fv);
-        }
-    DTB_CUDA(cudaMemcpyAsync(m->F[m->cur], hf, sizeof(float) * (size_t)n * B, cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaMemcpyAsync(m->C[m->cur], hc, sizeof(float) * (size_t)n * B, cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    const int n = (int)c->n_mom;
+    const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
+    if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
+    DTB_CUDA(cudaMemcpyAsync(m->io_all, f, bytes, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(launch_pack_f(m->io_all, m->Buser, n, m->Bcap, m->F[m->cur], m->C[m->cur], c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));  // the caller may reuse f on return
     return DTB_OK;
 }
 
@@ -773,16 +762,12 @@ int32_t dtb_batch_get_f_all(dtb_ctx* c, double* f) {
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f_all: null output");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
-    const int n = (int)c->n_mom, B = m->Bcap;
-    if (!m->pin_all) DTB_CUDA(cudaMallocHost(&m->pin_all, sizeof(float) * 2 * (size_t)n * B));
-    float* hf = m->pin_all;
-    float* hc = m->pin_all + (size_t)n * B;
-    DTB_CUDA(cudaMemcpyAsync(hf, m->F[m->cur], sizeof(float) * (size_t)n * B, cudaMemcpyDeviceToHost, c->stream));
-    DTB_CUDA(cudaMemcpyAsync(hc, m->C[m->cur], sizeof(float) * (size_t)n * B, cudaMemcpyDeviceToHost, c->stream));
+    const int n = (int)c->n_mom;
+    const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
+    if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
+    DTB_CUDA(launch_unpack_f(m->F[m->cur], m->C[m->cur], m->Buser, n, m->Bcap, m->io_all, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(f, m->io_all, bytes, cudaMemcpyDeviceToHost, c->stream));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
-    for (int a = 0; a < n; ++a)
-        for (int i = 0; i < m->Buser; ++i)
-            f[(size_t)i * n + a] = (double)hf[(size_t)a * B + i] + (double)hc[(size_t)a * B + i];
     return DTB_OK;
 }
 

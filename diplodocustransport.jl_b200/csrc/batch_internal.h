@@ -82,6 +82,8 @@ struct MixedRowOps {
 
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out,
                               float* C_out, unsigned long long* gstep, unsigned* ticket, cudaStream_t s);
+cudaError_t launch_pack_f(const double* io, int Buser, int n, int Bcap, float* F, float* C, cudaStream_t s);
+cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, int Bcap, double* io, cudaStream_t s);
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
                                 const float* sig1, const float* sig2, float* gsum, const int* active_hi,
                                 cudaStream_t s);

@@ -769,6 +769,57 @@ __global__ void batch_moments_kernel(const float* __restrict__ F, const float* _
     }
 }
 
+// Whole-batch state I/O: the user's slot-major f64 [Buser][n] <-> the slot-minor FP32 pair
+// (F, C) [n][Bcap], F = fl32(v), C = fl32(v - F), through 32 x 32 shared-memory transposes so
+// both sides are coalesced. Padding slots [Buser, Bcap) are written as zeros.
+__global__ void __launch_bounds__(256) pack_f_kernel(const double* __restrict__ io, int Buser, int n, int Bcap,
+                                                     float* __restrict__ F, float* __restrict__ C) {
+    __shared__ double t[32][33];
+    const int a0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = ty; k < 32; k += 8) {
+        const int i = i0 + k, a = a0 + tx;
+        t[k][tx] = (i < Buser && a < n) ? io[(size_t)i * n + a] : 0.0;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int a = a0 + k, i = i0 + tx;
+        if (a < n && i < Bcap) {
+            const double v = t[tx][k];
+            const float fv = __double2float_rn(v);
+            F[(size_t)a * Bcap + i] = fv;
+            C[(size_t)a * Bcap + i] = __double2float_rn(__dsub_rn(v, (double)fv));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) unpack_f_kernel(const float* __restrict__ F, const float* __restrict__ C,
+                                                       int Buser, int n, int Bcap, double* __restrict__ io) {
+    __shared__ double t[32][33];
+    const int a0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = ty; k < 32; k += 8) {
+        const int a = a0 + k, i = i0 + tx;
+        t[k][tx] = (a < n && i < Buser) ? __dadd_rn((double)F[(size_t)a * Bcap + i], (double)C[(size_t)a * Bcap + i])
+                                        : 0.0;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int i = i0 + k, a = a0 + tx;
+        if (i < Buser && a < n) io[(size_t)i * n + a] = t[tx][k];
+    }
+}
+
+cudaError_t launch_pack_f(const double* io, int Buser, int n, int Bcap, float* F, float* C, cudaStream_t s) {
+    pack_f_kernel<<<dim3((n + 31) / 32, (Bcap + 31) / 32), 256, 0, s>>>(io, Buser, n, Bcap, F, C);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, int Bcap, double* io, cudaStream_t s) {
+    unpack_f_kernel<<<dim3((n + 31) / 32, (Buser + 31) / 32), 256, 0, s>>>(F, C, Buser, n, Bcap, io);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
                                  const double* w, double* out, cudaStream_t s) {
     batch_moments_kernel<<<dim3(n_species, Bcap), 128, 0, s>>>(F, C, Bcap, sp_off, n_species, w, out);

@@ -169,3 +169,55 @@ def test_config3_full_size_moments(cuda):
             assert en1[i, s] == pytest.approx((f * wts)[s * ns:(s + 1) * ns].sum(), rel=1e-12)
     assert np.all(np.isfinite(num1)) and np.all(num1 > 0)
     m.close()
+
+
+def test_whole_batch_state_io(cuda):
+    """set_f_all / get_f_all move the slot-major FP64 batch through the device transpose: the
+    round trip keeps the FP32 hi+lo pair's precision, equals the per-slot reads, and a run
+    after set_f_all steps from the uploaded state (37 slots: the capacity pads to 40)."""
+    B = 37
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, B, seed=9)
+    n = w.ps.n_state
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    for i in range(B):
+        m.admit(i, w.f0[i], w.dt[i], 10)
+    rng = np.random.default_rng(3)
+    F = rng.lognormal(-2.0, 3.0, size=(B, n))
+    m.set_f_all(F)
+    G = m.get_f_all()
+    assert G.shape == (B, n)
+    assert float(np.max(np.abs(G - F) / F)) <= 2.0 ** -45
+    for i in (0, 17, B - 1):
+        np.testing.assert_array_equal(m.get_f(i), G[i])
+    m.set_f_all(w.f0)
+    m.run(10)
+    G = m.get_f_all()
+    ops = oracle.blocked_from_workload(w)
+    for i in (0, B - 1):
+        f = w.f0[i].copy()
+        for _ in range(10):
+            f, _, _ = ops.step(f, w.dt[i], 0)
+        assert rel_linf(G[i], f) <= TOL_RUN, i
+        np.testing.assert_array_equal(m.get_f(i), G[i])
+    m.close()
+
+
+def test_gemm_columns_follow_the_last_running_slot(cuda):
+    """The gain GEMM computes only up to the last running slot (rounded to 16 columns): a slot
+    alone at index 3 or 200 of 256, and the same slot with every slot running, give the same
+    f; finished slots keep their state while a higher slot runs on."""
+    B = 256
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, B, seed=12)
+    full = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    for i in range(B):
+        full.admit(i, w.f0[i], w.dt[i], 30)
+    full.run(30)
+    for slot in (3, 200):
+        one = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+        one.admit(slot, w.f0[slot], w.dt[slot], 30)
+        one.admit(0, w.f0[0], w.dt[0], 5)
+        one.run(30)
+        np.testing.assert_array_equal(one.get_f(slot), full.get_f(slot))
+        assert one.info(0)["steps_done"] == 5
+        one.close()
+    full.close()
