@@ -97,6 +97,10 @@ struct dtb_ctx {
     void* dfm_buf = nullptr;             // df_Momentum of the symplectic step
     std::vector<double> Ap, Vol, f_init, inj;
     bool have_vectors = false;
+    bool has_bin_domain = false;         // BinM.Domain !== nothing
+    std::vector<int64_t> bin_domain;     // its off_space entries
+    int n_bin_cells = 0;                 // cells the gain kernel runs (domain cells, or all)
+    int* bin_cells = nullptr;            // device list of those cells (null: 0..n_space-1)
     bool committed = false;
 
     // device memory

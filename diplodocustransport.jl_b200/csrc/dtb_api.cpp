@@ -320,6 +320,19 @@ int32_t dtb_upload_vectors(dtb_ctx* c, const double* Ap, const double* Vol, cons
     return DTB_OK;
 }
 
+int32_t dtb_set_bin_domain(dtb_ctx* c, const int64_t* off_space, int64_t n) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_set_bin_domain: null context");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_set_bin_domain: operators already committed");
+    if (!off_space || n < 0) {
+        c->has_bin_domain = false;
+        c->bin_domain.clear();
+        return DTB_OK;
+    }
+    c->has_bin_domain = true;
+    c->bin_domain.assign(off_space, off_space + n);
+    return DTB_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------ commit
@@ -603,6 +616,25 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     ops.n_units = c->n_units;
     ops.partial = c->partial;
     ops.thr = c->prec == DTB_F64 ? (double)1e-10f : (double)(T)1e-10f;
+    // binary domain: `in(off_space, Domain)` per cell (entries outside 0..n_space-1 match no cell)
+    ops.bin_on = nullptr;
+    c->n_bin_cells = c->n_space;
+    c->bin_cells = nullptr;
+    if (c->has_bin_domain) {
+        std::vector<int> on((size_t)c->n_space, 0), list;
+        for (int64_t k : c->bin_domain)
+            if (k >= 0 && k < c->n_space) on[(size_t)k] = 1;
+        for (int k = 0; k < c->n_space; ++k)
+            if (on[(size_t)k]) list.push_back(k);
+        std::vector<unsigned char> on8(on.begin(), on.end());
+        unsigned char* d_on;
+        DTB_TRY(c->alloc(&d_on, on8.size()));
+        DTB_CUDA(cudaMemcpyAsync(d_on, on8.data(), on8.size(), cudaMemcpyHostToDevice, c->stream));
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+        ops.bin_on = d_on;
+        c->n_bin_cells = (int)list.size();
+        if (!list.empty()) DTB_TRY(copy_host_ints(c, &c->bin_cells, list));
+    }
     ops.has_bin = c->has_bin;
     ops.has_emi = c->has_emi;
     return DTB_OK;
@@ -682,7 +714,7 @@ template <typename T>
 static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, int verbose, bool profile) {
     T* fin = reinterpret_cast<T*>(c->f_buf[c->cur]);
     T* fout = reinterpret_cast<T*>(c->f_buf[c->cur ^ 1]);
-    if (c->n_units > 0) {
+    if (c->n_units > 0 && c->n_bin_cells > 0) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile) {
             const size_t k = (size_t)c->prof_pending * 2;
@@ -696,8 +728,8 @@ static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, 
             DTB_CUDA(cudaEventRecord(e0, c->stream));
         }
         DTB_CUDA(launch_gain_stream<T>(reinterpret_cast<const T*>(c->G_all), c->units, c->n_units, fin, (int)c->n_mom,
-                                       c->sp_off_host, c->ns, c->f_smem_len, c->partial, c->n_space, c->gain_grid,
-                                       c->err, c->stream));
+                                       c->sp_off_host, c->ns, c->f_smem_len, c->partial, c->n_bin_cells,
+                                       c->gain_grid, c->err, c->stream, c->bin_cells));
         if (profile) {
             DTB_CUDA(cudaEventRecord(e1, c->stream));
             c->prof_n++;
@@ -1070,7 +1102,7 @@ int32_t dtb_selftest_bounded_wait(dtb_ctx* c, double limit_s) {
 int32_t dtb_gain_kernel_stats(dtb_ctx* c, double* avg_ms, double* bytes_per_launch) {
     DTB_CHECK(c, DTB_EINVAL, "dtb_gain_kernel_stats: null context");
     DTB_TRY(dtb_commit(c));
-    if (bytes_per_launch) *bytes_per_launch = c->gain_bytes * c->n_space;
+    if (bytes_per_launch) *bytes_per_launch = c->gain_bytes * c->n_bin_cells;
     if (avg_ms) *avg_ms = c->prof_n ? c->prof_ms / (double)c->prof_n : 0.0;
     return DTB_OK;
 }

@@ -76,6 +76,7 @@ struct RowOps {
     const int* unit_ptr;
     int n_units;
     const double* partial;                 // [n_space][n_units]
+    const unsigned char* bin_on;           // per cell: binary term applied (BinM.Domain); null = all
     // vectors
     const T* invAp;
     const T* inj;
@@ -96,7 +97,8 @@ struct RowOps {
 template <typename T>
 cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, const T* f,
                                int n_mom, const int* sp_offp_dev, int n_species, int f_smem_len,
-                               double* partial, int n_space, int grid_x, int* err, cudaStream_t s);
+                               double* partial, int n_space, int grid_x, int* err, cudaStream_t s,
+                               const int* cell_list = nullptr);
 
 template <typename T>
 cudaError_t launch_euler_rows(const RowOps<T>& ops, const T* f_in, T* f_out, double dt_imm,

@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(kGainThreads) gain_stream_kernel(const T* __re
                                                                    const GainUnit* __restrict__ units,
                                                                    int n_units, const T* __restrict__ f,
                                                                    int n_mom, SpOff so, int f_len,
-                                                                   double* __restrict__ partial, int* err) {
+                                                                   double* __restrict__ partial, int* err,
+                                                                   const int* __restrict__ cell_list) {
     using V = Vec<T>;
     using vec_t = typename V::type;
     constexpr int kTileElems = kGainTileBytes / sizeof(T);
@@ -145,7 +146,8 @@ __global__ void __launch_bounds__(kGainThreads) gain_stream_kernel(const T* __re
     volatile int* abort_flag = reinterpret_cast<volatile int*>(red + kRedRing * kGainConsumerWarps);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cell = blockIdx.y;
+    // the cells of the binary domain, or every cell when there is no list
+    const int cell = cell_list ? cell_list[blockIdx.y] : (int)blockIdx.y;
 
     if (tid == 0) {
         for (int s = 0; s < kGainStages; ++s) {
@@ -285,7 +287,8 @@ int gain_stream_blocks_per_sm(int elem_size, int f_smem_len) {
 template <typename T>
 cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, const T* f, int n_mom,
                                const int* sp_off_host, int n_species, int f_smem_len, double* partial,
-                               int n_space, int grid_x, int* err, cudaStream_t s) {
+                               int n_space, int grid_x, int* err, cudaStream_t s, const int* cell_list) {
+    // n_space: cells to run (grid y); cell_list maps them to cells, or null for 0..n_space-1
     // sp_off_host: [0..n_species] unpadded then [0..n_species] padded offsets (host array)
     SpOff so;
     so.n = n_species;
@@ -297,14 +300,16 @@ cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, c
     const int smem = gain_stream_smem_bytes(sizeof(T), f_smem_len);
     dim3 grid(grid_x, n_space);
     gain_stream_kernel<T><<<grid, kGainThreads, smem, s>>>(G, units, n_units, f, n_mom, so, f_smem_len, partial,
-                                                           err);
+                                                           err, cell_list);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_gain_stream<double>(const double*, const GainUnit*, int, const double*, int,
-                                                const int*, int, int, double*, int, int, int*, cudaStream_t);
+                                                const int*, int, int, double*, int, int, int*, cudaStream_t,
+                                                const int*);
 template cudaError_t launch_gain_stream<float>(const float*, const GainUnit*, int, const float*, int,
-                                               const int*, int, int, double*, int, int, int*, cudaStream_t);
+                                               const int*, int, int, double*, int, int, int*, cudaStream_t,
+                                               const int*);
 
 // ------------------------------------------------------------------ euler_rows
 constexpr int kRedFields = 7;  // min cr, cr_bin, cr_emi, cr_flux, sum_df, sum_f, nonfinite count
@@ -369,7 +374,9 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         }
         // loss bilinear term and gain partials
         double loss = 0.0, gain = 0.0;
-        if (ops.has_bin) {
+        // binary term of this cell (SteppingMethods.jl:369): outside BinM.Domain it is zero
+        const bool bin_here = ops.has_bin && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
+        if (bin_here) {
             const int la = a - ops.sp_off[s];
             for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
                 const T* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
@@ -390,7 +397,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
             const T fa = fc[a];
             T df = -(T)flux;
             if (ops.has_emi) df = df + (T)emi;
-            if (ops.has_bin) df = df + (T)((double)ops.vol[cell] * (gain - (double)fa * loss));
+            if (ops.has_bin) df = df + (bin_here ? (T)((double)ops.vol[cell] * (gain - (double)fa * loss)) : T(0));
             df = (T)((double)df * ((double)ops.invAp[i] * dt_scale));
             T fm = fa + df;
             fm = jl_mul_bool(fm, fm >= (T)ops.thr_mom);
@@ -401,7 +408,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
             const T fa = fc[a];
             const T dflux = (T)flux;
             const T demi = (T)emi;
-            const T dbin = (T)((double)ops.vol[cell] * (gain - (double)fa * loss));
+            const T dbin = bin_here ? (T)((double)ops.vol[cell] * (gain - (double)fa * loss)) : T(0);
             // SteppingMethods.jl:31-46
             T df = -dflux;
             if (ops.has_emi) df = df + demi;

@@ -124,6 +124,9 @@ class ForwardEulerStruct:
             for l in BinM.losses:
                 A = np.ascontiguousarray(l.L, dtype=np.float64)
                 check(L.dtb_add_loss_block(ctx, l.sp, l.other_sp, dptr(A)))
+            if BinM.Domain is not None:
+                D = np.ascontiguousarray(BinM.Domain, dtype=np.int64)
+                check(L.dtb_set_bin_domain(ctx, D.ctypes.data_as(_lib._ip), len(D)))
             if EmiM.M_Emi is not None:
                 M = np.asfortranarray(EmiM.M_Emi, dtype=np.float64)
                 check(L.dtb_upload_emi_ref(ctx, M.ctypes.data_as(_lib._dp), self.n))

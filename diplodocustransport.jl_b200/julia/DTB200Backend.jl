@@ -112,6 +112,11 @@ mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
             M = Matrix{Float64}(BinM.M_Bin)
             GC.@preserve M check(ccall((:dtb_upload_mbin_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
                                        ctx[], M, n_mom))
+            if !isnothing(BinM.Domain)   # Bin_Domain (SteppingStructs.jl:51, SteppingMethods.jl:369)
+                D = Vector{Int64}(BinM.Domain)
+                GC.@preserve D check(ccall((:dtb_set_bin_domain, libdtb), Int32, (Ptr{Cvoid}, Ptr{Int64}, Int64),
+                                           ctx[], D, length(D)))
+            end
         end
         if !isempty(EmiM.Emission_list)
             E = Matrix{Float64}(EmiM.M_Emi)

@@ -135,6 +135,12 @@ int32_t dtb_add_emi_block(dtb_ctx* ctx, int64_t row0, int64_t nrows, int64_t col
 int32_t dtb_upload_vectors(dtb_ctx* ctx, const double* Ap, const double* Vol,
                            const double* f_init, const double* inj);
 
+/* BinM.Domain (StructsAndDictionaries.jl:320, read at SteppingMethods.jl:355-369): the binary
+ * term is applied only in the space cells whose 0-based off_space is listed; n < 0 or a NULL
+ * list means `nothing` (every cell). Cells outside the domain get a zero binary term, which is
+ * what the reference's skipped cells hold for a finite M_Bin. Before dtb_commit. */
+int32_t dtb_set_bin_domain(dtb_ctx* ctx, const int64_t* off_space, int64_t n);
+
 /* Builds the device layouts. Called implicitly by the first step; calling it early moves
  * the upload cost out of the first step. */
 int32_t dtb_commit(dtb_ctx* ctx);

@@ -26,6 +26,7 @@ THR_F64 = float(np.float32(1e-10))  # Float64(1f-10): SteppingMethods.jl:99 comp
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int64)
+_bp = ctypes.POINTER(ctypes.c_uint8)
 
 
 class GainT(ctypes.Structure):
@@ -58,18 +59,18 @@ def lib():
         L.orc_step_ref.restype = ctypes.c_int
         L.orc_step_ref.argtypes = [ctypes.c_int64, ctypes.c_int64, _dp, _dp, _ip, _ip, _dp, ctypes.c_int,
                                    _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
-                                   _dp, _dp, _dp]
+                                   _dp, _dp, _dp, _bp]
         L.orc_step_blocked.restype = ctypes.c_int
         L.orc_step_blocked.argtypes = [ctypes.c_int32, _ip, ctypes.c_int64,
                                        ctypes.c_int, ctypes.POINTER(GainT), ctypes.c_int,
                                        ctypes.POINTER(LossT), ctypes.c_int, ctypes.POINTER(EmiT),
                                        _ip, _ip, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
-                                       ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+                                       ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _bp]
         L.orc_step_symplectic_ref.restype = ctypes.c_int
         L.orc_step_symplectic_ref.argtypes = [ctypes.c_int64, ctypes.c_int64, _dp, _dp,
                                               _ip, _ip, _dp, _ip, _ip, _dp, ctypes.c_int,
                                               _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
-                                              ctypes.c_double, ctypes.c_int, _dp, _dp]
+                                              ctypes.c_double, ctypes.c_int, _dp, _dp, _bp]
         L.orc_gain_rows.restype = None
         L.orc_gain_rows.argtypes = [_dp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                     _dp, _dp, _dp]
@@ -104,11 +105,31 @@ def _csc_arrays(F):
             np.ascontiguousarray(F.data, dtype=np.float64))
 
 
-class RefOperands:
-    """Reference-layout operands: M_Bin (n_mom^2 x n_mom, F-order), M_Emi (n x n, F-order), CSC F."""
+def domain_mask(domain, n_space: int):
+    """Bin_Domain (a list of 0-based off_space indices, or None for `nothing`) as one byte per
+    cell, or None."""
+    if domain is None:
+        return None
+    m = np.zeros(n_space, dtype=np.uint8)
+    for k in domain:
+        if 0 <= int(k) < n_space:
+            m[int(k)] = 1
+    return m
 
-    def __init__(self, n_mom: int, n_space: int, M_Bin, M_Emi, F, invAp, Vol, inj):
+
+def _b(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_bp)
+
+
+class RefOperands:
+    """Reference-layout operands: M_Bin (n_mom^2 x n_mom, F-order), M_Emi (n x n, F-order), CSC F;
+    ``domain`` is BinM.Domain (0-based off_space indices, or None)."""
+
+    def __init__(self, n_mom: int, n_space: int, M_Bin, M_Emi, F, invAp, Vol, inj, domain=None):
         self.n_mom, self.n_space = n_mom, n_space
+        self.dom = domain_mask(domain, n_space)
         self.M_Bin = None if M_Bin is None else np.asfortranarray(M_Bin, dtype=np.float64)
         self.M_Emi = None if M_Emi is None else np.asfortranarray(M_Emi, dtype=np.float64)
         self.colptr, self.rowval, self.nzval = _csc_arrays(F)
@@ -123,7 +144,7 @@ class RefOperands:
         rc = lib().orc_step_ref(self.n_mom, self.n_space, _d(self.M_Bin), _d(self.M_Emi),
                                 _i(self.colptr), _i(self.rowval), _d(self.nzval), 0,
                                 _d(self.invAp), _d(self.Vol), _d(self.inj), float(dt_scale), float(thr),
-                                int(verbose), _d(f), _d(diag), _d(df))
+                                int(verbose), _d(f), _d(diag), _d(df), _b(self.dom))
         assert rc == 0
         return f, diag, df
 
@@ -131,9 +152,11 @@ class RefOperands:
 class BlockedOperands:
     """Blocked operands (gain/loss/emission blocks); G, L, E are cast to FP64 once."""
 
-    def __init__(self, sp_size: Sequence[int], n_space: int, gains, losses, emis, F, invAp, Vol, inj):
+    def __init__(self, sp_size: Sequence[int], n_space: int, gains, losses, emis, F, invAp, Vol, inj,
+                 domain=None):
         self.sp_size = np.ascontiguousarray(sp_size, dtype=np.int64)
         self.n_space = n_space
+        self.dom = domain_mask(domain, n_space)
         self._keep = []
         self.gains = (GainT * max(1, len(gains)))()
         for i, g in enumerate(gains):
@@ -166,7 +189,8 @@ class BlockedOperands:
                                     self.n_gain, self.gains, self.n_loss, self.losses,
                                     self.n_emi, self.emis, _i(self.colptr), _i(self.rowval),
                                     _d(self.nzval), 0, _d(self.invAp), _d(self.Vol), _d(self.inj),
-                                    float(dt_scale), float(thr), int(verbose), _d(f), _d(diag), _d(df))
+                                    float(dt_scale), float(thr), int(verbose), _d(f), _d(diag), _d(df),
+                                    _b(self.dom))
         assert rc == 0
         return f, diag, df
 
@@ -174,7 +198,7 @@ class BlockedOperands:
 def blocked_from_workload(w) -> BlockedOperands:
     return BlockedOperands(w.ps.species_sizes, w.ps.n_space, w.binm.gains, w.binm.losses,
                            w.emim.blocks, w.fluxm.F_Flux, 1.0 / np.asarray(w.fluxm.Ap_Flux),
-                           w.fluxm.Vol, w.inj)
+                           w.fluxm.Vol, w.inj, domain=getattr(w.binm, "Domain", None))
 
 
 def ref_from_workload(w) -> RefOperands:
@@ -182,7 +206,8 @@ def ref_from_workload(w) -> RefOperands:
     M_Bin = w.binm.M_Bin if w.binm.M_Bin is not None else (
         blocked_to_ref(w.ps, w.binm) if w.binm.has_interactions else None)
     return RefOperands(w.ps.n_momentum, w.ps.n_space, M_Bin, emission_to_dense(w.ps, w.emim),
-                       w.fluxm.F_Flux, 1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj)
+                       w.fluxm.F_Flux, 1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj,
+                       domain=getattr(w.binm, "Domain", None))
 
 
 def gain_rows(G: np.ndarray, r0: int, r1: int, f1: np.ndarray, f2: np.ndarray) -> np.ndarray:

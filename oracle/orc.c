@@ -135,6 +135,18 @@ static void cfl_diag(int64_t n, int verbose, int has_bin, int has_emi,
     diag[0] = -m;
 }
 
+/* update_Big_Bin! skips a space cell (SteppingMethods.jl:369) unless the binary domain is
+ * `nothing` (dom == NULL), the cell's off_space is in the domain, or the cell's f has no
+ * nonzero entry (findfirst(!iszero, fView) === nothing; NaN counts as nonzero). A skipped
+ * cell keeps df_Bin from its last evaluation, which for a finite M_Bin is the all-zero f
+ * result: zeros. dom: one byte per cell, nonzero = in the domain. */
+static int bin_cell_on(const uint8_t* dom, int64_t cell, const double* fv, int64_t n_mom) {
+    if (!dom || dom[cell]) return 1;
+    for (int64_t k = 0; k < n_mom; ++k)
+        if (fv[k] != 0.0) return 0;
+    return 1;
+}
+
 /*
  * One ForwardEuler step in the reference layout (SteppingMethods.jl:12-107).
  *   M_Bin: (n_mom^2) x n_mom column-major, or NULL (no binary interactions)
@@ -144,11 +156,12 @@ static void cfl_diag(int64_t n, int verbose, int has_bin, int has_emi,
  *   thr: clamp threshold ((double)1e-10f for a Float64 state)
  *   f: state, updated in place; diag: 8 doubles (see cfl_diag)
  *   df_out: optional, receives the scaled df (length n)
+ *   bin_dom: NULL (Bin_Domain === nothing) or one byte per cell (see bin_cell_on)
  */
 int orc_step_ref(int64_t n_mom, int64_t n_space, const double* M_Bin, const double* M_Emi,
                  const int64_t* colptr, const int64_t* rowval, const double* nzval, int base,
                  const double* invAp, const double* Vol, const double* inj, double dt_scale,
-                 double thr, int verbose, double* f, double* diag, double* df_out) {
+                 double thr, int verbose, double* f, double* diag, double* df_out, const uint8_t* bin_dom) {
     int64_t n = n_mom * n_space;
     double* buf = (double*)malloc(sizeof(double) * (size_t)(4 * n + n_mom * n_mom));
     if (!buf) return ORC_ENOMEM;
@@ -170,6 +183,7 @@ int orc_step_ref(int64_t n_mom, int64_t n_space, const double* M_Bin, const doub
         for (int64_t cell = 0; cell < n_space; ++cell) {
             const double* fv = f + cell * n_mom;
             double* dv = df_bin + cell * n_mom;
+            if (!bin_cell_on(bin_dom, cell, fv, n_mom)) continue; /* :369 */
             gemv_colmajor(n_mom * n_mom, n_mom, M_Bin, fv, S); /* :372 */
             gemv_colmajor(n_mom, n_mom, S, fv, dv);             /* :373 */
             for (int64_t a = 0; a < n_mom; ++a) dv[a] *= Vol[cell]; /* :380 */
@@ -259,7 +273,8 @@ int orc_step_blocked(int32_t n_species, const int64_t* sp_size, int64_t n_space,
                      int n_emi, const orc_emi_t* emis,
                      const int64_t* colptr, const int64_t* rowval, const double* nzval, int base,
                      const double* invAp, const double* Vol, const double* inj, double dt_scale,
-                     double thr, int verbose, double* f, double* diag, double* df_out) {
+                     double thr, int verbose, double* f, double* diag, double* df_out,
+                     const uint8_t* bin_dom) {
     int64_t sp_off[64];
     if (n_species > 64) return ORC_EINVAL;
     int64_t n_mom = 0;
@@ -288,6 +303,7 @@ int orc_step_blocked(int32_t n_species, const int64_t* sp_size, int64_t n_space,
     int has_bin = (n_gain + n_loss) > 0;
     if (has_bin) {
         for (int64_t cell = 0; cell < n_space; ++cell) {
+            if (!bin_cell_on(bin_dom, cell, f + cell * n_mom, n_mom)) continue;
             blocked_bin_cell(n_species, sp_size, sp_off, n_gain, gains, n_loss, losses,
                              f + cell * n_mom, df_bin + cell * n_mom, n_mom);
             for (int64_t a = 0; a < n_mom; ++a) df_bin[cell * n_mom + a] *= Vol[cell];
@@ -314,7 +330,7 @@ int orc_step_symplectic_ref(int64_t n_mom, int64_t n_space, const double* M_Bin,
                             const int64_t* pcolptr, const int64_t* prowval, const double* pnzval,
                             int base, const double* invAp, const double* Vol, const double* inj,
                             double dt_scale, double thr_mom, double thr_space, int verbose,
-                            double* f, double* diag) {
+                            double* f, double* diag, const uint8_t* bin_dom) {
     int64_t n = n_mom * n_space;
     double* buf = (double*)malloc(sizeof(double) * (size_t)(8 * n + n_mom * n_mom));
     if (!buf) return ORC_ENOMEM;
@@ -334,6 +350,7 @@ int orc_step_symplectic_ref(int64_t n_mom, int64_t n_space, const double* M_Bin,
         for (int64_t cell = 0; cell < n_space; ++cell) {
             const double* fv = f + cell * n_mom;
             double* dv = dbin + cell * n_mom;
+            if (!bin_cell_on(bin_dom, cell, fv, n_mom)) continue;
             gemv_colmajor(n_mom * n_mom, n_mom, M_Bin, fv, S);
             gemv_colmajor(n_mom, n_mom, S, fv, dv);
             for (int64_t a = 0; a < n_mom; ++a) dv[a] *= Vol[cell];

@@ -31,7 +31,7 @@ def rel_linf(a, b):
 def make_method(w, precision=np.float64, ref_layout=False, **kw):
     binm, emim = w.binm, w.emim
     if ref_layout:
-        binm = BinaryMatrices(M_Bin=blocked_to_ref(w.ps, w.binm))
+        binm = BinaryMatrices(M_Bin=blocked_to_ref(w.ps, w.binm), Domain=w.binm.Domain)
         emim = EmissionMatrices(M_Emi=emission_to_dense(w.ps, w.emim))
     return ForwardEulerStruct(w.ps, w.f0, w.inj, binm, emim, w.fluxm, Precision=precision, **kw)
 
@@ -246,7 +246,7 @@ def test_symplectic_euler_matches_oracle(cuda, precision, tol):
                                        oracle._i(X[0]), oracle._i(X[1]), oracle._d(X[2]),
                                        oracle._i(P[0]), oracle._i(P[1]), oracle._d(P[2]), 0,
                                        oracle._d(r.invAp), oracle._d(r.Vol), oracle._d(r.inj), dt,
-                                       thr_m, thr_s, 1, oracle._d(f), oracle._d(d))
+                                       thr_m, thr_s, 1, oracle._d(f), oracle._d(d), oracle._b(r.dom))
         assert rc == 0
         assert m.last_diag.cr == pytest.approx(d[0], rel=1e-6 if precision == np.float32 else 1e-10)
     assert rel_linf(m.f, f) <= tol
@@ -265,3 +265,56 @@ def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
     f, _, _ = oracle.blocked_from_workload(w).step(w.f0, 1.0, 0)
     assert rel_linf(m.f, f) <= TOL64
     m.close()
+
+
+@pytest.mark.parametrize("precision,tol,domain", [(np.float64, TOL64, [0, 2]), (np.float32, TOL32, [1]),
+                                                  (np.float64, TOL64, []), (np.float64, TOL64, [2, 9, -1])])
+def test_bin_domain_matches_oracle(cuda, precision, tol, domain):
+    """BinM.Domain on 3 space cells: the gain kernel runs only the listed cells and the row
+    kernel adds a zero binary term elsewhere; 25 steps against the FP64 oracle with the same
+    domain, diagnostics included."""
+    w = synth.small(p_num=6, u_num=3, seed=23, n_space=3, randomize_vectors=True)
+    w.binm.Domain = domain
+    m = make_method(w, precision=precision)
+    ops = oracle.blocked_from_workload(w)
+    f = w.f0.copy()
+    for k in range(25):
+        _, _ = m(0.0, 1e9, 0.9 * m.dt0, 3)
+        f, diag, _ = ops.step(f, 0.9, 3, thr=oracle.THR_F64)
+        assert bool(m.last_diag.finite) == bool(diag[4])
+    assert m.last_diag.cr == pytest.approx(diag[0], rel=1e-6 if precision == np.float32 else 1e-10)
+    assert rel_linf(m.f, f) <= tol
+    m.close()
+
+
+def test_bin_domain_reference_layout_and_symplectic(cuda):
+    """The domain applies to a reference-layout M_Bin upload and to the symplectic step."""
+    from dtb.stepping import ForwardSymplecticEulerStruct
+    w = synth.small(p_num=5, u_num=2, seed=29, n_space=3, randomize_vectors=True)
+    w.binm.Domain = [1]
+    m = make_method(w, ref_layout=True)
+    r = oracle.ref_from_workload(w)
+    f = w.f0.copy()
+    for _ in range(20):
+        m(0.0, 1e9, 0.8 * m.dt0, 1)
+        f, _, _ = r.step(f, 0.8, 1)
+    assert rel_linf(m.f, f) <= TOL64
+    m.close()
+    w.fluxm.X_Flux = synth.space_flux(w.ps, np.random.default_rng(6), 1.0)
+    s = ForwardSymplecticEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, Precision=np.float64)
+    r = oracle.ref_from_workload(w)
+    X, P = (oracle._csc_arrays(M) for M in (w.fluxm.X_Flux, w.fluxm.P_Flux))
+    L = oracle.lib()
+    f = w.f0.copy()
+    d = np.zeros(8)
+    for _ in range(20):
+        s(0.0, 1e9, 0.8 * s.dt0, 1)
+        rc = L.orc_step_symplectic_ref(r.n_mom, r.n_space, oracle._d(r.M_Bin), oracle._d(r.M_Emi),
+                                       oracle._i(X[0]), oracle._i(X[1]), oracle._d(X[2]),
+                                       oracle._i(P[0]), oracle._i(P[1]), oracle._d(P[2]), 0,
+                                       oracle._d(r.invAp), oracle._d(r.Vol), oracle._d(r.inj), 0.8,
+                                       oracle.THR_F64, float(np.float32(1e-20)), 1, oracle._d(f), oracle._d(d),
+                                       oracle._b(r.dom))
+        assert rc == 0
+    assert rel_linf(s.f, f) <= TOL64
+    s.close()

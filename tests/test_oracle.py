@@ -148,7 +148,47 @@ def test_symplectic_reduces_to_euler_without_space_flux():
                                    oracle._i(zero), oracle._i(np.zeros(1, dtype=np.int64)), oracle._d(np.zeros(1)),
                                    oracle._i(r.colptr), oracle._i(r.rowval), oracle._d(r.nzval), 0,
                                    oracle._d(r.invAp), oracle._d(r.Vol), oracle._d(r.inj), 1.0,
-                                   oracle.THR_F64, float(np.float32(1e-20)), 1, oracle._d(fs), oracle._d(d))
+                                   oracle.THR_F64, float(np.float32(1e-20)), 1, oracle._d(fs), oracle._d(d),
+                                   oracle._b(r.dom))
     assert rc == 0
     fe, _, _ = r.step(f, 1.0)
     np.testing.assert_allclose(fs, fe, rtol=1e-14, atol=1e-300)
+
+
+def test_bin_domain_semantics():
+    """BinM.Domain (SteppingMethods.jl:355-369): the binary term acts only in listed cells; a
+    domain of every cell equals `nothing`; the blocked and reference layouts agree; a cell
+    outside the domain whose f is all zero is still evaluated (an Inf in M_Bin then makes
+    df non-finite there while the nonzero cells outside stay untouched)."""
+    from dtb.structs import BinaryMatrices
+    w = synth.small(p_num=5, u_num=3, seed=21, n_space=3, randomize_vectors=True)
+    n_mom = w.ps.n_momentum
+    f = w.f0.copy()
+    r_all = oracle.ref_from_workload(w)
+    w.binm.Domain = [0, 1, 2]
+    r_every = oracle.ref_from_workload(w)
+    np.testing.assert_array_equal(r_all.step(f, 0.8, 3)[0], r_every.step(f, 0.8, 3)[0])
+    w.binm.Domain = [1, 7, -2]  # entries that name no cell match nothing
+    r_dom = oracle.ref_from_workload(w)
+    b_dom = oracle.blocked_from_workload(w)
+    f_dom, d_dom, df_dom = r_dom.step(f, 0.8, 3)
+    fb, db, dfb = b_dom.step(f, 0.8, 3)
+    np.testing.assert_allclose(dfb, df_dom, rtol=1e-12, atol=1e-300)
+    w_nobin = synth.small(p_num=5, u_num=3, seed=21, n_space=3, randomize_vectors=True)
+    w_nobin.binm = BinaryMatrices()
+    _, _, df_nobin = oracle.ref_from_workload(w_nobin).step(f, 0.8, 3)
+    _, _, df_full = r_all.step(f, 0.8, 3)
+    cells = lambda v, k: v[k * n_mom:(k + 1) * n_mom]  # noqa: E731
+    for k in (0, 2):
+        np.testing.assert_array_equal(cells(df_dom, k), cells(df_nobin, k))
+    np.testing.assert_array_equal(cells(df_dom, 1), cells(df_full, 1))
+    # the all-zero exception
+    M = np.array(r_dom.M_Bin)
+    M[0, 0] = np.inf
+    f0 = f.copy()
+    f0[2 * n_mom:] = 0.0
+    rz = oracle.RefOperands(n_mom, 3, M, r_dom.M_Emi, w.fluxm.F_Flux, r_dom.invAp, r_dom.Vol, r_dom.inj,
+                            domain=[])
+    _, dz, dfz = rz.step(f0, 0.8, 1)
+    assert dz[4] == 0 and np.isnan(cells(dfz, 2)).any()
+    assert np.all(np.isfinite(cells(dfz, 0))) and np.all(np.isfinite(cells(dfz, 1)))
