@@ -1096,7 +1096,9 @@ int32_t dtb_selftest_bounded_wait(dtb_ctx* c, double limit_s) {
         }
         return DTB_OK;
     }
-    return check_kernel_err(c);
+    const int rc = check_kernel_err(c);
+    if (rc == DTB_ETIMEOUT) set_error("a bounded device wait gave up (self-test)");
+    return rc;
 }
 
 int32_t dtb_gain_kernel_stats(dtb_ctx* c, double* avg_ms, double* bytes_per_launch) {
