@@ -7,7 +7,6 @@
 // device step counter is below their stop step, so requests of different lengths share one
 // captured graph; a finished slot keeps its state until it is read and re-admitted.
 #include <cuda.h>
-#include <cudaTypedefs.h>
 
 #include <cstdio>
 #include <vector>
@@ -21,10 +20,8 @@ struct MixedGroup {
     int in1 = 0, in2 = 0;
     int M = 0, N1 = 0, n2 = 0, n2p = 0, n_cb = 0;
     std::vector<std::pair<int, int>> members;  // (output species, first stacked row)
-    __nv_bfloat16* hi = nullptr;
-    __nv_bfloat16* lo = nullptr;
+    unsigned char* gt = nullptr;  // G tiles [m_tiles][T][hi, lo][128 x 128 B], pre-swizzled
     float* row_scale = nullptr;
-    CUtensorMap tm_hi{}, tm_lo{};
     float* partial = nullptr;
     float* gsum = nullptr;  // [Bcap][M]
     int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256;
@@ -69,31 +66,6 @@ struct MixedState {
 }  // namespace dtb
 
 namespace {
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
-int make_map(CUtensorMap* tm, void* base, int64_t K, int64_t M) {
-    auto fn = encode_fn();
-    DTB_CHECK(fn, DTB_ECUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
-    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)M};
-    cuuint64_t strides[1] = {(cuuint64_t)K * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kMmaK, (cuuint32_t)kMmaM};
-    cuuint32_t es[2] = {1, 1};
-    CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    DTB_CHECK(r == CUDA_SUCCESS, DTB_ECUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
-    return DTB_OK;
-}
 
 unsigned long long ord_enc_host(double x) {
     unsigned long long u;
@@ -149,10 +121,11 @@ int commit_mixed(dtb_ctx* c) {
     for (auto& kv : c->gains) {
         GainStage& g = kv.second;
         MixedGroup& G = m->groups[(size_t)gidx[{g.in1, g.in2}]];
-        if (!G.hi) {
-            const size_t K = (size_t)G.N1 * G.n2p;
-            DTB_TRY(c->alloc(&G.hi, sizeof(__nv_bfloat16) * K * G.M));
-            DTB_TRY(c->alloc(&G.lo, sizeof(__nv_bfloat16) * K * G.M));
+        if (!G.gt) {
+            // whole m tiles, rows past M stay zero
+            const size_t bytes = (size_t)((G.M + kMmaM - 1) / kMmaM) * G.n_cb * G.N1 * kGTileBytes;
+            DTB_TRY(c->alloc(&G.gt, bytes));
+            DTB_CUDA(cudaMemsetAsync(G.gt, 0, bytes, s));
             DTB_TRY(c->alloc(&G.row_scale, sizeof(float) * G.M));
         }
         int roff = 0;
@@ -160,7 +133,6 @@ int commit_mixed(dtb_ctx* c) {
             if (mb.first == g.out) roff = mb.second;
         const int64_t no = c->sz[g.out];
         const size_t elems = (size_t)(no * G.N1 * G.n2);
-        const size_t K = (size_t)G.N1 * G.n2p;
         float* tmp = nullptr;
         const float* srcf = nullptr;
         if (!g.host.empty()) {
@@ -184,8 +156,7 @@ int commit_mixed(dtb_ctx* c) {
                 srcf = tmp;
             }
         }
-        DTB_CUDA(launch_split_rows(srcf, no, G.N1, G.n2, G.n2p, G.hi + (size_t)roff * K, G.lo + (size_t)roff * K,
-                                   G.row_scale + roff, nullptr, s));
+        DTB_CUDA(launch_split_rows(srcf, no, roff, G.N1, G.n2, G.n_cb, G.gt, G.row_scale + roff, s));
         DTB_CUDA(cudaStreamSynchronize(s));
         if (tmp) cudaFree(tmp);
         g.host.clear();
@@ -194,9 +165,6 @@ int commit_mixed(dtb_ctx* c) {
     DTB_CUDA(prepare_gain_gemm(bn));
     DTB_CUDA(prepare_mixed_rows());
     for (auto& G : m->groups) {
-        const int64_t K = (int64_t)G.N1 * G.n2p;
-        DTB_TRY(make_map(&G.tm_hi, G.hi, K, G.M));
-        DTB_TRY(make_map(&G.tm_lo, G.lo, K, G.M));
         G.bn = bn;
         G.n_tiles = (B + bn - 1) / bn;
         G.Bpad = G.n_tiles * bn;
@@ -492,6 +460,7 @@ int mixed_step(dtb_ctx* c, bool profile) {
     }
     for (auto& G : m->groups) {
         GemmArgs a;
+        a.gt = G.gt;
         a.M = G.M;
         a.N1 = G.N1;
         a.n2 = G.n2;
@@ -511,7 +480,7 @@ int mixed_step(dtb_ctx* c, bool profile) {
         a.partial = G.partial;
         a.err = c->err;
         a.active_hi = m->active_hi;
-        DTB_CUDA(launch_gain_gemm(G.bn, &G.tm_hi, &G.tm_lo, a, c->stream));
+        DTB_CUDA(launch_gain_gemm(G.bn, a, c->stream));
     }
     if (profile) {
         DTB_CUDA(cudaEventRecord(e1, c->stream));

@@ -17,6 +17,7 @@ constexpr int kMmaK = 64;   // K per stage: one 128-byte swizzle row of BF16
 // rows r of all gain blocks that share the input pair (in1, in2), with
 // X[b * n2p + c][i] = (f_in1[b][i] * isig1[i]) * (f_in2[c][i] * isig2[i]).
 struct GemmArgs {
+    const unsigned char* gt;  // G tiles [m_tiles][T][hi, lo][128 rows x 128 B], pre-swizzled (see split_rows)
     int M;          // stacked rows of the group
     int N1;         // states of input species 1
     int n2;         // states of input species 2 (unpadded)
@@ -34,8 +35,10 @@ struct GemmArgs {
     const int* active_hi;  // device: 1 + the highest slot that still steps (columns past it are skipped)
 };
 
-cudaError_t launch_gain_gemm(int bn, const CUtensorMap* tm_hi, const CUtensorMap* tm_lo, const GemmArgs& a,
-                             cudaStream_t s);
+cudaError_t launch_gain_gemm(int bn, const GemmArgs& a, cudaStream_t s);
+
+// Bytes of one K tile of one m tile of G: hi and lo halves of 128 rows x 64 BF16.
+constexpr int kGTileBytes = 2 * kMmaM * kMmaK * 2;
 int gain_gemm_smem_bytes(int bn);
 cudaError_t prepare_gain_gemm(int bn);
 
@@ -93,8 +96,8 @@ cudaError_t prepare_mixed_rows();
 cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
                                  const double* w, double* out, cudaStream_t s);
 
-cudaError_t launch_split_rows(const float* src, long long rows, int n1, int n2, int n2p, __nv_bfloat16* hi,
-                              __nv_bfloat16* lo, float* row_scale, int* err, cudaStream_t s);
+cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1, int n2, int n_cb,
+                              unsigned char* gt, float* row_scale, cudaStream_t s);
 cudaError_t launch_split_emi(const float* src, int rows, int ncols, int ld, __nv_bfloat162* dst, float* row_scale,
                              cudaStream_t s);
 

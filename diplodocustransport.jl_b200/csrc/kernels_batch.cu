@@ -55,11 +55,11 @@ __device__ __forceinline__ bool mb_wait(uint32_t bar, uint32_t parity, volatile 
         if (gtimer() - t0 > kWaitLimitNs) return false;
     }
 }
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, int x, int y, uint32_t bar) {
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
     asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
-            dst),
-        "l"(reinterpret_cast<uint64_t>(tm)), "r"(bar), "r"(x), "r"(y)
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
         : "memory");
 }
 // K-major operand tile in the canonical 128-byte swizzle layout: rows of 128 bytes, 8-row
@@ -115,7 +115,7 @@ struct GemmCfg {
 
 template <int BN>
 __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
-    gain_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, GemmArgs a) {
+    gain_gemm_kernel(GemmArgs a) {
     using C = GemmCfg<BN>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -140,7 +140,6 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     const int t0 = split * a.tiles_per_split;
     const int t1 = min(T, t0 + a.tiles_per_split);
     const int m0 = m_tile * kMmaM, n0 = n_tile * BN;
-    const int n2p = a.n_cb * kMmaK;
     // columns of this tile that belong to slots still stepping, rounded up to the MMA's N granule
     const int hi_cols = *reinterpret_cast<const volatile int*>(a.active_hi);
     const int n_eff = max(0, min(BN, (hi_cols - n0 + 15) / 16 * 16));
@@ -173,11 +172,12 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     const uint32_t tmem = *tmem_holder;
 
     if (warp == C::NPW) {
-        // ---------------- TMA producer of the G tiles
+        // ---------------- bulk-copy producer of the G tiles: the (m tile, K tile) pair is one
+        // contiguous, pre-swizzled 32 KB block (hi then lo), streamed in order
         if (lane == 0 && nt > 0) {
+            const unsigned char* src0 = a.gt + ((size_t)m_tile * T + t0) * kGTileBytes;
             int j = 0;
             for (; j < nt; ++j) {
-                const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
                 const int sa = j % C::SA;
                 const uint32_t ph = (j / C::SA) & 1u;
                 if (!mb_wait(smem_addr(&empty_a[sa]), ph ^ 1u, abort_flag)) {
@@ -186,9 +186,10 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                     break;
                 }
                 mb_expect_tx(smem_addr(&full_a[sa]), 2 * C::A_BYTES);
-                const int x = b * n2p + cb * kMmaK;
-                tma_load_2d(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), &tm_hi, x, m0, smem_addr(&full_a[sa]));
-                tma_load_2d(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), &tm_lo, x, m0, smem_addr(&full_a[sa]));
+                const unsigned char* src = src0 + (size_t)j * kGTileBytes;
+                bulk_load(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
+                bulk_load(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
+                          smem_addr(&full_a[sa]));
             }
             // drain: this block's own copies must land before it may exit
             for (int k = j > C::SA ? j - C::SA : 0; k < j; ++k) {
@@ -364,28 +365,31 @@ cudaError_t prepare_gain_gemm(int bn) {
 // The dynamic shared-memory limit is raised once per device by prepare_gain_gemm (commit time),
 // so launches stay legal inside a stream capture.
 template <int BN>
-static cudaError_t launch_gemm_bn(const CUtensorMap* hi, const CUtensorMap* lo, const GemmArgs& a, cudaStream_t s) {
+static cudaError_t launch_gemm_bn(const GemmArgs& a, cudaStream_t s) {
     using C = GemmCfg<BN>;
     const int grid = a.m_tiles * a.n_tiles * a.n_splits;
-    gain_gemm_kernel<BN><<<grid, C::THREADS, C::SMEM, s>>>(*hi, *lo, a);
+    gain_gemm_kernel<BN><<<grid, C::THREADS, C::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_gain_gemm(int bn, const CUtensorMap* tm_hi, const CUtensorMap* tm_lo, const GemmArgs& a,
-                             cudaStream_t s) {
+cudaError_t launch_gain_gemm(int bn, const GemmArgs& a, cudaStream_t s) {
     switch (bn) {
-        case 64: return launch_gemm_bn<64>(tm_hi, tm_lo, a, s);
-        case 128: return launch_gemm_bn<128>(tm_hi, tm_lo, a, s);
-        case 256: return launch_gemm_bn<256>(tm_hi, tm_lo, a, s);
+        case 64: return launch_gemm_bn<64>(a, s);
+        case 128: return launch_gemm_bn<128>(a, s);
+        case 256: return launch_gemm_bn<256>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 // ------------------------------------------------------------------ operand preparation
 // One block per row: scale = 2^floor(log2(max |g|)) (1 for an all-zero row), then
-// hi = bf16(g / scale), lo = bf16(g / scale - hi), written into K-padded rows.
-__global__ void split_rows_kernel(const float* __restrict__ src, int n1, int n2, int n2p, __nv_bfloat16* hi,
-                                  __nv_bfloat16* lo, float* row_scale) {
+// hi = bf16(g / scale), lo = bf16(g / scale - hi), written into the GEMM's tile-blocked layout:
+// K tile t = cb * n1 + b holds G[r][b][64 cb .. 64 cb + 63] (zero past n2); tile (m, t) is
+// 32 KB at ((m * T + t) * 2 + half) * 16 KB, row r % 128 at 128-byte pitch, and its 16-byte
+// chunk q (elements 8q .. 8q + 7) stored at chunk q ^ (r % 8): the 128-byte swizzle that the
+// UMMA descriptor expects of a 1024-byte aligned stage, so a flat bulk copy lands it ready.
+__global__ void split_rows_kernel(const float* __restrict__ src, int row0, int n1, int n2, int n_cb,
+                                  unsigned char* __restrict__ gt, float* row_scale) {
     __shared__ float s_max[256];
     const long long r = blockIdx.x;
     const float* g = src + (size_t)r * n1 * n2;
@@ -403,22 +407,41 @@ __global__ void split_rows_kernel(const float* __restrict__ src, int n1, int n2,
     const float scale = ldexpf(1.f, ex - 1);         // mx / scale in [1, 2)
     const float inv = ldexpf(1.f, 1 - ex);
     if (threadIdx.x == 0) row_scale[r] = scale;
-    __nv_bfloat16* dh = hi + (size_t)r * n1 * n2p;
-    __nv_bfloat16* dl = lo + (size_t)r * n1 * n2p;
-    for (long long k = threadIdx.x; k < (long long)n1 * n2p; k += blockDim.x) {
-        const long long b = k / n2p;
-        const int c = (int)(k - b * n2p);
-        const float v = c < n2 ? g[b * n2 + c] * inv : 0.f;
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        dh[k] = h;
-        dl[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+    const long long gr = row0 + r;  // stacked row of the group
+    const long long T = (long long)n_cb * n1;
+    const int rt = (int)(gr % kMmaM);
+    unsigned char* rowbase = gt + (size_t)(gr / kMmaM) * T * kGTileBytes + (size_t)rt * 128;
+    // one 16-byte chunk (8 elements) of hi and of lo per thread and iteration
+    const long long chunks = (long long)n1 * n_cb * 8;
+    for (long long q = threadIdx.x; q < chunks; q += blockDim.x) {
+        const long long bt = q >> 3;           // (b, cb) pair
+        const int cq = (int)(q & 7);           // chunk within the 64-wide block
+        const long long b = bt / n_cb;
+        const int cb = (int)(bt - b * n_cb);
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int c0 = cb * kMmaK + cq * 8 + 2 * e;
+            const float v0 = c0 < n2 ? g[b * n2 + c0] * inv : 0.f;
+            const float v1 = c0 + 1 < n2 ? g[b * n2 + c0 + 1] * inv : 0.f;
+            const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+            const __nv_bfloat162 hh = __halves2bfloat162(h0, h1);
+            const __nv_bfloat162 ll = __halves2bfloat162(__float2bfloat16_rn(v0 - __bfloat162float(h0)),
+                                                         __float2bfloat16_rn(v1 - __bfloat162float(h1)));
+            h[e] = *reinterpret_cast<const uint32_t*>(&hh);
+            l[e] = *reinterpret_cast<const uint32_t*>(&ll);
+        }
+        const long long t = (long long)cb * n1 + b;
+        unsigned char* tile = rowbase + (size_t)t * kGTileBytes;
+        const int phys = ((cq ^ (rt & 7)) << 4);
+        *reinterpret_cast<uint4*>(tile + phys) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(tile + kGTileBytes / 2 + phys) = make_uint4(l[0], l[1], l[2], l[3]);
     }
 }
 
-cudaError_t launch_split_rows(const float* src, long long rows, int n1, int n2, int n2p, __nv_bfloat16* hi,
-                              __nv_bfloat16* lo, float* row_scale, int* err, cudaStream_t s) {
-    (void)err;
-    split_rows_kernel<<<(unsigned)rows, 256, 0, s>>>(src, n1, n2, n2p, hi, lo, row_scale);
+cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1, int n2, int n_cb,
+                              unsigned char* gt, float* row_scale, cudaStream_t s) {
+    split_rows_kernel<<<(unsigned)rows, 256, 0, s>>>(src, row0, n1, n2, n_cb, gt, row_scale);
     return cudaGetLastError();
 }
 
