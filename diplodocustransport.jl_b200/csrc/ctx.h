@@ -140,6 +140,16 @@ struct dtb_ctx {
     int* pin_err = nullptr;
     float* pin_f32 = nullptr;  // FP32 state staging for dtb_get_f / dtb_set_f
 
+    // pipelined Solve (allocated on first use): dt staging and diagnostics read-back, double
+    // buffered; a ring of save slots on the device and in pinned memory; a copy stream
+    double* pin_dt2 = nullptr;          // [2][hist_cap]
+    StepDiagDev* pin_hist2 = nullptr;   // [2][hist_cap]
+    void* save_dev = nullptr;           // [kSaveRing][n_state] state elements
+    void* save_pin = nullptr;           // [kSaveRing][n_state]
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pipe_ev[16] = {};       // dt staging x2, hist x2, saved x kSaveRing, landed x kSaveRing
+    bool pipe_ready = false;
+
     // graphs
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 16;

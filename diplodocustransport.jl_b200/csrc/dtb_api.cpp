@@ -116,6 +116,14 @@ int32_t dtb_destroy(dtb_ctx* c) {
     if (c->pin_hist) cudaFreeHost(c->pin_hist);
     if (c->pin_err) cudaFreeHost(c->pin_err);
     if (c->pin_f32) cudaFreeHost(c->pin_f32);
+    if (c->pin_dt2) cudaFreeHost(c->pin_dt2);
+    if (c->pin_hist2) cudaFreeHost(c->pin_hist2);
+    if (c->save_pin) cudaFreeHost(c->save_pin);
+    if (c->pipe_ready) {
+        for (cudaEvent_t e : c->pipe_ev)
+            if (e) cudaEventDestroy(e);
+        cudaStreamDestroy(c->copy_stream);
+    }
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return DTB_OK;
@@ -971,54 +979,234 @@ int32_t dtb_reset(dtb_ctx* c) {
 int32_t dtb_solve(dtb_ctx* c, double dt_initial, const double* t_save, int64_t n_save, int32_t verbose, double* f_out,
                   int64_t* n_steps_out) {
     DTB_CHECK(c && t_save && f_out && n_save >= 1, DTB_EINVAL, "dtb_solve: null argument");
+    return dtb_solve_ex(c, dt_initial, t_save, n_save, verbose, f_out, nullptr, nullptr, nullptr, n_steps_out);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ pipelined Solve
+// Solver.jl:1-64 without a host round trip per save interval: the step schedule depends only
+// on dt and t_save, so it is generated on the host chunk by chunk (up to hist_cap steps, dt
+// staging double-buffered) and every chunk's steps are enqueued at once. At a save point the
+// state is copied on the device into a ring slot (and its moments computed there), and the
+// copy stream moves the slot to pinned memory while the next interval steps; the host copies
+// a slot out only when the ring wraps or at the end.
+constexpr int kSaveRing = 4;
+
+static int ensure_pipe(dtb_ctx* c) {
+    if (c->pipe_ready) return DTB_OK;
+    const size_t fb = c->esz * (size_t)c->n_state;
+    DTB_CUDA(cudaMallocHost(&c->pin_dt2, sizeof(double) * 2 * (size_t)c->hist_cap));
+    DTB_CUDA(cudaMallocHost(&c->save_pin, fb * kSaveRing));
+    DTB_TRY(c->alloc(&c->save_dev, fb * kSaveRing));
+    DTB_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 4 + 2 * kSaveRing; ++k) DTB_CUDA(cudaEventCreateWithFlags(&c->pipe_ev[k], cudaEventDisableTiming));
+    c->pipe_ready = true;
+    return DTB_OK;
+}
+
+// n steps through the device counter from its current value (graph replays where they fit).
+static int run_steps(dtb_ctx* c, int64_t n, int verbose) {
+    int64_t done = 0;
+    if (!c->profiling && n >= c->graph_steps) {
+        if (c->cur != 0) {
+            DTB_TRY(do_step(c, 0.0, true, verbose, false));
+            done++;
+        }
+        while (n - done >= c->graph_steps) {
+            DTB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+            done += c->graph_steps;
+            c->host_ctr += c->graph_steps;
+        }
+    }
+    for (; done < n; ++done) DTB_TRY(do_step(c, 0.0, true, verbose, c->profiling));
+    return DTB_OK;
+}
+
+namespace {
+struct StepInfo {
+    double t, dt, t_stop;
+};
+}  // namespace
+
+extern "C" int32_t dtb_solve_ex(dtb_ctx* c, double dt_initial, const double* t_save, int64_t n_save, int32_t verbose,
+                                double* f_out, const double* w, double* number, double* energy,
+                                int64_t* n_steps_out) {
+    DTB_CHECK(c && t_save && n_save >= 1, DTB_EINVAL, "dtb_solve_ex: null argument");
+    DTB_CHECK(!w || (number && energy), DTB_EINVAL, "dtb_solve_ex: moments need number and energy outputs");
     DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_solve: batched contexts use the dtb_batch_* entry points");
+    DTB_CHECK(dt_initial > 0 && std::isfinite(dt_initial), DTB_EINVAL, "dtb_solve: dt must be > 0");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
-    // Solver.jl:22 reset; :14 save the initial state
-    DTB_TRY(dtb_reset(c));
-    DTB_TRY(dtb_get_f(c, f_out));
-    double dt = dt_initial;
-    int64_t total = 0;
+    DTB_TRY(ensure_pipe(c));
+    const bool want_diag = verbose == 1 || verbose == 2 || verbose == 3;
+    if (want_diag && !c->pin_hist2)
+        DTB_CUDA(cudaMallocHost(&c->pin_hist2, sizeof(StepDiagDev) * 2 * (size_t)c->hist_cap));
+    if (!c->profiling) DTB_TRY(ensure_graph(c, verbose));
+    const size_t fb = c->esz * (size_t)c->n_state;
+    const size_t mstride = (size_t)2 * c->ns * c->n_space;
+    double* mom_all = nullptr;
+    if (w) {
+        DTB_CUDA(cudaMemcpyAsync(c->mom_w, w, sizeof(double) * (size_t)c->n_mom, cudaMemcpyHostToDevice, c->stream));
+        DTB_CUDA(cudaMallocAsync(&mom_all, sizeof(double) * mstride * (size_t)n_save, c->stream));
+    }
+    cudaEvent_t* ev_dt = c->pipe_ev;
+    cudaEvent_t* ev_hist = c->pipe_ev + 2;
+    cudaEvent_t* ev_saved = c->pipe_ev + 4;
+    cudaEvent_t* ev_landed = c->pipe_ev + 4 + kSaveRing;
+    int64_t owner[kSaveRing];
+    for (auto& o : owner) o = -1;
+    int rc = DTB_OK;
+
+    auto drain = [&](int sl) -> int {
+        if (owner[sl] < 0) return DTB_OK;
+        DTB_CUDA(cudaEventSynchronize(ev_landed[sl]));
+        double* dst = f_out + (size_t)owner[sl] * c->n_state;
+        const char* src = static_cast<const char*>(c->save_pin) + fb * sl;
+        if (c->prec == DTB_F64) {
+            std::memcpy(dst, src, fb);
+        } else {
+            const float* s32 = reinterpret_cast<const float*>(src);
+            for (int64_t k = 0; k < c->n_state; ++k) dst[k] = s32[k];
+        }
+        owner[sl] = -1;
+        return DTB_OK;
+    };
+    int64_t save_idx = 0;
+    auto save = [&]() -> int {
+        if (f_out) {
+            const int sl = (int)(save_idx % kSaveRing);
+            DTB_TRY(drain(sl));
+            void* dslot = static_cast<char*>(c->save_dev) + fb * sl;
+            DTB_CUDA(cudaMemcpyAsync(dslot, c->f_buf[c->cur], fb, cudaMemcpyDeviceToDevice, c->stream));
+            DTB_CUDA(cudaEventRecord(ev_saved[sl], c->stream));
+            DTB_CUDA(cudaStreamWaitEvent(c->copy_stream, ev_saved[sl], 0));
+            DTB_CUDA(cudaMemcpyAsync(static_cast<char*>(c->save_pin) + fb * sl, dslot, fb, cudaMemcpyDeviceToHost,
+                                     c->copy_stream));
+            DTB_CUDA(cudaEventRecord(ev_landed[sl], c->copy_stream));
+            owner[sl] = save_idx;
+        }
+        if (w) {
+            double* out = mom_all + mstride * (size_t)save_idx;
+            if (c->prec == DTB_F64)
+                DTB_CUDA(launch_moments_f64(reinterpret_cast<const double*>(c->f_buf[c->cur]), (int)c->n_mom,
+                                            c->n_space, c->sp_off_dev, c->ns, c->mom_w, out, c->stream));
+            else
+                DTB_CUDA(launch_moments_f32(reinterpret_cast<const float*>(c->f_buf[c->cur]), (int)c->n_mom,
+                                            c->n_space, c->sp_off_dev, c->ns, c->mom_w, out, c->stream));
+        }
+        ++save_idx;
+        return DTB_OK;
+    };
+    std::vector<StepInfo> info[2];
+    bool pending[2] = {false, false};
+    int64_t pending_n[2] = {0, 0};
+    auto print_chunk = [&](int b) -> int {
+        if (!pending[b]) return DTB_OK;
+        DTB_CUDA(cudaEventSynchronize(ev_hist[b]));
+        const StepDiagDev* h = c->pin_hist2 + (size_t)b * c->hist_cap;
+        for (int64_t k = 0; k < pending_n[b]; ++k) print_cr(verbose, h[k], info[b][k].t, info[b][k].t_stop, info[b][k].dt);
+        pending[b] = false;
+        return DTB_OK;
+    };
+
+    // Solver.jl:22 reset; :14 the initial state is the first save
+    rc = dtb_reset(c);
+    if (rc == DTB_OK) rc = save();
     const double d0 = dt0_eff(c);
-    std::vector<double> t_of, dt_of;
-    for (int64_t i = 1; i < n_save; ++i) {
-        double t_start = t_save[i - 1];
-        const double t_stop = t_save[i];
-        bool save = false;
-        std::vector<double> scales;
-        t_of.clear();
-        dt_of.clear();
-        while (!save) {
+    double dt = dt_initial;
+    int64_t interval = 1, total = 0;
+    double t_start = t_save[0];
+    int b = 0;
+    std::vector<int64_t> marks;
+    while (rc == DTB_OK && interval < n_save) {
+        // the staging buffer of two chunks ago is free once its upload has run
+        if ((rc = cudaEventSynchronize(ev_dt[b]) == cudaSuccess ? DTB_OK : DTB_ECUDA) != DTB_OK) break;
+        if ((rc = print_chunk(b)) != DTB_OK) break;
+        double* stage = c->pin_dt2 + (size_t)b * c->hist_cap;
+        info[b].clear();
+        marks.clear();
+        int64_t n = 0;
+        while (n < c->hist_cap && interval < n_save) {  // Solver.jl:25-37 with SteppingMethods.jl:18-23
+            const double t_stop = t_save[interval];
+            bool at_save = false;
             if (t_start + dt >= t_stop) {
                 dt = t_stop - t_start;
-                save = true;
+                at_save = true;
             }
-            scales.push_back(dt / d0);
-            t_of.push_back(t_start);
-            dt_of.push_back(dt);
+            stage[n] = dt / d0;
+            if (want_diag) info[b].push_back({t_start, dt, t_stop});
             t_start += dt;
-            DTB_CHECK(total + (int64_t)scales.size() <= kMaxScheduleSteps, DTB_EINVAL,
-                      "dtb_solve: more than 1e8 steps; the truncated dt of a save point is carried into later "
-                      "intervals (Solver.jl:35) and has become too small");
-        }
-        const bool want_diag = verbose == 1 || verbose == 2 || verbose == 3;
-        std::vector<dtb_step_diag> hist(want_diag ? scales.size() : 0);
-        DTB_TRY(dtb_run(c, scales.data(), (int64_t)scales.size(), verbose, want_diag ? hist.data() : nullptr));
-        if (want_diag) {
-            for (size_t k = 0; k < hist.size(); ++k) {
-                StepDiagDev d;
-                std::memcpy(&d, &hist[k], sizeof(d));
-                print_cr(verbose, d, t_of[k], t_stop, dt_of[k]);
+            ++n;
+            if (++total > kMaxScheduleSteps) {
+                set_error("dtb_solve: more than 1e8 steps; the truncated dt of a save point is carried into later "
+                          "intervals (Solver.jl:35) and has become too small");
+                rc = DTB_EINVAL;
+                break;
             }
-        } else {
-            DTB_TRY(check_kernel_err(c));
+            if (at_save) {
+                marks.push_back(n);
+                ++interval;
+                t_start = t_save[interval - 1];
+            }
         }
-        total += (int64_t)scales.size();
-        DTB_TRY(dtb_get_f(c, f_out + (size_t)i * c->n_state));
+        if (rc != DTB_OK) break;
+        DTB_CUDA(cudaMemcpyAsync(c->dt_arr, stage, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        DTB_CUDA(cudaEventRecord(ev_dt[b], c->stream));
+        DTB_CUDA(cudaMemsetAsync(c->ctr, 0, sizeof(unsigned long long), c->stream));
+        c->host_ctr = 0;
+        int64_t done = 0;
+        for (int64_t mk : marks) {
+            if ((rc = run_steps(c, mk - done, verbose)) != DTB_OK) break;
+            done = mk;
+            if ((rc = save()) != DTB_OK) break;
+        }
+        if (rc == DTB_OK && done < n) rc = run_steps(c, n - done, verbose);
+        if (rc != DTB_OK) break;
+        if (want_diag) {
+            DTB_CUDA(cudaMemcpyAsync(c->pin_hist2 + (size_t)b * c->hist_cap, c->hist, sizeof(StepDiagDev) * (size_t)n,
+                                     cudaMemcpyDeviceToHost, c->stream));
+            DTB_CUDA(cudaEventRecord(ev_hist[b], c->stream));
+            pending[b] = true;
+            pending_n[b] = n;
+        }
+        b ^= 1;
     }
+    // finish: diagnostics of the last two chunks in order, the save ring, the moments
+    cudaError_t e1 = cudaStreamSynchronize(c->stream);
+    cudaError_t e2 = cudaStreamSynchronize(c->copy_stream);
+    if (rc == DTB_OK && e1 != cudaSuccess) rc = (set_error(std::string("CUDA error: ") + cudaGetErrorString(e1)), DTB_ECUDA);
+    if (rc == DTB_OK && e2 != cudaSuccess) rc = (set_error(std::string("CUDA error: ") + cudaGetErrorString(e2)), DTB_ECUDA);
+    if (rc == DTB_OK) rc = print_chunk(b);
+    if (rc == DTB_OK) rc = print_chunk(b ^ 1);
+    for (int64_t k = std::max<int64_t>(0, save_idx - kSaveRing); rc == DTB_OK && k < save_idx; ++k)
+        rc = drain((int)(k % kSaveRing));
+    if (w) {
+        if (rc == DTB_OK) {
+            std::vector<double> hm(mstride * (size_t)n_save);
+            cudaError_t e = cudaMemcpyAsync(hm.data(), mom_all, sizeof(double) * hm.size(), cudaMemcpyDeviceToHost,
+                                            c->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+            if (e != cudaSuccess) {
+                set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
+                rc = DTB_ECUDA;
+            } else {
+                for (size_t k = 0; k < hm.size() / 2; ++k) {
+                    number[k] = hm[2 * k];
+                    energy[k] = hm[2 * k + 1];
+                }
+            }
+        }
+        cudaFreeAsync(mom_all, c->stream);
+        cudaStreamSynchronize(c->stream);
+    }
+    if (rc != DTB_OK) return rc;
+    DTB_TRY(check_kernel_err(c));
     if (n_steps_out) *n_steps_out = total;
     return DTB_OK;
 }
+
+extern "C" {
 
 int32_t dtb_moments(dtb_ctx* c, const double* w, double* number, double* energy) {
     DTB_CHECK(c && w && number && energy, DTB_EINVAL, "dtb_moments: null argument");

@@ -91,6 +91,7 @@ SIGNATURES = {
     "dtb_step": (_i32, [_P, _d, _d, _d, _i32, _dp, _i32p, ctypes.POINTER(StepDiag)]),
     "dtb_run": (_i32, [_P, _dp, _i64, _i32, ctypes.POINTER(StepDiag)]),
     "dtb_solve": (_i32, [_P, _d, _dp, _i64, _i32, _dp, _ip]),
+    "dtb_solve_ex": (_i32, [_P, _d, _dp, _i64, _i32, _dp, _dp, _dp, _dp, _ip]),
     "dtb_solve_schedule": (_i32, [_d, _dp, _i64, _d, _i32, _ip, _dp, _i64, _ip]),
     "dtb_get_f": (_i32, [_P, _dp]),
     "dtb_set_f": (_i32, [_P, _dp]),

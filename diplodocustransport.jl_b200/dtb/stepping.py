@@ -237,9 +237,12 @@ def solve_schedule(dt_initial: float, t_save: Sequence[float], dt0: float, preci
 
 def Solve(method: ForwardEulerStruct, dt_initial: float, t_save: Sequence[float], *, progress: bool = False,
           fileName: Optional[str] = None, fileLocation: Optional[str] = None, Verbose: int = 1,
-          stepwise: bool = False) -> OutputStruct:
+          stepwise: bool = False, moment_weights=None) -> OutputStruct:
     """Solver.jl:1-64. ``stepwise=True`` calls the functor once per step exactly like the
-    reference loop; the default runs each save interval as CUDA-graph replays (dtb_solve)."""
+    reference loop; the default enqueues the whole schedule as CUDA-graph replays with the save
+    points copied out behind the stepping (dtb_solve_ex). With ``moment_weights`` (one energy
+    weight per momentum state) the output also holds ``number`` and ``energy``, arrays
+    (n_save, n_space, n_species) of FP64 moments computed on the device at every save point."""
     t_save = [float(t) for t in t_save]
     n_save = len(t_save)
     out = OutputStruct()
@@ -260,8 +263,20 @@ def Solve(method: ForwardEulerStruct, dt_initial: float, t_save: Sequence[float]
     F = np.zeros((n_save, method.n))
     nsteps = ctypes.c_int64()
     t = np.ascontiguousarray(t_save, dtype=np.float64)
-    check(method.L.dtb_solve(method.ctx, float(dt_initial), dptr(t), n_save, int(Verbose), dptr(F),
-                             ctypes.byref(nsteps)))
+    if moment_weights is None:
+        check(method.L.dtb_solve(method.ctx, float(dt_initial), dptr(t), n_save, int(Verbose), dptr(F),
+                                 ctypes.byref(nsteps)))
+    else:
+        ps = method.PhaseSpace
+        w = np.ascontiguousarray(moment_weights, dtype=np.float64)
+        if w.shape != (ps.n_momentum,):
+            raise ValueError("moment_weights must hold one weight per momentum state")
+        shape = (n_save, ps.n_space, len(ps.species_sizes))
+        num = np.zeros(shape)
+        en = np.zeros(shape)
+        check(method.L.dtb_solve_ex(method.ctx, float(dt_initial), dptr(t), n_save, int(Verbose), dptr(F), dptr(w),
+                                    dptr(num), dptr(en), ctypes.byref(nsteps)))
+        out.number, out.energy = num, en
     out.f = [F[i].copy() for i in range(n_save)]
     out.t = list(t_save)
     out.n_steps = nsteps.value

@@ -167,6 +167,17 @@ int32_t dtb_solve(dtb_ctx* ctx, double dt_initial, const double* t_save, int64_t
 /* Step schedule of Solve, host only: per save interval the number of steps, and the
  * dt/dt0 of every step (capacity cap; n_total_out gets the total count). `precision`
  * selects how dt0 is rounded (Float32(dt0) for DTB_F32, SteppingStructs.jl:44). */
+/* Solve with the save points pipelined behind the stepping (Solver.jl:1-64; the copies of
+ * Solver.jl:40-43 made asynchronous) and the OutputStruct's moments computed on the device:
+ * the whole schedule is enqueued without a host round trip per interval; at each save point
+ * f is copied into a device ring slot that a second stream moves to pinned memory while the
+ * next interval steps. f_out: n_save x n (or NULL); w: n_mom energy weights (or NULL for no
+ * moments); number, energy: n_save x n_space x n_species, FP64 sums over each species slice
+ * (DistributionMoments.jl:33,145,162). dtb_solve is this call with no moments. */
+int32_t dtb_solve_ex(dtb_ctx* ctx, double dt_initial, const double* t_save, int64_t n_save,
+                     int32_t verbose, double* f_out, const double* w, double* number,
+                     double* energy, int64_t* n_steps);
+
 int32_t dtb_solve_schedule(double dt_initial, const double* t_save, int64_t n_save, double dt0,
                            int32_t precision, int64_t* steps_per_interval, double* dt_scales,
                            int64_t cap, int64_t* n_total_out);
