@@ -248,7 +248,9 @@ def Solve(method: ForwardEulerStruct, dt_initial: float, t_save: Sequence[float]
     out = OutputStruct()
     if stepwise:
         method.reset()
-        out.f.append(method.f_init.copy())
+        # Solver.jl:10-14 saves f_init, which the struct holds in its precision (SteppingStructs.jl:24,53)
+        single = _precision_code(method.Precision) == _lib.DTB_F32
+        out.f.append(method.f_init.astype(np.float32).astype(np.float64) if single else method.f_init.copy())
         out.t.append(t_save[0])
         dt = float(dt_initial)
         for i in range(1, n_save):

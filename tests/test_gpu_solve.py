@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from dtb import synth
-from dtb.stepping import ForwardEulerStruct, Solve
+from dtb.stepping import ForwardEulerStruct, Solve, solve_schedule
 from dtb.structs import energy_weights
 
 pytestmark = pytest.mark.gpu
@@ -22,14 +22,18 @@ def _method(w, precision=np.float64, **kw):
 
 @pytest.mark.parametrize("precision", [np.float64, np.float32])
 def test_many_irregular_saves_bitwise(cuda, precision):
-    """40 save points at irregular times, so intervals end mid-graph and the truncated dt of a
-    save is carried into the next interval (Solver.jl:35)."""
+    """40 save points at irregular times, so intervals end mid-graph and the truncated dt of the
+    first save (0.25) is carried into the later intervals (Solver.jl:35). Save times are
+    multiples of 0.25 so the carried dt stays 0.25 (an arbitrary grid would shrink it at every
+    save until the schedule explodes, as the reference would)."""
     w = synth.small(p_num=8, u_num=4, seed=41, randomize_vectors=True)
     rng = np.random.default_rng(3)
-    t_save = np.concatenate([[0.0], np.cumsum(rng.uniform(0.5, 9.0, 40))]).tolist()
+    t_save = [0.0, 3.25] + list(3.25 + 0.25 * np.cumsum(rng.integers(1, 40, 39)))
+    per, _ = solve_schedule(0.5, t_save, 1.0)
+    assert per.sum() < 2000
     m = _method(w, precision, graph_steps=8)
-    a = Solve(m, 0.7, t_save, Verbose=0, stepwise=True)
-    b = Solve(m, 0.7, t_save, Verbose=0)
+    a = Solve(m, 0.5, t_save, Verbose=0, stepwise=True)
+    b = Solve(m, 0.5, t_save, Verbose=0)
     assert len(b.f) == len(t_save)
     for x, y in zip(a.f, b.f):
         np.testing.assert_array_equal(x, y)
@@ -41,6 +45,7 @@ def test_schedule_longer_than_one_chunk(cuda):
     sides of the boundary."""
     w = synth.small(p_num=4, u_num=2, seed=42, randomize_vectors=True)
     t_save = [0.0, 10000.0, 33000.0, 65530.0, 65540.0, 70000.0]
+    assert solve_schedule(1.0, t_save, 1.0)[0].sum() == 70000
     m = _method(w)
     a = Solve(m, 1.0, t_save, Verbose=0, stepwise=True)
     b = Solve(m, 1.0, t_save, Verbose=0)
@@ -57,8 +62,9 @@ def test_device_moments_of_every_save(cuda, precision, rel):
     wts = energy_weights(w.ps)
     t_save = [0.0] + [3.0 * k + 0.5 for k in range(1, 12)]
     m = _method(w, precision)
-    out = Solve(m, 0.9, t_save, Verbose=0, moment_weights=wts)
-    ref = Solve(m, 0.9, t_save, Verbose=0)
+    out = Solve(m, 0.5, t_save, Verbose=0, moment_weights=wts)
+    ref = Solve(m, 0.5, t_save, Verbose=0)
+    assert out.n_steps == 67
     sizes = w.ps.species_sizes
     n_mom = w.ps.n_momentum
     assert out.number.shape == (len(t_save), 2, len(sizes))
