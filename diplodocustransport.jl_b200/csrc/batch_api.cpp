@@ -85,6 +85,21 @@ double ord_dec_host(unsigned long long e) {
 int commit_mixed(dtb_ctx* c) {
     DTB_CHECK(c->n_space == 1, DTB_EINVAL, "batched contexts hold single-cell instances (n_space must be 1)");
     DTB_CHECK(c->opts.batch >= 1, DTB_EINVAL, "batched context needs opts.batch >= 1");
+    // the tensor-core GEMM streams dense blocks: a sparse M_Bin is densified per block
+    for (auto& kv : c->sgains) {
+        const int so = std::get<0>(kv.first), s1 = std::get<1>(kv.first), s2 = std::get<2>(kv.first);
+        auto key = std::make_tuple(so, s1, s2);
+        GainStage& g = c->gains[key];
+        g.out = so;
+        g.in1 = s1;
+        g.in2 = s2;
+        DTB_CHECK(g.dev_src.empty(), DTB_EINVAL, "a sparse M_Bin cannot be summed with a device-resident gain block");
+        const int64_t n1 = c->sz[s1], n2 = c->sz[s2];
+        if (g.host.empty()) g.host.assign((size_t)(c->sz[so] * n1 * n2), 0.0);
+        const SparseGain& s = kv.second;
+        for (size_t q = 0; q < s.v.size(); ++q) g.host[(size_t)(((int64_t)s.a[q] * n1 + s.b[q]) * n2 + s.c[q])] += s.v[q];
+    }
+    c->sgains.clear();
     auto* m = new MixedState();
     c->mixed = m;
     m->Buser = c->opts.batch;

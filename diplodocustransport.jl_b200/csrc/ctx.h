@@ -57,6 +57,12 @@ struct GainStage {
     std::vector<std::pair<const void*, int>> dev_src;  // device sources (pointer, dtype), added in order
 };
 
+// Gain block entries from a sparse M_Bin: COO with local (output row, b, c) indices.
+struct SparseGain {
+    std::vector<int32_t> a, b, c;
+    std::vector<double> v;
+};
+
 struct EmiPiece {
     int64_t row0, nrows, col0, ncols;
     std::vector<double> data;  // row-major
@@ -86,6 +92,8 @@ struct dtb_ctx {
 
     // host staging
     std::map<std::tuple<int, int, int>, GainStage> gains;
+    std::map<std::tuple<int, int, int>, SparseGain> sgains;  // from dtb_upload_mbin_csc
+    std::vector<std::vector<char>> sparse_stage;              // commit-time host data of sparse blocks
     std::map<std::pair<int, int>, std::vector<double>> losses;
     std::vector<EmiPiece> emis;
     std::vector<int64_t> flux_r, flux_c;

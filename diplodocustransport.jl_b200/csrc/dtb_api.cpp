@@ -223,6 +223,49 @@ int32_t dtb_add_loss_block(dtb_ctx* c, int32_t sp, int32_t other_sp, const doubl
     return DTB_OK;
 }
 
+int32_t dtb_upload_mbin_csc(dtb_ctx* c, int64_t n_mom, const int64_t* colptr, const int64_t* rowval,
+                            const double* nzval) {
+    DTB_CHECK(c && colptr, DTB_EINVAL, "dtb_upload_mbin_csc: null argument");
+    DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_upload_mbin_csc: operators already committed");
+    DTB_CHECK(n_mom == c->n_mom, DTB_EINVAL, "dtb_upload_mbin_csc: M_Bin must be n_mom^2 x n_mom (SteppingMethods.jl:349)");
+    const int64_t N = n_mom, base = c->opts.index_base;
+    DTB_CHECK(colptr[0] == base, DTB_EINVAL, "dtb_upload_mbin_csc: colptr[0] must equal index_base");
+    DTB_CHECK(colptr[N] == colptr[0] || (rowval && nzval), DTB_EINVAL, "dtb_upload_mbin_csc: null rowval/nzval");
+    for (int64_t k = 0; k < N; ++k) {
+        DTB_CHECK(colptr[k + 1] >= colptr[k], DTB_EINVAL, "dtb_upload_mbin_csc: colptr not monotone");
+        const int sk = species_of(c, k);
+        for (int64_t p = colptr[k] - base; p < colptr[k + 1] - base; ++p) {
+            const int64_t row = rowval[p] - base;
+            DTB_CHECK(row >= 0 && row < N * N, DTB_EINVAL, "dtb_upload_mbin_csc: row index out of range");
+            const double v = nzval[p];
+            if (v == 0.0) continue;
+            // M_Bin[(j - 1) N + a, k] is T[a, j, k]: df_a += T[a, j, k] f_j f_k
+            const int64_t j = row / N, a = row - j * N;
+            const int so = species_of(c, a), sj = species_of(c, j);
+            const int64_t al = a - c->off[so];
+            if (j == a || k == a) {
+                // loss form: f_a * L'[a, c] f_c with c the other index (the row kernel subtracts)
+                const int64_t o = j == a ? k : j;
+                const int so2 = j == a ? sk : sj;
+                auto& L = c->losses[{so, so2}];
+                if (L.empty()) L.assign((size_t)(c->sz[so] * c->sz[so2]), 0.0);
+                L[(size_t)(al * c->sz[so2] + (o - c->off[so2]))] -= v;
+                continue;
+            }
+            // gain, folded to in1 <= in2 (G[a][b][c] = T[a,b,c] + T[a,c,b] across species)
+            const bool swap = sj > sk;
+            const int s1 = swap ? sk : sj, s2 = swap ? sj : sk;
+            const int64_t b = swap ? k : j, cc = swap ? j : k;
+            SparseGain& g = c->sgains[std::make_tuple(so, s1, s2)];
+            g.a.push_back((int32_t)al);
+            g.b.push_back((int32_t)(b - c->off[s1]));
+            g.c.push_back((int32_t)(cc - c->off[s2]));
+            g.v.push_back(v);
+        }
+    }
+    return DTB_OK;
+}
+
 int32_t dtb_upload_mbin_ref(dtb_ctx* c, const double* M, int64_t n_mom) {
     DTB_CHECK(c && M, DTB_EINVAL, "dtb_upload_mbin_ref: null argument");
     DTB_CHECK(!c->committed, DTB_ESTATE, "dtb_upload_mbin_ref: operators already committed");
@@ -383,9 +426,95 @@ static int build_ell(dtb_ctx* c, const std::vector<int64_t>& fr, const std::vect
     return DTB_OK;
 }
 
+// Sparse gain block layout: per output row, runs of consecutive nonzero b-rows, each run
+// trimmed to the union of its rows' c-spans (8-element aligned). A run is cut where the union
+// would pad the stored rows by more than half, where b skips a row, or at max_elems.
+struct SparseRun {
+    int al, b0, nb, c0, w;  // output row, first b, b-rows, first c, row width (elements)
+    int64_t elem_off;       // within the sparse data
+};
+
+static void sparse_runs(const SparseGain& g, int64_t n2p, int64_t max_elems, std::vector<SparseRun>& runs,
+                        std::vector<double>& data) {
+    std::vector<size_t> idx(g.v.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+        if (g.a[x] != g.a[y]) return g.a[x] < g.a[y];
+        if (g.b[x] != g.b[y]) return g.b[x] < g.b[y];
+        return g.c[x] < g.c[y];
+    });
+    // rows (a, b) with their c-span
+    struct Row {
+        int a, b, c0, c1;
+        size_t i0, i1;
+    };
+    std::vector<Row> rows;
+    for (size_t k = 0; k < idx.size();) {
+        size_t e = k;
+        const int a = g.a[idx[k]], b = g.b[idx[k]];
+        while (e < idx.size() && g.a[idx[e]] == a && g.b[idx[e]] == b) ++e;
+        const int c0 = g.c[idx[k]] / 8 * 8;
+        const int c1 = (int)std::min<int64_t>(n2p, round_up(g.c[idx[e - 1]] + 1, 8));
+        rows.push_back({a, b, c0, c1, k, e});
+        k = e;
+    }
+    auto flush = [&](size_t r0, size_t r1, int c0, int c1) {
+        SparseRun R;
+        R.al = rows[r0].a;
+        R.b0 = rows[r0].b;
+        R.nb = (int)(r1 - r0);
+        R.c0 = c0;
+        R.w = c1 - c0;
+        R.elem_off = (int64_t)data.size();
+        data.resize(data.size() + (size_t)R.nb * R.w, 0.0);
+        for (size_t r = r0; r < r1; ++r)
+            for (size_t q = rows[r].i0; q < rows[r].i1; ++q)
+                data[(size_t)(R.elem_off + (int64_t)(r - r0) * R.w + (g.c[idx[q]] - c0))] += g.v[idx[q]];
+        runs.push_back(R);
+    };
+    size_t r0 = 0;
+    int u0 = 0, u1 = 0;
+    int64_t own = 0;  // sum of the run's own row widths
+    for (size_t r = 0; r < rows.size(); ++r) {
+        if (r > r0) {
+            const bool adj = rows[r].a == rows[r - 1].a && rows[r].b == rows[r - 1].b + 1;
+            const int n0 = std::min(u0, rows[r].c0), n1 = std::max(u1, rows[r].c1);
+            const int64_t padded = (int64_t)(r - r0 + 1) * (n1 - n0);
+            const int64_t own2 = own + (rows[r].c1 - rows[r].c0);
+            if (adj && 2 * padded <= 3 * own2 && padded <= max_elems) {
+                u0 = n0;
+                u1 = n1;
+                own = own2;
+                continue;
+            }
+            flush(r0, r, u0, u1);
+        }
+        r0 = r;
+        u0 = rows[r].c0;
+        u1 = rows[r].c1;
+        own = u1 - u0;
+    }
+    if (!rows.empty()) flush(r0, rows.size(), u0, u1);
+}
+
 template <typename T>
 static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     const size_t esz = sizeof(T);
+    // sparse entries of a block that also has dense host uploads are folded into the dense block
+    for (auto it = c->sgains.begin(); it != c->sgains.end();) {
+        auto dn = c->gains.find(it->first);
+        if (dn == c->gains.end()) {
+            ++it;
+            continue;
+        }
+        GainStage& g = dn->second;
+        DTB_CHECK(g.dev_src.empty(), DTB_EINVAL, "a sparse M_Bin cannot be summed with a device-resident gain block");
+        const int64_t n1 = c->sz[g.in1], n2 = c->sz[g.in2];
+        if (g.host.empty()) g.host.assign((size_t)(c->sz[g.out] * n1 * n2), 0.0);
+        const SparseGain& s = it->second;
+        for (size_t q = 0; q < s.v.size(); ++q) g.host[(size_t)(((int64_t)s.a[q] * n1 + s.b[q]) * n2 + s.c[q])] += s.v[q];
+        it = c->sgains.erase(it);
+    }
     // ---------------- gain blocks
     struct BlkInfo {
         int out, in1, in2;
@@ -404,10 +533,50 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
         total_elems += b.no * b.n1 * b.n2p;
         blks.push_back(b);
     }
-    c->has_bin = !c->gains.empty() || !c->losses.empty();
-    if (!blks.empty()) {
+    // sparse blocks: runs built on the host, their data placed after the dense blocks
+    struct SpBlk {
+        int out, in1, in2;
+        std::vector<SparseRun> runs;
+        int64_t elem_off;
+    };
+    std::vector<SpBlk> sblks;
+    std::vector<double> sdata;
+    double sparse_bytes = 0;
+    for (auto& kv : c->sgains) {
+        SpBlk sb;
+        sb.out = std::get<0>(kv.first);
+        sb.in1 = std::get<1>(kv.first);
+        sb.in2 = std::get<2>(kv.first);
+        const int64_t n2p = round_up(c->sz[sb.in2], 8);
+        DTB_CHECK(n2p * (int64_t)esz <= kGainTileBytes, DTB_EINVAL,
+                  "gain block input-2 species has too many states for one staged b-row");
+        sdata.clear();
+        sparse_runs(kv.second, n2p, (int64_t)(64 * 1024 / esz), sb.runs, sdata);
+        total_elems = round_up(total_elems, 256 / (int64_t)esz);
+        sb.elem_off = total_elems;
+        total_elems += (int64_t)sdata.size();
+        sparse_bytes += (double)sdata.size() * esz;
+        // staged now: the host copy of this block's data goes with it
+        std::vector<T> tv(sdata.size());
+        for (size_t i = 0; i < sdata.size(); ++i) tv[i] = (T)sdata[i];
+        sb.runs.shrink_to_fit();
+        sblks.push_back(std::move(sb));
+        c->sparse_stage.emplace_back(reinterpret_cast<const char*>(tv.data()),
+                                     reinterpret_cast<const char*>(tv.data()) + tv.size() * esz);
+    }
+    c->has_bin = !c->gains.empty() || !c->losses.empty() || !c->sgains.empty();
+    if (!blks.empty() || !sblks.empty()) {
         DTB_TRY(c->alloc(&c->G_all, esz * (size_t)total_elems));
         DTB_CUDA(cudaMemsetAsync(c->G_all, 0, esz * (size_t)total_elems, c->stream));
+        for (size_t k = 0; k < sblks.size(); ++k) {
+            const auto& st = c->sparse_stage[k];
+            if (!st.empty())
+                DTB_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(c->G_all) + esz * (size_t)sblks[k].elem_off, st.data(),
+                                         st.size(), cudaMemcpyHostToDevice, c->stream));
+        }
+        DTB_CUDA(cudaStreamSynchronize(c->stream));
+        c->sparse_stage.clear();
+        c->sgains.clear();
         size_t bi = 0;
         for (auto& kv : c->gains) {
             GainStage& g = kv.second;
@@ -449,14 +618,19 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
     // work units, ordered by output row
     c->f_smem_len = (int)c->offp[c->ns];
     int bps = gain_stream_blocks_per_sm((int)esz, c->f_smem_len);
-    DTB_CHECK(bps >= 1 || blks.empty(), DTB_EINVAL, "gain kernel does not fit on an SM (state vector too long)");
+    DTB_CHECK(bps >= 1 || (blks.empty() && sblks.empty()), DTB_EINVAL,
+              "gain kernel does not fit on an SM (state vector too long)");
     if (bps < 1) bps = 1;
     std::vector<GainUnit> units;
     std::vector<int> unit_ptr((size_t)c->n_mom + 1, 0);
     {
-        double tot_bytes = 0;
+        double tot_bytes = sparse_bytes;
         for (auto& b : blks) tot_bytes += (double)b.no * b.n1 * b.n2 * esz;
         c->gain_bytes = tot_bytes;
+        // sparse runs per output row (global momentum index)
+        std::vector<std::vector<std::pair<const SpBlk*, const SparseRun*>>> srow((size_t)c->n_mom);
+        for (auto& sb : sblks)
+            for (auto& R : sb.runs) srow[(size_t)(c->off[sb.out] + R.al)].push_back({&sb, &R});
         const double target = std::min(256.0 * 1024, std::max((double)kGainTileBytes,
                                                                tot_bytes / ((double)c->num_sms * bps * 8)));
         for (int64_t a = 0; a < c->n_mom; ++a) {
@@ -479,6 +653,20 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
                     u.row = (int)a;
                     units.push_back(u);
                 }
+            }
+            for (auto& pr : srow[(size_t)a]) {
+                const SpBlk& sb = *pr.first;
+                const SparseRun& R = *pr.second;
+                const int tile_b = (int)std::max<int64_t>(1, std::min<int64_t>(R.nb, kGainTileBytes / (R.w * (int64_t)esz)));
+                GainUnit u;
+                u.g_off = sb.elem_off + R.elem_off;
+                u.b_off = (int)(c->offp[sb.in1] + R.b0);
+                u.c_off = (int)(c->offp[sb.in2] + R.c0);
+                u.nb = R.nb;
+                u.n2p = R.w;
+                u.tile_b = tile_b;
+                u.row = (int)a;
+                units.push_back(u);
             }
         }
         unit_ptr[(size_t)c->n_mom] = (int)units.size();

@@ -87,6 +87,7 @@ SIGNATURES = {
     "dtb_add_emi_block": (_i32, [_P, _i64, _i64, _i64, _i64, _dp]),
     "dtb_upload_vectors": (_i32, [_P, _dp, _dp, _dp, _dp]),
     "dtb_set_bin_domain": (_i32, [_P, _ip, _i64]),
+    "dtb_upload_mbin_csc": (_i32, [_P, _i64, _ip, _ip, _dp]),
     "dtb_commit": (_i32, [_P]),
     "dtb_step": (_i32, [_P, _d, _d, _d, _i32, _dp, _i32p, ctypes.POINTER(StepDiag)]),
     "dtb_run": (_i32, [_P, _dp, _i64, _i32, ctypes.POINTER(StepDiag)]),

@@ -15,6 +15,7 @@ from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
 import numpy as np
+import scipy.sparse as sp
 
 from . import _lib
 from ._lib import check, dptr, iptr
@@ -116,7 +117,13 @@ class ForwardEulerStruct:
             L = self.L
             _upload_csc_part(L, ctx, FluxM.X_Flux, _lib.DTB_FLUX_X)
             _upload_csc_part(L, ctx, FluxM.P_Flux, _lib.DTB_FLUX_P)
-            if BinM.M_Bin is not None:
+            if BinM.M_Bin is not None and sp.issparse(BinM.M_Bin):  # Bin_sparse (BuildBinaryMatrices.jl:44-52)
+                M = sp.csc_matrix(BinM.M_Bin)
+                colptr = np.ascontiguousarray(M.indptr, dtype=np.int64)
+                rowval = np.ascontiguousarray(M.indices, dtype=np.int64)
+                nzval = np.ascontiguousarray(M.data, dtype=np.float64)
+                check(L.dtb_upload_mbin_csc(ctx, PhaseSpace.n_momentum, iptr(colptr), iptr(rowval), dptr(nzval)))
+            elif BinM.M_Bin is not None:
                 M = np.asfortranarray(BinM.M_Bin, dtype=np.float64)
                 check(L.dtb_upload_mbin_ref(ctx, M.ctypes.data_as(_lib._dp), PhaseSpace.n_momentum))
             for g in BinM.gains:

@@ -135,6 +135,14 @@ int32_t dtb_add_emi_block(dtb_ctx* ctx, int64_t row0, int64_t nrows, int64_t col
 int32_t dtb_upload_vectors(dtb_ctx* ctx, const double* Ap, const double* Vol,
                            const double* f_init, const double* inj);
 
+/* M_Bin as a sparse matrix (BuildBinaryMatrices.jl:44-52, Bin_sparse = true): CSC of the
+ * n_mom^2 x n_mom matrix (colptr n_mom + 1 entries, indices with opts.index_base; duplicate
+ * entries are summed like sparse(I, J, V)). Decomposed like dtb_upload_mbin_ref, but the gain
+ * part stays sparse: the kernel streams only the nonzero b-rows of each output row, each run
+ * of consecutive b-rows trimmed to the c-span of its nonzeros. */
+int32_t dtb_upload_mbin_csc(dtb_ctx* ctx, int64_t n_mom, const int64_t* colptr, const int64_t* rowval,
+                            const double* nzval);
+
 /* BinM.Domain (StructsAndDictionaries.jl:320, read at SteppingMethods.jl:355-369): the binary
  * term is applied only in the space cells whose 0-based off_space is listed; n < 0 or a NULL
  * list means `nothing` (every cell). Cells outside the domain get a zero binary term, which is

@@ -130,6 +130,8 @@ class RefOperands:
     def __init__(self, n_mom: int, n_space: int, M_Bin, M_Emi, F, invAp, Vol, inj, domain=None):
         self.n_mom, self.n_space = n_mom, n_space
         self.dom = domain_mask(domain, n_space)
+        if M_Bin is not None and hasattr(M_Bin, "toarray"):  # a scipy sparse M_Bin (Bin_sparse)
+            M_Bin = M_Bin.toarray()
         self.M_Bin = None if M_Bin is None else np.asfortranarray(M_Bin, dtype=np.float64)
         self.M_Emi = None if M_Emi is None else np.asfortranarray(M_Emi, dtype=np.float64)
         self.colptr, self.rowval, self.nzval = _csc_arrays(F)
