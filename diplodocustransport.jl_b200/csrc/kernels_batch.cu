@@ -549,22 +549,32 @@ __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict
     }
 }
 
-// One 32-row x 32-instance tile per block, 256 threads, a 2 x 2 (row x instance) micro-tile per
-// thread. Loss and emission are tile products through double-buffered shared memory when the
-// tile's rows belong to one species and every emission piece touching them covers them all
-// (tile_fast); other tiles take direct loads.
-__global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
-                                                         const float* __restrict__ Cc, float* __restrict__ Fo,
-                                                         float* __restrict__ Co, unsigned long long* gstep,
-                                                         unsigned* ticket) {
+// One 32-row x 32-instance tile per block, 512 threads. Loss and emission are tile products
+// through double-buffered shared memory when the tile's rows belong to one species and every
+// emission piece touching them covers them all (tile_fast): the two halves of the block take
+// the two halves of each K chunk with a 2 x 2 (row x instance) micro-tile per thread, and the
+// halves' sums are added in a fixed order. The update then gives each thread one row and two
+// instances, with every load it needs issued before the arithmetic (flux columns and values,
+// state, vectors), so the latency of the L2 round trips overlaps.
+constexpr int kRowsThreads = 512;
+constexpr int kEllFast = 8;  // ELL widths up to this take the hoisted-load flux path
+
+__global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
+                                                                  const float* __restrict__ Cc,
+                                                                  float* __restrict__ Fo, float* __restrict__ Co,
+                                                                  unsigned long long* gstep, unsigned* ticket) {
     __shared__ float s_gain[kRT][kIT + 1];
     extern __shared__ __align__(16) float rows_dyn[];
     float(*s_F)[kCK][kIT] = reinterpret_cast<float(*)[kCK][kIT]>(rows_dyn);
     float(*s_L)[kRT][kCK + 1] = reinterpret_cast<float(*)[kRT][kCK + 1]>(rows_dyn + 2 * kCK * kIT);
-    __shared__ double s_min[16][kIT];
+    // after the products the same memory holds the two halves' loss and emission tiles
+    float(*s_pl)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn);
+    float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + 2 * kRT * (kIT + 1));
+    __shared__ double s_min[kRT][kIT];
     __shared__ int s_nonfin[kIT];
     __shared__ int s_last;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x;
+    const int half = tid >> 8, ht = tid & 255, tx = ht & 15, ty = ht >> 4;
     const int a0 = blockIdx.x * kRT, i0 = blockIdx.y * kIT;
     const int n = ops.n_mom, B = ops.Bcap;
     const long long step = (long long)*reinterpret_cast<volatile unsigned long long*>(gstep);
@@ -574,8 +584,9 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
         const int r = tid & (kRT - 1);
         const int a = a0 + r;
         const int s = a < n ? species_of_row(ops, a) : 0;
-        for (int q = 0; q < kIT / 8; ++q) {
-            const int il = (tid >> 5) + 8 * q;
+#pragma unroll
+        for (int q = 0; q < kIT / 16; ++q) {
+            const int il = (tid >> 5) + 16 * q;
             const int i = i0 + il;
             float g = 0.f;
             if (a < n && i < B) {
@@ -594,15 +605,14 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
     const bool fast = ops.tile_fast[blockIdx.x] != 0;
     if (fast) {
         const int s = species_of_row(ops, a0);
-        // acc[r][i] += sum_c T[a0 + r][c] * F[col0 + c][i0 + i], chunks of kCK columns; the next
-        // chunk is loaded into registers while the current one is multiplied
+        // acc[r][i] += sum_c T[a0 + r][c] * F[col0 + c][i0 + i] over this half's part of each chunk
         auto tile_product = [&](auto load_T, int col0, int nc, float(&acc)[2][2]) {
-            constexpr int PER = (kRT * kCK) / 256;  // elements of each operand per thread and chunk
+            constexpr int PER = (kRT * kCK) / kRowsThreads;  // elements of each operand per thread and chunk
             float rl[PER], rf[PER];
             auto fetch = [&](int c0) {
 #pragma unroll
                 for (int q = 0; q < PER; ++q) {
-                    const int e = tid + 256 * q;
+                    const int e = tid + kRowsThreads * q;
                     const int cc = e & (kCK - 1), rr = e / kCK;
                     const int a = a0 + rr, c = c0 + cc;
                     rl[q] = (a < n && c < nc) ? load_T(a, c) : 0.f;
@@ -614,7 +624,7 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
             auto stash = [&](int buf) {
 #pragma unroll
                 for (int q = 0; q < PER; ++q) {
-                    const int e = tid + 256 * q;
+                    const int e = tid + kRowsThreads * q;
                     s_L[buf][e / kCK][e & (kCK - 1)] = rl[q];
                     s_F[buf][e / kIT][e & (kIT - 1)] = rf[q];
                 }
@@ -625,11 +635,12 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
             __syncthreads();  // the previous product's last reads of both buffers are done
             stash(0);
             __syncthreads();
+            const int k0 = half * (kCK / 2);
             for (int k = 0; k < nch; ++k) {
                 const int buf = k & 1;
                 if (k + 1 < nch) fetch((k + 1) * kCK);
 #pragma unroll 8
-                for (int cc = 0; cc < kCK; ++cc) {
+                for (int cc = k0; cc < k0 + kCK / 2; ++cc) {
                     const float2 fv = *reinterpret_cast<const float2*>(&s_F[buf][cc][tx * 2]);
                     const float l0 = s_L[buf][ty * 2][cc], l1 = s_L[buf][ty * 2 + 1][cc];
                     acc[0][0] += l0 * fv.x;
@@ -663,35 +674,68 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
                     ops.emi_col0[pc], ops.emi_ncols[pc], acc_e);
             }
         }
+        __syncthreads();  // the chunk buffers are free: park both halves' sums
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                s_pl[half][ty * 2 + k][tx * 2 + j] = acc_l[k][j];
+                s_pe[half][ty * 2 + k][tx * 2 + j] = acc_e[k][j];
+            }
     }
     __syncthreads();
 
-    // ---- update of the thread's 2 x 2 (row, instance) pairs
+    // ---- update: one row, two instances per thread
+    const int r = tid >> 4;
+    const int a = a0 + r;
+    const int jb = (tid & 15) * 2;
+    const int ib = i0 + jb;
     double rmin[2] = {CUDART_INF, CUDART_INF};
     int nonfin[2] = {0, 0};
-    const int ib = i0 + tx * 2;
-    bool act[2];
-    double dts[2];
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const int i = ib + j;
-        act[j] = i < B && step < ops.stop_step[i];
-        dts[j] = i < B ? ops.dt_scale[i] : 0.0;
-    }
-    for (int k = 0; k < 2; ++k) {
-        const int a = a0 + ty * 2 + k;
-        if (a >= n || ib >= B) continue;
+    if (a < n && ib < B) {
         const size_t idx = (size_t)a * B + ib;  // B and ib are even
+        // every independent load first
         const float2 fa2 = *reinterpret_cast<const float2*>(F + idx);
         const float2 ca2 = *reinterpret_cast<const float2*>(Cc + idx);
+        const double inv_ap = (double)__ldg(ops.invAp + a), injv = (double)__ldg(ops.inj + a);
+        bool act[2];
+        double dts[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = ib + j;
+            act[j] = i < B && step < ops.stop_step[i];
+            dts[j] = i < B ? ops.dt_scale[i] : 0.0;
+        }
         float flux[2] = {0.f, 0.f};
-        for (int e = 0; e < ops.ell_w; ++e) {
-            const int col = __ldg(ops.ell_col + (size_t)a * ops.ell_w + e);
-            if (col < 0) continue;
-            const float v = __ldg(ops.ell_val + (size_t)a * ops.ell_w + e);
-            const float2 f2 = *reinterpret_cast<const float2*>(F + (size_t)col * B + ib);
-            flux[0] += v * f2.x;
-            flux[1] += v * f2.y;
+        const int* crow = ops.ell_col + (size_t)a * ops.ell_w;
+        const float* vrow = ops.ell_val + (size_t)a * ops.ell_w;
+        if (ops.ell_w <= kEllFast) {
+            int cols[kEllFast];
+            float vals[kEllFast];
+#pragma unroll
+            for (int e = 0; e < kEllFast; ++e) {
+                cols[e] = e < ops.ell_w ? __ldg(crow + e) : -1;
+                vals[e] = e < ops.ell_w ? __ldg(vrow + e) : 0.f;
+            }
+            float2 fv[kEllFast];
+#pragma unroll
+            for (int e = 0; e < kEllFast; ++e)
+                fv[e] = cols[e] >= 0 ? *reinterpret_cast<const float2*>(F + (size_t)cols[e] * B + ib) : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int e = 0; e < kEllFast; ++e) {
+                if (cols[e] < 0) continue;  // padding: only stored entries take part
+                flux[0] += vals[e] * fv[e].x;
+                flux[1] += vals[e] * fv[e].y;
+            }
+        } else {
+            for (int e = 0; e < ops.ell_w; ++e) {
+                const int col = __ldg(crow + e);
+                if (col < 0) continue;
+                const float v = __ldg(vrow + e);
+                const float2 f2 = *reinterpret_cast<const float2*>(F + (size_t)col * B + ib);
+                flux[0] += v * f2.x;
+                flux[1] += v * f2.y;
+            }
         }
         const int s = species_of_row(ops, a);
         const float fa[2] = {fa2.x, fa2.y};
@@ -704,16 +748,21 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
                 co[j] = ca[j];
                 continue;
             }
-            float loss = acc_l[k][j], emi = acc_e[k][j];
-            if (!fast) row_terms_direct(ops, F, a, s, ib + j, loss, emi);
-            const float gain = ops.has_bin ? s_gain[ty * 2 + k][tx * 2 + j] : 0.f;
+            float loss, emi;
+            if (fast) {
+                loss = s_pl[0][r][jb + j] + s_pl[1][r][jb + j];
+                emi = s_pe[0][r][jb + j] + s_pe[1][r][jb + j];
+            } else {
+                row_terms_direct(ops, F, a, s, ib + j, loss, emi);
+            }
+            const float gain = ops.has_bin ? s_gain[r][jb + j] : 0.f;
             // SteppingMethods.jl:31-46 in FP32, the scaling in FP64
             float df = -flux[j];
             if (ops.has_emi) df += emi;
             if (ops.has_bin) df += ops.vol * (gain - fa[j] * loss);
-            const double dfs = (double)df * ((double)ops.invAp[a] * dts[j]);
+            const double dfs = (double)df * (inv_ap * dts[j]);
             // :97-101 with an FP64 compensated sum: the state is fa + ca
-            double t = ((double)fa[j] + (double)ca[j]) + (dfs + (double)ops.inj[a] * dts[j]);
+            double t = ((double)fa[j] + (double)ca[j]) + (dfs + injv * dts[j]);
             t = (t >= ops.thr) ? t : copysign(0.0, t);
             t = (t != CUDART_INF) ? t : copysign(0.0, t);
             fo[j] = (float)t;
@@ -729,13 +778,13 @@ __global__ void __launch_bounds__(256) mixed_rows_kernel(MixedRowOps ops, const 
     // ---- per-instance diagnostics over the tile's rows, then one atomic per instance
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-        s_min[ty][tx * 2 + j] = rmin[j];
-        if (nonfin[j]) atomicOr(&s_nonfin[tx * 2 + j], 1);
+        s_min[r][jb + j] = rmin[j];
+        if (nonfin[j]) atomicOr(&s_nonfin[jb + j], 1);
     }
     __syncthreads();
     if (tid < kIT) {
         double m = CUDART_INF;
-        for (int y = 0; y < 16; ++y) {
+        for (int y = 0; y < kRT; ++y) {
             const double v = s_min[y][tid];
             if (v < m || (v == m && signbit(v))) m = v;
         }
@@ -852,7 +901,7 @@ cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
                               unsigned long long* gstep, unsigned* ticket, cudaStream_t s) {
     dim3 grid((ops.n_mom + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
-    mixed_rows_kernel<<<grid, 256, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
+    mixed_rows_kernel<<<grid, kRowsThreads, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
     return cudaGetLastError();
 }
 
