@@ -220,12 +220,16 @@ int commit_mixed(dtb_ctx* c) {
             for (auto& kv : c->losses) {
                 if (kv.first.first != sp) continue;
                 const int oth = kv.first.second;
-                const int64_t nr = c->sz[sp], nc = c->sz[oth];
+                const int64_t nr = c->sz[sp], nc = c->sz[oth], l = round_up(nc, 4);
+                // rows padded with zeros to a multiple of 4 (16-byte rows for the epilogue's async copies)
                 doff.push_back((long long)data.size());
-                ld.push_back((int)nc);
+                ld.push_back((int)l);
                 coff.push_back((int)c->off[oth]);
                 ncols.push_back((int)nc);
-                data.insert(data.end(), kv.second.begin(), kv.second.begin() + nr * nc);
+                const size_t base = data.size();
+                data.resize(base + (size_t)(nr * l), 0.0);
+                for (int64_t r = 0; r < nr; ++r)
+                    for (int64_t k = 0; k < nc; ++k) data[base + (size_t)(r * l + k)] = kv.second[(size_t)(r * nc + k)];
             }
         }
         ops.loss_ptr[c->ns] = (int)doff.size();
@@ -243,47 +247,37 @@ int commit_mixed(dtb_ctx* c) {
         ops.loss_ncols = d_nc;
         ops.loss_data = d_data;
     }
-    // ---------------- emission pieces: BF16 hi+lo with a power-of-two scale per piece row
+    // ---------------- emission pieces: FP32 rows padded with zeros to a multiple of 4
     {
         c->has_emi = !c->emis.empty();
         std::vector<long long> doff;
-        std::vector<int> ld, r0v, c0v, ncv, soff;
+        std::vector<int> ld, r0v, c0v, ncv;
         std::vector<std::vector<int>> rows((size_t)n_mom);
-        long long total = 0;
-        int srows = 0;
+        std::vector<double> data;
         for (size_t p = 0; p < c->emis.size(); ++p) {
             const EmiPiece& e = c->emis[p];
-            doff.push_back(total);
-            ld.push_back((int)e.ncols);
+            const int64_t l = round_up(e.ncols, 4);
+            doff.push_back((long long)data.size());
+            ld.push_back((int)l);
             r0v.push_back((int)e.row0);
             c0v.push_back((int)e.col0);
             ncv.push_back((int)e.ncols);
-            soff.push_back(srows);
-            total += e.nrows * e.ncols;
-            srows += (int)e.nrows;
-            for (int64_t r = 0; r < e.nrows; ++r) rows[(size_t)(e.row0 + r)].push_back((int)p);
+            const size_t base = data.size();
+            data.resize(base + (size_t)(e.nrows * l), 0.0);
+            for (int64_t r = 0; r < e.nrows; ++r) {
+                for (int64_t k = 0; k < e.ncols; ++k) data[base + (size_t)(r * l + k)] = e.data[(size_t)(r * e.ncols + k)];
+                rows[(size_t)(e.row0 + r)].push_back((int)p);
+            }
         }
-        __nv_bfloat162* d_data = nullptr;
-        float* d_scale = nullptr;
-        DTB_TRY(c->alloc(&d_data, sizeof(__nv_bfloat162) * (size_t)std::max<long long>(1, total)));
-        DTB_TRY(c->alloc(&d_scale, sizeof(float) * (size_t)std::max(1, srows)));
-        for (size_t p = 0; p < c->emis.size(); ++p) {
-            const EmiPiece& e = c->emis[p];
-            std::vector<float> h(e.data.begin(), e.data.end());
-            float* tmp = nullptr;
-            DTB_CUDA(cudaMalloc(&tmp, sizeof(float) * h.size()));
-            DTB_CUDA(cudaMemcpyAsync(tmp, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, s));
-            DTB_CUDA(launch_split_emi(tmp, (int)e.nrows, (int)e.ncols, (int)e.ncols, d_data + doff[p], d_scale + soff[p], s));
-            DTB_CUDA(cudaStreamSynchronize(s));
-            cudaFree(tmp);
-        }
+        float* d_data = nullptr;
+        DTB_TRY(copy_host_vec(c, &d_data, data));
         std::vector<int> rptr((size_t)n_mom + 1, 0), piece;
         for (int i = 0; i < n_mom; ++i) {
             rptr[(size_t)i] = (int)piece.size();
             for (int p : rows[(size_t)i]) piece.push_back(p);
         }
         rptr[(size_t)n_mom] = (int)piece.size();
-        int *d_rptr, *d_piece, *d_ld, *d_r0, *d_c0, *d_nc, *d_soff;
+        int *d_rptr, *d_piece, *d_ld, *d_r0, *d_c0, *d_nc;
         long long* d_doff;
         DTB_TRY(copy_host_ints(c, &d_rptr, rptr));
         DTB_TRY(copy_host_ints(c, &d_piece, piece));
@@ -292,7 +286,6 @@ int commit_mixed(dtb_ctx* c) {
         DTB_TRY(copy_host_ints(c, &d_r0, r0v));
         DTB_TRY(copy_host_ints(c, &d_c0, c0v));
         DTB_TRY(copy_host_ints(c, &d_nc, ncv));
-        DTB_TRY(copy_host_ints(c, &d_soff, soff));
         ops.emi_rptr = d_rptr;
         ops.emi_piece = d_piece;
         ops.emi_data_off = d_doff;
@@ -301,8 +294,6 @@ int commit_mixed(dtb_ctx* c) {
         ops.emi_col0 = d_c0;
         ops.emi_ncols = d_nc;
         ops.emi_data = d_data;
-        ops.emi_scale = d_scale;
-        ops.emi_scale_off = d_soff;
     }
     // ---------------- flux: CSR with duplicates summed, banded ELL (FP32), padding column -1
     {
@@ -417,6 +408,12 @@ int commit_mixed(dtb_ctx* c) {
             const int s0 = species_of(c, a0);
             for (int a = a0; a < a1; ++a)
                 if (species_of(c, a) != s0 || emi_rows[(size_t)a] != emi_rows[(size_t)a0]) fast[(size_t)t] = 0;
+            // and whose K chunks fit the kernel's job list
+            int64_t jobs = 0;
+            for (auto& kv : c->losses)
+                if (kv.first.first == s0) jobs += (c->sz[kv.first.second] + kRowsChunk - 1) / kRowsChunk;
+            for (int p : emi_rows[(size_t)a0]) jobs += (c->emis[(size_t)p].ncols + kRowsChunk - 1) / kRowsChunk;
+            if (jobs > kRowsMaxJobs) fast[(size_t)t] = 0;
         }
         unsigned char* d_fast;
         DTB_TRY(copy_host_ints(c, &d_fast, fast));

@@ -56,9 +56,7 @@ struct MixedRowOps {
     const int* emi_row0;
     const int* emi_col0;
     const int* emi_ncols;
-    const __nv_bfloat162* emi_data;  // (hi, lo) pairs of E / scale of the piece row
-    const float* emi_scale;          // per piece row
-    const int* emi_scale_off;        // per piece: index of its first row in emi_scale
+    const float* emi_data;           // E rows, FP32, each row padded with zeros to emi_ld (a multiple of 4)
     int loss_ptr[DTB_MAX_SPECIES + 1];
     const long long* loss_data_off;
     const int* loss_ld;
@@ -98,7 +96,8 @@ cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const
 
 cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1, int n2, int n_cb,
                               unsigned char* gt, float* row_scale, cudaStream_t s);
-cudaError_t launch_split_emi(const float* src, int rows, int ncols, int ld, __nv_bfloat162* dst, float* row_scale,
-                             cudaStream_t s);
+// K chunks of loss / emission tile products one fast epilogue tile may run (more: direct path).
+constexpr int kRowsMaxJobs = 32;
+constexpr int kRowsChunk = 128;
 
 }  // namespace dtb

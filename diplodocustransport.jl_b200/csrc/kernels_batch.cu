@@ -445,35 +445,6 @@ cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1
     return cudaGetLastError();
 }
 
-// Emission rows: (hi, lo) pairs of E / scale[row] with the same power-of-two row scale.
-__global__ void split_emi_kernel(const float* __restrict__ src, int ncols, int ld, __nv_bfloat162* dst, float* row_scale) {
-    __shared__ float s_max[128];
-    const int r = blockIdx.x;
-    float m = 0.f;
-    for (int k = threadIdx.x; k < ncols; k += blockDim.x) m = fmaxf(m, fabsf(src[(size_t)r * ncols + k]));
-    s_max[threadIdx.x] = m;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) s_max[threadIdx.x] = fmaxf(s_max[threadIdx.x], s_max[threadIdx.x + o]);
-        __syncthreads();
-    }
-    int ex = 0;
-    if (s_max[0] > 0.f && isfinite(s_max[0])) frexpf(s_max[0], &ex);
-    const float inv = ldexpf(1.f, 1 - ex);
-    if (threadIdx.x == 0) row_scale[r] = ldexpf(1.f, ex - 1);
-    for (int k = threadIdx.x; k < ld; k += blockDim.x) {
-        const float v = k < ncols ? src[(size_t)r * ncols + k] * inv : 0.f;
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        dst[(size_t)r * ld + k] = __halves2bfloat162(h, __float2bfloat16_rn(v - __bfloat162float(h)));
-    }
-}
-
-cudaError_t launch_split_emi(const float* src, int rows, int ncols, int ld, __nv_bfloat162* dst, float* row_scale,
-                             cudaStream_t s) {
-    split_emi_kernel<<<rows, 128, 0, s>>>(src, ncols, ld, dst, row_scale);
-    return cudaGetLastError();
-}
-
 // ------------------------------------------------------------------ batched Euler epilogue
 namespace {
 
@@ -486,8 +457,11 @@ __device__ __forceinline__ unsigned long long ord_enc(double x) {
 
 constexpr int kRT = 32;   // rows per tile
 constexpr int kIT = 32;   // instances per tile
-constexpr int kCK = 128;  // K chunk of the loss / emission tile products
-constexpr int kRowsSmem = (2 * kRT * (kCK + 1) + 2 * kCK * kIT) * 4;  // dynamic: two L and two F chunks
+constexpr int kCK = kRowsChunk;  // K chunk of the loss / emission tile products
+constexpr int kLS = kCK + 4;      // row pitch of a staged operand chunk (16-byte aligned rows)
+constexpr int kRowStages = 3;     // cp.async ring depth
+constexpr int kStageFloats = kRT * kLS + kCK * kIT;
+constexpr int kRowsSmem = kRowStages * kStageFloats * 4;  // dynamic: the operand / state chunk ring
 
 // Sum of the split-K partial tiles of one gain group, scaled back to G and f units:
 // gsum[i][r] = row_scale[r] * sig1[i] * sig2[i] * sum_s partial[s][i][r]. Fixed summation order.
@@ -537,22 +511,38 @@ __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict
     if (ops.has_emi) {
         for (int p = ops.emi_rptr[a]; p < ops.emi_rptr[a + 1]; ++p) {
             const int pc = ops.emi_piece[p];
-            const __nv_bfloat162* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
+            const float* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
             const int col0 = ops.emi_col0[pc], nc = ops.emi_ncols[pc];
-            float acc = 0.f;
-            for (int c = 0; c < nc; ++c) {
-                const float2 e2 = __bfloat1622float2(row[c]);
-                acc += (e2.x + e2.y) * F[(size_t)(col0 + c) * B + i];
-            }
-            emi += acc * ops.emi_scale[ops.emi_scale_off[pc] + (a - ops.emi_row0[pc])];
+            for (int c = 0; c < nc; ++c) emi += row[c] * F[(size_t)(col0 + c) * B + i];
         }
     }
 }
 
+// 16-byte asynchronous copy global -> shared; src_bytes 0 fills the destination with zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One K chunk of a tile product: kCK columns of a row-major FP32 operand (loss or emission rows)
+// against the same kCK state rows of the tile's instances.
+struct RowJob {
+    const float* T;  // operand row of the tile's first row, at column 0
+    int ld;          // operand row pitch (a multiple of 4)
+    int col0;        // state row of operand column 0
+    int nc;          // operand columns
+    int c0;          // first column of the chunk
+    int which;       // 0: loss, 1: emission
+};
+
 // One 32-row x 32-instance tile per block, 512 threads. Loss and emission are tile products
-// through double-buffered shared memory when the tile's rows belong to one species and every
-// emission piece touching them covers them all (tile_fast): the two halves of the block take
-// the two halves of each K chunk with a 2 x 2 (row x instance) micro-tile per thread, and the
+// when the tile's rows belong to one species and every emission piece touching them covers
+// them all (tile_fast): all their K chunks form one job list streamed through a 3-stage
+// cp.async ring (operand chunk 32 x 128, state chunk 128 x 32); the two halves of the block take
+// the two halves of each chunk with a 2 x 2 (row x instance) micro-tile per thread, and the
 // halves' sums are added in a fixed order. The update then gives each thread one row and two
 // instances, with every load it needs issued before the arithmetic (flux columns and values,
 // state, vectors), so the latency of the L2 round trips overlaps.
@@ -564,9 +554,9 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                                                                   float* __restrict__ Fo, float* __restrict__ Co,
                                                                   unsigned long long* gstep, unsigned* ticket) {
     __shared__ float s_gain[kRT][kIT + 1];
+    __shared__ RowJob s_job[kRowsMaxJobs];
+    __shared__ int s_njob;
     extern __shared__ __align__(16) float rows_dyn[];
-    float(*s_F)[kCK][kIT] = reinterpret_cast<float(*)[kCK][kIT]>(rows_dyn);
-    float(*s_L)[kRT][kCK + 1] = reinterpret_cast<float(*)[kRT][kCK + 1]>(rows_dyn + 2 * kCK * kIT);
     // after the products the same memory holds the two halves' loss and emission tiles
     float(*s_pl)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn);
     float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + 2 * kRT * (kIT + 1));
@@ -578,6 +568,27 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     const int a0 = blockIdx.x * kRT, i0 = blockIdx.y * kIT;
     const int n = ops.n_mom, B = ops.Bcap;
     const long long step = (long long)*reinterpret_cast<volatile unsigned long long*>(gstep);
+    const bool fast = ops.tile_fast[blockIdx.x] != 0;
+
+    if (fast && tid == 0) {
+        // the tile's product chunks: loss blocks of its species, then the emission pieces of its rows
+        const int s = species_of_row(ops, a0);
+        int nj = 0;
+        if (ops.has_bin)
+            for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
+                const float* T = ops.loss_data + ops.loss_data_off[b] + (size_t)(a0 - ops.sp_off[s]) * ops.loss_ld[b];
+                for (int c0 = 0; c0 < ops.loss_ncols[b] && nj < kRowsMaxJobs; c0 += kCK)
+                    s_job[nj++] = {T, ops.loss_ld[b], ops.loss_col_off[b], ops.loss_ncols[b], c0, 0};
+            }
+        if (ops.has_emi && a0 < n)
+            for (int p = ops.emi_rptr[a0]; p < ops.emi_rptr[a0 + 1]; ++p) {
+                const int pc = ops.emi_piece[p];
+                const float* T = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a0 - ops.emi_row0[pc]) * ops.emi_ld[pc];
+                for (int c0 = 0; c0 < ops.emi_ncols[pc] && nj < kRowsMaxJobs; c0 += kCK)
+                    s_job[nj++] = {T, ops.emi_ld[pc], ops.emi_col0[pc], ops.emi_ncols[pc], c0, 1};
+            }
+        s_njob = nj;
+    }
 
     // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
     if (ops.has_bin) {
@@ -599,82 +610,61 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         }
     }
     if (tid < kIT) s_nonfin[tid] = 0;
+    __syncthreads();
 
     float acc_l[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
     float acc_e[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-    const bool fast = ops.tile_fast[blockIdx.x] != 0;
     if (fast) {
-        const int s = species_of_row(ops, a0);
-        // acc[r][i] += sum_c T[a0 + r][c] * F[col0 + c][i0 + i] over this half's part of each chunk
-        auto tile_product = [&](auto load_T, int col0, int nc, float(&acc)[2][2]) {
-            constexpr int PER = (kRT * kCK) / kRowsThreads;  // elements of each operand per thread and chunk
-            float rl[PER], rf[PER];
-            auto fetch = [&](int c0) {
+        const int nj = s_njob;
+        // a chunk into ring stage st: 1024 16-byte pieces of operand and 1024 of state, 2 + 2 per thread
+        auto issue = [&](int k, int st) {
+            float* sL = rows_dyn + st * kStageFloats;
+            float* sF = sL + kRT * kLS;
+            const RowJob J = s_job[k];
 #pragma unroll
-                for (int q = 0; q < PER; ++q) {
-                    const int e = tid + kRowsThreads * q;
-                    const int cc = e & (kCK - 1), rr = e / kCK;
-                    const int a = a0 + rr, c = c0 + cc;
-                    rl[q] = (a < n && c < nc) ? load_T(a, c) : 0.f;
-                    const int ii = e & (kIT - 1), cf = e / kIT;
-                    const int i = i0 + ii, c2 = c0 + cf;
-                    rf[q] = (c2 < nc && i < B) ? F[(size_t)(col0 + c2) * B + i] : 0.f;
-                }
-            };
-            auto stash = [&](int buf) {
-#pragma unroll
-                for (int q = 0; q < PER; ++q) {
-                    const int e = tid + kRowsThreads * q;
-                    s_L[buf][e / kCK][e & (kCK - 1)] = rl[q];
-                    s_F[buf][e / kIT][e & (kIT - 1)] = rf[q];
-                }
-            };
-            const int nch = (nc + kCK - 1) / kCK;
-            if (nch == 0) return;
-            fetch(0);
-            __syncthreads();  // the previous product's last reads of both buffers are done
-            stash(0);
-            __syncthreads();
-            const int k0 = half * (kCK / 2);
-            for (int k = 0; k < nch; ++k) {
-                const int buf = k & 1;
-                if (k + 1 < nch) fetch((k + 1) * kCK);
-#pragma unroll 8
-                for (int cc = k0; cc < k0 + kCK / 2; ++cc) {
-                    const float2 fv = *reinterpret_cast<const float2*>(&s_F[buf][cc][tx * 2]);
-                    const float l0 = s_L[buf][ty * 2][cc], l1 = s_L[buf][ty * 2 + 1][cc];
-                    acc[0][0] += l0 * fv.x;
-                    acc[0][1] += l0 * fv.y;
-                    acc[1][0] += l1 * fv.x;
-                    acc[1][1] += l1 * fv.y;
-                }
-                if (k + 1 < nch) stash(buf ^ 1);
-                __syncthreads();
+            for (int q2 = 0; q2 < 2; ++q2) {
+                const int q = tid + kRowsThreads * q2;
+                const int rr = q >> 5, c4 = (q & 31) * 4;
+                const bool ok = a0 + rr < n && J.c0 + c4 < J.nc;
+                const float* src = ok ? J.T + (size_t)rr * J.ld + J.c0 + c4 : J.T;
+                cp_async16(sL + rr * kLS + c4, src, ok ? 16 : 0);
+                const int cr = q >> 3, i4 = (q & 7) * 4;
+                const bool okf = J.c0 + cr < J.nc && i0 + i4 < B;
+                const float* srcf = okf ? F + (size_t)(J.col0 + J.c0 + cr) * B + i0 + i4 : F;
+                cp_async16(sF + cr * kIT + i4, srcf, okf ? 16 : 0);
             }
         };
-        if (ops.has_bin) {
-            for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
-                const float* base = ops.loss_data + ops.loss_data_off[b];
-                const int ld = ops.loss_ld[b], off = ops.sp_off[s];
-                tile_product([&](int a, int c) { return __ldg(base + (size_t)(a - off) * ld + c); }, ops.loss_col_off[b],
-                             ops.loss_ncols[b], acc_l);
+#pragma unroll
+        for (int k = 0; k < kRowStages - 1; ++k) {
+            if (k < nj) issue(k, k);
+            cp_async_commit();  // empty groups keep the group count uniform
+        }
+        const int k0 = half * (kCK / 2);
+        for (int k = 0; k < nj; ++k) {
+            cp_async_wait<kRowStages - 2>();
+            __syncthreads();  // chunk k landed for every thread; chunk k - 1's stage is free
+            if (k + kRowStages - 1 < nj) issue(k + kRowStages - 1, (k + kRowStages - 1) % kRowStages);
+            cp_async_commit();
+            const float* sL = rows_dyn + (k % kRowStages) * kStageFloats;
+            const float* sF = sL + kRT * kLS;
+            float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;
+#pragma unroll 8
+            for (int cc = k0; cc < k0 + kCK / 2; ++cc) {
+                const float2 fv = *reinterpret_cast<const float2*>(sF + cc * kIT + tx * 2);
+                const float l0 = sL[(ty * 2) * kLS + cc], l1 = sL[(ty * 2 + 1) * kLS + cc];
+                a00 += l0 * fv.x;
+                a01 += l0 * fv.y;
+                a10 += l1 * fv.x;
+                a11 += l1 * fv.y;
+            }
+            if (s_job[k].which) {
+                acc_e[0][0] += a00; acc_e[0][1] += a01; acc_e[1][0] += a10; acc_e[1][1] += a11;
+            } else {
+                acc_l[0][0] += a00; acc_l[0][1] += a01; acc_l[1][0] += a10; acc_l[1][1] += a11;
             }
         }
-        if (ops.has_emi && a0 < n) {
-            for (int p = ops.emi_rptr[a0]; p < ops.emi_rptr[a0 + 1]; ++p) {
-                const int pc = ops.emi_piece[p];
-                const __nv_bfloat162* base = ops.emi_data + ops.emi_data_off[pc];
-                const int ld = ops.emi_ld[pc], r0 = ops.emi_row0[pc];
-                const float* sc = ops.emi_scale + ops.emi_scale_off[pc];
-                tile_product(
-                    [&](int a, int c) {
-                        const float2 e2 = __bfloat1622float2(base[(size_t)(a - r0) * ld + c]);
-                        return (e2.x + e2.y) * sc[a - r0];
-                    },
-                    ops.emi_col0[pc], ops.emi_ncols[pc], acc_e);
-            }
-        }
-        __syncthreads();  // the chunk buffers are free: park both halves' sums
+        cp_async_wait<0>();
+        __syncthreads();  // the ring is free: park both halves' sums
 #pragma unroll
         for (int k = 0; k < 2; ++k)
 #pragma unroll
