@@ -418,6 +418,53 @@ int commit_mixed(dtb_ctx* c) {
         unsigned char* d_fast;
         DTB_TRY(copy_host_ints(c, &d_fast, fast));
         ops.tile_fast = d_fast;
+        // the fast tiles' product chunks, in the layout of the loss and emission data above:
+        // the loss blocks of the tile's species, then the emission pieces of its rows
+        std::vector<RowJob> jobs((size_t)n_tiles_r * kRowsMaxJobs);
+        std::vector<int> njobs((size_t)n_tiles_r, 0);
+        std::vector<std::vector<RowJob>> loss_of((size_t)c->ns);  // per species: (T at row 0, ld, col0, nc)
+        {
+            long long off = 0;
+            for (int sp = 0; sp < c->ns; ++sp)
+                for (auto& kv : c->losses) {
+                    if (kv.first.first != sp) continue;
+                    const int64_t nr = c->sz[sp], nc = c->sz[kv.first.second], l = round_up(nc, 4);
+                    loss_of[(size_t)sp].push_back({ops.loss_data + off, (int)l, (int)c->off[kv.first.second], (int)nc, 0, 0, 0});
+                    off += nr * l;
+                }
+        }
+        std::vector<long long> emi_off(c->emis.size());
+        {
+            long long off = 0;
+            for (size_t p = 0; p < c->emis.size(); ++p) {
+                emi_off[p] = off;
+                off += c->emis[p].nrows * round_up(c->emis[p].ncols, 4);
+            }
+        }
+        for (int t = 0; t < n_tiles_r; ++t) {
+            if (!fast[(size_t)t]) continue;
+            const int a0 = t * tr, s0 = species_of(c, a0);
+            RowJob* J = jobs.data() + (size_t)t * kRowsMaxJobs;
+            int k = 0;
+            if (c->has_bin)
+                for (const RowJob& L : loss_of[(size_t)s0])
+                    for (int c0 = 0; c0 < L.nc; c0 += kRowsChunk)
+                        J[k++] = {L.T + (size_t)(a0 - c->off[s0]) * L.ld, L.ld, L.col0, L.nc, c0, 0, 0};
+            for (int p : emi_rows[(size_t)a0]) {
+                const EmiPiece& e = c->emis[(size_t)p];
+                const int l = (int)round_up(e.ncols, 4);
+                for (int c0 = 0; c0 < e.ncols; c0 += kRowsChunk)
+                    J[k++] = {ops.emi_data + emi_off[(size_t)p] + (size_t)(a0 - e.row0) * l, l, (int)e.col0, (int)e.ncols,
+                              c0, 1, 0};
+            }
+            njobs[(size_t)t] = k;
+        }
+        RowJob* d_jobs;
+        int* d_nj;
+        DTB_TRY(copy_host_ints(c, &d_jobs, jobs));
+        DTB_TRY(copy_host_ints(c, &d_nj, njobs));
+        ops.jobs = d_jobs;
+        ops.njobs = d_nj;
     }
     ops.thr = (double)1e-10f;
     ops.has_bin = c->has_bin;

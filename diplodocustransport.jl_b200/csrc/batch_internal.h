@@ -42,6 +42,23 @@ constexpr int kGTileBytes = 2 * kMmaM * kMmaK * 2;
 int gain_gemm_smem_bytes(int bn);
 cudaError_t prepare_gain_gemm(int bn);
 
+// K chunks of loss / emission tile products one fast epilogue tile may run (more: direct path).
+constexpr int kRowsMaxJobs = 32;
+constexpr int kRowsChunk = 128;
+
+// One K chunk of an epilogue tile product: kRowsChunk columns of a row-major FP32 operand
+// (loss or emission rows) against the same state rows of the tile's instances. Built on the
+// host per 32-row tile.
+struct RowJob {
+    const float* T;  // operand row of the tile's first row, at column 0
+    int ld;          // operand row pitch (a multiple of 4)
+    int col0;        // state row of operand column 0
+    int nc;          // operand columns
+    int c0;          // first column of the chunk
+    int which;       // 0: loss, 1: emission
+    int pad;
+};
+
 // Per-row operands of the batched Euler epilogue.
 struct MixedRowOps {
     int n_mom, Bcap, n_species;  // Bcap: slots in the state matrix (a multiple of 4), its row stride
@@ -69,7 +86,9 @@ struct MixedRowOps {
     int gain_roff[64];
     const float* grp_gsum[16];    // [Bcap][M] reduced, rescaled gain sums of the group
     int grp_M[16];
-    const unsigned char* tile_fast;  // per 64-row tile: loss/emission as shared-memory tile products
+    const unsigned char* tile_fast;  // per 32-row tile: loss/emission as shared-memory tile products
+    const RowJob* jobs;              // [tile][kRowsMaxJobs] product chunks of the fast tiles
+    const int* njobs;                // [tile]
     const float* invAp;
     const float* inj;
     float vol;
@@ -96,8 +115,5 @@ cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const
 
 cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1, int n2, int n_cb,
                               unsigned char* gt, float* row_scale, cudaStream_t s);
-// K chunks of loss / emission tile products one fast epilogue tile may run (more: direct path).
-constexpr int kRowsMaxJobs = 32;
-constexpr int kRowsChunk = 128;
 
 }  // namespace dtb

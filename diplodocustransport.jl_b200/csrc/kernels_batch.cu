@@ -527,17 +527,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// One K chunk of a tile product: kCK columns of a row-major FP32 operand (loss or emission rows)
-// against the same kCK state rows of the tile's instances.
-struct RowJob {
-    const float* T;  // operand row of the tile's first row, at column 0
-    int ld;          // operand row pitch (a multiple of 4)
-    int col0;        // state row of operand column 0
-    int nc;          // operand columns
-    int c0;          // first column of the chunk
-    int which;       // 0: loss, 1: emission
-};
-
 // One 32-row x 32-instance tile per block, 512 threads. Loss and emission are tile products
 // when the tile's rows belong to one species and every emission piece touching them covers
 // them all (tile_fast): all their K chunks form one job list streamed through a 3-stage
@@ -570,24 +559,51 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     const long long step = (long long)*reinterpret_cast<volatile unsigned long long*>(gstep);
     const bool fast = ops.tile_fast[blockIdx.x] != 0;
 
-    if (fast && tid == 0) {
-        // the tile's product chunks: loss blocks of its species, then the emission pieces of its rows
-        const int s = species_of_row(ops, a0);
-        int nj = 0;
-        if (ops.has_bin)
-            for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
-                const float* T = ops.loss_data + ops.loss_data_off[b] + (size_t)(a0 - ops.sp_off[s]) * ops.loss_ld[b];
-                for (int c0 = 0; c0 < ops.loss_ncols[b] && nj < kRowsMaxJobs; c0 += kCK)
-                    s_job[nj++] = {T, ops.loss_ld[b], ops.loss_col_off[b], ops.loss_ncols[b], c0, 0};
+    if (fast) {  // the tile's product chunks (host-built job list)
+        if (tid < kRowsMaxJobs) s_job[tid] = ops.jobs[(size_t)blockIdx.x * kRowsMaxJobs + tid];
+        if (tid == 0) s_njob = ops.njobs[blockIdx.x];
+    }
+    // ---- update operands, loaded ahead of the products so their latency overlaps them
+    const int r = tid >> 4;
+    const int a = a0 + r;
+    const int jb = (tid & 15) * 2;
+    const int ib = i0 + jb;
+    const bool mine = a < n && ib < B;
+    const bool ell_fast = ops.ell_w <= kEllFast;
+    float2 fa2 = make_float2(0.f, 0.f), ca2 = make_float2(0.f, 0.f);
+    double inv_ap = 0.0, injv = 0.0;
+    bool act[2] = {false, false};
+    double dts[2] = {0.0, 0.0};
+    int cols[kEllFast];
+    float vals[kEllFast];
+#pragma unroll
+    for (int e = 0; e < kEllFast; ++e) {
+        cols[e] = -1;
+        vals[e] = 0.f;
+    }
+    if (mine) {
+        const size_t idx = (size_t)a * B + ib;  // B and ib are even
+        fa2 = *reinterpret_cast<const float2*>(F + idx);
+        ca2 = *reinterpret_cast<const float2*>(Cc + idx);
+        inv_ap = (double)__ldg(ops.invAp + a);
+        injv = (double)__ldg(ops.inj + a);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = ib + j;
+            act[j] = i < B && step < ops.stop_step[i];
+            dts[j] = i < B ? ops.dt_scale[i] : 0.0;
+        }
+        if (ell_fast) {
+            const int* crow = ops.ell_col + (size_t)a * ops.ell_w;
+            const float* vrow = ops.ell_val + (size_t)a * ops.ell_w;
+#pragma unroll
+            for (int e = 0; e < kEllFast; ++e) {
+                if (e < ops.ell_w) {
+                    cols[e] = __ldg(crow + e);
+                    vals[e] = __ldg(vrow + e);
+                }
             }
-        if (ops.has_emi && a0 < n)
-            for (int p = ops.emi_rptr[a0]; p < ops.emi_rptr[a0 + 1]; ++p) {
-                const int pc = ops.emi_piece[p];
-                const float* T = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a0 - ops.emi_row0[pc]) * ops.emi_ld[pc];
-                for (int c0 = 0; c0 < ops.emi_ncols[pc] && nj < kRowsMaxJobs; c0 += kCK)
-                    s_job[nj++] = {T, ops.emi_ld[pc], ops.emi_col0[pc], ops.emi_ncols[pc], c0, 1};
-            }
-        s_njob = nj;
+        }
     }
 
     // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
@@ -611,6 +627,11 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     }
     if (tid < kIT) s_nonfin[tid] = 0;
     __syncthreads();
+    float2 fv[kEllFast];
+#pragma unroll
+    for (int e = 0; e < kEllFast; ++e)
+        fv[e] = (mine && cols[e] >= 0) ? *reinterpret_cast<const float2*>(F + (size_t)cols[e] * B + ib)
+                                       : make_float2(0.f, 0.f);
 
     float acc_l[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
     float acc_e[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
@@ -676,41 +697,12 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     __syncthreads();
 
     // ---- update: one row, two instances per thread
-    const int r = tid >> 4;
-    const int a = a0 + r;
-    const int jb = (tid & 15) * 2;
-    const int ib = i0 + jb;
     double rmin[2] = {CUDART_INF, CUDART_INF};
     int nonfin[2] = {0, 0};
-    if (a < n && ib < B) {
-        const size_t idx = (size_t)a * B + ib;  // B and ib are even
-        // every independent load first
-        const float2 fa2 = *reinterpret_cast<const float2*>(F + idx);
-        const float2 ca2 = *reinterpret_cast<const float2*>(Cc + idx);
-        const double inv_ap = (double)__ldg(ops.invAp + a), injv = (double)__ldg(ops.inj + a);
-        bool act[2];
-        double dts[2];
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int i = ib + j;
-            act[j] = i < B && step < ops.stop_step[i];
-            dts[j] = i < B ? ops.dt_scale[i] : 0.0;
-        }
+    if (mine) {
+        const size_t idx = (size_t)a * B + ib;
         float flux[2] = {0.f, 0.f};
-        const int* crow = ops.ell_col + (size_t)a * ops.ell_w;
-        const float* vrow = ops.ell_val + (size_t)a * ops.ell_w;
-        if (ops.ell_w <= kEllFast) {
-            int cols[kEllFast];
-            float vals[kEllFast];
-#pragma unroll
-            for (int e = 0; e < kEllFast; ++e) {
-                cols[e] = e < ops.ell_w ? __ldg(crow + e) : -1;
-                vals[e] = e < ops.ell_w ? __ldg(vrow + e) : 0.f;
-            }
-            float2 fv[kEllFast];
-#pragma unroll
-            for (int e = 0; e < kEllFast; ++e)
-                fv[e] = cols[e] >= 0 ? *reinterpret_cast<const float2*>(F + (size_t)cols[e] * B + ib) : make_float2(0.f, 0.f);
+        if (ell_fast) {
 #pragma unroll
             for (int e = 0; e < kEllFast; ++e) {
                 if (cols[e] < 0) continue;  // padding: only stored entries take part
@@ -718,6 +710,8 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                 flux[1] += vals[e] * fv[e].y;
             }
         } else {
+            const int* crow = ops.ell_col + (size_t)a * ops.ell_w;
+            const float* vrow = ops.ell_val + (size_t)a * ops.ell_w;
             for (int e = 0; e < ops.ell_w; ++e) {
                 const int col = __ldg(crow + e);
                 if (col < 0) continue;
