@@ -24,7 +24,7 @@ struct MixedGroup {
     float* row_scale = nullptr;
     float* partial = nullptr;
     float* gsum = nullptr;  // [Bcap][M]
-    int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256;
+    int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256, splits_per_cb = 0;
     double flops = 0;  // 3 MMAs x 2 x M x K x Bcap
     double bytes = 0;  // hi + lo bytes of G
 };
@@ -189,6 +189,14 @@ int commit_mixed(dtb_ctx* c) {
         S = std::min(S, T);
         G.tiles_per_split = (T + S - 1) / S;
         G.n_splits = (T + G.tiles_per_split - 1) / G.tiles_per_split;
+        // splits aligned to the 64-wide input-2 blocks when that keeps nearly every SM busy: a
+        // split then never reloads its f2 block in mid-stream
+        const int k_cb = S / G.n_cb;
+        G.splits_per_cb = 0;
+        if (k_cb >= 1 && k_cb <= G.N1 && (double)(k_cb * G.n_cb) >= 0.95 * S) {
+            G.splits_per_cb = k_cb;
+            G.n_splits = k_cb * G.n_cb;
+        }
         DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
         DTB_TRY(c->alloc(&G.gsum, sizeof(float) * (size_t)B * G.M));
         G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * m->Buser;
@@ -528,6 +536,7 @@ int mixed_step(dtb_ctx* c, bool profile) {
         a.off2 = (int)c->off[G.in2];
         a.tiles_per_split = G.tiles_per_split;
         a.n_splits = G.n_splits;
+        a.splits_per_cb = G.splits_per_cb;
         a.m_tiles = G.m_tiles;
         a.n_tiles = G.n_tiles;
         a.Bcap = m->Buser;

@@ -24,6 +24,7 @@ struct GemmArgs {
     int n_cb;       // 64-wide blocks of input species 2 (n2 padded to 64)
     int off1, off2; // state offsets of the two input species
     int tiles_per_split, n_splits, m_tiles, n_tiles;
+    int splits_per_cb;  // > 0: every split lies inside one 64-wide input-2 block (K tiles cb-major)
     int Bcap;       // instances that exist (columns >= Bcap are zero in X)
     int Bst;        // row stride of the state matrix F[n][Bst]
     int Bpad;       // n_tiles * BN, instance stride of the partial rows

@@ -109,7 +109,7 @@ struct GemmCfg {
     static constexpr int SB = 2;
     static constexpr int SA = BN == 256 ? 3 : (BN == 128 ? 4 : 6);
     static constexpr int DATA = SA * 2 * A_BYTES + SB * 2 * B_BYTES;
-    static constexpr int BARS = (2 * SA + 2 * SB + 2) * 8;
+    static constexpr int BARS = (2 * SA + 2 * SB + 3) * 8;
     static constexpr int SMEM = 1024 + DATA + BARS + 16;   // 1024: alignment slack
 };
 
@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     uint64_t* empty_b = full_b + C::SB;
     uint64_t* acc_bar = empty_b + C::SB;
     uint64_t* drain_bar = acc_bar + 1;
-    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain_bar + 1);
+    uint64_t* x0_bar = drain_bar + 1;  // the first X tile is written (its state loads are done)
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(x0_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -137,8 +138,17 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     const int m_tile = (task / a.n_tiles) % a.m_tiles;
     const int split = task / (a.n_tiles * a.m_tiles);
     const int T = a.n_cb * a.N1;
-    const int t0 = split * a.tiles_per_split;
-    const int t1 = min(T, t0 + a.tiles_per_split);
+    // K range of this split: within one input-2 block when the splits are aligned to them (the
+    // producers then load that block's f2 once), else an even cut of all K tiles
+    int t0, t1;
+    if (a.splits_per_cb > 0) {
+        const int cb = split / a.splits_per_cb, piece = split - cb * a.splits_per_cb;
+        t0 = cb * a.N1 + (int)((long long)piece * a.N1 / a.splits_per_cb);
+        t1 = cb * a.N1 + (int)((long long)(piece + 1) * a.N1 / a.splits_per_cb);
+    } else {
+        t0 = split * a.tiles_per_split;
+        t1 = min(T, t0 + a.tiles_per_split);
+    }
     const int m0 = m_tile * kMmaM, n0 = n_tile * BN;
     // columns of this tile that belong to slots still stepping, rounded up to the MMA's N granule
     const int hi_cols = *reinterpret_cast<const volatile int*>(a.active_hi);
@@ -156,6 +166,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
         }
         mb_init(smem_addr(acc_bar), 1);
         mb_init(smem_addr(drain_bar), 1);
+        mb_init(smem_addr(x0_bar), BN / 32);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -190,6 +201,14 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 bulk_load(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
                 bulk_load(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
                           smem_addr(&full_a[sa]));
+                // the producers' state loads come first: the rest of the G ring waits for the first
+                // X tile, so those loads do not queue behind every CTA's full ring of G traffic
+                if (j == 0 && nt > 1 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+                    *abort_flag = 1;
+                    ++j;
+                    break;
+                }
             }
             // drain: this block's own copies must land before it may exit
             for (int k = j > C::SA ? j - C::SA : 0; k < j; ++k) {
@@ -298,7 +317,10 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 // arrive per warp once every lane has fenced
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                if (lane == 0) mb_arrive(smem_addr(&full_b[sb]));
+                if (lane == 0) {
+                    mb_arrive(smem_addr(&full_b[sb]));
+                    if (j == 0) mb_arrive(smem_addr(x0_bar));
+                }
             }
         }
         // epilogue: TMEM lanes 32*(warp%4).. hold rows m0 + 32*(warp%4) + lane
