@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             for (int j = 0; j < nt; ++j) {
                 const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
                 const int sb = j % C::SB;
-                const float x1 = x1_next * s1;
+                const float x1 = (x1_next * s1) * s2;  // both scales are powers of two: exact
                 if (valid && j + 1 < nt) {
                     const int tn = t + 1, bn = tn - (tn / a.N1) * a.N1;
                     x1_next = __ldg(a.F + (size_t)(a.off1 + bn) * a.Bst + inst);
@@ -288,11 +288,17 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                     break;
                 }
                 if (cb != cur_cb) {
+                    // 64 unconditional loads (clamped in bounds) issued back to back, the padding
+                    // zeroed afterwards: one round trip instead of a load-use chain
+                    const float* fb = a.F + (valid ? inst : 0);
 #pragma unroll
                     for (int c = 0; c < kMmaK; ++c) {
-                        const int cc = cb * kMmaK + c;
-                        f2r[c] = (valid && cc < a.n2) ? __ldg(a.F + (size_t)(a.off2 + cc) * a.Bst + inst) * s2 : 0.f;
+                        const int cc = min(cb * kMmaK + c, a.n2 - 1);
+                        f2r[c] = __ldg(fb + (size_t)(a.off2 + cc) * a.Bst);
                     }
+#pragma unroll
+                    for (int c = 0; c < kMmaK; ++c)
+                        if (!valid || cb * kMmaK + c >= a.n2) f2r[c] = 0.f;
                     cur_cb = cb;
                 }
                 unsigned char* rhi = b_base + (size_t)(sb * 2) * C::B_BYTES + (size_t)p * 128;
