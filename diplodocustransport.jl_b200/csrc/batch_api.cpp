@@ -43,7 +43,6 @@ struct MixedState {
     unsigned long long* min_ratio = nullptr;
     int* nonfinite = nullptr;
     unsigned long long* gstep = nullptr;
-    unsigned* ticket = nullptr;
     int* active_hi = nullptr;  // device: 1 + the highest slot that still steps
     int last_active_hi = -1;
     long long host_step = 0;
@@ -370,13 +369,11 @@ int commit_mixed(dtb_ctx* c) {
     DTB_CUDA(cudaMemsetAsync(m->active_hi, 0, sizeof(int), s));
     m->last_active_hi = 0;
     DTB_TRY(c->alloc(&m->gstep, sizeof(unsigned long long)));
-    DTB_TRY(c->alloc(&m->ticket, sizeof(unsigned)));
     DTB_TRY(c->alloc(&c->err, sizeof(int)));
     DTB_CUDA(cudaMemsetAsync(m->dt_scale, 0, sizeof(double) * B, s));
     DTB_CUDA(cudaMemsetAsync(m->stop_step, 0, sizeof(long long) * B, s));
     DTB_CUDA(cudaMemsetAsync(m->nonfinite, 0, sizeof(int) * B, s));
     DTB_CUDA(cudaMemsetAsync(m->gstep, 0, sizeof(unsigned long long), s));
-    DTB_CUDA(cudaMemsetAsync(m->ticket, 0, sizeof(unsigned), s));
     DTB_CUDA(cudaMemsetAsync(c->err, 0, sizeof(int), s));
     {
         std::vector<unsigned long long> inf((size_t)B, ord_enc_host(INFINITY));
@@ -510,7 +507,9 @@ int mixed_flush_profile(MixedState* m) {
     return DTB_OK;
 }
 
-int mixed_step(dtb_ctx* c, bool profile) {
+// One batched step; kpos is its place in a launch sequence whose last step advances the device
+// step counter by the sequence length (advance), so no kernel needs a grid-wide ticket.
+int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
     MixedState* m = c->mixed;
     const float* Fin = m->F[m->cur];
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -559,8 +558,9 @@ int mixed_step(dtb_ctx* c, bool profile) {
         DTB_CUDA(launch_split_reduce(G.partial, G.n_splits, G.Bpad, G.M, m->Bcap, G.row_scale,
                                      m->sig + (size_t)G.in1 * m->Bcap, m->sig + (size_t)G.in2 * m->Bcap, G.gsum,
                                      m->active_hi, c->stream));
-    DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, m->ticket,
+    DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, kpos,
                                c->stream));
+    if (advance > 0) DTB_CUDA(launch_advance_step(m->gstep, advance, c->stream));
     m->cur ^= 1;
     m->host_step++;
     return DTB_OK;
@@ -573,7 +573,8 @@ int ensure_mixed_graph(dtb_ctx* c) {
     cudaGraph_t gr;
     DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = DTB_OK;
-    for (int k = 0; k < m->graph_steps && rc == DTB_OK; ++k) rc = mixed_step(c, false);
+    for (int k = 0; k < m->graph_steps && rc == DTB_OK; ++k)
+        rc = mixed_step(c, false, k, k == m->graph_steps - 1 ? m->graph_steps : 0);
     cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
     m->host_step = hs;
     m->cur = 0;
@@ -634,7 +635,7 @@ int batch_launch(dtb_ctx* c, int64_t nsteps) {
     int64_t done = 0;
     if (nsteps >= m->graph_steps) {
         if (m->cur != 0) {
-            DTB_TRY(mixed_step(c, false));
+            DTB_TRY(mixed_step(c, false, 0, 1));
             done++;
         }
         DTB_TRY(ensure_mixed_graph(c));
@@ -644,7 +645,7 @@ int batch_launch(dtb_ctx* c, int64_t nsteps) {
             m->host_step += m->graph_steps;
         }
     }
-    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, false));
+    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, false, 0, 1));
     return DTB_OK;
 }
 
@@ -715,7 +716,7 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
     int64_t done = 0;
     if (!m->profiling && nsteps >= m->graph_steps) {
         if (m->cur != 0) {
-            DTB_TRY(mixed_step(c, false));
+            DTB_TRY(mixed_step(c, false, 0, 1));
             done++;
         }
         DTB_TRY(ensure_mixed_graph(c));
@@ -725,7 +726,7 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
             m->host_step += m->graph_steps;
         }
     }
-    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, m->profiling));
+    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, m->profiling, 0, 1));
     if (m->profiling) DTB_TRY(mixed_flush_profile(m));
     return mixed_check_err(c);
 }

@@ -102,7 +102,8 @@ struct MixedRowOps {
 };
 
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out,
-                              float* C_out, unsigned long long* gstep, unsigned* ticket, cudaStream_t s);
+                              float* C_out, const unsigned long long* gstep, int kpos, cudaStream_t s);
+cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s);
 cudaError_t launch_pack_f(const double* io, int Buser, int n, int Bcap, float* F, float* C, cudaStream_t s);
 cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, int Bcap, double* io, cudaStream_t s);
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,

@@ -564,27 +564,32 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // instances, with every load it needs issued before the arithmetic (flux columns and values,
 // state, vectors), so the latency of the L2 round trips overlaps.
 constexpr int kRowsThreads = 512;
+constexpr int kKGroups = kRowsThreads / 64;  // K-slices of each product chunk
+static_assert(2 * kKGroups * kRT * (kIT + 1) <= kRowStages * kStageFloats, "partial tiles fit the ring");
 constexpr int kEllFast = 8;  // ELL widths up to this take the hoisted-load flux path
 
 __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
                                                                   const float* __restrict__ Cc,
                                                                   float* __restrict__ Fo, float* __restrict__ Co,
-                                                                  unsigned long long* gstep, unsigned* ticket) {
+                                                                  const unsigned long long* gstep, int kpos) {
     __shared__ float s_gain[kRT][kIT + 1];
     __shared__ RowJob s_job[kRowsMaxJobs];
     __shared__ int s_njob;
     extern __shared__ __align__(16) float rows_dyn[];
     // after the products the same memory holds the two halves' loss and emission tiles
     float(*s_pl)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn);
-    float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + 2 * kRT * (kIT + 1));
+    float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + kKGroups * kRT * (kIT + 1));
     __shared__ double s_min[kRT][kIT];
     __shared__ int s_nonfin[kIT];
-    __shared__ int s_last;
     const int tid = threadIdx.x;
-    const int half = tid >> 8, ht = tid & 255, tx = ht & 15, ty = ht >> 4;
+    // products: 8 groups of 64 threads split each K chunk; a 4 x 4 micro-tile per thread (rows
+    // ty + 8k, instances 4 tx .. 4 tx + 3), so a 16-wide slice of K costs 5 shared loads per 16 FMAs
+    const int kg = tid >> 6, lt = tid & 63, tx = lt & 7, ty = lt >> 3;
     const int a0 = blockIdx.x * kRT, i0 = blockIdx.y * kIT;
     const int n = ops.n_mom, B = ops.Bcap;
-    const long long step = (long long)*reinterpret_cast<volatile unsigned long long*>(gstep);
+    // the device step counter advances once per launch sequence (advance_step); kpos is this
+    // launch's place in the sequence
+    const long long step = (long long)*reinterpret_cast<const volatile unsigned long long*>(gstep) + kpos;
     const bool fast = ops.tile_fast[blockIdx.x] != 0;
 
     if (fast) {  // the tile's product chunks (host-built job list)
@@ -661,8 +666,14 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         fv[e] = (mine && cols[e] >= 0) ? *reinterpret_cast<const float2*>(F + (size_t)cols[e] * B + ib)
                                        : make_float2(0.f, 0.f);
 
-    float acc_l[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-    float acc_e[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    float acc_l[4][4], acc_e[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            acc_l[k][j] = 0.f;
+            acc_e[k][j] = 0.f;
+        }
     if (fast) {
         const int nj = s_njob;
         // a chunk into ring stage st: 1024 16-byte pieces of operand and 1024 of state, 2 + 2 per thread
@@ -688,7 +699,7 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             if (k < nj) issue(k, k);
             cp_async_commit();  // empty groups keep the group count uniform
         }
-        const int k0 = half * (kCK / 2);
+        const int k0 = kg * (kCK / kKGroups);
         for (int k = 0; k < nj; ++k) {
             cp_async_wait<kRowStages - 2>();
             __syncthreads();  // chunk k landed for every thread; chunk k - 1's stage is free
@@ -696,30 +707,42 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             cp_async_commit();
             const float* sL = rows_dyn + (k % kRowStages) * kStageFloats;
             const float* sF = sL + kRT * kLS;
-            float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;
-#pragma unroll 8
-            for (int cc = k0; cc < k0 + kCK / 2; ++cc) {
-                const float2 fv = *reinterpret_cast<const float2*>(sF + cc * kIT + tx * 2);
-                const float l0 = sL[(ty * 2) * kLS + cc], l1 = sL[(ty * 2 + 1) * kLS + cc];
-                a00 += l0 * fv.x;
-                a01 += l0 * fv.y;
-                a10 += l1 * fv.x;
-                a11 += l1 * fv.y;
+            float t[4][4];
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+                for (int j2 = 0; j2 < 4; ++j2) t[k2][j2] = 0.f;
+#pragma unroll
+            for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
+                const float4 f4 = *reinterpret_cast<const float4*>(sF + cc * kIT + tx * 4);
+                const float fvv[4] = {f4.x, f4.y, f4.z, f4.w};
+#pragma unroll
+                for (int k2 = 0; k2 < 4; ++k2) {
+                    const float l = sL[(ty + 8 * k2) * kLS + cc];
+#pragma unroll
+                    for (int j2 = 0; j2 < 4; ++j2) t[k2][j2] += l * fvv[j2];
+                }
             }
             if (s_job[k].which) {
-                acc_e[0][0] += a00; acc_e[0][1] += a01; acc_e[1][0] += a10; acc_e[1][1] += a11;
+#pragma unroll
+                for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+                    for (int j2 = 0; j2 < 4; ++j2) acc_e[k2][j2] += t[k2][j2];
             } else {
-                acc_l[0][0] += a00; acc_l[0][1] += a01; acc_l[1][0] += a10; acc_l[1][1] += a11;
+#pragma unroll
+                for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+                    for (int j2 = 0; j2 < 4; ++j2) acc_l[k2][j2] += t[k2][j2];
             }
         }
         cp_async_wait<0>();
-        __syncthreads();  // the ring is free: park both halves' sums
+        __syncthreads();  // the ring is free: park the groups' sums
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < 4; ++k)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                s_pl[half][ty * 2 + k][tx * 2 + j] = acc_l[k][j];
-                s_pe[half][ty * 2 + k][tx * 2 + j] = acc_e[k][j];
+            for (int j = 0; j < 4; ++j) {
+                s_pl[kg][ty + 8 * k][tx * 4 + j] = acc_l[k][j];
+                s_pe[kg][ty + 8 * k][tx * 4 + j] = acc_e[k][j];
             }
     }
     __syncthreads();
@@ -762,8 +785,13 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             }
             float loss, emi;
             if (fast) {
-                loss = s_pl[0][r][jb + j] + s_pl[1][r][jb + j];
-                emi = s_pe[0][r][jb + j] + s_pe[1][r][jb + j];
+                loss = 0.f;
+                emi = 0.f;
+#pragma unroll
+                for (int g = 0; g < kKGroups; ++g) {  // fixed order
+                    loss += s_pl[g][r][jb + j];
+                    emi += s_pe[g][r][jb + j];
+                }
             } else {
                 row_terms_direct(ops, F, a, s, ib + j, loss, emi);
             }
@@ -794,31 +822,22 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         if (nonfin[j]) atomicOr(&s_nonfin[jb + j], 1);
     }
     __syncthreads();
-    if (tid < kIT) {
-        double m = CUDART_INF;
-        for (int y = 0; y < kRT; ++y) {
-            const double v = s_min[y][tid];
+    {
+        // 16 lanes per instance, two rows each, then a shuffle tree (min with -0.0 below +0.0)
+        const int il = tid >> 4, rg = tid & 15;
+        double m = s_min[rg][il];
+        const double v2 = s_min[rg + 16][il];
+        if (v2 < m || (v2 == m && signbit(v2))) m = v2;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            const double v = __shfl_xor_sync(0xffffffffu, m, o);
             if (v < m || (v == m && signbit(v))) m = v;
         }
-        const int i = i0 + tid;
-        if (i < B && step < ops.stop_step[i]) {
+        const int i = i0 + il;
+        if (rg == 0 && i < B && step < ops.stop_step[i]) {
             atomicMin(&ops.min_ratio[i], ord_enc(m));
-            if (s_nonfin[tid]) atomicOr(&ops.nonfinite[i], 1);
+            if (s_nonfin[il]) atomicOr(&ops.nonfinite[i], 1);
         }
-    }
-    // the last block to finish advances the global step counter
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        const unsigned total = gridDim.x * gridDim.y;
-        const unsigned t = atomicAdd(ticket, 1u);
-        s_last = (t == total - 1);
-    }
-    __syncthreads();
-    if (s_last && tid == 0) {
-        *ticket = 0u;
-        __threadfence();
-        *reinterpret_cast<volatile unsigned long long*>(gstep) = (unsigned long long)(step + 1);
     }
 }
 
@@ -910,10 +929,17 @@ cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const
     return cudaGetLastError();
 }
 
+__global__ void advance_step_kernel(unsigned long long* gstep, int n) { *gstep += (unsigned long long)n; }
+
+cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s) {
+    advance_step_kernel<<<1, 1, 0, s>>>(gstep, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
-                              unsigned long long* gstep, unsigned* ticket, cudaStream_t s) {
+                              const unsigned long long* gstep, int kpos, cudaStream_t s) {
     dim3 grid((ops.n_mom + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
-    mixed_rows_kernel<<<grid, kRowsThreads, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, ticket);
+    mixed_rows_kernel<<<grid, kRowsThreads, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, kpos);
     return cudaGetLastError();
 }
 
