@@ -82,7 +82,6 @@ double ord_dec_host(unsigned long long e) {
 
 // Builds the device layouts of a DTB_MIXED context.
 int commit_mixed(dtb_ctx* c) {
-    DTB_CHECK(c->n_space == 1, DTB_EINVAL, "batched contexts hold single-cell instances (n_space must be 1)");
     DTB_CHECK(c->opts.batch >= 1, DTB_EINVAL, "batched context needs opts.batch >= 1");
     // the tensor-core GEMM streams dense blocks: a sparse M_Bin is densified per block
     for (auto& kv : c->sgains) {
@@ -107,6 +106,10 @@ int commit_mixed(dtb_ctx* c) {
     MixedRowOps& ops = m->ops;
     const int B = m->Bcap;
     const int n_mom = (int)c->n_mom;
+    // a slot holds n_space cells of n_mom states: the state matrix has n_state rows, and the gain
+    // GEMM takes every (cell, slot) pair as a column
+    const int n_st = (int)c->n_state, nsp = c->n_space;
+    const int Bcols = nsp * B;
     cudaStream_t s = c->stream;
 
     // ---------------- gain groups
@@ -131,7 +134,7 @@ int commit_mixed(dtb_ctx* c) {
     }
     DTB_CHECK(m->groups.size() <= 16, DTB_EINVAL, "at most 16 input pairs in a batched context");
     c->has_bin = !c->gains.empty() || !c->losses.empty();
-    const int bn = B >= 192 ? 256 : (B > 64 ? 128 : 64);
+    const int bn = Bcols >= 192 ? 256 : (Bcols > 64 ? 128 : 64);
     for (auto& kv : c->gains) {
         GainStage& g = kv.second;
         MixedGroup& G = m->groups[(size_t)gidx[{g.in1, g.in2}]];
@@ -180,7 +183,7 @@ int commit_mixed(dtb_ctx* c) {
     DTB_CUDA(prepare_mixed_rows());
     for (auto& G : m->groups) {
         G.bn = bn;
-        G.n_tiles = (B + bn - 1) / bn;
+        G.n_tiles = (Bcols + bn - 1) / bn;
         G.Bpad = G.n_tiles * bn;
         G.m_tiles = (G.M + kMmaM - 1) / kMmaM;
         const int T = G.n_cb * G.N1;
@@ -197,8 +200,8 @@ int commit_mixed(dtb_ctx* c) {
             G.n_splits = k_cb * G.n_cb;
         }
         DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
-        DTB_TRY(c->alloc(&G.gsum, sizeof(float) * (size_t)B * G.M));
-        G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * m->Buser;
+        DTB_TRY(c->alloc(&G.gsum, sizeof(float) * (size_t)Bcols * G.M));
+        G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * m->Buser * nsp;
         G.bytes = 4.0 * G.M * (double)G.N1 * G.n2;
     }
     // ---------------- gain lookup per species
@@ -259,7 +262,7 @@ int commit_mixed(dtb_ctx* c) {
         c->has_emi = !c->emis.empty();
         std::vector<long long> doff;
         std::vector<int> ld, r0v, c0v, ncv;
-        std::vector<std::vector<int>> rows((size_t)n_mom);
+        std::vector<std::vector<int>> rows((size_t)n_st);
         std::vector<double> data;
         for (size_t p = 0; p < c->emis.size(); ++p) {
             const EmiPiece& e = c->emis[p];
@@ -278,12 +281,12 @@ int commit_mixed(dtb_ctx* c) {
         }
         float* d_data = nullptr;
         DTB_TRY(copy_host_vec(c, &d_data, data));
-        std::vector<int> rptr((size_t)n_mom + 1, 0), piece;
-        for (int i = 0; i < n_mom; ++i) {
+        std::vector<int> rptr((size_t)n_st + 1, 0), piece;
+        for (int i = 0; i < n_st; ++i) {
             rptr[(size_t)i] = (int)piece.size();
             for (int p : rows[(size_t)i]) piece.push_back(p);
         }
-        rptr[(size_t)n_mom] = (int)piece.size();
+        rptr[(size_t)n_st] = (int)piece.size();
         int *d_rptr, *d_piece, *d_ld, *d_r0, *d_c0, *d_nc;
         long long* d_doff;
         DTB_TRY(copy_host_ints(c, &d_rptr, rptr));
@@ -304,7 +307,7 @@ int commit_mixed(dtb_ctx* c) {
     }
     // ---------------- flux: CSR with duplicates summed, banded ELL (FP32), padding column -1
     {
-        std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)n_mom);
+        std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)n_st);
         for (size_t p = 0; p < c->flux_r.size(); ++p) rows[(size_t)c->flux_r[p]].push_back({c->flux_c[p], c->flux_v[p]});
         int w = 0;
         for (auto& r : rows) {
@@ -320,9 +323,9 @@ int commit_mixed(dtb_ctx* c) {
             w = std::max<int>(w, (int)r.size());
         }
         w = std::max(w, 1);
-        std::vector<double> val((size_t)n_mom * w, 0.0);
-        std::vector<int> col((size_t)n_mom * w, -1);
-        for (int i = 0; i < n_mom; ++i)
+        std::vector<double> val((size_t)n_st * w, 0.0);
+        std::vector<int> col((size_t)n_st * w, -1);
+        for (int i = 0; i < n_st; ++i)
             for (size_t k = 0; k < rows[(size_t)i].size(); ++k) {
                 col[(size_t)i * w + k] = (int)rows[(size_t)i][k].first;
                 val[(size_t)i * w + k] = rows[(size_t)i][k].second;
@@ -344,9 +347,22 @@ int commit_mixed(dtb_ctx* c) {
         DTB_TRY(copy_host_vec(c, &d_inj, c->inj));
         ops.invAp = d_inv;
         ops.inj = d_inj;
-        ops.vol = (float)c->Vol[0];
+        // per-cell Vol and BinM.Domain
+        std::vector<double> vol(c->Vol.begin(), c->Vol.end());
+        float* d_vol;
+        DTB_TRY(copy_host_vec(c, &d_vol, vol));
+        ops.vol_cell = d_vol;
+        ops.bin_on = nullptr;
+        if (c->has_bin_domain) {
+            std::vector<unsigned char> on((size_t)nsp, 0);
+            for (int64_t k : c->bin_domain)
+                if (k >= 0 && k < nsp) on[(size_t)k] = 1;
+            unsigned char* d_on;
+            DTB_TRY(copy_host_ints(c, &d_on, on));
+            ops.bin_on = d_on;
+        }
     }
-    const size_t nb = (size_t)n_mom * B;
+    const size_t nb = (size_t)n_st * B;
     for (int k = 0; k < 2; ++k) {
         DTB_TRY(c->alloc(&m->F[k], sizeof(float) * nb));
         DTB_TRY(c->alloc(&m->C[k], sizeof(float) * nb));
@@ -384,13 +400,15 @@ int commit_mixed(dtb_ctx* c) {
         std::vector<int> spo(c->off, c->off + c->ns + 1);
         DTB_TRY(copy_host_ints(c, &m->sp_off, spo));
         DTB_TRY(c->alloc(&m->mom_w, sizeof(double) * (size_t)n_mom));
-        DTB_TRY(c->alloc(&m->mom_out, sizeof(double) * 2 * (size_t)c->ns * B));
+        DTB_TRY(c->alloc(&m->mom_out, sizeof(double) * 2 * (size_t)c->ns * B * nsp));
     }
-    DTB_CUDA(cudaMallocHost(&m->pin_col, sizeof(float) * 2 * (size_t)n_mom));
+    DTB_CUDA(cudaMallocHost(&m->pin_col, sizeof(float) * 2 * (size_t)n_st));
     DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));
     m->h_stop.assign((size_t)B, 0);
     m->h_start.assign((size_t)B, 0);
     ops.n_mom = n_mom;
+    ops.n_state = n_st;
+    ops.n_space = nsp;
     ops.Bcap = B;
     ops.n_species = c->ns;
     for (int sp = 0; sp <= c->ns; ++sp) ops.sp_off[sp] = (int)c->off[sp];
@@ -403,16 +421,17 @@ int commit_mixed(dtb_ctx* c) {
     // them take the shared-memory tile products
     {
         const int tr = mixed_rows_tile_rows();
-        const int n_tiles_r = (n_mom + tr - 1) / tr;
-        std::vector<std::vector<int>> emi_rows((size_t)n_mom);
+        const int n_tiles_r = (n_st + tr - 1) / tr;
+        std::vector<std::vector<int>> emi_rows((size_t)n_st);
         for (size_t p = 0; p < c->emis.size(); ++p)
             for (int64_t r = 0; r < c->emis[p].nrows; ++r) emi_rows[(size_t)(c->emis[p].row0 + r)].push_back((int)p);
         std::vector<unsigned char> fast((size_t)n_tiles_r, 1);
         for (int t = 0; t < n_tiles_r; ++t) {
-            const int a0 = t * tr, a1 = std::min(n_mom, a0 + tr);
-            const int s0 = species_of(c, a0);
+            const int a0 = t * tr, a1 = std::min(n_st, a0 + tr);
+            const int s0 = species_of(c, a0 % n_mom);
+            if (a0 / n_mom != (a1 - 1) / n_mom) fast[(size_t)t] = 0;  // the tile lies in one cell
             for (int a = a0; a < a1; ++a)
-                if (species_of(c, a) != s0 || emi_rows[(size_t)a] != emi_rows[(size_t)a0]) fast[(size_t)t] = 0;
+                if (species_of(c, a % n_mom) != s0 || emi_rows[(size_t)a] != emi_rows[(size_t)a0]) fast[(size_t)t] = 0;
             // and whose K chunks fit the kernel's job list
             int64_t jobs = 0;
             for (auto& kv : c->losses)
@@ -448,13 +467,14 @@ int commit_mixed(dtb_ctx* c) {
         }
         for (int t = 0; t < n_tiles_r; ++t) {
             if (!fast[(size_t)t]) continue;
-            const int a0 = t * tr, s0 = species_of(c, a0);
+            const int a0 = t * tr, cell = a0 / n_mom, s0 = species_of(c, a0 % n_mom);
             RowJob* J = jobs.data() + (size_t)t * kRowsMaxJobs;
             int k = 0;
-            if (c->has_bin)
+            if (c->has_bin)  // the loss of a cell reads that cell's states
                 for (const RowJob& L : loss_of[(size_t)s0])
                     for (int c0 = 0; c0 < L.nc; c0 += kRowsChunk)
-                        J[k++] = {L.T + (size_t)(a0 - c->off[s0]) * L.ld, L.ld, L.col0, L.nc, c0, 0, 0};
+                        J[k++] = {L.T + (size_t)(a0 - cell * n_mom - c->off[s0]) * L.ld, L.ld, L.col0 + cell * n_mom, L.nc,
+                                  c0, 0, 0};
             for (int p : emi_rows[(size_t)a0]) {
                 const EmiPiece& e = c->emis[(size_t)p];
                 const int l = (int)round_up(e.ncols, 4);
@@ -540,6 +560,8 @@ int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
         a.n_tiles = G.n_tiles;
         a.Bcap = m->Buser;
         a.Bst = m->Bcap;
+        a.n_space = c->n_space;
+        a.n_mom = (int)c->n_mom;
         a.Bpad = G.Bpad;
         a.F = Fin;
         a.isig1 = m->isig + (size_t)G.in1 * m->Bcap;
@@ -557,7 +579,7 @@ int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
     for (auto& G : m->groups)
         DTB_CUDA(launch_split_reduce(G.partial, G.n_splits, G.Bpad, G.M, m->Bcap, G.row_scale,
                                      m->sig + (size_t)G.in1 * m->Bcap, m->sig + (size_t)G.in2 * m->Bcap, G.gsum,
-                                     m->active_hi, c->stream));
+                                     m->active_hi, c->n_space, c->stream));
     DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, kpos,
                                c->stream));
     if (advance > 0) DTB_CUDA(launch_advance_step(m->gstep, advance, c->stream));
@@ -667,7 +689,7 @@ int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_sc
     DTB_CHECK(n_steps >= 0 && std::isfinite(dt_scale), DTB_EINVAL, "dtb_batch_admit: bad dt_scale or step count");
     DeviceGuard g(c->device);
     DTB_CUDA(cudaStreamSynchronize(c->stream));
-    const int n = (int)c->n_mom, B = m->Bcap;
+    const int n = (int)c->n_state, B = m->Bcap;
     for (int i = 0; i < n; ++i) {
         m->pin_col[i] = (float)f0[i];
         m->pin_col[n + i] = (float)(f0[i] - (double)(float)f0[i]);  // exact remainder as the compensation
@@ -682,7 +704,8 @@ int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_sc
     std::vector<float> sg((size_t)c->ns), isg((size_t)c->ns);
     for (int sp = 0; sp < c->ns; ++sp) {
         double mx = 0;
-        for (int64_t k = c->off[sp]; k < c->off[sp + 1]; ++k) mx = std::max(mx, std::fabs(f0[k]));
+        for (int cl = 0; cl < c->n_space; ++cl)
+            for (int64_t k = c->off[sp]; k < c->off[sp + 1]; ++k) mx = std::max(mx, std::fabs(f0[cl * c->n_mom + k]));
         int ex = 0;
         if (mx > 0 && std::isfinite(mx)) std::frexp(mx, &ex);
         sg[(size_t)sp] = std::ldexp(1.0f, ex);
@@ -737,7 +760,7 @@ int32_t dtb_batch_get_f(dtb_ctx* c, int32_t slot, double* f) {
     DTB_CHECK(slot >= 0 && slot < m->Buser, DTB_ENOTFOUND, "dtb_batch_get_f: slot out of range");
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f: null output");
     DeviceGuard g(c->device);
-    const int n = (int)c->n_mom, B = m->Bcap;
+    const int n = (int)c->n_state, B = m->Bcap;
     DTB_CUDA(cudaMemcpy2DAsync(m->pin_col, sizeof(float), m->F[m->cur] + slot, sizeof(float) * B, sizeof(float), n,
                                cudaMemcpyDeviceToHost, c->stream));
     DTB_CUDA(cudaMemcpy2DAsync(m->pin_col + n, sizeof(float), m->C[m->cur] + slot, sizeof(float) * B, sizeof(float), n,
@@ -786,7 +809,7 @@ int32_t dtb_batch_set_f_all(dtb_ctx* c, const double* f) {
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_set_f_all: null input");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
-    const int n = (int)c->n_mom;
+    const int n = (int)c->n_state;
     const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
     if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
     DTB_CUDA(cudaMemcpyAsync(m->io_all, f, bytes, cudaMemcpyHostToDevice, c->stream));
@@ -800,7 +823,7 @@ int32_t dtb_batch_get_f_all(dtb_ctx* c, double* f) {
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f_all: null output");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
-    const int n = (int)c->n_mom;
+    const int n = (int)c->n_state;
     const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
     if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
     DTB_CUDA(launch_unpack_f(m->F[m->cur], m->C[m->cur], m->Buser, n, m->Bcap, m->io_all, c->stream));
@@ -816,11 +839,12 @@ int32_t dtb_batch_moments(dtb_ctx* c, const double* w, double* number, double* e
     DeviceGuard g(c->device);
     const int B = m->Bcap, ns = c->ns;
     DTB_CUDA(cudaMemcpyAsync(m->mom_w, w, sizeof(double) * (size_t)c->n_mom, cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(launch_batch_moments(m->F[m->cur], m->C[m->cur], B, m->sp_off, ns, m->mom_w, m->mom_out, c->stream));
-    std::vector<double> out((size_t)2 * ns * B);
+    DTB_CUDA(launch_batch_moments(m->F[m->cur], m->C[m->cur], B, m->sp_off, ns, (int)c->n_mom, c->n_space, m->mom_w,
+                                  m->mom_out, c->stream));
+    std::vector<double> out((size_t)2 * ns * B * c->n_space);
     DTB_CUDA(cudaMemcpyAsync(out.data(), m->mom_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c->stream));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
-    for (size_t k = 0; k < (size_t)m->Buser * ns; ++k) {
+    for (size_t k = 0; k < (size_t)m->Buser * c->n_space * ns; ++k) {
         number[k] = out[2 * k];
         energy[k] = out[2 * k + 1];
     }

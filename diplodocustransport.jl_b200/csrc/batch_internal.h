@@ -26,7 +26,9 @@ struct GemmArgs {
     int tiles_per_split, n_splits, m_tiles, n_tiles;
     int splits_per_cb;  // > 0: every split lies inside one 64-wide input-2 block (K tiles cb-major)
     int Bcap;       // instances that exist (columns >= Bcap are zero in X)
-    int Bst;        // row stride of the state matrix F[n][Bst]
+    int Bst;        // row stride of the state matrix F[n_state][Bst]
+    int n_space;    // space cells: column j of X is cell j / Bst of slot j % Bst
+    int n_mom;      // states of one cell
     int Bpad;       // n_tiles * BN, instance stride of the partial rows
     const float* F;
     const float* isig1;  // [Bst] reciprocal power-of-two scale of species in1 per instance
@@ -63,6 +65,9 @@ struct RowJob {
 // Per-row operands of the batched Euler epilogue.
 struct MixedRowOps {
     int n_mom, Bcap, n_species;  // Bcap: slots in the state matrix (a multiple of 4), its row stride
+    int n_state, n_space;        // rows of the state matrix = n_space cells of n_mom states
+    const float* vol_cell;       // per cell: Vol (SteppingMethods.jl:380)
+    const unsigned char* bin_on; // per cell: the binary term applies (BinM.Domain); null = every cell
     int sp_off[DTB_MAX_SPECIES + 1];
     int ell_w;
     const float* ell_val;
@@ -92,7 +97,6 @@ struct MixedRowOps {
     const int* njobs;                // [tile]
     const float* invAp;
     const float* inj;
-    float vol;
     double thr;
     int has_bin, has_emi;
     const double* dt_scale;          // [Bcap]
@@ -108,12 +112,12 @@ cudaError_t launch_pack_f(const double* io, int Buser, int n, int Bcap, float* F
 cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, int Bcap, double* io, cudaStream_t s);
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
                                 const float* sig1, const float* sig2, float* gsum, const int* active_hi,
-                                cudaStream_t s);
+                                int n_space, cudaStream_t s);
 int mixed_rows_tile_rows();
 cudaError_t prepare_mixed_rows();
 
 cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
-                                 const double* w, double* out, cudaStream_t s);
+                                 int n_mom, int n_space, const double* w, double* out, cudaStream_t s);
 
 cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1, int n2, int n_cb,
                               unsigned char* gt, float* row_scale, cudaStream_t s);

@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     }
     const int m0 = m_tile * kMmaM, n0 = n_tile * BN;
     // columns of this tile that belong to slots still stepping, rounded up to the MMA's N granule
-    const int hi_cols = *reinterpret_cast<const volatile int*>(a.active_hi);
+    const int hi_cols = a.n_space > 1 ? a.n_space * a.Bst : *reinterpret_cast<const volatile int*>(a.active_hi);
     const int n_eff = max(0, min(BN, (hi_cols - n0 + 15) / 16 * 16));
     const int nt = (n_eff > 0 && t1 > t0) ? t1 - t0 : 0;
 
@@ -260,8 +260,13 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
         // ---------------- X producers (one instance row per thread), then the epilogue
         const int p = tid;  // row of the B tile
         if (p < BN && nt > 0) {
-            const int inst = n0 + p;
-            const bool valid = inst < a.Bcap && p < n_eff;
+            // column n0 + p: cell (n0 + p) / Bst of slot (n0 + p) % Bst; the cell's states start at
+            // row cell * n_mom of F
+            const int col = n0 + p;
+            const int cell = col / a.Bst;
+            const int inst = col - cell * a.Bst;
+            const bool valid = cell < a.n_space && inst < a.Bcap && p < n_eff;
+            const float* Fc = a.F + (size_t)(valid ? cell : 0) * a.n_mom * a.Bst;
             const float s1 = valid ? a.isig1[inst] : 0.f;
             const float s2 = valid ? a.isig2[inst] : 0.f;
             float f2r[kMmaK];
@@ -271,7 +276,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             float x1_next = 0.f;
             if (valid) {
                 const int b0 = t0 - (t0 / a.N1) * a.N1;
-                x1_next = __ldg(a.F + (size_t)(a.off1 + b0) * a.Bst + inst);
+                x1_next = __ldg(Fc + (size_t)(a.off1 + b0) * a.Bst + inst);
             }
             for (int j = 0; j < nt; ++j) {
                 const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
@@ -279,7 +284,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 const float x1 = (x1_next * s1) * s2;  // both scales are powers of two: exact
                 if (valid && j + 1 < nt) {
                     const int tn = t + 1, bn = tn - (tn / a.N1) * a.N1;
-                    x1_next = __ldg(a.F + (size_t)(a.off1 + bn) * a.Bst + inst);
+                    x1_next = __ldg(Fc + (size_t)(a.off1 + bn) * a.Bst + inst);
                 }
                 (void)b;
                 if (!mb_wait(smem_addr(&empty_b[sb]), ((j / C::SB) & 1u) ^ 1u, abort_flag)) {
@@ -290,7 +295,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 if (cb != cur_cb) {
                     // 64 unconditional loads (clamped in bounds) issued back to back, the padding
                     // zeroed afterwards: one round trip instead of a load-use chain
-                    const float* fb = a.F + (valid ? inst : 0);
+                    const float* fb = Fc + (valid ? inst : 0);
 #pragma unroll
                     for (int c = 0; c < kMmaK; ++c) {
                         const int cc = min(cb * kMmaK + c, a.n2 - 1);
@@ -496,10 +501,11 @@ constexpr int kRowsSmem = kRowStages * kStageFloats * 4;  // dynamic: the operan
 __global__ void split_reduce_kernel(const float* __restrict__ partial, int n_splits, int Bpad, int M, int Bcap,
                                     const float* __restrict__ row_scale, const float* __restrict__ sig1,
                                     const float* __restrict__ sig2, float* __restrict__ gsum,
-                                    const int* __restrict__ active_hi) {
+                                    const int* __restrict__ active_hi, int n_space) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (r >= M || i >= Bcap || i >= *active_hi) return;
+    const int i = blockIdx.y;  // column: cell i / Bcap, slot i % Bcap
+    if (r >= M || i >= Bcap * n_space || (n_space == 1 && i >= *active_hi)) return;
+    const int slot = i % Bcap;
     const float* p = partial + (size_t)i * M + r;
     const size_t stride = (size_t)Bpad * M;
     float acc = 0.f;
@@ -513,7 +519,7 @@ __global__ void split_reduce_kernel(const float* __restrict__ partial, int n_spl
         acc += v3;
     }
     for (; sp < n_splits; ++sp) acc += p[(size_t)sp * stride];
-    gsum[(size_t)i * M + r] = acc * row_scale[r] * sig1[i] * sig2[i];
+    gsum[(size_t)i * M + r] = acc * row_scale[r] * sig1[slot] * sig2[slot];
 }
 
 __device__ __forceinline__ int species_of_row(const MixedRowOps& ops, int a) {
@@ -523,16 +529,17 @@ __device__ __forceinline__ int species_of_row(const MixedRowOps& ops, int a) {
 }
 
 // Loss and emission of one (row, instance) pair with direct loads (tiles the fast path cannot take).
-__device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict__ F, int a, int s, int i,
-                                 float& loss, float& emi) {
+// a: state row (global), am: its momentum index within cell `cell`, s: its species.
+__device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict__ F, int a, int am, int cell, int s,
+                                 int i, float& loss, float& emi) {
     const int B = ops.Bcap;
     loss = 0.f;
     emi = 0.f;
     if (ops.has_bin) {
-        const int la = a - ops.sp_off[s];
+        const int la = am - ops.sp_off[s];
         for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
             const float* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
-            const int co = ops.loss_col_off[b], nc = ops.loss_ncols[b];
+            const int co = ops.loss_col_off[b] + cell * ops.n_mom, nc = ops.loss_ncols[b];
             for (int c = 0; c < nc; ++c) loss += row[c] * F[(size_t)(co + c) * B + i];
         }
     }
@@ -586,7 +593,7 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     // ty + 8k, instances 4 tx .. 4 tx + 3), so a 16-wide slice of K costs 5 shared loads per 16 FMAs
     const int kg = tid >> 6, lt = tid & 63, tx = lt & 7, ty = lt >> 3;
     const int a0 = blockIdx.x * kRT, i0 = blockIdx.y * kIT;
-    const int n = ops.n_mom, B = ops.Bcap;
+    const int n = ops.n_state, B = ops.Bcap;
     // the device step counter advances once per launch sequence (advance_step); kpos is this
     // launch's place in the sequence
     const long long step = (long long)*reinterpret_cast<const volatile unsigned long long*>(gstep) + kpos;
@@ -643,16 +650,19 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     if (ops.has_bin) {
         const int r = tid & (kRT - 1);
         const int a = a0 + r;
-        const int s = a < n ? species_of_row(ops, a) : 0;
+        const int cell = a / ops.n_mom, am = a - cell * ops.n_mom;
+        const int s = a < n ? species_of_row(ops, am) : 0;
+        const bool on = a < n && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
 #pragma unroll
         for (int q = 0; q < kIT / 16; ++q) {
             const int il = (tid >> 5) + 16 * q;
             const int i = i0 + il;
             float g = 0.f;
-            if (a < n && i < B) {
+            if (on && i < B) {
+                // group sums are [cell * Bcap + slot][stacked row]
                 for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
                     const int gi = ops.gain_grp[e];
-                    g += ops.grp_gsum[gi][(size_t)i * ops.grp_M[gi] + ops.gain_roff[e] + (a - ops.sp_off[s])];
+                    g += ops.grp_gsum[gi][((size_t)cell * B + i) * ops.grp_M[gi] + ops.gain_roff[e] + (am - ops.sp_off[s])];
                 }
             }
             s_gain[r][il] = g;
@@ -772,7 +782,12 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                 flux[1] += v * f2.y;
             }
         }
-        const int s = species_of_row(ops, a);
+        const int cell = a / ops.n_mom, am = a - cell * ops.n_mom;
+        const int s = species_of_row(ops, am);
+        // the binary term of this cell (SteppingMethods.jl:369-380): Vol of the cell, zero outside
+        // BinM.Domain
+        const bool bin_here = ops.has_bin && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
+        const float vol = ops.vol_cell[cell];
         const float fa[2] = {fa2.x, fa2.y};
         const float ca[2] = {ca2.x, ca2.y};
         float fo[2], co[2];
@@ -793,13 +808,13 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                     emi += s_pe[g][r][jb + j];
                 }
             } else {
-                row_terms_direct(ops, F, a, s, ib + j, loss, emi);
+                row_terms_direct(ops, F, a, am, cell, s, ib + j, loss, emi);
             }
             const float gain = ops.has_bin ? s_gain[r][jb + j] : 0.f;
             // SteppingMethods.jl:31-46 in FP32, the scaling in FP64
             float df = -flux[j];
             if (ops.has_emi) df += emi;
-            if (ops.has_bin) df += ops.vol * (gain - fa[j] * loss);
+            if (ops.has_bin) df += bin_here ? vol * (gain - fa[j] * loss) : 0.f;
             const double dfs = (double)df * (inv_ap * dts[j]);
             // :97-101 with an FP64 compensated sum: the state is fa + ca
             double t = ((double)fa[j] + (double)ca[j]) + (dfs + injv * dts[j]);
@@ -846,13 +861,14 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
 // Per (slot, species) FP64 number sum(f) and energy sum(f * w) of the compensated state F + C
 // (DistributionMoments.jl:33,145,162); out[(slot * n_species + s) * 2 + {0, 1}].
 __global__ void batch_moments_kernel(const float* __restrict__ F, const float* __restrict__ C, int Bcap,
-                                     const int* __restrict__ sp_off, int n_species, const double* __restrict__ w,
-                                     double* __restrict__ out) {
+                                     const int* __restrict__ sp_off, int n_species, int n_mom,
+                                     const double* __restrict__ w, double* __restrict__ out) {
     __shared__ double s_n[128], s_e[128];
-    const int sp = blockIdx.x, slot = blockIdx.y;
+    const int sp = blockIdx.x, slot = blockIdx.y, cell = blockIdx.z;
     double a = 0.0, e = 0.0;
+    const size_t row0 = (size_t)cell * n_mom;
     for (int k = sp_off[sp] + threadIdx.x; k < sp_off[sp + 1]; k += blockDim.x) {
-        const double v = (double)F[(size_t)k * Bcap + slot] + (double)C[(size_t)k * Bcap + slot];
+        const double v = (double)F[(row0 + k) * Bcap + slot] + (double)C[(row0 + k) * Bcap + slot];
         a += v;
         e += v * w[k];
     }
@@ -866,9 +882,10 @@ __global__ void batch_moments_kernel(const float* __restrict__ F, const float* _
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[((size_t)slot * n_species + sp) * 2 + 0] = s_n[0];
-        out[((size_t)slot * n_species + sp) * 2 + 1] = s_e[0];
+    if (threadIdx.x == 0) {  // out[slot][cell][species][number, energy]
+        const size_t o = (((size_t)slot * gridDim.z + cell) * n_species + sp) * 2;
+        out[o + 0] = s_n[0];
+        out[o + 1] = s_e[0];
     }
 }
 
@@ -924,8 +941,8 @@ cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, in
 }
 
 cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const int* sp_off, int n_species,
-                                 const double* w, double* out, cudaStream_t s) {
-    batch_moments_kernel<<<dim3(n_species, Bcap), 128, 0, s>>>(F, C, Bcap, sp_off, n_species, w, out);
+                                 int n_mom, int n_space, const double* w, double* out, cudaStream_t s) {
+    batch_moments_kernel<<<dim3(n_species, Bcap, n_space), 128, 0, s>>>(F, C, Bcap, sp_off, n_species, n_mom, w, out);
     return cudaGetLastError();
 }
 
@@ -945,10 +962,10 @@ cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const f
 
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
                                 const float* sig1, const float* sig2, float* gsum, const int* active_hi,
-                                cudaStream_t s) {
-    dim3 grid((M + 255) / 256, Bcap);
+                                int n_space, cudaStream_t s) {
+    dim3 grid((M + 255) / 256, Bcap * n_space);
     split_reduce_kernel<<<grid, 256, 0, s>>>(partial, n_splits, Bpad, M, Bcap, row_scale, sig1, sig2, gsum,
-                                             active_hi);
+                                             active_hi, n_space);
     return cudaGetLastError();
 }
 

@@ -4,7 +4,9 @@
 operators once (as ``ForwardEulerStruct`` does for a single solve, SteppingStructs.jl:33-100)
 and holds ``capacity`` slots. Each admitted slot runs the explicit Euler step of
 SteppingMethods.jl:12-107 with its own initial f, dt and step count; ``run(k)`` advances every
-slot with steps left by k batched steps. The gain contraction of all slots is a tensor-core
+slot with steps left by k batched steps. A slot may hold several space cells (PhaseSpace.n_space):
+every (cell, slot) pair is then a column of the gain GEMM, with the cell's Vol and BinM.Domain
+applied per cell, and the flux coupling the cells. The gain contraction of all slots is a tensor-core
 GEMM with G in BF16 hi + lo (three MMAs, FP32 accumulation) and f is updated with an FP64
 compensated sum.
 """
@@ -14,6 +16,7 @@ import ctypes
 from typing import Optional
 
 import numpy as np
+import scipy.sparse as sp
 
 from . import _lib
 from ._lib import check, dptr
@@ -25,17 +28,15 @@ class BatchedEuler:
     def __init__(self, PhaseSpace: PhaseSpace, Injection, BinM: BinaryMatrices, EmiM: EmissionMatrices,
                  FluxM: FluxMatrices, capacity: int, *, device: int = 0, stream: Optional[int] = None,
                  graph_steps: int = 16):
-        if PhaseSpace.n_space != 1:
-            raise ValueError("batched instances are single-cell")
         self.L = _lib.load()
         self.PhaseSpace = PhaseSpace
         self.capacity = int(capacity)
         self.dt0 = float(PhaseSpace.dt0)
-        self.n = PhaseSpace.n_momentum
+        self.n = PhaseSpace.n_state
         dims = _lib.Dims()
         sizes = PhaseSpace.species_sizes
         dims.n_species = len(sizes)
-        dims.n_space = 1
+        dims.n_space = PhaseSpace.n_space
         for i, s in enumerate(sizes):
             dims.species_size[i] = s
         opts = _lib.Opts(precision=_lib.DTB_MIXED, device=device, stream=stream, index_base=0,
@@ -47,14 +48,23 @@ class BatchedEuler:
             L = self.L
             _upload_csc(L, ctx, FluxM.X_Flux)
             _upload_csc(L, ctx, FluxM.P_Flux)
-            if BinM.M_Bin is not None:
+            if BinM.M_Bin is not None and sp.issparse(BinM.M_Bin):
+                M = sp.csc_matrix(BinM.M_Bin)
+                ip = [np.ascontiguousarray(x, dtype=np.int64) for x in (M.indptr, M.indices)]
+                nz = np.ascontiguousarray(M.data, dtype=np.float64)
+                check(L.dtb_upload_mbin_csc(ctx, PhaseSpace.n_momentum, ip[0].ctypes.data_as(_lib._ip),
+                                            ip[1].ctypes.data_as(_lib._ip), dptr(nz)))
+            elif BinM.M_Bin is not None:
                 M = np.asfortranarray(BinM.M_Bin, dtype=np.float64)
-                check(L.dtb_upload_mbin_ref(ctx, M.ctypes.data_as(_lib._dp), self.n))
+                check(L.dtb_upload_mbin_ref(ctx, M.ctypes.data_as(_lib._dp), PhaseSpace.n_momentum))
             for g in BinM.gains:
                 _upload_gain(L, ctx, g)
             for l in BinM.losses:
                 A = np.ascontiguousarray(l.L, dtype=np.float64)
                 check(L.dtb_add_loss_block(ctx, l.sp, l.other_sp, dptr(A)))
+            if BinM.Domain is not None:
+                D = np.ascontiguousarray(BinM.Domain, dtype=np.int64)
+                check(L.dtb_set_bin_domain(ctx, D.ctypes.data_as(_lib._ip), len(D)))
             if EmiM.M_Emi is not None:
                 M = np.asfortranarray(EmiM.M_Emi, dtype=np.float64)
                 check(L.dtb_upload_emi_ref(ctx, M.ctypes.data_as(_lib._dp), self.n))
@@ -97,12 +107,16 @@ class BatchedEuler:
         return out
 
     def moments(self, weights) -> tuple:
-        """FP64 number and energy per (slot, species) on the device."""
+        """FP64 number and energy per (slot, species) on the device, or per (slot, cell, species)
+        when the slots hold several space cells; weights: one per momentum state."""
         w = np.ascontiguousarray(weights, dtype=np.float64)
         ns = len(self.PhaseSpace.species_sizes)
-        num = np.zeros((self.capacity, ns))
+        nsp = self.PhaseSpace.n_space
+        num = np.zeros((self.capacity, nsp, ns))
         en = np.zeros_like(num)
         check(self.L.dtb_batch_moments(self.ctx, dptr(w), dptr(num), dptr(en)))
+        if nsp == 1:
+            return num[:, 0, :], en[:, 0, :]
         return num, en
 
     def info(self, slot: int) -> dict:

@@ -224,9 +224,12 @@ int32_t dtb_set_profiling(dtb_ctx* ctx, int32_t on);
  * all slots is one tensor-core GEMM per input pair with G stored as BF16 hi + lo with a
  * power-of-two scale per row (three MMAs: hi*hi + hi*lo + lo*hi, FP32 accumulation), f in
  * FP32 with a power-of-two scale per (slot, species) inside the GEMM operand, and the update
- * f += df of SteppingMethods.jl:97-101 accumulated in FP64 with a compensation term. */
+ * f += df of SteppingMethods.jl:97-101 accumulated in FP64 with a compensation term. A slot
+ * holds dims.n_space cells (n_state = n_space * n_mom values): every (cell, slot) pair is a
+ * column of the gain GEMM (update_Big_Bin!'s loop over cells, SteppingMethods.jl:360-386),
+ * each cell with its Vol and BinM.Domain, the flux coupling the cells. */
 
-/* Starts a solve in `slot`: f = f0 (n_mom values), dt_scale = dt/dt0, n_steps steps from the
+/* Starts a solve in `slot`: f = f0 (n_state values), dt_scale = dt/dt0, n_steps steps from the
  * current batched step. A slot that finished (or was never admitted) does not step. */
 int32_t dtb_batch_admit(dtb_ctx* ctx, int32_t slot, const double* f0, double dt_scale, int64_t n_steps);
 
@@ -242,14 +245,14 @@ int32_t dtb_batch_get_f(dtb_ctx* ctx, int32_t slot, double* f);
 int32_t dtb_batch_slot_info(dtb_ctx* ctx, int32_t slot, int64_t* steps_done, int64_t* steps_left,
                             double* cr_max, int32_t* finite);
 
-/* The whole batch's state in or out: f is [batch][n_mom] Float64 (slot-major). set_f_all
+/* The whole batch's state in or out: f is [batch][n_state] Float64 (slot-major). set_f_all
  * replaces every slot's f (steps left and dt are kept); get_f_all reads every slot's f. */
 int32_t dtb_batch_set_f_all(dtb_ctx* ctx, const double* f);
 int32_t dtb_batch_get_f_all(dtb_ctx* ctx, double* f);
 
-/* FP64 number sum(f) and energy sum(f * w) of every slot and species, on the device
+/* FP64 number sum(f) and energy sum(f * w) of every slot, space cell and species, on the device
  * (DistributionMoments.jl:33,145,162); w is the per-state energy weight (n_mom). Outputs are
- * batch x n_species, slot-major. */
+ * batch x n_space x n_species, slot-major. */
 int32_t dtb_batch_moments(dtb_ctx* ctx, const double* w, double* number, double* energy);
 
 /* Stops a slot (it no longer steps). */

@@ -221,3 +221,66 @@ def test_gemm_columns_follow_the_last_running_slot(cuda):
         assert one.info(0)["steps_done"] == 5
         one.close()
     full.close()
+
+
+def _multicell(n_space, seed, domain=None):
+    w = synth.small(p_num=8, u_num=4, seed=seed, n_space=n_space, randomize_vectors=True)
+    w.fluxm.X_Flux = synth.space_flux(w.ps, np.random.default_rng(seed + 1), 1.0)
+    w.binm.Domain = domain
+    for g in w.binm.gains:  # a gain term that matters at this step count
+        g.G = np.asarray(g.G) * 20.0
+    return w
+
+
+@pytest.mark.parametrize("n_space,domain", [(3, None), (4, [0, 2]), (2, [])])
+def test_multicell_slots_match_oracle(cuda, n_space, domain):
+    """Slots of several space cells (update_Big_Bin!'s loop over cells, SteppingMethods.jl:360-386):
+    every (cell, slot) pair is a gain-GEMM column, each cell with its Vol and BinM.Domain, a
+    space flux coupling the cells; 6 slots with their own f0 and dt, 30 steps, against the FP64
+    oracle of the same multi-cell grid."""
+    w = _multicell(n_space, 60 + n_space, domain)
+    n = w.ps.n_state
+    rng = np.random.default_rng(5)
+    f0s = [w.f0 * rng.uniform(0.7, 1.3, n) for _ in range(6)]
+    dts = rng.uniform(0.5, 1.0, 6)
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 6)
+    for i in range(6):
+        m.admit(i, f0s[i], dts[i], 30)
+    m.run(30)
+    ops = oracle.blocked_from_workload(w)
+    for i in range(6):
+        f = f0s[i].copy()
+        for _ in range(30):
+            f, _, _ = ops.step(f, dts[i], 0)
+        assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
+    m.close()
+
+
+def test_multicell_moments_and_bulk_io(cuda):
+    """Per-(slot, cell, species) FP64 moments and whole-batch state I/O with cells."""
+    from dtb.structs import energy_weights
+    w = _multicell(3, 71)
+    n = w.ps.n_state
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 5)
+    rng = np.random.default_rng(2)
+    F = np.stack([w.f0 * rng.uniform(0.5, 1.5, n) for _ in range(5)])
+    for i in range(5):
+        m.admit(i, F[i], 0.8, 10)
+    m.run(10)
+    G = m.get_f_all()
+    assert G.shape == (5, n)
+    wts = energy_weights(w.ps)
+    num, en = m.moments(wts)
+    sizes = w.ps.species_sizes
+    nm = w.ps.n_momentum
+    assert num.shape == (5, 3, len(sizes))
+    for i in range(5):
+        np.testing.assert_array_equal(m.get_f(i), G[i])
+        for cell in range(3):
+            for s in range(len(sizes)):
+                lo = cell * nm + sum(sizes[:s])
+                sl = slice(lo, lo + sizes[s])
+                assert num[i, cell, s] == pytest.approx(G[i][sl].sum(), rel=1e-12)
+                assert en[i, cell, s] == pytest.approx((G[i][sl] * wts[sum(sizes[:s]):sum(sizes[:s]) + sizes[s]]).sum(),
+                                                       rel=1e-12)
+    m.close()
