@@ -955,7 +955,7 @@ cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s
 
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
                               const unsigned long long* gstep, int kpos, cudaStream_t s) {
-    dim3 grid((ops.n_mom + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
+    dim3 grid((ops.n_state + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
     mixed_rows_kernel<<<grid, kRowsThreads, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, kpos);
     return cudaGetLastError();
 }

@@ -227,8 +227,6 @@ def _multicell(n_space, seed, domain=None):
     w = synth.small(p_num=8, u_num=4, seed=seed, n_space=n_space, randomize_vectors=True)
     w.fluxm.X_Flux = synth.space_flux(w.ps, np.random.default_rng(seed + 1), 1.0)
     w.binm.Domain = domain
-    for g in w.binm.gains:  # a gain term that matters at this step count
-        g.G = np.asarray(g.G) * 20.0
     return w
 
 
