@@ -48,6 +48,7 @@ struct MixedState {
     long long host_step = 0;
     MixedRowOps ops{};
     cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step from state buffer 0 / 1
     int graph_steps = 16;
     std::vector<long long> h_stop, h_start;
     float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation
@@ -507,6 +508,8 @@ void destroy_mixed(dtb_ctx* c) {
     MixedState* m = c->mixed;
     if (!m) return;
     if (m->graph) cudaGraphExecDestroy(m->graph);
+    for (auto& g1 : m->graph1)
+        if (g1) cudaGraphExecDestroy(g1);
     for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
     if (m->pin_col) cudaFreeHost(m->pin_col);
     delete m;
@@ -605,6 +608,43 @@ int ensure_mixed_graph(dtb_ctx* c) {
     e = cudaGraphInstantiate(&m->graph, gr, 0);
     cudaGraphDestroy(gr);
     DTB_CUDA(e);
+    return DTB_OK;
+}
+
+// One batched step as a graph (one per state buffer), for runs shorter than a full graph.
+int ensure_mixed_graph1(dtb_ctx* c) {
+    MixedState* m = c->mixed;
+    const int cur = m->cur;
+    if (m->graph1[cur]) return DTB_OK;
+    const long long hs = m->host_step;
+    cudaGraph_t gr;
+    DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = mixed_step(c, false, 0, 1);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+    m->host_step = hs;
+    m->cur = cur;
+    if (rc != DTB_OK) return rc;
+    DTB_CUDA(e);
+    e = cudaGraphInstantiate(&m->graph1[cur], gr, 0);
+    cudaGraphDestroy(gr);
+    DTB_CUDA(e);
+    return DTB_OK;
+}
+
+// Device error flag of earlier batched launches: read behind a call's own synchronisation.
+int mixed_err_enqueue(dtb_ctx* c) {
+    DTB_CUDA(cudaMemcpyAsync(c->pin_err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return DTB_OK;
+}
+int mixed_err_take(dtb_ctx* c) {  // after the stream was synchronised
+    if (*c->pin_err) {
+        const int e = *c->pin_err;
+        *c->pin_err = 0;
+        cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
+        set_error("a bounded device wait gave up in the batched step (kernel error flags " + std::to_string(e) + ")");
+        return DTB_ETIMEOUT;
+    }
     return DTB_OK;
 }
 
@@ -749,9 +789,19 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
             m->host_step += m->graph_steps;
         }
     }
-    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, m->profiling, 0, 1));
-    if (m->profiling) DTB_TRY(mixed_flush_profile(m));
-    return mixed_check_err(c);
+    if (m->profiling) {
+        for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, true, 0, 1));
+        DTB_TRY(mixed_flush_profile(m));
+        return mixed_check_err(c);
+    }
+    for (; done < nsteps; ++done) {
+        DTB_TRY(ensure_mixed_graph1(c));
+        DTB_CUDA(cudaGraphLaunch(m->graph1[m->cur], c->stream));
+        m->cur ^= 1;
+        m->host_step++;
+    }
+    // enqueued only: a device error surfaces at the next call that reads results
+    return DTB_OK;
 }
 
 int32_t dtb_batch_get_f(dtb_ctx* c, int32_t slot, double* f) {
@@ -765,7 +815,9 @@ int32_t dtb_batch_get_f(dtb_ctx* c, int32_t slot, double* f) {
                                cudaMemcpyDeviceToHost, c->stream));
     DTB_CUDA(cudaMemcpy2DAsync(m->pin_col + n, sizeof(float), m->C[m->cur] + slot, sizeof(float) * B, sizeof(float), n,
                                cudaMemcpyDeviceToHost, c->stream));
+    DTB_TRY(mixed_err_enqueue(c));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
+    DTB_TRY(mixed_err_take(c));
     for (int i = 0; i < n; ++i) f[i] = (double)m->pin_col[i] + (double)m->pin_col[n + i];
     return DTB_OK;
 }
@@ -785,7 +837,9 @@ int32_t dtb_batch_slot_info(dtb_ctx* c, int32_t slot, int64_t* steps_done, int64
         int nf = 0;
         DTB_CUDA(cudaMemcpyAsync(&e, m->min_ratio + slot, sizeof(e), cudaMemcpyDeviceToHost, c->stream));
         DTB_CUDA(cudaMemcpyAsync(&nf, m->nonfinite + slot, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DTB_TRY(mixed_err_enqueue(c));
         DTB_CUDA(cudaStreamSynchronize(c->stream));
+        DTB_TRY(mixed_err_take(c));
         if (cr_max) *cr_max = -ord_dec_host(e);
         if (finite) *finite = nf ? 0 : 1;
     }
@@ -828,7 +882,9 @@ int32_t dtb_batch_get_f_all(dtb_ctx* c, double* f) {
     if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
     DTB_CUDA(launch_unpack_f(m->F[m->cur], m->C[m->cur], m->Buser, n, m->Bcap, m->io_all, c->stream));
     DTB_CUDA(cudaMemcpyAsync(f, m->io_all, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DTB_TRY(mixed_err_enqueue(c));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
+    DTB_TRY(mixed_err_take(c));
     return DTB_OK;
 }
 
@@ -843,7 +899,9 @@ int32_t dtb_batch_moments(dtb_ctx* c, const double* w, double* number, double* e
                                   m->mom_out, c->stream));
     std::vector<double> out((size_t)2 * ns * B * c->n_space);
     DTB_CUDA(cudaMemcpyAsync(out.data(), m->mom_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c->stream));
+    DTB_TRY(mixed_err_enqueue(c));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
+    DTB_TRY(mixed_err_take(c));
     for (size_t k = 0; k < (size_t)m->Buser * c->n_space * ns; ++k) {
         number[k] = out[2 * k];
         energy[k] = out[2 * k + 1];

@@ -586,7 +586,7 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     // after the products the same memory holds the two halves' loss and emission tiles
     float(*s_pl)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn);
     float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + kKGroups * kRT * (kIT + 1));
-    __shared__ double s_min[kRT][kIT];
+    __shared__ double s_min[kRT][kIT + 1];  // padded: the per-instance reduction reads down columns
     __shared__ int s_nonfin[kIT];
     const int tid = threadIdx.x;
     // products: 8 groups of 64 threads split each K chunk; a 4 x 4 micro-tile per thread (rows

@@ -109,9 +109,16 @@ mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
         upload_csc!(ctx[], FluxM.P_Flux)
         n_mom = sum(sizes)
         if !isempty(BinM.Binary_list)
-            M = Matrix{Float64}(BinM.M_Bin)
-            GC.@preserve M check(ccall((:dtb_upload_mbin_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
-                                       ctx[], M, n_mom))
+            if BinM.M_Bin isa SparseMatrixCSC   # Bin_sparse (BuildBinaryMatrices.jl:44-52), 1-based CSC
+                S = SparseMatrixCSC{Float64,Int64}(BinM.M_Bin)
+                GC.@preserve S check(ccall((:dtb_upload_mbin_csc, libdtb), Int32,
+                                           (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}),
+                                           ctx[], n_mom, S.colptr, S.rowval, S.nzval))
+            else
+                M = Matrix{Float64}(BinM.M_Bin)
+                GC.@preserve M check(ccall((:dtb_upload_mbin_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
+                                           ctx[], M, n_mom))
+            end
             if !isnothing(BinM.Domain)   # Bin_Domain (SteppingStructs.jl:51, SteppingMethods.jl:369)
                 D = Vector{Int64}(BinM.Domain)
                 GC.@preserve D check(ccall((:dtb_set_bin_domain, libdtb), Int32, (Ptr{Cvoid}, Ptr{Int64}, Int64),

@@ -233,8 +233,11 @@ int32_t dtb_set_profiling(dtb_ctx* ctx, int32_t on);
  * current batched step. A slot that finished (or was never admitted) does not step. */
 int32_t dtb_batch_admit(dtb_ctx* ctx, int32_t slot, const double* f0, double dt_scale, int64_t n_steps);
 
-/* nsteps batched steps of every slot that still has steps left, replayed from a captured
- * CUDA graph. */
+/* nsteps batched steps of every slot that still has steps left, replayed from captured CUDA
+ * graphs. Returns once the steps are enqueued on the context's stream; a device-side error of
+ * these steps (a bounded wait that gave up) is reported by the next call that reads results
+ * (dtb_batch_get_f, dtb_batch_get_f_all, dtb_batch_slot_info, dtb_batch_moments) or by dtb_sync.
+ * With profiling on (dtb_batch_set_profiling) the call waits for the steps and checks them. */
 int32_t dtb_batch_run(dtb_ctx* ctx, int64_t nsteps);
 
 /* The slot's current f (FP32 state plus its compensation term, as Float64). */
