@@ -16,6 +16,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "batch_internal.h"
 
 namespace dtb {
@@ -23,6 +25,29 @@ namespace dtb {
 namespace {
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Programmatic dependent launch: the kernels of a batched step are launched so that the next
+// one may start while the previous one runs. Each waits for its predecessor (grid completion and
+// memory) before it reads what the predecessor wrote, and lets its own dependents launch only
+// after that wait, so a chain of early launches never skips a completion.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -259,6 +284,8 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     } else {
         // ---------------- X producers (one instance row per thread), then the epilogue
         const int p = tid;  // row of the B tile
+        pdl_wait();  // F is the previous step's output
+        if (tid == 0) pdl_trigger();
         if (p < BN && nt > 0) {
             // column n0 + p: cell (n0 + p) / Bst of slot (n0 + p) % Bst; the cell's states start at
             // row cell * n_mom of F
@@ -401,8 +428,7 @@ template <int BN>
 static cudaError_t launch_gemm_bn(const GemmArgs& a, cudaStream_t s) {
     using C = GemmCfg<BN>;
     const int grid = a.m_tiles * a.n_tiles * a.n_splits;
-    gain_gemm_kernel<BN><<<grid, C::THREADS, C::SMEM, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(gain_gemm_kernel<BN>, dim3(grid), dim3(C::THREADS), C::SMEM, s, a);
 }
 
 cudaError_t launch_gain_gemm(int bn, const GemmArgs& a, cudaStream_t s) {
@@ -504,6 +530,8 @@ __global__ void split_reduce_kernel(const float* __restrict__ partial, int n_spl
                                     const int* __restrict__ active_hi, int n_space) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;  // column: cell i / Bcap, slot i % Bcap
+    pdl_wait();  // the partials of this step's GEMM
+    pdl_trigger();
     if (r >= M || i >= Bcap * n_space || (n_space == 1 && i >= *active_hi)) return;
     const int slot = i % Bcap;
     const float* p = partial + (size_t)i * M + r;
@@ -622,9 +650,6 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         vals[e] = 0.f;
     }
     if (mine) {
-        const size_t idx = (size_t)a * B + ib;  // B and ib are even
-        fa2 = *reinterpret_cast<const float2*>(F + idx);
-        ca2 = *reinterpret_cast<const float2*>(Cc + idx);
         inv_ap = (double)__ldg(ops.invAp + a);
         injv = (double)__ldg(ops.inj + a);
 #pragma unroll
@@ -646,6 +671,15 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         }
     }
 
+    // everything above is static or written by the host; the state and the group sums below are
+    // outputs of the previous step's epilogue and this step's split_reduce
+    pdl_wait();
+    if (tid == 0) pdl_trigger();
+    if (mine) {
+        const size_t idx = (size_t)a * B + ib;  // B and ib are even
+        fa2 = *reinterpret_cast<const float2*>(F + idx);
+        ca2 = *reinterpret_cast<const float2*>(Cc + idx);
+    }
     // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
     if (ops.has_bin) {
         const int r = tid & (kRT - 1);
@@ -956,17 +990,16 @@ cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out, float* C_out,
                               const unsigned long long* gstep, int kpos, cudaStream_t s) {
     dim3 grid((ops.n_state + kRT - 1) / kRT, (ops.Bcap + kIT - 1) / kIT);
-    mixed_rows_kernel<<<grid, kRowsThreads, kRowsSmem, s>>>(ops, F_in, C_in, F_out, C_out, gstep, kpos);
-    return cudaGetLastError();
+    return launch_pdl(mixed_rows_kernel, grid, dim3(kRowsThreads), (size_t)kRowsSmem, s, ops, F_in, C_in, F_out, C_out,
+                      gstep, kpos);
 }
 
 cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
                                 const float* sig1, const float* sig2, float* gsum, const int* active_hi,
                                 int n_space, cudaStream_t s) {
     dim3 grid((M + 255) / 256, Bcap * n_space);
-    split_reduce_kernel<<<grid, 256, 0, s>>>(partial, n_splits, Bpad, M, Bcap, row_scale, sig1, sig2, gsum,
-                                             active_hi, n_space);
-    return cudaGetLastError();
+    return launch_pdl(split_reduce_kernel, grid, dim3(256), 0, s, partial, n_splits, Bpad, M, Bcap, row_scale, sig1,
+                      sig2, gsum, active_hi, n_space);
 }
 
 int mixed_rows_tile_rows() { return kRT; }
