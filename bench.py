@@ -511,7 +511,7 @@ def run_batched(args):
             "config": dict(_config_dict(args.config, w), parallelism=f"batch replicas x{world}"),
             "e2e": {"value": world * B * K2 / (ms_e2e / 1e3), "unit": "instance-steps/s",
                     "h2d_bytes_per_step": B * n * 8, "d2h_bytes_per_step": B * n * 8},
-            "gpu_launches": int(st["launches_per_step"]) * K,
+            "gpu_launches": int(st["launches_per_step"]) * K + (K + 15) // 16,  # + one step-counter advance per graph
             "roofline": roof,
             "plain_fp64": {"value": plain_sps, "unit": "steps/s", "workload": "same grid, one instance, FP64"},
             "speedup_vs_plain_fp64": value / plain_sps,

@@ -23,7 +23,6 @@ struct MixedGroup {
     unsigned char* gt = nullptr;  // G tiles [m_tiles][T][hi, lo][128 x 128 B], pre-swizzled
     float* row_scale = nullptr;
     float* partial = nullptr;
-    float* gsum = nullptr;  // [Bcap][M]
     int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256, splits_per_cb = 0;
     double flops = 0;  // 3 MMAs x 2 x M x K x Bcap
     double bytes = 0;  // hi + lo bytes of G
@@ -201,7 +200,6 @@ int commit_mixed(dtb_ctx* c) {
             G.n_splits = k_cb * G.n_cb;
         }
         DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
-        DTB_TRY(c->alloc(&G.gsum, sizeof(float) * (size_t)Bcols * G.M));
         G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * m->Buser * nsp;
         G.bytes = 4.0 * G.M * (double)G.N1 * G.n2;
     }
@@ -415,8 +413,13 @@ int commit_mixed(dtb_ctx* c) {
     for (int sp = 0; sp <= c->ns; ++sp) ops.sp_off[sp] = (int)c->off[sp];
     for (size_t gi = 0; gi < m->groups.size(); ++gi) {
         const MixedGroup& G = m->groups[gi];
-        ops.grp_gsum[gi] = G.gsum;
+        ops.grp_partial[gi] = G.partial;
+        ops.grp_stride[gi] = (long long)G.Bpad * G.M;
+        ops.grp_nsplit[gi] = G.n_splits;
         ops.grp_M[gi] = G.M;
+        ops.grp_rscale[gi] = G.row_scale;
+        ops.grp_sig1[gi] = m->sig + (size_t)G.in1 * B;
+        ops.grp_sig2[gi] = m->sig + (size_t)G.in2 * B;
     }
     // tiles whose rows share one species and one list of emission pieces that cover all of
     // them take the shared-memory tile products
@@ -579,10 +582,6 @@ int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
         m->prof_n++;
         if (++m->prof_pending == 256) DTB_TRY(mixed_flush_profile(m));
     }
-    for (auto& G : m->groups)
-        DTB_CUDA(launch_split_reduce(G.partial, G.n_splits, G.Bpad, G.M, m->Bcap, G.row_scale,
-                                     m->sig + (size_t)G.in1 * m->Bcap, m->sig + (size_t)G.in2 * m->Bcap, G.gsum,
-                                     m->active_hi, c->n_space, c->stream));
     DTB_CUDA(launch_mixed_rows(m->ops, Fin, m->C[m->cur], m->F[m->cur ^ 1], m->C[m->cur ^ 1], m->gstep, kpos,
                                c->stream));
     if (advance > 0) DTB_CUDA(launch_advance_step(m->gstep, advance, c->stream));
@@ -939,7 +938,7 @@ int32_t dtb_batch_gemm_stats(dtb_ctx* c, double* avg_ms, double* flops_per_step,
     if (avg_ms) *avg_ms = m->prof_n ? m->prof_ms / (double)m->prof_n : 0.0;
     if (flops_per_step) *flops_per_step = fl;
     if (bytes_per_step) *bytes_per_step = by;
-    if (launches_per_step) *launches_per_step = 2 * (int32_t)m->groups.size() + 1;
+    if (launches_per_step) *launches_per_step = (int32_t)m->groups.size() + 1;  // + advance_step per graph
     return DTB_OK;
 }
 

@@ -90,8 +90,15 @@ struct MixedRowOps {
     int gain_ptr[DTB_MAX_SPECIES + 1];
     int gain_grp[64];
     int gain_roff[64];
-    const float* grp_gsum[16];    // [Bcap][M] reduced, rescaled gain sums of the group
+    // split-K partial sums of each gain group's GEMM: partial[split][column][M]; the epilogue sums
+    // the splits in order and scales back by row_scale[r] * sig1[slot] * sig2[slot]
+    const float* grp_partial[16];
+    long long grp_stride[16];     // Bpad * M: elements between splits
+    int grp_nsplit[16];
     int grp_M[16];
+    const float* grp_rscale[16];
+    const float* grp_sig1[16];    // [Bcap] power-of-two scale of input 1 per slot
+    const float* grp_sig2[16];
     const unsigned char* tile_fast;  // per 32-row tile: loss/emission as shared-memory tile products
     const RowJob* jobs;              // [tile][kRowsMaxJobs] product chunks of the fast tiles
     const int* njobs;                // [tile]
@@ -110,9 +117,6 @@ cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const f
 cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s);
 cudaError_t launch_pack_f(const double* io, int Buser, int n, int Bcap, float* F, float* C, cudaStream_t s);
 cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, int Bcap, double* io, cudaStream_t s);
-cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
-                                const float* sig1, const float* sig2, float* gsum, const int* active_hi,
-                                int n_space, cudaStream_t s);
 int mixed_rows_tile_rows();
 cudaError_t prepare_mixed_rows();
 

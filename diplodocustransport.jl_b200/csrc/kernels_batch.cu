@@ -522,33 +522,6 @@ constexpr int kRowStages = 3;     // cp.async ring depth
 constexpr int kStageFloats = kRT * kLS + kCK * kIT;
 constexpr int kRowsSmem = kRowStages * kStageFloats * 4;  // dynamic: the operand / state chunk ring
 
-// Sum of the split-K partial tiles of one gain group, scaled back to G and f units:
-// gsum[i][r] = row_scale[r] * sig1[i] * sig2[i] * sum_s partial[s][i][r]. Fixed summation order.
-__global__ void split_reduce_kernel(const float* __restrict__ partial, int n_splits, int Bpad, int M, int Bcap,
-                                    const float* __restrict__ row_scale, const float* __restrict__ sig1,
-                                    const float* __restrict__ sig2, float* __restrict__ gsum,
-                                    const int* __restrict__ active_hi, int n_space) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;  // column: cell i / Bcap, slot i % Bcap
-    pdl_wait();  // the partials of this step's GEMM
-    pdl_trigger();
-    if (r >= M || i >= Bcap * n_space || (n_space == 1 && i >= *active_hi)) return;
-    const int slot = i % Bcap;
-    const float* p = partial + (size_t)i * M + r;
-    const size_t stride = (size_t)Bpad * M;
-    float acc = 0.f;
-    int sp = 0;
-    for (; sp + 4 <= n_splits; sp += 4) {
-        const float v0 = p[(size_t)sp * stride], v1 = p[(size_t)(sp + 1) * stride];
-        const float v2 = p[(size_t)(sp + 2) * stride], v3 = p[(size_t)(sp + 3) * stride];
-        acc += v0;
-        acc += v1;
-        acc += v2;
-        acc += v3;
-    }
-    for (; sp < n_splits; ++sp) acc += p[(size_t)sp * stride];
-    gsum[(size_t)i * M + r] = acc * row_scale[r] * sig1[slot] * sig2[slot];
-}
 
 __device__ __forceinline__ int species_of_row(const MixedRowOps& ops, int a) {
     int s = 0;
@@ -671,8 +644,8 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         }
     }
 
-    // everything above is static or written by the host; the state and the group sums below are
-    // outputs of the previous step's epilogue and this step's split_reduce
+    // everything above is static or written by the host; the state and the split partials below
+    // are outputs of the previous step's epilogue and this step's gain GEMM
     pdl_wait();
     if (tid == 0) pdl_trigger();
     if (mine) {
@@ -693,10 +666,25 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             const int i = i0 + il;
             float g = 0.f;
             if (on && i < B) {
-                // group sums are [cell * Bcap + slot][stacked row]
+                // the group's split partials of column cell * Bcap + slot, summed in split order
                 for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
                     const int gi = ops.gain_grp[e];
-                    g += ops.grp_gsum[gi][((size_t)cell * B + i) * ops.grp_M[gi] + ops.gain_roff[e] + (am - ops.sp_off[s])];
+                    const int row = ops.gain_roff[e] + (am - ops.sp_off[s]);
+                    const float* pp = ops.grp_partial[gi] + ((size_t)cell * B + i) * ops.grp_M[gi] + row;
+                    const size_t st = (size_t)ops.grp_stride[gi];
+                    const int nsp = ops.grp_nsplit[gi];
+                    float acc = 0.f;
+                    int sp = 0;
+                    for (; sp + 4 <= nsp; sp += 4) {
+                        const float v0 = pp[(size_t)sp * st], v1 = pp[(size_t)(sp + 1) * st];
+                        const float v2 = pp[(size_t)(sp + 2) * st], v3 = pp[(size_t)(sp + 3) * st];
+                        acc += v0;
+                        acc += v1;
+                        acc += v2;
+                        acc += v3;
+                    }
+                    for (; sp < nsp; ++sp) acc += pp[(size_t)sp * st];
+                    g += acc * ops.grp_rscale[gi][row] * ops.grp_sig1[gi][i] * ops.grp_sig2[gi][i];
                 }
             }
             s_gain[r][il] = g;
@@ -994,13 +982,6 @@ cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const f
                       gstep, kpos);
 }
 
-cudaError_t launch_split_reduce(const float* partial, int n_splits, int Bpad, int M, int Bcap, const float* row_scale,
-                                const float* sig1, const float* sig2, float* gsum, const int* active_hi,
-                                int n_space, cudaStream_t s) {
-    dim3 grid((M + 255) / 256, Bcap * n_space);
-    return launch_pdl(split_reduce_kernel, grid, dim3(256), 0, s, partial, n_splits, Bpad, M, Bcap, row_scale, sig1,
-                      sig2, gsum, active_hi, n_space);
-}
 
 int mixed_rows_tile_rows() { return kRT; }
 
