@@ -925,7 +925,7 @@ static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, 
         }
         DTB_CUDA(launch_gain_stream<T>(reinterpret_cast<const T*>(c->G_all), c->units, c->n_units, fin, (int)c->n_mom,
                                        c->sp_off_host, c->ns, c->f_smem_len, c->partial, c->n_bin_cells,
-                                       c->gain_grid, c->err, c->stream, c->bin_cells));
+                                       c->gain_grid, c->err, c->stream, c->bin_cells, true));
         if (profile) {
             DTB_CUDA(cudaEventRecord(e1, c->stream));
             c->prof_n++;

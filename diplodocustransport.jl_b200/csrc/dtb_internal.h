@@ -98,7 +98,7 @@ template <typename T>
 cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, const T* f,
                                int n_mom, const int* sp_offp_dev, int n_species, int f_smem_len,
                                double* partial, int n_space, int grid_x, int* err, cudaStream_t s,
-                               const int* cell_list = nullptr);
+                               const int* cell_list = nullptr, bool pdl = false);
 
 template <typename T>
 cudaError_t launch_euler_rows(const RowOps<T>& ops, const T* f_in, T* f_out, double dt_imm,

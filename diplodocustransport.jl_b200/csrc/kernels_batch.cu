@@ -19,6 +19,7 @@
 #include <utility>
 
 #include "batch_internal.h"
+#include "pdl.cuh"
 
 namespace dtb {
 
@@ -26,28 +27,6 @@ namespace {
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
-// Programmatic dependent launch: the kernels of a batched step are launched so that the next
-// one may start while the previous one runs. Each waits for its predecessor (grid completion and
-// memory) before it reads what the predecessor wrote, and lets its own dependents launch only
-// after that wait, so a chain of early launches never skips a completion.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-template <typename... KArgs, typename... Args>
-static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                              Args&&... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -107,18 +86,17 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+
+// 16 columns of this warp's 32 TMEM lanes without waiting (tcgen05.wait::ld before using r).
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
           "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
     __nv_bfloat162 h = __floats2bfloat162_rn(lo_elem, hi_elem);
@@ -374,17 +352,23 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
         }
         if (ok && !*abort_flag) {
             float* dst = a.partial + (size_t)split * a.Bpad * a.M;
-            for (int cc = 0; cc < ncol; cc += 16) {
-                float v[16];
-                if (nt > 0 && c0 + cc < n_eff) {
-                    tmem_ld16(tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc), v);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 16; ++k) v[k] = 0.f;
-                }
+            // two 16-column loads in flight per wait
+            for (int cc = 0; cc < ncol; cc += 32) {
+                uint32_t r0[16], r1[16];
+                const bool ok0 = nt > 0 && c0 + cc < n_eff, ok1 = nt > 0 && c0 + cc + 16 < n_eff && cc + 16 < ncol;
+                const uint32_t ta = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc);
+                if (ok0) tmem_ld16_issue(ta, r0);
+                if (ok1) tmem_ld16_issue(ta + 16, r1);
+                if (ok0 || ok1) tmem_ld_wait();
                 if (row < a.M) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = v[k];
+                    for (int k = 0; k < 16; ++k)
+                        dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = ok0 ? __uint_as_float(r0[k]) : 0.f;
+                    if (cc + 16 < ncol) {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k)
+                            dst[(size_t)(n0 + c0 + cc + 16 + k) * a.M + row] = ok1 ? __uint_as_float(r1[k]) : 0.f;
+                    }
                 }
             }
         }

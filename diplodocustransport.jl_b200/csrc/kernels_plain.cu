@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "dtb_internal.h"
+#include "pdl.cuh"
 
 namespace dtb {
 
@@ -159,18 +160,7 @@ __global__ void __launch_bounds__(kGainThreads) gain_stream_kernel(const T* __re
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    if (warp < kGainConsumerWarps) {
-        // f of this cell in the padded per-species layout; zeros in the padding.
-        const T* fc = f + (size_t)cell * n_mom;
-        for (int i = tid; i < f_len; i += kNC) {
-            int s = 0;
-            while (s + 1 < so.n && i >= so.offp[s + 1]) ++s;
-            const int j = i - so.offp[s];
-            const int ns = so.off[s + 1] - so.off[s];
-            f_s[i] = (j < ns) ? fc[so.off[s] + j] : T(0);
-        }
-    }
-    __syncthreads();
+    __syncthreads();  // barriers initialised; the producer may stream G before f is ready
 
     if (warp == kGainConsumerWarps) {
         // ---------------- producer: one thread issues the bulk copies
@@ -214,6 +204,22 @@ __global__ void __launch_bounds__(kGainThreads) gain_stream_kernel(const T* __re
     }
 
     // ---------------- consumers: 8 warps
+    // f is the previous step's output and the previous step still reads the partials this
+    // kernel writes: wait for it (the G tiles already stream in meanwhile)
+    pdl_wait();
+    if (tid == 0) pdl_trigger();
+    {
+        // f of this cell in the padded per-species layout; zeros in the padding.
+        const T* fc = f + (size_t)cell * n_mom;
+        for (int i = tid; i < f_len; i += kNC) {
+            int s = 0;
+            while (s + 1 < so.n && i >= so.offp[s + 1]) ++s;
+            const int j = i - so.offp[s];
+            const int ns = so.off[s + 1] - so.off[s];
+            f_s[i] = (j < ns) ? fc[so.off[s] + j] : T(0);
+        }
+    }
+    asm volatile("bar.sync 1, %0;" ::"n"(kNC) : "memory");  // the consumer warps only
     uint32_t it = 0;
     uint32_t lk = 0;  // units done by this block
     for (int u = blockIdx.x; u < n_units; u += gridDim.x, ++lk) {
@@ -287,7 +293,7 @@ int gain_stream_blocks_per_sm(int elem_size, int f_smem_len) {
 template <typename T>
 cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, const T* f, int n_mom,
                                const int* sp_off_host, int n_species, int f_smem_len, double* partial,
-                               int n_space, int grid_x, int* err, cudaStream_t s, const int* cell_list) {
+                               int n_space, int grid_x, int* err, cudaStream_t s, const int* cell_list, bool pdl) {
     // n_space: cells to run (grid y); cell_list maps them to cells, or null for 0..n_space-1
     // sp_off_host: [0..n_species] unpadded then [0..n_species] padded offsets (host array)
     SpOff so;
@@ -299,17 +305,22 @@ cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, c
     // the dynamic shared-memory limit was raised by gain_stream_blocks_per_sm at commit
     const int smem = gain_stream_smem_bytes(sizeof(T), f_smem_len);
     dim3 grid(grid_x, n_space);
-    gain_stream_kernel<T><<<grid, kGainThreads, smem, s>>>(G, units, n_units, f, n_mom, so, f_smem_len, partial,
-                                                           err, cell_list);
+    // pdl: a step's own sequence (its G is static); a caller's G may be its predecessor's output,
+    // which the producer (it starts before the dependency wait) must not read early
+    if (pdl)
+        return launch_pdl(gain_stream_kernel<T>, grid, dim3(kGainThreads), (size_t)smem, s, G, units, n_units, f, n_mom,
+                          so, f_smem_len, partial, err, cell_list);
+    gain_stream_kernel<T><<<grid, kGainThreads, smem, s>>>(G, units, n_units, f, n_mom, so, f_smem_len, partial, err,
+                                                           cell_list);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_gain_stream<double>(const double*, const GainUnit*, int, const double*, int,
                                                 const int*, int, int, double*, int, int, int*, cudaStream_t,
-                                                const int*);
+                                                const int*, bool);
 template cudaError_t launch_gain_stream<float>(const float*, const GainUnit*, int, const float*, int,
                                                const int*, int, int, double*, int, int, int*, cudaStream_t,
-                                               const int*);
+                                               const int*, bool);
 
 // ------------------------------------------------------------------ euler_rows
 constexpr int kRedFields = 7;  // min cr, cr_bin, cr_emi, cr_flux, sum_df, sum_f, nonfinite count
@@ -324,6 +335,8 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
     __shared__ double s_red[kRowsWarps][kRedFields];
     __shared__ double s_fin[6][kRowsWarps * 32];
     __shared__ int s_last;
+    pdl_wait();  // this step's inputs (gain partials, momentum pass) and the previous step's state and counter
+    if (threadIdx.x == 0) pdl_trigger();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
     const double dt_scale = dt_arr ? dt_arr[step] : dt_imm;
@@ -504,9 +517,8 @@ cudaError_t launch_euler_rows(const RowOps<T>& ops, const T* f_in, T* f_out, dou
                               unsigned long long* ctr, StepDiagDev* hist, long long hist_cap, int verbose,
                               double* blk_red, unsigned* ticket, cudaStream_t s) {
     const int grid = (ops.n_state + kRowsWarps - 1) / kRowsWarps;
-    euler_rows_kernel<T><<<grid, kRowsWarps * 32, 0, s>>>(ops, f_in, f_out, dt_imm, dt_arr, ctr, hist, hist_cap,
-                                                          verbose, blk_red, ticket);
-    return cudaGetLastError();
+    return launch_pdl(euler_rows_kernel<T>, grid, dim3(kRowsWarps * 32), 0, s, ops, f_in, f_out, dt_imm, dt_arr, ctr,
+                      hist, hist_cap, verbose, blk_red, ticket);
 }
 
 template cudaError_t launch_euler_rows<double>(const RowOps<double>&, const double*, double*, double, const double*,
@@ -532,6 +544,8 @@ __global__ void __launch_bounds__(kRowsWarps * 32) sympl_space_kernel(RowOps<T> 
     __shared__ double s_red[kRowsWarps][2];
     __shared__ double s_fin[2][kRowsWarps * 32];
     __shared__ int s_last;
+    pdl_wait();  // this step's inputs (gain partials, momentum pass) and the previous step's state and counter
+    if (threadIdx.x == 0) pdl_trigger();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
     const double dt_scale = dt_arr ? dt_arr[step] : dt_imm;
@@ -615,9 +629,8 @@ cudaError_t launch_sympl_space(const RowOps<T>& ops, const T* f_old, const T* fm
                                double dt_imm, const double* dt_arr, unsigned long long* ctr, StepDiagDev* hist,
                                long long hist_cap, int verbose, double* blk_red, unsigned* ticket, cudaStream_t s) {
     const int grid = (ops.n_state + kRowsWarps - 1) / kRowsWarps;
-    sympl_space_kernel<T><<<grid, kRowsWarps * 32, 0, s>>>(ops, f_old, fm, dfm, f_out, dt_imm, dt_arr, ctr, hist,
-                                                           hist_cap, verbose, blk_red, ticket);
-    return cudaGetLastError();
+    return launch_pdl(sympl_space_kernel<T>, grid, dim3(kRowsWarps * 32), 0, s, ops, f_old, fm, dfm, f_out, dt_imm,
+                      dt_arr, ctr, hist, hist_cap, verbose, blk_red, ticket);
 }
 template cudaError_t launch_sympl_space<double>(const RowOps<double>&, const double*, const double*, const double*,
                                                 double*, double, const double*, unsigned long long*, StepDiagDev*,
