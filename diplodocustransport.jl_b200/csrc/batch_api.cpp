@@ -450,14 +450,18 @@ int commit_mixed(dtb_ctx* c) {
         // the loss blocks of the tile's species, then the emission pieces of its rows
         std::vector<RowJob> jobs((size_t)n_tiles_r * kRowsMaxJobs);
         std::vector<int> njobs((size_t)n_tiles_r, 0);
-        std::vector<std::vector<RowJob>> loss_of((size_t)c->ns);  // per species: (T at row 0, ld, col0, nc)
+        struct Opnd {
+            const float* T;  // row 0 of the operand block, column 0
+            int ld, col0, nc;
+        };
+        std::vector<std::vector<Opnd>> loss_of((size_t)c->ns);  // per species
         {
             long long off = 0;
             for (int sp = 0; sp < c->ns; ++sp)
                 for (auto& kv : c->losses) {
                     if (kv.first.first != sp) continue;
                     const int64_t nr = c->sz[sp], nc = c->sz[kv.first.second], l = round_up(nc, 4);
-                    loss_of[(size_t)sp].push_back({ops.loss_data + off, (int)l, (int)c->off[kv.first.second], (int)nc, 0, 0, 0});
+                    loss_of[(size_t)sp].push_back({ops.loss_data + off, (int)l, (int)c->off[kv.first.second], (int)nc});
                     off += nr * l;
                 }
         }
@@ -472,19 +476,34 @@ int commit_mixed(dtb_ctx* c) {
         for (int t = 0; t < n_tiles_r; ++t) {
             if (!fast[(size_t)t]) continue;
             const int a0 = t * tr, cell = a0 / n_mom, s0 = species_of(c, a0 % n_mom);
-            RowJob* J = jobs.data() + (size_t)t * kRowsMaxJobs;
-            int k = 0;
-            if (c->has_bin)  // the loss of a cell reads that cell's states
-                for (const RowJob& L : loss_of[(size_t)s0])
-                    for (int c0 = 0; c0 < L.nc; c0 += kRowsChunk)
-                        J[k++] = {L.T + (size_t)(a0 - cell * n_mom - c->off[s0]) * L.ld, L.ld, L.col0 + cell * n_mom, L.nc,
-                                  c0, 0, 0};
+            // the tile's operands at its first row: loss blocks read the tile's cell, emission
+            // pieces their global columns; a loss block and an emission piece over the same state
+            // rows share jobs
+            std::vector<Opnd> L, E;
+            if (c->has_bin)
+                for (const Opnd& o : loss_of[(size_t)s0])
+                    L.push_back({o.T + (size_t)(a0 - cell * n_mom - c->off[s0]) * o.ld, o.ld, o.col0 + cell * n_mom, o.nc});
             for (int p : emi_rows[(size_t)a0]) {
                 const EmiPiece& e = c->emis[(size_t)p];
                 const int l = (int)round_up(e.ncols, 4);
-                for (int c0 = 0; c0 < e.ncols; c0 += kRowsChunk)
-                    J[k++] = {ops.emi_data + emi_off[(size_t)p] + (size_t)(a0 - e.row0) * l, l, (int)e.col0, (int)e.ncols,
-                              c0, 1, 0};
+                E.push_back({ops.emi_data + emi_off[(size_t)p] + (size_t)(a0 - e.row0) * l, l, (int)e.col0, (int)e.ncols});
+            }
+            RowJob* J = jobs.data() + (size_t)t * kRowsMaxJobs;
+            int k = 0;
+            std::vector<bool> e_used(E.size(), false);
+            for (const Opnd& lo : L) {
+                int pair = -1;
+                for (size_t q = 0; q < E.size() && pair < 0; ++q)
+                    if (!e_used[q] && E[q].col0 == lo.col0 && E[q].nc == lo.nc) pair = (int)q;
+                if (pair >= 0) e_used[(size_t)pair] = true;
+                for (int c0 = 0; c0 < lo.nc; c0 += kRowsChunk)
+                    J[k++] = {lo.T, pair >= 0 ? E[(size_t)pair].T : nullptr, lo.ld, pair >= 0 ? E[(size_t)pair].ld : 0,
+                              lo.col0, lo.nc, c0, 0};
+            }
+            for (size_t q = 0; q < E.size(); ++q) {
+                if (e_used[q]) continue;
+                for (int c0 = 0; c0 < E[q].nc; c0 += kRowsChunk)
+                    J[k++] = {nullptr, E[q].T, 0, E[q].ld, E[q].col0, E[q].nc, c0, 0};
             }
             njobs[(size_t)t] = k;
         }

@@ -53,12 +53,13 @@ constexpr int kRowsChunk = 128;
 // (loss or emission rows) against the same state rows of the tile's instances. Built on the
 // host per 32-row tile.
 struct RowJob {
-    const float* T;  // operand row of the tile's first row, at column 0
-    int ld;          // operand row pitch (a multiple of 4)
-    int col0;        // state row of operand column 0
-    int nc;          // operand columns
-    int c0;          // first column of the chunk
-    int which;       // 0: loss, 1: emission
+    const float* TL;  // loss operand row of the tile's first row at column 0, or null
+    const float* TE;  // emission operand row likewise, or null (loss and emission over the
+                      // same state rows share one job and one staged state chunk)
+    int ldl, lde;     // operand row pitches (multiples of 4)
+    int col0;         // state row of operand column 0
+    int nc;           // operand columns
+    int c0;           // first column of the chunk
     int pad;
 };
 

@@ -503,7 +503,7 @@ constexpr int kIT = 32;   // instances per tile
 constexpr int kCK = kRowsChunk;  // K chunk of the loss / emission tile products
 constexpr int kLS = kCK + 4;      // row pitch of a staged operand chunk (16-byte aligned rows)
 constexpr int kRowStages = 3;     // cp.async ring depth
-constexpr int kStageFloats = kRT * kLS + kCK * kIT;
+constexpr int kStageFloats = 2 * kRT * kLS + kCK * kIT;  // loss chunk, emission chunk, state chunk
 constexpr int kRowsSmem = kRowStages * kStageFloats * 4;  // dynamic: the operand / state chunk ring
 
 
@@ -695,15 +695,16 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         // a chunk into ring stage st: 1024 16-byte pieces of operand and 1024 of state, 2 + 2 per thread
         auto issue = [&](int k, int st) {
             float* sL = rows_dyn + st * kStageFloats;
-            float* sF = sL + kRT * kLS;
+            float* sE = sL + kRT * kLS;
+            float* sF = sE + kRT * kLS;
             const RowJob J = s_job[k];
 #pragma unroll
             for (int q2 = 0; q2 < 2; ++q2) {
                 const int q = tid + kRowsThreads * q2;
                 const int rr = q >> 5, c4 = (q & 31) * 4;
                 const bool ok = a0 + rr < n && J.c0 + c4 < J.nc;
-                const float* src = ok ? J.T + (size_t)rr * J.ld + J.c0 + c4 : J.T;
-                cp_async16(sL + rr * kLS + c4, src, ok ? 16 : 0);
+                if (J.TL) cp_async16(sL + rr * kLS + c4, ok ? J.TL + (size_t)rr * J.ldl + J.c0 + c4 : J.TL, ok ? 16 : 0);
+                if (J.TE) cp_async16(sE + rr * kLS + c4, ok ? J.TE + (size_t)rr * J.lde + J.c0 + c4 : J.TE, ok ? 16 : 0);
                 const int cr = q >> 3, i4 = (q & 7) * 4;
                 const bool okf = J.c0 + cr < J.nc && i0 + i4 < B;
                 const float* srcf = okf ? F + (size_t)(J.col0 + J.c0 + cr) * B + i0 + i4 : F;
@@ -722,33 +723,34 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             if (k + kRowStages - 1 < nj) issue(k + kRowStages - 1, (k + kRowStages - 1) % kRowStages);
             cp_async_commit();
             const float* sL = rows_dyn + (k % kRowStages) * kStageFloats;
-            const float* sF = sL + kRT * kLS;
-            float t[4][4];
+            const float* sE = sL + kRT * kLS;
+            const float* sF = sE + kRT * kLS;
+            const bool hl = s_job[k].TL != nullptr, he = s_job[k].TE != nullptr;
+            if (hl) {
 #pragma unroll
-            for (int k2 = 0; k2 < 4; ++k2)
+                for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
+                    const float4 f4 = *reinterpret_cast<const float4*>(sF + cc * kIT + tx * 4);
+                    const float fvv[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
-                for (int j2 = 0; j2 < 4; ++j2) t[k2][j2] = 0.f;
+                    for (int k2 = 0; k2 < 4; ++k2) {
+                        const float l = sL[(ty + 8 * k2) * kLS + cc];
 #pragma unroll
-            for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
-                const float4 f4 = *reinterpret_cast<const float4*>(sF + cc * kIT + tx * 4);
-                const float fvv[4] = {f4.x, f4.y, f4.z, f4.w};
-#pragma unroll
-                for (int k2 = 0; k2 < 4; ++k2) {
-                    const float l = sL[(ty + 8 * k2) * kLS + cc];
-#pragma unroll
-                    for (int j2 = 0; j2 < 4; ++j2) t[k2][j2] += l * fvv[j2];
+                        for (int j2 = 0; j2 < 4; ++j2) acc_l[k2][j2] += l * fvv[j2];
+                    }
                 }
             }
-            if (s_job[k].which) {
+            if (he) {
 #pragma unroll
-                for (int k2 = 0; k2 < 4; ++k2)
+                for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
+                    const float4 f4 = *reinterpret_cast<const float4*>(sF + cc * kIT + tx * 4);
+                    const float fvv[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
-                    for (int j2 = 0; j2 < 4; ++j2) acc_e[k2][j2] += t[k2][j2];
-            } else {
+                    for (int k2 = 0; k2 < 4; ++k2) {
+                        const float e = sE[(ty + 8 * k2) * kLS + cc];
 #pragma unroll
-                for (int k2 = 0; k2 < 4; ++k2)
-#pragma unroll
-                    for (int j2 = 0; j2 < 4; ++j2) acc_l[k2][j2] += t[k2][j2];
+                        for (int j2 = 0; j2 < 4; ++j2) acc_e[k2][j2] += e * fvv[j2];
+                    }
+                }
             }
         }
         cp_async_wait<0>();
