@@ -282,3 +282,59 @@ def test_multicell_moments_and_bulk_io(cuda):
                 assert en[i, cell, s] == pytest.approx((G[i][sl] * wts[sum(sizes[:s]):sum(sizes[:s]) + sizes[s]]).sum(),
                                                        rel=1e-12)
     m.close()
+
+
+def test_number_conservation_plain_and_batched(cuda):
+    """Known answer: gain and loss built to conserve number per species (flux and emission off)
+    keep sum(f) of each species over 50 steps: to FP64 rounding on the plain FP64 path, and to
+    the BF16 hi+lo contraction's accuracy on the batched path, with FP64 device moments."""
+    from dtb.stepping import ForwardEulerStruct
+    from dtb.structs import FluxMatrices
+    w = synth.small(p_num=8, u_num=4, seed=8, with_emission=False)
+    ns = w.ps.species_sizes[0]
+    n = w.ps.n_state
+    Ge = np.asarray(w.binm.gains[0].G)
+    Gg = np.asarray(w.binm.gains[1].G)
+    w.binm.losses = [LossBlock(0, 1, Ge.sum(axis=0)), LossBlock(1, 0, Gg.sum(axis=0).T)]
+    w.fluxm = FluxMatrices(Ap_Flux=np.ones(n), Am_Flux=-np.ones(n), X_Flux=sp.csc_matrix((n, n)),
+                           P_Flux=sp.csc_matrix((n, n)), Vol=np.ones(1))
+    w.inj = np.zeros(n)
+    n0 = [w.f0[:ns].sum(), w.f0[ns:].sum()]
+    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, Precision=np.float64)
+    for _ in range(50):
+        m(0.0, 1e9, 1.0, 0)
+    f = m.f
+    assert f.min() > 0
+    assert abs(f[:ns].sum() - n0[0]) / n0[0] < 1e-12
+    assert abs(f[ns:].sum() - n0[1]) / n0[1] < 1e-12
+    m.close()
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 4)
+    for i in range(4):
+        b.admit(i, w.f0 * (1.0 + 0.1 * i), 1.0, 50)
+    b.run(50)
+    num, _ = b.moments(np.ones(w.ps.n_momentum))
+    for i in range(4):
+        for s_ in range(2):
+            assert abs(num[i, s_] - n0[s_] * (1.0 + 0.1 * i)) / (n0[s_] * (1.0 + 0.1 * i)) < 1e-5
+    b.close()
+
+
+def test_batched_cr_and_finite_flags_match_oracle(cuda):
+    """Per-slot diagnostics: the largest Cr = -min(df ./ f) over a slot's steps
+    (SteppingMethods.jl:48-94) and the finite flag, against the FP64 oracle's per-step Cr."""
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, 5, seed=14)
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 5)
+    for i in range(5):
+        m.admit(i, w.f0[i], w.dt[i], 20)
+    m.run(20)
+    ops = oracle.blocked_from_workload(w)
+    for i in range(5):
+        f = w.f0[i].copy()
+        crs = []
+        for _ in range(20):
+            f, d, _ = ops.step(f, w.dt[i], 1)
+            crs.append(d[0])
+        info = m.info(i)
+        assert info["finite"]
+        assert info["cr_max"] == pytest.approx(max(crs), rel=1e-4), i
+    m.close()
