@@ -632,6 +632,35 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     // are outputs of the previous step's epilogue and this step's gain GEMM
     pdl_wait();
     if (tid == 0) pdl_trigger();
+    __syncthreads();  // the job table is visible
+    // a chunk into ring stage st: 1024 16-byte pieces of each operand and of the state, 2 + 2 + 2
+    // per thread
+    auto issue = [&](int k, int st) {
+        float* sL = rows_dyn + st * kStageFloats;
+        float* sE = sL + kRT * kLS;
+        float* sF = sE + kRT * kLS;
+        const RowJob J = s_job[k];
+#pragma unroll
+        for (int q2 = 0; q2 < 2; ++q2) {
+            const int q = tid + kRowsThreads * q2;
+            const int rr = q >> 5, c4 = (q & 31) * 4;
+            const bool ok = a0 + rr < n && J.c0 + c4 < J.nc;
+            if (J.TL) cp_async16(sL + rr * kLS + c4, ok ? J.TL + (size_t)rr * J.ldl + J.c0 + c4 : J.TL, ok ? 16 : 0);
+            if (J.TE) cp_async16(sE + rr * kLS + c4, ok ? J.TE + (size_t)rr * J.lde + J.c0 + c4 : J.TE, ok ? 16 : 0);
+            const int cr = q >> 3, i4 = (q & 7) * 4;
+            const bool okf = J.c0 + cr < J.nc && i0 + i4 < B;
+            const float* srcf = okf ? F + (size_t)(J.col0 + J.c0 + cr) * B + i0 + i4 : F;
+            cp_async16(sF + cr * kIT + i4, srcf, okf ? 16 : 0);
+        }
+    };
+    // the first chunks are in flight while the gain partials are gathered below
+    if (fast) {
+#pragma unroll
+        for (int k = 0; k < kRowStages - 1; ++k) {
+            if (k < s_njob) issue(k, k);
+            cp_async_commit();  // empty groups keep the group count uniform
+        }
+    }
     if (mine) {
         const size_t idx = (size_t)a * B + ib;  // B and ib are even
         fa2 = *reinterpret_cast<const float2*>(F + idx);
@@ -692,30 +721,6 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         }
     if (fast) {
         const int nj = s_njob;
-        // a chunk into ring stage st: 1024 16-byte pieces of operand and 1024 of state, 2 + 2 per thread
-        auto issue = [&](int k, int st) {
-            float* sL = rows_dyn + st * kStageFloats;
-            float* sE = sL + kRT * kLS;
-            float* sF = sE + kRT * kLS;
-            const RowJob J = s_job[k];
-#pragma unroll
-            for (int q2 = 0; q2 < 2; ++q2) {
-                const int q = tid + kRowsThreads * q2;
-                const int rr = q >> 5, c4 = (q & 31) * 4;
-                const bool ok = a0 + rr < n && J.c0 + c4 < J.nc;
-                if (J.TL) cp_async16(sL + rr * kLS + c4, ok ? J.TL + (size_t)rr * J.ldl + J.c0 + c4 : J.TL, ok ? 16 : 0);
-                if (J.TE) cp_async16(sE + rr * kLS + c4, ok ? J.TE + (size_t)rr * J.lde + J.c0 + c4 : J.TE, ok ? 16 : 0);
-                const int cr = q >> 3, i4 = (q & 7) * 4;
-                const bool okf = J.c0 + cr < J.nc && i0 + i4 < B;
-                const float* srcf = okf ? F + (size_t)(J.col0 + J.c0 + cr) * B + i0 + i4 : F;
-                cp_async16(sF + cr * kIT + i4, srcf, okf ? 16 : 0);
-            }
-        };
-#pragma unroll
-        for (int k = 0; k < kRowStages - 1; ++k) {
-            if (k < nj) issue(k, k);
-            cp_async_commit();  // empty groups keep the group count uniform
-        }
         const int k0 = kg * (kCK / kKGroups);
         for (int k = 0; k < nj; ++k) {
             cp_async_wait<kRowStages - 2>();
