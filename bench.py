@@ -489,16 +489,20 @@ def run_batched(args):
     peak_s = float(pj.get("bf16_tflops_sustained", 1400.0))
     achieved = st["flops_per_step"] / (st["avg_ms"] / 1e3) / 1e12 if st["avg_ms"] > 0 else None
     traffic = _profile_traffic(f"gain_gemm_config{args.config}.md")
+    # 256-column tiles over an even number of 128-row m tiles run on SM pairs (cta_group::2)
+    pairs = B * w.ps.n_space >= 192 and (sum(w.ps.species_sizes) + 127) // 128 % 2 == 0
+    GEMM_LABEL = ("gain_gemm_pair (tcgen05.mma.cta_group::2, BF16 hi+lo x3)" if pairs
+                  else "gain_gemm (tcgen05, BF16 hi+lo x3)")
     # the GEMM's bound: the slower of its tensor time and its operator-streaming time
     hbm = float(pj.get("hbm_gbs", 6650.0))
     hbm_bound = st["bytes_per_step"] / (hbm * 1e9) > st["flops_per_step"] / (peak * 1e12)
     if hbm_bound:
         gbs = st["bytes_per_step"] / (st["avg_ms"] / 1e3) / 1e9 if st["avg_ms"] > 0 else None
-        roof = {"bound": "hbm", "kernel": "gain_gemm (tcgen05, BF16 hi+lo x3)", "achieved": gbs, "peak": hbm,
+        roof = {"bound": "hbm", "kernel": GEMM_LABEL, "achieved": gbs, "peak": hbm,
                 "peak_kind": "measured" if pj else "fallback", "unit": "GB/s", "frac": gbs / hbm if gbs else None,
                 "tensor_tflops": achieved}
     else:
-        roof = {"bound": "tensor", "kernel": "gain_gemm (tcgen05, BF16 hi+lo x3)", "achieved": achieved,
+        roof = {"bound": "tensor", "kernel": GEMM_LABEL, "achieved": achieved,
                 "peak": peak, "peak_kind": "measured burst" if pj else "fallback", "unit": "TFLOP/s",
                 "frac": achieved / peak if achieved else None,
                 "frac_of_sustained": achieved / peak_s if achieved else None}

@@ -24,6 +24,7 @@ struct MixedGroup {
     float* row_scale = nullptr;
     float* partial = nullptr;
     int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256, splits_per_cb = 0;
+    bool pair = false;  // the CTA-pair kernel (cta_group::2) runs this group
     double flops = 0;  // 3 MMAs x 2 x M x K x Bcap
     double bytes = 0;  // hi + lo bytes of G
 };
@@ -181,13 +182,21 @@ int commit_mixed(dtb_ctx* c) {
     }
     DTB_CUDA(prepare_gain_gemm(bn));
     DTB_CUDA(prepare_mixed_rows());
+    // 256-column tiles over an even number of m tiles run on SM pairs (DTB_GEMM=classic keeps
+    // the one-SM kernel)
+    const char* gk = std::getenv("DTB_GEMM");
+    int max_pairs = 0;
+    if (bn == 256 && !(gk && std::string(gk) == "classic")) DTB_CUDA(prepare_gain_gemm_pair(&max_pairs));
     for (auto& G : m->groups) {
         G.bn = bn;
         G.n_tiles = (Bcols + bn - 1) / bn;
         G.Bpad = G.n_tiles * bn;
         G.m_tiles = (G.M + kMmaM - 1) / kMmaM;
+        G.pair = max_pairs > 0 && G.m_tiles % 2 == 0;
         const int T = G.n_cb * G.N1;
-        int S = std::max(1, (int)std::lround((double)c->num_sms / (G.m_tiles * G.n_tiles)));
+        // K splits: one CTA per SM, or one pair per co-resident cluster of two
+        int S = G.pair ? std::max(1, (int)std::lround((double)max_pairs / (G.m_tiles / 2 * G.n_tiles)))
+                       : std::max(1, (int)std::lround((double)c->num_sms / (G.m_tiles * G.n_tiles)));
         S = std::min(S, T);
         G.tiles_per_split = (T + S - 1) / S;
         G.n_splits = (T + G.tiles_per_split - 1) / G.tiles_per_split;
@@ -594,7 +603,10 @@ int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
         a.partial = G.partial;
         a.err = c->err;
         a.active_hi = m->active_hi;
-        DTB_CUDA(launch_gain_gemm(G.bn, a, c->stream));
+        if (G.pair)
+            DTB_CUDA(launch_gain_gemm_pair(a, c->stream));
+        else
+            DTB_CUDA(launch_gain_gemm(G.bn, a, c->stream));
     }
     if (profile) {
         DTB_CUDA(cudaEventRecord(e1, c->stream));

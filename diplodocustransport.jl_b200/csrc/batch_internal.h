@@ -39,6 +39,11 @@ struct GemmArgs {
 };
 
 cudaError_t launch_gain_gemm(int bn, const GemmArgs& a, cudaStream_t s);
+// The CTA-pair variant (BN = 256, m_tiles even): grid m_tiles x n_tiles x n_splits CTAs in
+// clusters of two. prepare_gain_gemm_pair raises the shared-memory limit and reports how many
+// pairs fit on the device at once.
+cudaError_t prepare_gain_gemm_pair(int* max_pairs);
+cudaError_t launch_gain_gemm_pair(const GemmArgs& a, cudaStream_t s);
 
 // Bytes of one K tile of one m tile of G: hi and lo halves of 128 rows x 64 BF16.
 constexpr int kGTileBytes = 2 * kMmaM * kMmaK * 2;

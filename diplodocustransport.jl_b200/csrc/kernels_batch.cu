@@ -381,6 +381,342 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     }
 }
 
+// ------------------------------------------------------------------ CTA-pair gain GEMM
+// The same contraction with the MMA spread over the two SMs of a cluster pair
+// (tcgen05.mma.cta_group::2, M = 256 = two m tiles, N = 256 columns of X): each CTA stages its
+// own 128 G rows and HALF of the X tile, and the pair's tensor cores read both halves, so an SM
+// forms 128 instead of 256 columns of X and its shared memory serves A plus half of B per MMA
+// (104 instead of 157 bytes per clock at the full MMA rate, against the 128 an SM delivers).
+// The even CTA (rank 0) issues the MMAs for the pair. The odd CTA's producer warps arrive on the
+// even CTA's X barrier directly and one odd-CTA thread forwards the landing of each of its G
+// stages; the even CTA commits stage releases and the final accumulator to the barriers of
+// both. TMA multicast is not used.
+struct PairCfg {
+    static constexpr int BN = 256;               // X columns of a pair (the MMA's N)
+    static constexpr int HN = BN / 2;            // X columns staged by each CTA
+    static constexpr int NPW = 8;                // producer / epilogue warps
+    static constexpr int THREADS = (NPW + 2) * 32;
+    static constexpr int A_BYTES = kMmaM * 128;  // hi or lo of this CTA's 128 G rows x 64 K
+    static constexpr int B_BYTES = HN * 128;     // hi or lo of this CTA's half of the X tile
+    static constexpr int SA = 4;
+    static constexpr int SB = 3;
+    static constexpr int DATA = SA * 2 * A_BYTES + SB * 2 * B_BYTES;
+    static constexpr int BARS = (3 * SA + 2 * SB + 3) * 8;
+    static constexpr int SMEM = 1024 + DATA + BARS + 16;
+};
+static_assert(PairCfg::SMEM <= 232448, "pair GEMM shared memory");
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// shared::cluster address of the same shared-memory location in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// arrive on a barrier of the other CTA of the pair (shared::cluster address)
+__device__ __forceinline__ void mb_arrive_remote(uint32_t cluster_bar) {
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+__device__ __forceinline__ void umma2_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// arrive on one barrier (this CTA's or the peer's, by shared::cluster address) once the pair
+// MMAs issued so far by this thread have completed
+__device__ __forceinline__ void umma2_commit(uint32_t cluster_bar) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(cluster_bar)
+                 : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
+    gain_gemm_pair_kernel(GemmArgs a) {
+    using C = PairCfg;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* a_base = smem;                           // [SA][hi, lo][128 rows x 128 B]
+    unsigned char* b_base = smem + C::SA * 2 * C::A_BYTES;  // [SB][hi, lo][HN rows x 128 B]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + C::DATA);
+    uint64_t* full_a = bars;             // this CTA's G stage landed
+    uint64_t* empty_a = full_a + C::SA;  // the pair's MMAs are done with the stage
+    uint64_t* pfull_a = empty_a + C::SA; // rank 0 only: the odd CTA's G stage landed
+    uint64_t* full_b = pfull_a + C::SA;  // rank 0: both CTAs' X halves of the stage are written
+    uint64_t* empty_b = full_b + C::SB;
+    uint64_t* acc_bar = empty_b + C::SB;
+    uint64_t* drain_bar = acc_bar + 1;
+    uint64_t* x0_bar = drain_bar + 1;
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(x0_bar + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_rank();
+    const int pair = blockIdx.x >> 1;
+    const int m_pairs = a.m_tiles >> 1;
+    const int n_tile = pair % a.n_tiles;
+    const int mp = (pair / a.n_tiles) % m_pairs;
+    const int split = pair / (a.n_tiles * m_pairs);
+    const int m_tile = 2 * mp + (int)rank;
+    const int T = a.n_cb * a.N1;
+    int t0, t1;
+    if (a.splits_per_cb > 0) {
+        const int cb = split / a.splits_per_cb, piece = split - cb * a.splits_per_cb;
+        t0 = cb * a.N1 + (int)((long long)piece * a.N1 / a.splits_per_cb);
+        t1 = cb * a.N1 + (int)((long long)(piece + 1) * a.N1 / a.splits_per_cb);
+    } else {
+        t0 = split * a.tiles_per_split;
+        t1 = min(T, t0 + a.tiles_per_split);
+    }
+    const int m0 = m_tile * kMmaM, n0 = n_tile * C::BN;
+    // active columns rounded up to 32, so each CTA's half is a whole number of 16-row groups
+    const int hi_cols = a.n_space > 1 ? a.n_space * a.Bst : *reinterpret_cast<const volatile int*>(a.active_hi);
+    const int n_eff = max(0, min(C::BN, (hi_cols - n0 + 31) / 32 * 32));
+    const int hn = n_eff / 2;
+    const int nt = (n_eff > 0 && t1 > t0) ? t1 - t0 : 0;
+
+    if (tid == 0) {
+        for (int s = 0; s < C::SA; ++s) {
+            mb_init(smem_addr(&full_a[s]), 1);
+            mb_init(smem_addr(&empty_a[s]), 1);
+            mb_init(smem_addr(&pfull_a[s]), 1);
+        }
+        for (int s = 0; s < C::SB; ++s) {
+            mb_init(smem_addr(&full_b[s]), 2 * C::NPW);  // one arrive per producing warp of the pair
+            mb_init(smem_addr(&empty_b[s]), 1);
+        }
+        mb_init(smem_addr(acc_bar), 1);
+        mb_init(smem_addr(drain_bar), 1);
+        mb_init(smem_addr(x0_bar), C::NPW);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == C::NPW + 1) {  // same warp in both CTAs: BN fp32 columns x 128 lanes in each
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_holder)),
+                     "r"(C::BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    // both CTAs' barriers are initialised before either CTA signals the other
+    tc_fence_before();
+    cluster_sync_all();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp == C::NPW) {
+        // ---------------- bulk-copy producer of this CTA's G tiles
+        if (lane == 0 && nt > 0) {
+            const unsigned char* src0 = a.gt + ((size_t)m_tile * T + t0) * kGTileBytes;
+            int j = 0;
+            for (; j < nt; ++j) {
+                const int sa = j % C::SA;
+                const uint32_t ph = (j / C::SA) & 1u;
+                if (!mb_wait(smem_addr(&empty_a[sa]), ph ^ 1u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_EMPTY);
+                    *abort_flag = 1;
+                    break;
+                }
+                mb_expect_tx(smem_addr(&full_a[sa]), 2 * C::A_BYTES);
+                const unsigned char* src = src0 + (size_t)j * kGTileBytes;
+                bulk_load(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
+                bulk_load(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
+                          smem_addr(&full_a[sa]));
+                if (j == 0 && nt > 1 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+                    *abort_flag = 1;
+                    ++j;
+                    break;
+                }
+            }
+            for (int k = j > C::SA ? j - C::SA : 0; k < j; ++k) {
+                if (!mb_wait(smem_addr(&full_a[k % C::SA]), (k / C::SA) & 1u, nullptr)) atomicOr(a.err, KERR_TIMEOUT_DRAIN);
+            }
+        }
+    } else if (warp == C::NPW + 1) {
+        if (lane == 0 && nt > 0 && rank == 0) {
+            // ---------------- MMA issuer of the pair
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_eff >> 3) << 17) |
+                                   ((uint32_t)((2 * kMmaM) >> 4) << 24);
+            int issued = 0;
+            for (int j = 0; j < nt; ++j) {
+                const int sa = j % C::SA, sb = j % C::SB;
+                const uint32_t pa = (j / C::SA) & 1u, pb = (j / C::SB) & 1u;
+                if (!mb_wait(smem_addr(&full_a[sa]), pa, abort_flag) ||
+                    !mb_wait(smem_addr(&pfull_a[sa]), pa, abort_flag) ||
+                    !mb_wait(smem_addr(&full_b[sb]), pb, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ahi = smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES);
+                const uint32_t alo = smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES);
+                const uint32_t bhi = smem_addr(b_base + (size_t)(sb * 2) * C::B_BYTES);
+                const uint32_t blo = smem_addr(b_base + (size_t)(sb * 2 + 1) * C::B_BYTES);
+                const uint64_t dahi = umma_desc_sw128(ahi), dalo = umma_desc_sw128(alo);
+                const uint64_t dbhi = umma_desc_sw128(bhi), dblo = umma_desc_sw128(blo);
+#pragma unroll
+                for (int kk = 0; kk < kMmaK / 16; ++kk) {
+                    const uint64_t o = (uint64_t)(kk * 2);
+                    umma2_bf16(tmem, dahi + o, dbhi + o, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+                    umma2_bf16(tmem, dahi + o, dblo + o, idesc, 1u);
+                    umma2_bf16(tmem, dalo + o, dbhi + o, idesc, 1u);
+                }
+                umma2_commit(smem_addr(&empty_a[sa]));
+                umma2_commit(peer_addr(smem_addr(&empty_a[sa]), 1u));
+                umma2_commit(smem_addr(&empty_b[sb]));
+                umma2_commit(peer_addr(smem_addr(&empty_b[sb]), 1u));
+                ++issued;
+            }
+            if (*abort_flag) {
+                if (issued > 0) {  // the MMAs already issued read both CTAs' shared memory
+                    umma2_commit(smem_addr(drain_bar));
+                    if (!mb_wait(smem_addr(drain_bar), 0u, nullptr)) atomicOr(a.err, KERR_TIMEOUT_DRAIN);
+                }
+            } else {
+                umma2_commit(smem_addr(acc_bar));
+                umma2_commit(peer_addr(smem_addr(acc_bar), 1u));
+            }
+        } else if (lane == 0 && nt > 0) {
+            // ---------------- odd CTA: forward each landed G stage to the even CTA, in order
+            for (int j = 0; j < nt; ++j) {
+                const int sa = j % C::SA;
+                if (!mb_wait(smem_addr(&full_a[sa]), (j / C::SA) & 1u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+                    *abort_flag = 1;
+                    break;
+                }
+                mb_arrive_remote(peer_addr(smem_addr(&pfull_a[sa]), 0u));
+            }
+        }
+    } else {
+        // ---------------- X producers: row c of this CTA's half (column n0 + rank * hn + c),
+        // two threads per row, each converting one 32-wide half of the 64-wide K tile
+        const int p = tid;
+        const int c = p & (C::HN - 1), kh = p / C::HN;
+        pdl_wait();  // F is the previous step's output
+        if (tid == 0) pdl_trigger();
+        if (nt > 0) {
+            const int col = n0 + (int)rank * hn + c;
+            const int cell = col / a.Bst;
+            const int inst = col - cell * a.Bst;
+            const bool valid = c < hn && cell < a.n_space && inst < a.Bcap;
+            const float* Fc = a.F + (size_t)(valid ? cell : 0) * a.n_mom * a.Bst;
+            const float s1 = valid ? a.isig1[inst] : 0.f;
+            const float s2 = valid ? a.isig2[inst] : 0.f;
+            float f2r[kMmaK / 2];
+            int cur_cb = -1;
+            float x1_next = 0.f;
+            if (valid) {
+                const int b0 = t0 - (t0 / a.N1) * a.N1;
+                x1_next = __ldg(Fc + (size_t)(a.off1 + b0) * a.Bst + inst);
+            }
+            for (int j = 0; j < nt; ++j) {
+                const int t = t0 + j, cb = t / a.N1;
+                const int sb = j % C::SB;
+                const float x1 = (x1_next * s1) * s2;  // both scales are powers of two: exact
+                if (valid && j + 1 < nt) {
+                    const int tn = t + 1, bn = tn - (tn / a.N1) * a.N1;
+                    x1_next = __ldg(Fc + (size_t)(a.off1 + bn) * a.Bst + inst);
+                }
+                if (!mb_wait(smem_addr(&empty_b[sb]), ((j / C::SB) & 1u) ^ 1u, abort_flag)) {
+                    if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_EMPTY);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (cb != cur_cb) {
+                    const float* fb = Fc + (valid ? inst : 0);
+                    const int cbase = cb * kMmaK + kh * (kMmaK / 2);
+#pragma unroll
+                    for (int e = 0; e < kMmaK / 2; ++e) {
+                        const int cc = min(cbase + e, a.n2 - 1);
+                        f2r[e] = __ldg(fb + (size_t)(a.off2 + cc) * a.Bst);
+                    }
+#pragma unroll
+                    for (int e = 0; e < kMmaK / 2; ++e)
+                        if (!valid || cbase + e >= a.n2) f2r[e] = 0.f;
+                    cur_cb = cb;
+                }
+                unsigned char* rhi = b_base + (size_t)(sb * 2) * C::B_BYTES + (size_t)c * 128;
+                unsigned char* rlo = b_base + (size_t)(sb * 2 + 1) * C::B_BYTES + (size_t)c * 128;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t h[4], l[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float v0 = x1 * f2r[8 * q + 2 * e];
+                        const float v1 = x1 * f2r[8 * q + 2 * e + 1];
+                        const __nv_bfloat162 hh = __floats2bfloat162_rn(v0, v1);
+                        const float2 hf = __bfloat1622float2(hh);
+                        h[e] = *reinterpret_cast<const uint32_t*>(&hh);
+                        l[e] = pack_bf16x2(v0 - hf.x, v1 - hf.y);
+                    }
+                    const int phys = (((kh * 4 + q) ^ (c & 7)) << 4);
+                    *reinterpret_cast<uint4*>(rhi + phys) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(rlo + phys) = make_uint4(l[0], l[1], l[2], l[3]);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    if (rank == 0)
+                        mb_arrive(smem_addr(&full_b[sb]));
+                    else
+                        mb_arrive_remote(peer_addr(smem_addr(&full_b[sb]), 0u));
+                    if (j == 0) mb_arrive(smem_addr(x0_bar));
+                }
+            }
+        }
+        // epilogue: this CTA's TMEM holds its 128 G rows x the pair's n_eff columns
+        const int lg = warp & 3;
+        const int ncol = C::BN / (C::NPW / 4);
+        const int c0 = (warp >> 2) * ncol;
+        const int row = m0 + lg * 32 + lane;
+        bool ok = true;
+        if (nt > 0) {
+            ok = mb_wait(smem_addr(acc_bar), 0u, abort_flag);
+            if (!ok && !*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
+            tc_fence_after();
+        }
+        if (ok && !*abort_flag) {
+            float* dst = a.partial + (size_t)split * a.Bpad * a.M;
+            for (int cc = 0; cc < ncol; cc += 32) {
+                uint32_t r0[16], r1[16];
+                const bool ok0 = nt > 0 && c0 + cc < n_eff, ok1 = nt > 0 && c0 + cc + 16 < n_eff;
+                const uint32_t ta = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc);
+                if (ok0) tmem_ld16_issue(ta, r0);
+                if (ok1) tmem_ld16_issue(ta + 16, r1);
+                if (ok0 || ok1) tmem_ld_wait();
+                if (row < a.M) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k)
+                        dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = ok0 ? __uint_as_float(r0[k]) : 0.f;
+#pragma unroll
+                    for (int k = 0; k < 16; ++k)
+                        dst[(size_t)(n0 + c0 + cc + 16 + k) * a.M + row] = ok1 ? __uint_as_float(r1[k]) : 0.f;
+                }
+            }
+        }
+    }
+    // neither CTA leaves (or frees tensor memory) while the other may still touch its shared
+    // memory, barriers or tensor memory
+    __syncwarp();
+    tc_fence_before();
+    cluster_sync_all();
+    if (warp == C::NPW + 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::BN) : "memory");
+    }
+}
+
 }  // namespace
 
 int gain_gemm_smem_bytes(int bn) {
@@ -413,6 +749,22 @@ static cudaError_t launch_gemm_bn(const GemmArgs& a, cudaStream_t s) {
     using C = GemmCfg<BN>;
     const int grid = a.m_tiles * a.n_tiles * a.n_splits;
     return launch_pdl(gain_gemm_kernel<BN>, dim3(grid), dim3(C::THREADS), C::SMEM, s, a);
+}
+
+cudaError_t prepare_gain_gemm_pair(int* max_pairs) {
+    cudaError_t e = cudaFuncSetAttribute(gain_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         PairCfg::SMEM);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2);
+    cfg.blockDim = dim3(PairCfg::THREADS);
+    cfg.dynamicSmemBytes = PairCfg::SMEM;
+    return cudaOccupancyMaxActiveClusters(max_pairs, gain_gemm_pair_kernel, &cfg);
+}
+
+cudaError_t launch_gain_gemm_pair(const GemmArgs& a, cudaStream_t s) {
+    const int grid = a.m_tiles * a.n_tiles * a.n_splits;  // m_tiles is even: grid pairs up
+    return launch_pdl(gain_gemm_pair_kernel, dim3(grid), dim3(PairCfg::THREADS), (size_t)PairCfg::SMEM, s, a);
 }
 
 cudaError_t launch_gain_gemm(int bn, const GemmArgs& a, cudaStream_t s) {

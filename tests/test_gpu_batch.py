@@ -32,10 +32,13 @@ def _gain_only(w):
     return w
 
 
-@pytest.mark.parametrize("p,u,batch", [(8, 4, 8), (16, 8, 100), (8, 8, 300), (12, 6, 40)])
+@pytest.mark.parametrize("p,u,batch", [(8, 4, 8), (16, 8, 100), (8, 8, 300), (12, 6, 40), (10, 8, 300),
+                                       (16, 8, 260)])
 def test_batched_gain_term_matches_fp64(cuda, p, u, batch):
     """One step with only the gain term: f1 - f0 = gain; covers BN = 64, 128, 256, several N
-    tiles, n2 padded to 64 (p*u = 32, 72) and more than one M tile."""
+    tiles, n2 padded to 64 (p*u = 32, 72, 80) and more than one M tile. (10, 8, 300) and
+    (16, 8, 260) have two m tiles and 256-column tiles, so they run on SM pairs: rows past M in
+    the second m tile (M = 160), and a second column tile with 44 or 4 running columns."""
     w = _gain_only(synth.batched_two_species(p, 1e-2, 1e2, u, batch, seed=p * 100 + u))
     for g in w.binm.gains:  # make the gain dominate the step
         g.G = np.asarray(g.G) * 50.0
@@ -202,12 +205,14 @@ def test_whole_batch_state_io(cuda):
     m.close()
 
 
-def test_gemm_columns_follow_the_last_running_slot(cuda):
-    """The gain GEMM computes only up to the last running slot (rounded to 16 columns): a slot
-    alone at index 3 or 200 of 256, and the same slot with every slot running, give the same
-    f; finished slots keep their state while a higher slot runs on."""
+@pytest.mark.parametrize("p,u", [(8, 4), (10, 8)])
+def test_gemm_columns_follow_the_last_running_slot(cuda, p, u):
+    """The gain GEMM computes only up to the last running slot (rounded to 16 columns, 32 on SM
+    pairs): a slot alone at index 3 or 200 of 256, and the same slot with every slot running,
+    give the same f; finished slots keep their state while a higher slot runs on. (10, 8) has
+    two m tiles and runs on SM pairs."""
     B = 256
-    w = synth.batched_two_species(8, 1e-2, 1e2, 4, B, seed=12)
+    w = synth.batched_two_species(p, 1e-2, 1e2, u, B, seed=12)
     full = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
     for i in range(B):
         full.admit(i, w.f0[i], w.dt[i], 30)
@@ -221,6 +226,35 @@ def test_gemm_columns_follow_the_last_running_slot(cuda):
         assert one.info(0)["steps_done"] == 5
         one.close()
     full.close()
+
+
+def test_sm_pair_gemm_agrees_with_one_sm_gemm(cuda, monkeypatch):
+    """The SM-pair gain GEMM (two m tiles per MMA) and the one-SM kernel (DTB_GEMM=classic) form
+    the same products in the same K order: 8 steps of every operator on 300 slots agree to
+    1e-6 (relative L-infinity per slot), and both stay within the FP64 oracle's tolerance."""
+    B = 300
+    w = synth.batched_two_species(10, 1e-2, 1e2, 8, B, seed=21)
+    out = {}
+    for kind in ("pair", "classic"):
+        if kind == "classic":
+            monkeypatch.setenv("DTB_GEMM", "classic")
+        else:
+            monkeypatch.delenv("DTB_GEMM", raising=False)
+        m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+        for i in range(B):
+            m.admit(i, w.f0[i], w.dt[i], 8)
+        m.run(8)
+        out[kind] = m.get_f_all()
+        m.close()
+    a, b = out["pair"], out["classic"]
+    for i in range(B):
+        assert rel_linf(a[i], b[i]) <= 1e-6, i
+    ops = oracle.blocked_from_workload(w)
+    for i in (0, 257, B - 1):
+        f = w.f0[i].copy()
+        for _ in range(8):
+            f, _, _ = ops.step(f, w.dt[i], 0)
+        assert rel_linf(a[i], f) <= TOL_RUN, i
 
 
 def _multicell(n_space, seed, domain=None):
