@@ -450,6 +450,9 @@ def run_batched(args):
     torch.cuda.synchronize()
     ms_prof = e4.elapsed_time(e5)
     st = m.gemm_stats()
+    plans = []
+    while (pl := m.gemm_plan(len(plans))) is not None:
+        plans.append(pl)
     m.set_profiling(False)
     # ---- e2e: the whole batch state from pinned host memory in and out every step
     Fh = torch.empty((B, n), dtype=torch.float64).pin_memory().numpy()
@@ -490,8 +493,7 @@ def run_batched(args):
     achieved = st["flops_per_step"] / (st["avg_ms"] / 1e3) / 1e12 if st["avg_ms"] > 0 else None
     traffic = _profile_traffic(f"gain_gemm_config{args.config}.md")
     # 256-column tiles over an even number of 128-row m tiles run on SM pairs (cta_group::2)
-    pairs = B * w.ps.n_space >= 192 and (sum(w.ps.species_sizes) + 127) // 128 % 2 == 0
-    GEMM_LABEL = ("gain_gemm_pair (tcgen05.mma.cta_group::2, BF16 hi+lo x3)" if pairs
+    GEMM_LABEL = ("gain_gemm_pair (tcgen05.mma.cta_group::2, BF16 hi+lo x3)" if all(p["pair"] for p in plans)
                   else "gain_gemm (tcgen05, BF16 hi+lo x3)")
     # the GEMM's bound: the slower of its tensor time and its operator-streaming time
     hbm = float(pj.get("hbm_gbs", 6650.0))
@@ -506,7 +508,7 @@ def run_batched(args):
                 "peak": peak, "peak_kind": "measured burst" if pj else "fallback", "unit": "TFLOP/s",
                 "frac": achieved / peak if achieved else None,
                 "frac_of_sustained": achieved / peak_s if achieved else None}
-    roof.update({"traffic": traffic, "algorithmic_flops_per_step": st["flops_per_step"],
+    roof.update({"gemm_plans": [dict(p, tuned_us=round(p["tuned_us"], 2)) for p in plans], "traffic": traffic, "algorithmic_flops_per_step": st["flops_per_step"],
                  "operator_bytes_per_step": st["bytes_per_step"], "avg_gemm_ms_per_step": st["avg_ms"],
                  "profiled_ms_per_step": ms_prof / K})
     line = {"metric": METRIC, "value": value, "unit": "instance-steps/s", "n_gpus": world, "steps": K, "warmup": W,

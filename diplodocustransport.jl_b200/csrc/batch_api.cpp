@@ -3,12 +3,18 @@
 //
 // Per batched step: for every gain group (gain blocks sharing an input pair) one tcgen05 GEMM
 // of the stacked G rows (BF16 hi+lo, per-row power-of-two scale) against the batch of
-// vec(f1 x f2), then one epilogue kernel over all (row, instance) pairs. Slots step while the
+// vec(f1 x f2), then one epilogue kernel over all (row, instance) pairs. The GEMM's plan
+// (column tile, one SM or an SM pair per tile, K splits) is autotuned at commit per shape. Slots step while the
 // device step counter is below their stop step, so requests of different lengths share one
 // captured graph; a finished slot keeps its state until it is read and re-admitted.
 #include <cuda.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "batch_internal.h"
@@ -25,6 +31,7 @@ struct MixedGroup {
     float* partial = nullptr;
     int bn = 256, n_tiles = 1, m_tiles = 1, n_splits = 1, tiles_per_split = 1, Bpad = 256, splits_per_cb = 0;
     bool pair = false;  // the CTA-pair kernel (cta_group::2) runs this group
+    double tuned_us = 0;  // autotuner: measured GEMM time of the chosen plan (0: not timed here)
     double flops = 0;  // 3 MMAs x 2 x M x K x Bcap
     double bytes = 0;  // hi + lo bytes of G
 };
@@ -81,6 +88,223 @@ double ord_dec_host(unsigned long long e) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- gain GEMM plans
+namespace {
+
+// One way to run a group's gain GEMM: the kernel (one SM per tile, or an SM pair sharing a
+// 256 x 256 MMA), the column tile width and the requested number of K splits.
+struct GemmPlan {
+    int pair = 0;
+    int bn = 256;
+    int splits = 1;
+    double us = 0;  // measured time of one GEMM with this plan (0: not measured)
+};
+
+// Plans chosen so far in this process, by shape; a cache file (dtb_set_tune_cache) seeds it and
+// records what the autotuner measures, one line per shape:
+//   sm<SMs>:M<rows>:N1<n1>:n2<n2>:cols<columns>:cells<cells> <pair> <bn> <splits> <us>
+std::mutex g_plan_mu;
+std::map<std::string, GemmPlan> g_plans;
+std::string g_plan_file;
+
+std::string plan_key(const dtb_ctx* c, const MixedGroup& G, int Bcols) {
+    char k[160];
+    std::snprintf(k, sizeof(k), "sm%d:M%d:N1%d:n2%d:cols%d:cells%d", c->num_sms, G.M, G.N1, G.n2, Bcols,
+                  (int)c->n_space);
+    return k;
+}
+
+bool plan_valid(const MixedGroup& G, const GemmPlan& p, int max_pairs) {
+    if (p.bn != 64 && p.bn != 128 && p.bn != 256) return false;
+    if (p.splits < 1) return false;
+    if (p.pair && (p.bn != 256 || G.m_tiles % 2 != 0 || max_pairs <= 0)) return false;
+    return true;
+}
+
+// Tile counts and K splits of a plan. The splits are aligned to the 64-wide input-2 blocks
+// when that keeps nearly every requested split: a split then never reloads its f2 block in
+// mid-stream.
+void apply_plan(MixedGroup& G, const GemmPlan& p, int Bcols) {
+    G.pair = p.pair != 0;
+    G.bn = p.bn;
+    G.n_tiles = (Bcols + p.bn - 1) / p.bn;
+    G.Bpad = G.n_tiles * p.bn;
+    const int T = G.n_cb * G.N1;
+    const int S = std::max(1, std::min(p.splits, T));
+    G.tiles_per_split = (T + S - 1) / S;
+    G.n_splits = (T + G.tiles_per_split - 1) / G.tiles_per_split;
+    const int k_cb = S / G.n_cb;
+    G.splits_per_cb = 0;
+    if (k_cb >= 1 && k_cb <= G.N1 && (double)(k_cb * G.n_cb) >= 0.95 * S) {
+        G.splits_per_cb = k_cb;
+        G.n_splits = k_cb * G.n_cb;
+    }
+}
+
+// Splits that fill the device once: one CTA per SM, or one pair per co-resident cluster.
+int fill_splits(const dtb_ctx* c, const MixedGroup& G, int pair, int bn, int Bcols, int max_pairs) {
+    const int n_tiles = (Bcols + bn - 1) / bn;
+    const double units = pair ? (double)(G.m_tiles / 2 * n_tiles) : (double)(G.m_tiles * n_tiles);
+    return std::max(1, (int)std::lround((pair ? max_pairs : c->num_sms) / units));
+}
+
+// Without timing: the widest tile the columns fill, on SM pairs when the rows pair up.
+GemmPlan heuristic_plan(const dtb_ctx* c, const MixedGroup& G, int Bcols, int max_pairs) {
+    GemmPlan p;
+    p.bn = Bcols >= 192 ? 256 : (Bcols > 64 ? 128 : 64);
+    p.pair = (p.bn == 256 && G.m_tiles % 2 == 0 && max_pairs > 0) ? 1 : 0;
+    p.splits = fill_splits(c, G, p.pair, p.bn, Bcols, max_pairs);
+    return p;
+}
+
+}  // namespace
+
+GemmArgs gemm_args(const dtb_ctx* c, const MixedGroup& G, const float* Fin) {
+    const MixedState* m = c->mixed;
+    GemmArgs a;
+    a.gt = G.gt;
+    a.M = G.M;
+    a.N1 = G.N1;
+    a.n2 = G.n2;
+    a.n_cb = G.n_cb;
+    a.off1 = (int)c->off[G.in1];
+    a.off2 = (int)c->off[G.in2];
+    a.tiles_per_split = G.tiles_per_split;
+    a.n_splits = G.n_splits;
+    a.splits_per_cb = G.splits_per_cb;
+    a.m_tiles = G.m_tiles;
+    a.n_tiles = G.n_tiles;
+    a.Bcap = m->Buser;
+    a.Bst = m->Bcap;
+    a.n_space = c->n_space;
+    a.n_mom = (int)c->n_mom;
+    a.Bpad = G.Bpad;
+    a.F = Fin;
+    a.isig1 = m->isig + (size_t)G.in1 * m->Bcap;
+    a.isig2 = m->isig + (size_t)G.in2 * m->Bcap;
+    a.partial = G.partial;
+    a.err = c->err;
+    a.active_hi = m->active_hi;
+    return a;
+}
+
+cudaError_t launch_group_gemm(const dtb_ctx* c, const MixedGroup& G, const float* Fin) {
+    const GemmArgs a = gemm_args(c, G, Fin);
+    return G.pair ? launch_gain_gemm_pair(a, c->stream) : launch_gain_gemm(G.bn, a, c->stream);
+}
+
+// Times each candidate plan of one group on the device (every column running, the state at its
+// committed zeros: tensor-core time does not depend on the values) and returns the fastest.
+int tune_group(dtb_ctx* c, MixedGroup& G, int Bcols, int max_pairs, GemmPlan* best) {
+    MixedState* m = c->mixed;
+    std::vector<GemmPlan> cands;
+    for (int bn : {64, 128, 256}) {
+        if (bn > 64 && bn / 2 >= Bcols) continue;  // half the tile or more would be padding
+        GemmPlan p;
+        p.bn = bn;
+        p.splits = fill_splits(c, G, 0, bn, Bcols, max_pairs);
+        cands.push_back(p);
+        if (bn == 256 && G.m_tiles % 2 == 0 && max_pairs > 0) {
+            p.pair = 1;
+            p.splits = fill_splits(c, G, 1, bn, Bcols, max_pairs);
+            cands.push_back(p);
+        }
+    }
+    *best = heuristic_plan(c, G, Bcols, max_pairs);
+    if (cands.size() < 2) return DTB_OK;
+    size_t scratch = 0;
+    for (const GemmPlan& p : cands) {
+        apply_plan(G, p, Bcols);
+        scratch = std::max(scratch, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M);
+    }
+    float* part = nullptr;
+    DTB_CUDA(cudaMalloc(&part, scratch));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DTB_CUDA(cudaEventCreate(&e0));
+    DTB_CUDA(cudaEventCreate(&e1));
+    const int all = Bcols;
+    DTB_CUDA(cudaMemcpyAsync(m->active_hi, &all, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    double best_ms = 1e30;
+    int rc = DTB_OK;
+    for (const GemmPlan& p : cands) {
+        apply_plan(G, p, Bcols);
+        G.partial = part;
+        constexpr int kWarm = 2, kRep = 5;
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < kWarm && e == cudaSuccess; ++k) e = launch_group_gemm(c, G, m->F[0]);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+        for (int k = 0; k < kRep && e == cudaSuccess; ++k) e = launch_group_gemm(c, G, m->F[0]);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {  // a plan this device cannot launch is skipped
+            cudaGetLastError();
+            continue;
+        }
+        const double per = ms / kRep;
+        if (per < best_ms) {
+            best_ms = per;
+            *best = p;
+            best->us = per * 1e3;
+        }
+    }
+    const int zero = 0;
+    cudaError_t e = cudaMemcpyAsync(m->active_hi, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    int kerr = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&kerr, c->err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(part);
+    G.partial = nullptr;
+    DTB_CUDA(e);
+    if (kerr != 0) {
+        set_error("gain GEMM autotuning: a bounded device wait gave up (code " + std::to_string(kerr) + ")");
+        rc = DTB_ETIMEOUT;
+    }
+    return rc;
+}
+
+// Plan of every gain group: a plan already chosen for the shape in this process (or read from
+// the cache file), else the autotuner's (or, with DTB_FLAG_NO_AUTOTUNE, the heuristic's).
+int plan_gemms(dtb_ctx* c, int Bcols, int max_pairs) {
+    MixedState* m = c->mixed;
+    const bool tune = (c->opts.flags & DTB_FLAG_NO_AUTOTUNE) == 0;
+    for (auto& G : m->groups) {
+        GemmPlan p;
+        bool have = false;
+        const std::string key = plan_key(c, G, Bcols);
+        if (tune) {
+            std::lock_guard<std::mutex> lk(g_plan_mu);
+            auto it = g_plans.find(key);
+            if (it != g_plans.end() && plan_valid(G, it->second, max_pairs)) {
+                p = it->second;
+                have = true;
+            }
+        }
+        if (!have) {
+            if (tune) {
+                DTB_TRY(tune_group(c, G, Bcols, max_pairs, &p));
+                std::lock_guard<std::mutex> lk(g_plan_mu);
+                g_plans[key] = p;
+                if (!g_plan_file.empty()) {
+                    if (FILE* f = std::fopen(g_plan_file.c_str(), "a")) {
+                        std::fprintf(f, "%s %d %d %d %.3f\n", key.c_str(), p.pair, p.bn, p.splits, p.us);
+                        std::fclose(f);
+                    }
+                }
+            } else {
+                p = heuristic_plan(c, G, Bcols, max_pairs);
+            }
+        }
+        apply_plan(G, p, Bcols);
+        G.tuned_us = p.us;
+        DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
+    }
+    return DTB_OK;
+}
+
 // Builds the device layouts of a DTB_MIXED context.
 int commit_mixed(dtb_ctx* c) {
     DTB_CHECK(c->opts.batch >= 1, DTB_EINVAL, "batched context needs opts.batch >= 1");
@@ -135,7 +359,6 @@ int commit_mixed(dtb_ctx* c) {
     }
     DTB_CHECK(m->groups.size() <= 16, DTB_EINVAL, "at most 16 input pairs in a batched context");
     c->has_bin = !c->gains.empty() || !c->losses.empty();
-    const int bn = Bcols >= 192 ? 256 : (Bcols > 64 ? 128 : 64);
     for (auto& kv : c->gains) {
         GainStage& g = kv.second;
         MixedGroup& G = m->groups[(size_t)gidx[{g.in1, g.in2}]];
@@ -180,35 +403,15 @@ int commit_mixed(dtb_ctx* c) {
         g.host.clear();
         g.host.shrink_to_fit();
     }
-    DTB_CUDA(prepare_gain_gemm(bn));
+    for (int b : {64, 128, 256}) DTB_CUDA(prepare_gain_gemm(b));
     DTB_CUDA(prepare_mixed_rows());
-    // 256-column tiles over an even number of m tiles run on SM pairs (DTB_GEMM=classic keeps
-    // the one-SM kernel)
-    const char* gk = std::getenv("DTB_GEMM");
     int max_pairs = 0;
-    if (bn == 256 && !(gk && std::string(gk) == "classic")) DTB_CUDA(prepare_gain_gemm_pair(&max_pairs));
+    if (prepare_gain_gemm_pair(&max_pairs) != cudaSuccess) {  // no cluster pairs: one-SM plans only
+        cudaGetLastError();
+        max_pairs = 0;
+    }
     for (auto& G : m->groups) {
-        G.bn = bn;
-        G.n_tiles = (Bcols + bn - 1) / bn;
-        G.Bpad = G.n_tiles * bn;
         G.m_tiles = (G.M + kMmaM - 1) / kMmaM;
-        G.pair = max_pairs > 0 && G.m_tiles % 2 == 0;
-        const int T = G.n_cb * G.N1;
-        // K splits: one CTA per SM, or one pair per co-resident cluster of two
-        int S = G.pair ? std::max(1, (int)std::lround((double)max_pairs / (G.m_tiles / 2 * G.n_tiles)))
-                       : std::max(1, (int)std::lround((double)c->num_sms / (G.m_tiles * G.n_tiles)));
-        S = std::min(S, T);
-        G.tiles_per_split = (T + S - 1) / S;
-        G.n_splits = (T + G.tiles_per_split - 1) / G.tiles_per_split;
-        // splits aligned to the 64-wide input-2 blocks when that keeps nearly every SM busy: a
-        // split then never reloads its f2 block in mid-stream
-        const int k_cb = S / G.n_cb;
-        G.splits_per_cb = 0;
-        if (k_cb >= 1 && k_cb <= G.N1 && (double)(k_cb * G.n_cb) >= 0.95 * S) {
-            G.splits_per_cb = k_cb;
-            G.n_splits = k_cb * G.n_cb;
-        }
-        DTB_TRY(c->alloc(&G.partial, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M));
         G.flops = 3.0 * 2.0 * G.M * (double)G.N1 * G.n2 * m->Buser * nsp;
         G.bytes = 4.0 * G.M * (double)G.N1 * G.n2;
     }
@@ -414,6 +617,8 @@ int commit_mixed(dtb_ctx* c) {
     DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));
     m->h_stop.assign((size_t)B, 0);
     m->h_start.assign((size_t)B, 0);
+    // ---------------- GEMM plan per group: tile width, kernel and K splits (autotuned)
+    DTB_TRY(plan_gemms(c, Bcols, max_pairs));
     ops.n_mom = n_mom;
     ops.n_state = n_st;
     ops.n_space = nsp;
@@ -578,36 +783,7 @@ int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
         e1 = m->ev[k + 1];
         DTB_CUDA(cudaEventRecord(e0, c->stream));
     }
-    for (auto& G : m->groups) {
-        GemmArgs a;
-        a.gt = G.gt;
-        a.M = G.M;
-        a.N1 = G.N1;
-        a.n2 = G.n2;
-        a.n_cb = G.n_cb;
-        a.off1 = (int)c->off[G.in1];
-        a.off2 = (int)c->off[G.in2];
-        a.tiles_per_split = G.tiles_per_split;
-        a.n_splits = G.n_splits;
-        a.splits_per_cb = G.splits_per_cb;
-        a.m_tiles = G.m_tiles;
-        a.n_tiles = G.n_tiles;
-        a.Bcap = m->Buser;
-        a.Bst = m->Bcap;
-        a.n_space = c->n_space;
-        a.n_mom = (int)c->n_mom;
-        a.Bpad = G.Bpad;
-        a.F = Fin;
-        a.isig1 = m->isig + (size_t)G.in1 * m->Bcap;
-        a.isig2 = m->isig + (size_t)G.in2 * m->Bcap;
-        a.partial = G.partial;
-        a.err = c->err;
-        a.active_hi = m->active_hi;
-        if (G.pair)
-            DTB_CUDA(launch_gain_gemm_pair(a, c->stream));
-        else
-            DTB_CUDA(launch_gain_gemm(G.bn, a, c->stream));
-    }
+    for (auto& G : m->groups) DTB_CUDA(launch_group_gemm(c, G, Fin));
     if (profile) {
         DTB_CUDA(cudaEventRecord(e1, c->stream));
         m->prof_n++;
@@ -954,6 +1130,34 @@ int32_t dtb_batch_set_profiling(dtb_ctx* c, int32_t on) {
     m->prof_ms = 0;
     m->prof_n = 0;
     m->prof_pending = 0;
+    return DTB_OK;
+}
+
+int32_t dtb_set_tune_cache(const char* path) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plans.clear();
+    g_plan_file = path ? path : "";
+    if (!path) return DTB_OK;
+    if (FILE* f = std::fopen(path, "r")) {
+        char key[160];
+        GemmPlan p;
+        while (std::fscanf(f, "%159s %d %d %d %lf", key, &p.pair, &p.bn, &p.splits, &p.us) == 5) g_plans[key] = p;
+        std::fclose(f);
+    }
+    return DTB_OK;
+}
+
+int32_t dtb_batch_gemm_plan(dtb_ctx* c, int32_t group, int32_t* pair, int32_t* bn, int32_t* n_splits,
+                            double* tuned_us) {
+    DTB_TRY(mixed_ready(c));
+    MixedState* m = c->mixed;
+    DTB_CHECK(group >= 0, DTB_EINVAL, "negative group index");
+    if (group >= (int32_t)m->groups.size()) return DTB_ENOTFOUND;
+    const MixedGroup& G = m->groups[(size_t)group];
+    if (pair) *pair = G.pair ? 1 : 0;
+    if (bn) *bn = G.bn;
+    if (n_splits) *n_splits = G.n_splits;
+    if (tuned_us) *tuned_us = G.tuned_us;
     return DTB_OK;
 }
 

@@ -16,6 +16,7 @@ DTB_OK, DTB_EINVAL, DTB_ENOMEM, DTB_ECUDA, DTB_ETIMEOUT, DTB_ESTATE, DTB_ENODEV,
 DTB_F64, DTB_F32, DTB_MIXED = 0, 1, 2
 DTB_DTYPE_F64, DTB_DTYPE_F32 = 0, 1
 DTB_FLAG_SYMPLECTIC = 1
+DTB_FLAG_NO_AUTOTUNE = 2
 DTB_FLUX_X, DTB_FLUX_P = 0, 1
 MAX_SPECIES = 16
 
@@ -124,6 +125,8 @@ SIGNATURES = {
     "dtb_batch_capacity": (_i32, [_P, _i32p, _ip]),
     "dtb_batch_set_profiling": (_i32, [_P, _i32]),
     "dtb_batch_gemm_stats": (_i32, [_P, _dp, _dp, _dp, _i32p]),
+    "dtb_set_tune_cache": (_i32, [ctypes.c_char_p]),
+    "dtb_batch_gemm_plan": (_i32, [_P, _i32, _i32p, _i32p, _i32p, _dp]),
     "dtb_gain_contract_noalloc": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
 }
 

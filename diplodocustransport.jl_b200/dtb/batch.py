@@ -27,7 +27,7 @@ from .structs import BinaryMatrices, EmissionMatrices, FluxMatrices, PhaseSpace
 class BatchedEuler:
     def __init__(self, PhaseSpace: PhaseSpace, Injection, BinM: BinaryMatrices, EmiM: EmissionMatrices,
                  FluxM: FluxMatrices, capacity: int, *, device: int = 0, stream: Optional[int] = None,
-                 graph_steps: int = 16):
+                 graph_steps: int = 16, autotune: bool = True):
         self.L = _lib.load()
         self.PhaseSpace = PhaseSpace
         self.capacity = int(capacity)
@@ -40,7 +40,8 @@ class BatchedEuler:
         for i, s in enumerate(sizes):
             dims.species_size[i] = s
         opts = _lib.Opts(precision=_lib.DTB_MIXED, device=device, stream=stream, index_base=0,
-                         graph_steps=graph_steps, dt0=self.dt0, batch=self.capacity, flags=0)
+                         graph_steps=graph_steps, dt0=self.dt0, batch=self.capacity,
+                         flags=0 if autotune else _lib.DTB_FLAG_NO_AUTOTUNE)
         ctx = ctypes.c_void_p()
         check(self.L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)))
         self.ctx = ctx
@@ -139,6 +140,18 @@ class BatchedEuler:
     def set_profiling(self, on: bool) -> None:
         check(self.L.dtb_batch_set_profiling(self.ctx, 1 if on else 0))
 
+    def gemm_plan(self, group: int = 0) -> Optional[dict]:
+        """The gain-GEMM plan of one gain group (None past the last group): SM pairs or not,
+        column tile width, K splits, measured microseconds of one GEMM (0 if not timed)."""
+        pair, bn, ns = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        us = ctypes.c_double()
+        rc = self.L.dtb_batch_gemm_plan(self.ctx, group, ctypes.byref(pair), ctypes.byref(bn), ctypes.byref(ns),
+                                        ctypes.byref(us))
+        if rc == _lib.DTB_ENOTFOUND:
+            return None
+        check(rc)
+        return {"pair": bool(pair.value), "bn": bn.value, "n_splits": ns.value, "tuned_us": us.value}
+
     def gemm_stats(self) -> dict:
         ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         lps = ctypes.c_int32()
@@ -162,3 +175,9 @@ class BatchedEuler:
             self.close()
         except Exception:
             pass
+
+
+def set_tune_cache(path: Optional[str]) -> None:
+    """Seeds the process-wide gain-GEMM plans from a cache file and records new measurements in
+    it; None forgets the plans chosen so far."""
+    check(_lib.load().dtb_set_tune_cache(None if path is None else str(path).encode()))

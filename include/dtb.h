@@ -41,6 +41,8 @@ extern "C" {
 /* dtb_opts.flags */
 #define DTB_FLAG_SYMPLECTIC 1  /* ForwardSymplecticEulerStruct (SteppingStructs.jl:104-229):
                                   momentum update, then space update (SteppingMethods.jl:120-243) */
+#define DTB_FLAG_NO_AUTOTUNE 2 /* batched contexts: plan the gain GEMM by a fixed rule instead of
+                                  timing the candidate plans on the device at commit */
 
 /* flux parts (FluxMatricesStruct.X_Flux / P_Flux, StructsAndDictionaries.jl:346-347) */
 #define DTB_FLUX_X 0
@@ -271,6 +273,25 @@ int32_t dtb_batch_set_profiling(dtb_ctx* ctx, int32_t on);
  * and operator bytes per step, and the kernel launches per batched step. */
 int32_t dtb_batch_gemm_stats(dtb_ctx* ctx, double* avg_ms, double* flops_per_step, double* bytes_per_step,
                              int32_t* launches_per_step);
+
+/* Gain-GEMM autotuning. At commit a batched context times, for each gain group (the gain
+ * blocks of one input pair), the candidate plans on the device with CUDA events: the column
+ * tile width (64, 128 or 256 instances), one SM per tile or an SM pair sharing 256 x 256 MMAs
+ * (cta_group::2, when the group's 128-row tiles pair up) and the K splits that fill the device,
+ * and keeps the fastest. A plan is chosen once per shape and process, so contexts of one shape
+ * run the same plan (and round alike). dtb_set_tune_cache names a text file that seeds the
+ * plans and records every measured one, one line per shape:
+ *   sm<SMs>:M<rows>:N1<n1>:n2<n2>:cols<columns>:cells<cells> <pair 0|1> <bn> <splits> <us>
+ * NULL forgets the plans chosen so far and stops recording. Process-wide; replaces the
+ * per-stage tile choices of a hand-tuned build (no reference counterpart: the reference's
+ * mul! calls, SteppingMethods.jl:372-373, leave this to MKL / cuBLAS). */
+int32_t dtb_set_tune_cache(const char* path);
+
+/* The plan a committed batched context runs for gain group `group` (DTB_ENOTFOUND past the
+ * last group): SM pairs or not, column tile width, K splits, and the measured time of one
+ * GEMM with it in microseconds (0 when the plan came from the cache or the fixed rule). */
+int32_t dtb_batch_gemm_plan(dtb_ctx* ctx, int32_t group, int32_t* pair, int32_t* bn, int32_t* n_splits,
+                            double* tuned_us);
 
 /* ---- serving: continuous batching of solve requests ----
  * A server owns a host thread that admits queued requests into free slots of their grid's

@@ -9,7 +9,7 @@ import scipy.sparse as sp
 
 import oracle
 from dtb import synth
-from dtb.batch import BatchedEuler
+from dtb.batch import BatchedEuler, set_tune_cache
 from dtb.structs import BinaryMatrices, EmissionMatrices, LossBlock
 
 pytestmark = pytest.mark.gpu
@@ -228,25 +228,38 @@ def test_gemm_columns_follow_the_last_running_slot(cuda, p, u):
     full.close()
 
 
-def test_sm_pair_gemm_agrees_with_one_sm_gemm(cuda, monkeypatch):
-    """The SM-pair gain GEMM (two m tiles per MMA) and the one-SM kernel (DTB_GEMM=classic) form
-    the same products in the same K order: 8 steps of every operator on 300 slots agree to
-    1e-6 (relative L-infinity per slot), and both stay within the FP64 oracle's tolerance."""
+def _plan_key(w, batch):
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n1, n2 = w.ps.species_sizes[0], w.ps.species_sizes[1]
+    cols = w.ps.n_space * ((batch + 3) // 4 * 4)
+    return f"sm{sms}:M{sum(w.ps.species_sizes)}:N1{n1}:n2{n2}:cols{cols}:cells{w.ps.n_space}"
+
+
+def test_sm_pair_gemm_agrees_with_one_sm_gemm(cuda, tmp_path):
+    """The SM-pair gain GEMM (two m tiles per MMA) and the one-SM kernel, each forced through a
+    plan cache file, form the same products in the same K order: 8 steps of every operator on
+    300 slots agree to 1e-6 (relative L-infinity per slot), and both stay within the FP64
+    oracle's tolerance."""
     B = 300
     w = synth.batched_two_species(10, 1e-2, 1e2, 8, B, seed=21)
+    cache = tmp_path / "plans.txt"
     out = {}
-    for kind in ("pair", "classic"):
-        if kind == "classic":
-            monkeypatch.setenv("DTB_GEMM", "classic")
-        else:
-            monkeypatch.delenv("DTB_GEMM", raising=False)
-        m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
-        for i in range(B):
-            m.admit(i, w.f0[i], w.dt[i], 8)
-        m.run(8)
-        out[kind] = m.get_f_all()
-        m.close()
-    a, b = out["pair"], out["classic"]
+    try:
+        for pair in (1, 0):
+            cache.write_text(f"{_plan_key(w, B)} {pair} 256 37 0\n")
+            set_tune_cache(str(cache))
+            m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+            plan = m.gemm_plan(0)
+            assert plan["pair"] == bool(pair) and plan["bn"] == 256 and plan["tuned_us"] == 0.0
+            for i in range(B):
+                m.admit(i, w.f0[i], w.dt[i], 8)
+            m.run(8)
+            out[pair] = m.get_f_all()
+            m.close()
+    finally:
+        set_tune_cache(None)
+    a, b = out[1], out[0]
     for i in range(B):
         assert rel_linf(a[i], b[i]) <= 1e-6, i
     ops = oracle.blocked_from_workload(w)
@@ -255,6 +268,40 @@ def test_sm_pair_gemm_agrees_with_one_sm_gemm(cuda, monkeypatch):
         for _ in range(8):
             f, _, _ = ops.step(f, w.dt[i], 0)
         assert rel_linf(a[i], f) <= TOL_RUN, i
+
+
+def test_autotuned_plan_is_measured_shared_and_recorded(cuda, tmp_path):
+    """The autotuner times the candidate plans of a new shape once (the chosen plan carries its
+    measured time), a second context of the same shape reuses it and steps bit-identically, the
+    cache file gets one line for the shape, and DTB_FLAG_NO_AUTOTUNE takes the fixed rule."""
+    B = 260
+    w = synth.batched_two_species(16, 1e-2, 1e2, 8, B, seed=22)
+    cache = tmp_path / "plans.txt"
+    set_tune_cache(str(cache))
+    try:
+        a = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+        pa = a.gemm_plan(0)
+        assert a.gemm_plan(1) is None
+        assert pa["tuned_us"] > 0 and pa["bn"] in (64, 128, 256) and pa["n_splits"] >= 1
+        b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+        assert b.gemm_plan(0) == pa
+        lines = [ln for ln in cache.read_text().splitlines() if ln.strip()]
+        assert len(lines) == 1 and lines[0].startswith(_plan_key(w, B) + " ")
+        fields = lines[0].split()
+        assert (int(fields[1]) == 1) == pa["pair"] and int(fields[2]) == pa["bn"]
+        for m in (a, b):
+            for i in range(B):
+                m.admit(i, w.f0[i], w.dt[i], 6)
+            m.run(6)
+        np.testing.assert_array_equal(a.get_f_all(), b.get_f_all())
+        a.close()
+        b.close()
+        c = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B, autotune=False)
+        pc = c.gemm_plan(0)
+        assert pc["tuned_us"] == 0.0 and pc["bn"] == 256 and pc["pair"]  # M = 256: two m tiles
+        c.close()
+    finally:
+        set_tune_cache(None)
 
 
 def _multicell(n_space, seed, domain=None):
