@@ -911,6 +911,7 @@ constexpr int kRowsThreads = 512;
 constexpr int kKGroups = kRowsThreads / 64;  // K-slices of each product chunk
 static_assert(2 * kKGroups * kRT * (kIT + 1) <= kRowStages * kStageFloats, "partial tiles fit the ring");
 constexpr int kEllFast = 8;  // ELL widths up to this take the hoisted-load flux path
+constexpr int kGatherChunk = 18;  // split partials in flight per instance in the gain gather
 
 __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
                                                                   const float* __restrict__ Cc,
@@ -980,11 +981,15 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         }
     }
 
-    // everything above is static or written by the host; the state and the split partials below
-    // are outputs of the previous step's epilogue and this step's gain GEMM
-    pdl_wait();
-    if (tid == 0) pdl_trigger();
+    // Everything up to the gain gather reads only static operands and the state F, C of this
+    // step, which the previous step's epilogue wrote before this step's GEMM passed its own wait
+    // (and so before this grid could launch). The products and the update's loads therefore run
+    // before this grid waits for the GEMM, on SMs as the GEMM's blocks leave them; only the
+    // gather of the GEMM's split partials follows the wait.
     __syncthreads();  // the job table is visible
+    // the next step's GEMM may launch now: it waits for this grid's completion before it reads
+    // the new state, so only its set-up (barriers, tensor memory, its first G tile) overlaps
+    if (tid == 0) pdl_trigger();
     // a chunk into ring stage st: 1024 16-byte pieces of each operand and of the state, 2 + 2 + 2
     // per thread
     auto issue = [&](int k, int st) {
@@ -1005,7 +1010,7 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             cp_async16(sF + cr * kIT + i4, srcf, okf ? 16 : 0);
         }
     };
-    // the first chunks are in flight while the gain partials are gathered below
+    // the first chunks are in flight while the update's operands are loaded below
     if (fast) {
 #pragma unroll
         for (int k = 0; k < kRowStages - 1; ++k) {
@@ -1017,43 +1022,6 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         const size_t idx = (size_t)a * B + ib;  // B and ib are even
         fa2 = *reinterpret_cast<const float2*>(F + idx);
         ca2 = *reinterpret_cast<const float2*>(Cc + idx);
-    }
-    // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
-    if (ops.has_bin) {
-        const int r = tid & (kRT - 1);
-        const int a = a0 + r;
-        const int cell = a / ops.n_mom, am = a - cell * ops.n_mom;
-        const int s = a < n ? species_of_row(ops, am) : 0;
-        const bool on = a < n && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
-#pragma unroll
-        for (int q = 0; q < kIT / 16; ++q) {
-            const int il = (tid >> 5) + 16 * q;
-            const int i = i0 + il;
-            float g = 0.f;
-            if (on && i < B) {
-                // the group's split partials of column cell * Bcap + slot, summed in split order
-                for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
-                    const int gi = ops.gain_grp[e];
-                    const int row = ops.gain_roff[e] + (am - ops.sp_off[s]);
-                    const float* pp = ops.grp_partial[gi] + ((size_t)cell * B + i) * ops.grp_M[gi] + row;
-                    const size_t st = (size_t)ops.grp_stride[gi];
-                    const int nsp = ops.grp_nsplit[gi];
-                    float acc = 0.f;
-                    int sp = 0;
-                    for (; sp + 4 <= nsp; sp += 4) {
-                        const float v0 = pp[(size_t)sp * st], v1 = pp[(size_t)(sp + 1) * st];
-                        const float v2 = pp[(size_t)(sp + 2) * st], v3 = pp[(size_t)(sp + 3) * st];
-                        acc += v0;
-                        acc += v1;
-                        acc += v2;
-                        acc += v3;
-                    }
-                    for (; sp < nsp; ++sp) acc += pp[(size_t)sp * st];
-                    g += acc * ops.grp_rscale[gi][row] * ops.grp_sig1[gi][i] * ops.grp_sig2[gi][i];
-                }
-            }
-            s_gain[r][il] = g;
-        }
     }
     if (tid < kIT) s_nonfin[tid] = 0;
     __syncthreads();
@@ -1119,6 +1087,55 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                 s_pl[kg][ty + 8 * k][tx * 4 + j] = acc_l[k][j];
                 s_pe[kg][ty + 8 * k][tx * 4 + j] = acc_e[k][j];
             }
+    }
+    pdl_wait();  // this step's gain GEMM has completed: its split partials are visible
+    // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
+    if (ops.has_bin) {
+        const int r = tid & (kRT - 1);
+        const int a = a0 + r;
+        const int cell = a / ops.n_mom, am = a - cell * ops.n_mom;
+        const int s = a < n ? species_of_row(ops, am) : 0;
+        const bool on = a < n && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
+        // the thread's two instances il0 and il0 + 16; their partials are loaded kGatherChunk
+        // splits at a time for both instances at once (one L2 round trip per chunk), then summed
+        // in split order
+        const int il0 = tid >> 5;
+        const bool ok0 = on && i0 + il0 < B, ok1 = on && i0 + il0 + 16 < B;
+        float g0 = 0.f, g1 = 0.f;
+        if (ok0 || ok1) {
+            for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
+                const int gi = ops.gain_grp[e];
+                const int row = ops.gain_roff[e] + (am - ops.sp_off[s]);
+                const int Mg = ops.grp_M[gi];
+                // column cell * Bcap + slot of the group's partials
+                const float* pp0 = ops.grp_partial[gi] + ((size_t)cell * B + i0 + il0) * Mg + row;
+                const float* pp1 = pp0 + (size_t)16 * Mg;
+                const size_t st = (size_t)ops.grp_stride[gi];
+                const int nsp = ops.grp_nsplit[gi];
+                float acc0 = 0.f, acc1 = 0.f;
+                for (int sp0 = 0; sp0 < nsp; sp0 += kGatherChunk) {
+                    float v0[kGatherChunk], v1[kGatherChunk];
+#pragma unroll
+                    for (int k = 0; k < kGatherChunk; ++k) {
+                        const bool in = sp0 + k < nsp;
+                        v0[k] = (in && ok0) ? pp0[(size_t)(sp0 + k) * st] : 0.f;
+                        v1[k] = (in && ok1) ? pp1[(size_t)(sp0 + k) * st] : 0.f;
+                    }
+#pragma unroll
+                    for (int k = 0; k < kGatherChunk; ++k) {
+                        if (sp0 + k < nsp) {
+                            acc0 += v0[k];
+                            acc1 += v1[k];
+                        }
+                    }
+                }
+                const float rs = ops.grp_rscale[gi][row];
+                if (ok0) g0 += acc0 * rs * ops.grp_sig1[gi][i0 + il0] * ops.grp_sig2[gi][i0 + il0];
+                if (ok1) g1 += acc1 * rs * ops.grp_sig1[gi][i0 + il0 + 16] * ops.grp_sig2[gi][i0 + il0 + 16];
+            }
+        }
+        s_gain[r][il0] = g0;
+        s_gain[r][il0 + 16] = g1;
     }
     __syncthreads();
 

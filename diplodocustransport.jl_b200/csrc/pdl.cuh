@@ -2,8 +2,11 @@
 //
 // The kernels of a step are launched so that the next one may start while the previous one
 // runs. Each waits for its predecessor (grid completion and memory) before it reads what the
-// predecessor wrote or writes what the predecessor reads, and lets its own dependents launch only
-// after that wait, so a chain of early launches never skips a completion.
+// predecessor wrote or writes what the predecessor reads. A grid completes only after its own
+// wait returned, so waiting on the predecessor's completion also covers every grid before it.
+// Most kernels let their dependents launch right after that wait; the batched epilogue
+// (mixed_rows) does so at its start, since everything the next GEMM does before its own wait
+// (barriers, tensor memory, static G tiles) touches nothing the epilogue reads or writes.
 #pragma once
 
 #include <cuda_runtime.h>
