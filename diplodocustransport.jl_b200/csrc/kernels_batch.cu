@@ -687,21 +687,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
             tc_fence_after();
         }
         if (ok && !*abort_flag) {
-            float* dst = a.partial + (size_t)split * a.Bpad * a.M;
-            for (int cc = 0; cc < ncol; cc += 32) {
-                uint32_t r0[16], r1[16];
-                const bool ok0 = nt > 0 && c0 + cc < n_eff, ok1 = nt > 0 && c0 + cc + 16 < n_eff;
-                const uint32_t ta = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc);
-                if (ok0) tmem_ld16_issue(ta, r0);
-                if (ok1) tmem_ld16_issue(ta + 16, r1);
-                if (ok0 || ok1) tmem_ld_wait();
-                if (row < a.M) {
+            // the warp's 128 columns: every tensor-memory load in flight before one wait
+            static_assert(C::BN / (C::NPW / 4) == 128, "epilogue covers 128 columns per warp");
+            float* dst = a.partial + (size_t)split * a.Bpad * a.M + (size_t)(n0 + c0) * a.M + row;
+            uint32_t rv[8][16];
+            const uint32_t ta = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)c0;
+            if (nt > 0 && c0 < n_eff) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k)
-                        dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = ok0 ? __uint_as_float(r0[k]) : 0.f;
+                for (int q = 0; q < 8; ++q) tmem_ld16_issue(ta + 16 * q, rv[q]);
+                tmem_ld_wait();
+            }
+            if (row < a.M) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k)
-                        dst[(size_t)(n0 + c0 + cc + 16 + k) * a.M + row] = ok1 ? __uint_as_float(r1[k]) : 0.f;
+                for (int q = 0; q < 8; ++q) {
+                    const bool live = nt > 0 && c0 + 16 * q < n_eff;
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) dst[(size_t)(16 * q + k) * a.M] = live ? __uint_as_float(rv[q][k]) : 0.f;
                 }
             }
         }
