@@ -1,24 +1,28 @@
 """Benchmark of the explicit Euler step on B200 (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1|0]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 2|3|0|1|4]
 
-Workload (default, --config 1): the plain single instance with two species (electron,
-photon) of 64 log p bins x 16 u bins = 1024 states each; FP32 gain tensor 1024 x 1,048,576
-per output species (8.6 GB, streamed from HBM every step, larger than L2), flux, loss and
-emission as in the config recipe (dtb/synth.py). A step is one Euler step. --config 0 is the
-FP64 N_s = 128 case (L2-resident, launch-bound).
+Workload (default, --config 2): batching, 256 independent instances on one grid of two
+species (electron, photon) of 32 log p bins x 8 u bins = 256 states each, sharing one gain
+tensor 2 x 256 x 65,536 stored as BF16 hi+lo with per-row scales (134 MB, streamed every step,
+larger than L2), loss, emission and flux as in the config recipe (dtb/synth.py); per-instance
+f0 and dt. A step is one batched Euler step of all instances (the autotuned tcgen05 gain GEMM
+and the epilogue kernel). --config 3: three species, 64 instances, 4.59 GB of G per step.
+--config 1: the plain single instance (FP32 G 8.6 GB); --config 0: the FP64 N_s = 128 case
+(L2-resident, launch-bound); --config 4: serving (Poisson request stream, p50/p99).
 
-value: Euler steps/s over the timed steps, inputs resident in HBM, device-timed with CUDA
-events on the library's stream; N GPUs run independent replicas (weak scaling) and the
-whole-job value is the sum over ranks (total steps / max time over ranks).
-e2e: the same steps through the public API with host buffers: every step uploads f from
-pinned host memory, steps, and reads f back (dtb_set_f / dtb_step / dtb_get_f).
-roofline: the gain kernel (dominant), algorithmic bytes = every G element read once per
-step, duration from CUDA events around each gain launch in the timed region.
+value: instance-steps/s over the timed steps, inputs resident in HBM, device-timed with CUDA
+events on the library's stream (a captured graph replayed); N GPUs run independent batch
+replicas (weak scaling) and the whole-job value is the sum over ranks (total instance-steps /
+max time over ranks).
+e2e: the same steps through the public API with host buffers: every step uploads the whole
+batch's f (FP64) from pinned host memory, steps, and reads it back.
+roofline: the gain GEMM (dominant), algorithmic FLOPs = 3 MMAs x 2 x M x K x instances per
+step (tensor-bound; config 3: operator bytes, HBM-bound), duration from CUDA events around
+every GEMM launch over a second run of the same steps.
 cpu_baseline / --impl reference: the FP64 oracle port timed on the host cores with OpenMP on
-a bounded sample (a subset of gain rows scaled to the full row count, plus the full O(N^2)
-rest), reported in steps/s.
-"""
+one instance for a few steps, scaled to instance-steps/s.
+""""""
 from __future__ import annotations
 
 import argparse
