@@ -22,7 +22,7 @@ step (tensor-bound; config 3: operator bytes, HBM-bound), duration from CUDA eve
 every GEMM launch over a second run of the same steps.
 cpu_baseline / --impl reference: the FP64 oracle port timed on the host cores with OpenMP on
 one instance for a few steps, scaled to instance-steps/s.
-""""""
+"""
 from __future__ import annotations
 
 import argparse
