@@ -145,3 +145,17 @@ def test_server_host_errors_without_a_device():
     st = _lib.RequestStats()
     assert L.dtb_serve_wait(srv, 7, 0.01, None, ctypes.byref(st)) == _lib.DTB_ENOTFOUND
     assert L.dtb_serve_destroy(srv) == _lib.DTB_OK
+
+
+def test_entry_scripts_compile_and_bench_parses_its_arguments():
+    """bench.py and __graft_entry__.py are valid Python, and bench.py answers --help without a
+    device (its argument parser is reachable before any CUDA call)."""
+    import py_compile
+    import subprocess
+    import sys
+    for name in ("bench.py", "__graft_entry__.py"):
+        py_compile.compile(os.path.join(ROOT, name), doraise=True)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True, text=True,
+                         timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert "--config" in out.stdout and "--impl" in out.stdout
