@@ -388,10 +388,12 @@ def run_batched(args):
     import torch
     import torch.distributed as dist
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from dtb.batch import BatchedEuler
+    from dtb.batch import BatchedEuler, set_tune_cache
     from dtb.stepping import ForwardEulerStruct
     rank, local, world = _env_rank()
     torch.cuda.set_device(local)
+    if args.tune_cache:
+        set_tune_cache(args.tune_cache)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
@@ -654,6 +656,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="p_bins x u_bins override of the config-1 grid, e.g. 32x16")
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 accuracy check of the batched run")
+    ap.add_argument("--tune-cache", default=None,
+                    help="gain-GEMM plan cache file: plans recorded there are reused, new ones are measured and "
+                         "appended (a profiling run can replay the plan a plain run chose)")
     ap.add_argument("--requests", type=int, default=2000, help="serving stream length (--config 4)")
     ap.add_argument("--rate", type=float, default=20.0, help="mean request arrival rate per second (--config 4)")
     ap.add_argument("--capacity", type=int, default=256, help="slots per grid (--config 4)")
