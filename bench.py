@@ -16,7 +16,8 @@ events on the library's stream (a captured graph replayed); N GPUs run independe
 replicas (weak scaling) and the whole-job value is the sum over ranks (total instance-steps /
 max time over ranks).
 e2e: the same steps through the public API with host buffers: every step uploads the whole
-batch's f (FP64) from pinned host memory, steps, and reads it back.
+batch's f (FP64) from pinned host memory, steps, and reads it back (dtb_batch_run_io, one
+call and one wait per step).
 roofline: the gain GEMM (dominant), algorithmic FLOPs = 3 MMAs x 2 x M x K x instances per
 step (tensor-bound; config 3: operator bytes, HBM-bound), duration from CUDA events around
 every GEMM launch over a second run of the same steps.
@@ -470,9 +471,7 @@ def run_batched(args):
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(K2):
-        m.set_f_all(Fh)
-        m.run(1)
-        m.get_f_all(Fh)
+        m.run_io(Fh, 1, Fh)  # upload, one batched step, download: one call, one wait
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)

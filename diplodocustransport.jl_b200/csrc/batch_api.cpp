@@ -1010,6 +1010,45 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
     return DTB_OK;
 }
 
+namespace {
+
+// Every slot's f from the caller's host array into the state pair (F, C), enqueued.
+int upload_all(dtb_ctx* c, const double* f) {
+    MixedState* m = c->mixed;
+    const int n = (int)c->n_state;
+    const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
+    if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
+    DTB_CUDA(cudaMemcpyAsync(m->io_all, f, bytes, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(launch_pack_f(m->io_all, m->Buser, n, m->Bcap, m->F[m->cur], m->C[m->cur], c->stream));
+    return DTB_OK;
+}
+
+// Every slot's f (F + C in FP64) into the caller's host array, enqueued.
+int download_all(dtb_ctx* c, double* f) {
+    MixedState* m = c->mixed;
+    const int n = (int)c->n_state;
+    const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
+    if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
+    DTB_CUDA(launch_unpack_f(m->F[m->cur], m->C[m->cur], m->Buser, n, m->Bcap, m->io_all, c->stream));
+    DTB_CUDA(cudaMemcpyAsync(f, m->io_all, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return DTB_OK;
+}
+
+}  // namespace
+
+int32_t dtb_batch_run_io(dtb_ctx* c, const double* f_in, int64_t nsteps, double* f_out) {
+    DTB_TRY(mixed_ready(c));
+    DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_batch_run_io: nsteps < 0");
+    DeviceGuard g(c->device);
+    if (f_in) DTB_TRY(upload_all(c, f_in));
+    if (nsteps > 0) DTB_TRY(dtb_batch_run(c, nsteps));
+    if (f_out) DTB_TRY(download_all(c, f_out));
+    DTB_TRY(mixed_err_enqueue(c));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));  // one wait for the whole round trip
+    DTB_TRY(mixed_err_take(c));
+    return DTB_OK;
+}
+
 int32_t dtb_batch_get_f(dtb_ctx* c, int32_t slot, double* f) {
     DTB_TRY(mixed_ready(c));
     MixedState* m = c->mixed;
@@ -1067,13 +1106,8 @@ int32_t dtb_batch_release(dtb_ctx* c, int32_t slot) {
 int32_t dtb_batch_set_f_all(dtb_ctx* c, const double* f) {
     DTB_TRY(mixed_ready(c));
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_set_f_all: null input");
-    MixedState* m = c->mixed;
     DeviceGuard g(c->device);
-    const int n = (int)c->n_state;
-    const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
-    if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
-    DTB_CUDA(cudaMemcpyAsync(m->io_all, f, bytes, cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(launch_pack_f(m->io_all, m->Buser, n, m->Bcap, m->F[m->cur], m->C[m->cur], c->stream));
+    DTB_TRY(upload_all(c, f));
     DTB_CUDA(cudaStreamSynchronize(c->stream));  // the caller may reuse f on return
     return DTB_OK;
 }
@@ -1081,13 +1115,8 @@ int32_t dtb_batch_set_f_all(dtb_ctx* c, const double* f) {
 int32_t dtb_batch_get_f_all(dtb_ctx* c, double* f) {
     DTB_TRY(mixed_ready(c));
     DTB_CHECK(f, DTB_EINVAL, "dtb_batch_get_f_all: null output");
-    MixedState* m = c->mixed;
     DeviceGuard g(c->device);
-    const int n = (int)c->n_state;
-    const size_t bytes = sizeof(double) * (size_t)n * m->Buser;
-    if (!m->io_all) DTB_TRY(c->alloc(&m->io_all, bytes));
-    DTB_CUDA(launch_unpack_f(m->F[m->cur], m->C[m->cur], m->Buser, n, m->Bcap, m->io_all, c->stream));
-    DTB_CUDA(cudaMemcpyAsync(f, m->io_all, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DTB_TRY(download_all(c, f));
     DTB_TRY(mixed_err_enqueue(c));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
     DTB_TRY(mixed_err_take(c));

@@ -126,6 +126,7 @@ SIGNATURES = {
     "dtb_batch_set_profiling": (_i32, [_P, _i32]),
     "dtb_batch_gemm_stats": (_i32, [_P, _dp, _dp, _dp, _i32p]),
     "dtb_set_tune_cache": (_i32, [ctypes.c_char_p]),
+    "dtb_batch_run_io": (_i32, [_P, _P, _i64, _P]),
     "dtb_batch_gemm_plan": (_i32, [_P, _i32, _i32p, _i32p, _i32p, _dp]),
     "dtb_gain_contract_noalloc": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
 }

@@ -107,6 +107,15 @@ class BatchedEuler:
         check(self.L.dtb_batch_get_f_all(self.ctx, dptr(out)))
         return out
 
+    def run_io(self, F_in, nsteps: int, out: Optional[np.ndarray] = None) -> Optional[np.ndarray]:
+        """Every slot's f from F_in (None: keep the device state), nsteps batched steps, every
+        slot's f into `out` (allocated when None), with one wait for the whole round trip."""
+        A = None if F_in is None else np.ascontiguousarray(F_in, dtype=np.float64)
+        if out is None:
+            out = np.empty((self.capacity, self.n))
+        check(self.L.dtb_batch_run_io(self.ctx, None if A is None else dptr(A), int(nsteps), dptr(out)))
+        return out
+
     def moments(self, weights) -> tuple:
         """FP64 number and energy per (slot, species) on the device, or per (slot, cell, species)
         when the slots hold several space cells; weights: one per momentum state."""

@@ -255,6 +255,12 @@ int32_t dtb_batch_slot_info(dtb_ctx* ctx, int32_t slot, int64_t* steps_done, int
 int32_t dtb_batch_set_f_all(dtb_ctx* ctx, const double* f);
 int32_t dtb_batch_get_f_all(dtb_ctx* ctx, double* f);
 
+/* The host round trip of a caller that steps from host memory, in one call and one wait:
+ * dtb_batch_set_f_all(f_in) (skipped when f_in is NULL), dtb_batch_run(nsteps), then
+ * dtb_batch_get_f_all(f_out) (skipped when f_out is NULL). f_in and f_out may be the same
+ * array. Device errors of the steps are reported by this call. */
+int32_t dtb_batch_run_io(dtb_ctx* ctx, const double* f_in, int64_t nsteps, double* f_out);
+
 /* FP64 number sum(f) and energy sum(f * w) of every slot, space cell and species, on the device
  * (DistributionMoments.jl:33,145,162); w is the per-state energy weight (n_mom). Outputs are
  * batch x n_space x n_species, slot-major. */

@@ -205,6 +205,59 @@ def test_whole_batch_state_io(cuda):
     m.close()
 
 
+def test_run_io_equals_separate_io_calls(cuda):
+    """dtb_batch_run_io (upload, steps, download under one wait) gives bit-identical states to
+    set_f_all + run + get_f_all on a second context; the same array may be input and output,
+    and a None input keeps the device state."""
+    B = 37
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, B, seed=23)
+    a = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    for m in (a, b):
+        for i in range(B):
+            m.admit(i, w.f0[i], w.dt[i], 40)
+    F = np.array(w.f0, dtype=np.float64)
+    b.set_f_all(F)
+    for nsteps in (1, 3, 20):
+        b.run(nsteps)
+        ref = b.get_f_all()
+        F = a.run_io(F, nsteps, F)
+        np.testing.assert_array_equal(F, ref)
+    b.run(2)
+    np.testing.assert_array_equal(a.run_io(None, 2), b.get_f_all())
+    a.close()
+    b.close()
+
+
+def test_page_locked_and_pageable_host_arrays_agree(cuda):
+    """Batch I/O through page-locked host arrays (an array that starts inside a larger pinned
+    buffer) and through pageable arrays gives bit-identical states, through run_io and
+    set_f_all / get_f_all."""
+    import torch
+    B = 37
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, B, seed=24)
+    n = w.ps.n_state
+    a = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    for m in (a, b):
+        for i in range(B):
+            m.admit(i, w.f0[i], w.dt[i], 40)
+    big = torch.zeros((B + 3) * n, dtype=torch.float64).pin_memory().numpy()
+    P = big[n:n + B * n].reshape(B, n)
+    P[:] = w.f0
+    F = np.array(w.f0, dtype=np.float64)
+    for nsteps in (1, 5):
+        a.run_io(P, nsteps, P)
+        F = b.run_io(F, nsteps, F)
+        np.testing.assert_array_equal(P, F)
+    Q = torch.empty((B, n), dtype=torch.float64).pin_memory().numpy()
+    a.set_f_all(P)
+    a.get_f_all(Q)
+    np.testing.assert_array_equal(Q, P)
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("p,u", [(8, 4), (10, 8)])
 def test_gemm_columns_follow_the_last_running_slot(cuda, p, u):
     """The gain GEMM computes only up to the last running slot (rounded to 16 columns, 32 on SM
