@@ -1,6 +1,7 @@
 """Benchmark of the explicit Euler step on B200 (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 2|3|0|1|4]
+    python bench.py [--gpus N] [--steps K (2000)] [--warmup W (5; at least 32 are run)] [--impl ours|reference]
+                    [--config 2|3|0|1|4]
 
 Workload (default, --config 2): batching, 256 independent instances on one grid of two
 species (electron, photon) of 32 log p bins x 8 u bins = 256 states each, sharing one gain
@@ -39,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "diplodocustransport.jl_b200"))
 
 METRIC = "steps/s & p99 latency, batched BF16-split vs plain FP64, at ≤1e-5 rel err"
+GRAPH_WARMUP = 32  # two captured graphs of 16 steps
 
 
 def _env_rank():
@@ -306,9 +308,10 @@ def run_ours(args):
     w.binm.gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, None) for g in w.binm.gains]
     torch.cuda.empty_cache()
     L = m.L
-    K, W = args.steps, args.warmup
+    # warm-up: at least two graphs' worth of steps, so the 16-step graph is captured and
+    # instantiated before the timed region
+    K, W = args.steps, max(args.warmup, GRAPH_WARMUP)
     scales = np.ones(K)
-    # warm-up (also captures graphs)
     m.run(np.ones(W))
     lps = _lib.ctypes.c_int32()
     L.dtb_launches_per_step(m.ctx, _lib.ctypes.byref(lps))
@@ -402,7 +405,9 @@ def run_batched(args):
     w = build_batched(args.config, dev)
     B = w.f0.shape[0]
     n = w.ps.n_state
-    K, W = args.steps, args.warmup
+    # warm-up: at least two graphs' worth of steps (the 16-step graph is captured and instantiated
+    # before the timed region)
+    K, W = args.steps, max(args.warmup, GRAPH_WARMUP)
     stream = torch.cuda.Stream()
     m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B, device=local, stream=stream.cuda_stream)
     for i in range(B):
@@ -426,7 +431,7 @@ def run_batched(args):
     del gains64, binm64
     w.binm.gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, None) for g in w.binm.gains]
     torch.cuda.empty_cache()
-    m.run(W)  # warm-up (captures the graph)
+    m.run(W)  # warm-up (captures and instantiates the graphs)
     if rank == 0 and not args.no_check:
         errs = []
         for i in (0, B - 1):
@@ -648,7 +653,7 @@ def run_serving(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)

@@ -530,7 +530,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
                 bulk_load(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
                 bulk_load(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
                           smem_addr(&full_a[sa]));
-                if (j == 0 && nt > 1 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
+                // the first two G tiles go out at once, the rest after the first X tile (so the
+                // producers' state loads do not queue behind the whole ring of G traffic)
+                if (j == 1 && nt > 2 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
                     if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
                     *abort_flag = 1;
                     ++j;
