@@ -275,8 +275,10 @@ int plan_gemms(dtb_ctx* c, int Bcols, int max_pairs) {
         GemmPlan p;
         bool have = false;
         const std::string key = plan_key(c, G, Bcols);
+        // held across lookup, tuning and store: concurrent commits of one shape get one plan
+        std::unique_lock<std::mutex> lk(g_plan_mu, std::defer_lock);
         if (tune) {
-            std::lock_guard<std::mutex> lk(g_plan_mu);
+            lk.lock();
             auto it = g_plans.find(key);
             if (it != g_plans.end() && plan_valid(G, it->second, max_pairs)) {
                 p = it->second;
@@ -286,7 +288,6 @@ int plan_gemms(dtb_ctx* c, int Bcols, int max_pairs) {
         if (!have) {
             if (tune) {
                 DTB_TRY(tune_group(c, G, Bcols, max_pairs, &p));
-                std::lock_guard<std::mutex> lk(g_plan_mu);
                 g_plans[key] = p;
                 if (!g_plan_file.empty()) {
                     if (FILE* f = std::fopen(g_plan_file.c_str(), "a")) {
