@@ -893,6 +893,19 @@ __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict
     }
 }
 
+// Two FP32 FMAs in one instruction: acc.{lo, hi} = fma(a, b.{lo, hi}, acc.{lo, hi}), each
+// rounded to nearest like the scalar fma (a pair of floats packed in 64 bits, lo first).
+__device__ __forceinline__ void ffma2(unsigned long long& acc, float a, unsigned long long b) {
+    unsigned long long aa;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(aa) : "f"(a));
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(aa), "l"(b));
+}
+__device__ __forceinline__ float2 unpack_f32x2(unsigned long long v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+
 // 16-byte asynchronous copy global -> shared; src_bytes 0 fills the destination with zeros.
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(src_bytes)
@@ -1034,13 +1047,14 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         fv[e] = (mine && cols[e] >= 0) ? *reinterpret_cast<const float2*>(F + (size_t)cols[e] * B + ib)
                                        : make_float2(0.f, 0.f);
 
-    float acc_l[4][4], acc_e[4][4];
+    // accumulators as packed pairs of instances (tx * 4 + {0, 1} and {2, 3}) for the f32x2 FMAs
+    unsigned long long acc_l[4][2], acc_e[4][2];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            acc_l[k][j] = 0.f;
-            acc_e[k][j] = 0.f;
+        for (int j = 0; j < 2; ++j) {
+            acc_l[k][j] = 0ull;
+            acc_e[k][j] = 0ull;
         }
     if (fast) {
         const int nj = s_njob;
@@ -1057,26 +1071,24 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
             if (hl) {
 #pragma unroll
                 for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
-                    const float4 f4 = *reinterpret_cast<const float4*>(sF + cc * kIT + tx * 4);
-                    const float fvv[4] = {f4.x, f4.y, f4.z, f4.w};
+                    const ulonglong2 f4 = *reinterpret_cast<const ulonglong2*>(sF + cc * kIT + tx * 4);
 #pragma unroll
                     for (int k2 = 0; k2 < 4; ++k2) {
                         const float l = sL[(ty + 8 * k2) * kLS + cc];
-#pragma unroll
-                        for (int j2 = 0; j2 < 4; ++j2) acc_l[k2][j2] += l * fvv[j2];
+                        ffma2(acc_l[k2][0], l, f4.x);
+                        ffma2(acc_l[k2][1], l, f4.y);
                     }
                 }
             }
             if (he) {
 #pragma unroll
                 for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
-                    const float4 f4 = *reinterpret_cast<const float4*>(sF + cc * kIT + tx * 4);
-                    const float fvv[4] = {f4.x, f4.y, f4.z, f4.w};
+                    const ulonglong2 f4 = *reinterpret_cast<const ulonglong2*>(sF + cc * kIT + tx * 4);
 #pragma unroll
                     for (int k2 = 0; k2 < 4; ++k2) {
                         const float e = sE[(ty + 8 * k2) * kLS + cc];
-#pragma unroll
-                        for (int j2 = 0; j2 < 4; ++j2) acc_e[k2][j2] += e * fvv[j2];
+                        ffma2(acc_e[k2][0], e, f4.x);
+                        ffma2(acc_e[k2][1], e, f4.y);
                     }
                 }
             }
@@ -1086,9 +1098,12 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                s_pl[kg][ty + 8 * k][tx * 4 + j] = acc_l[k][j];
-                s_pe[kg][ty + 8 * k][tx * 4 + j] = acc_e[k][j];
+            for (int j = 0; j < 2; ++j) {
+                const float2 pl = unpack_f32x2(acc_l[k][j]), pe = unpack_f32x2(acc_e[k][j]);
+                s_pl[kg][ty + 8 * k][tx * 4 + 2 * j] = pl.x;
+                s_pl[kg][ty + 8 * k][tx * 4 + 2 * j + 1] = pl.y;
+                s_pe[kg][ty + 8 * k][tx * 4 + 2 * j] = pe.x;
+                s_pe[kg][ty + 8 * k][tx * 4 + 2 * j + 1] = pe.y;
             }
     }
     pdl_wait();  // this step's gain GEMM has completed: its split partials are visible
