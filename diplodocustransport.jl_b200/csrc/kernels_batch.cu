@@ -59,11 +59,17 @@ __device__ __forceinline__ bool mb_wait(uint32_t bar, uint32_t parity, volatile 
         if (gtimer() - t0 > kWaitLimitNs) return false;
     }
 }
-// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16) of a stream
+// read once per step (the G tiles, larger than L2): the lines are marked evict-first, so the
+// step's small working set (state, split partials, loss and emission operands) stays in L2
+// across the stream.
+__device__ __forceinline__ void bulk_load_stream(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-        "l"(src), "r"(bytes), "r"(bar)
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(bar), "l"(pol)
         : "memory");
 }
 // K-major operand tile in the canonical 128-byte swizzle layout: rows of 128 bytes, 8-row
@@ -201,8 +207,8 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 }
                 mb_expect_tx(smem_addr(&full_a[sa]), 2 * C::A_BYTES);
                 const unsigned char* src = src0 + (size_t)j * kGTileBytes;
-                bulk_load(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
-                bulk_load(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
+                bulk_load_stream(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
+                bulk_load_stream(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
                           smem_addr(&full_a[sa]));
                 // the producers' state loads come first: the rest of the G ring waits for the first
                 // X tile, so those loads do not queue behind every CTA's full ring of G traffic
@@ -527,8 +533,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
                 }
                 mb_expect_tx(smem_addr(&full_a[sa]), 2 * C::A_BYTES);
                 const unsigned char* src = src0 + (size_t)j * kGTileBytes;
-                bulk_load(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
-                bulk_load(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
+                bulk_load_stream(smem_addr(a_base + (size_t)(sa * 2) * C::A_BYTES), src, C::A_BYTES, smem_addr(&full_a[sa]));
+                bulk_load_stream(smem_addr(a_base + (size_t)(sa * 2 + 1) * C::A_BYTES), src + C::A_BYTES, C::A_BYTES,
                           smem_addr(&full_a[sa]));
                 // the first two G tiles go out at once, the rest after the first X tile (so the
                 // producers' state loads do not queue behind the whole ring of G traffic)
