@@ -3,6 +3,8 @@
 Tolerances: the gain term alone within 2e-5 (normwise relative) of the FP64 contraction; whole
 runs within relative L-infinity 1e-5 of the FP64 oracle run with the same dt per instance.
 """
+import contextlib
+
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -16,6 +18,31 @@ pytestmark = pytest.mark.gpu
 
 TOL_GAIN = 2e-5
 TOL_RUN = 1e-5
+
+
+def _plan_key(w, batch):
+    """Autotuner key of the two-species workloads' one gain group (e, gamma inputs)."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n1, n2 = w.ps.species_sizes[0], w.ps.species_sizes[1]
+    cols = w.ps.n_space * ((batch + 3) // 4 * 4)
+    return f"sm{sms}:M{sum(w.ps.species_sizes)}:N1{n1}:n2{n2}:cols{cols}:cells{w.ps.n_space}"
+
+
+@contextlib.contextmanager
+def forced_plan(tmp_path, w, batch, plan):
+    """Commits inside the block use the gain GEMM plan `plan` = (pair, bn, splits) for this
+    shape, read from a plan cache file instead of measured (None: the autotuner's choice)."""
+    if plan is None:
+        yield
+        return
+    cache = tmp_path / "plans.txt"
+    cache.write_text(f"{_plan_key(w, batch)} {plan[0]} {plan[1]} {plan[2]} 0\n")
+    set_tune_cache(str(cache))
+    try:
+        yield
+    finally:
+        set_tune_cache(None)
 
 
 def rel_linf(a, b):
@@ -32,17 +59,28 @@ def _gain_only(w):
     return w
 
 
-@pytest.mark.parametrize("p,u,batch", [(8, 4, 8), (16, 8, 100), (8, 8, 300), (12, 6, 40), (10, 8, 300),
-                                       (16, 8, 260)])
-def test_batched_gain_term_matches_fp64(cuda, p, u, batch):
-    """One step with only the gain term: f1 - f0 = gain; covers BN = 64, 128, 256, several N
-    tiles, n2 padded to 64 (p*u = 32, 72, 80) and more than one M tile. (10, 8, 300) and
-    (16, 8, 260) have two m tiles and 256-column tiles, so they run on SM pairs: rows past M in
-    the second m tile (M = 160), and a second column tile with 44 or 4 running columns."""
+@pytest.mark.parametrize("p,u,batch,plan", [
+    (8, 4, 8, None), (16, 8, 100, None), (8, 8, 300, None), (12, 6, 40, None),
+    (16, 8, 100, (0, 128, 37)), (8, 8, 300, (0, 256, 37)), (8, 8, 300, (0, 128, 20)),
+    (10, 8, 300, (1, 256, 37)), (16, 8, 260, (1, 256, 37)), (16, 8, 260, (1, 256, 13)),
+    (10, 8, 300, (0, 64, 37))])
+def test_batched_gain_term_matches_fp64(cuda, tmp_path, p, u, batch, plan):
+    """One step with only the gain term: f1 - f0 = gain; covers BN = 64, 128, 256 on one SM and
+    the SM-pair kernel (plans forced through the cache file, or the autotuner's choice), several
+    N tiles, n2 padded to 64 (p*u = 32, 72, 80), more than one M tile, K splits aligned to the
+    input-2 blocks and not (13 splits of 20 K tiles, one crossing the block boundary). On SM
+    pairs: rows past M in the second m tile (M = 160), and a second column tile with 44 or 4
+    running columns. The gain's error grows with the K range of a split (each split sums its
+    range in one FP32 tensor-memory accumulator): a forced 5-split plan (3,328 K values per
+    accumulator) reached 2.003e-5 here, the autotuner's plans fill the device with 36-37 splits."""
     w = _gain_only(synth.batched_two_species(p, 1e-2, 1e2, u, batch, seed=p * 100 + u))
     for g in w.binm.gains:  # make the gain dominate the step
         g.G = np.asarray(g.G) * 50.0
-    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, batch)
+    with forced_plan(tmp_path, w, batch, plan):
+        m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, batch)
+    if plan is not None:
+        got = m.gemm_plan(0)
+        assert (got["pair"], got["bn"]) == (bool(plan[0]), plan[1])
     for i in range(batch):
         m.admit(i, w.f0[i], 1.0, 1)
     m.run(1)
@@ -258,35 +296,32 @@ def test_page_locked_and_pageable_host_arrays_agree(cuda):
     b.close()
 
 
-@pytest.mark.parametrize("p,u", [(8, 4), (10, 8)])
-def test_gemm_columns_follow_the_last_running_slot(cuda, p, u):
+@pytest.mark.parametrize("p,u,plan", [(8, 4, None), (10, 8, (1, 256, 37)), (10, 8, (0, 256, 37)),
+                                      (10, 8, (0, 128, 37))])
+def test_gemm_columns_follow_the_last_running_slot(cuda, tmp_path, p, u, plan):
     """The gain GEMM computes only up to the last running slot (rounded to 16 columns, 32 on SM
     pairs): a slot alone at index 3 or 200 of 256, and the same slot with every slot running,
     give the same f; finished slots keep their state while a higher slot runs on. (10, 8) has
-    two m tiles and runs on SM pairs."""
+    two m tiles and runs, forced, on SM pairs and on one SM."""
     B = 256
     w = synth.batched_two_species(p, 1e-2, 1e2, u, B, seed=12)
-    full = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
-    for i in range(B):
-        full.admit(i, w.f0[i], w.dt[i], 30)
-    full.run(30)
-    for slot in (3, 200):
-        one = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
-        one.admit(slot, w.f0[slot], w.dt[slot], 30)
-        one.admit(0, w.f0[0], w.dt[0], 5)
-        one.run(30)
-        np.testing.assert_array_equal(one.get_f(slot), full.get_f(slot))
-        assert one.info(0)["steps_done"] == 5
-        one.close()
-    full.close()
-
-
-def _plan_key(w, batch):
-    import torch
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
-    n1, n2 = w.ps.species_sizes[0], w.ps.species_sizes[1]
-    cols = w.ps.n_space * ((batch + 3) // 4 * 4)
-    return f"sm{sms}:M{sum(w.ps.species_sizes)}:N1{n1}:n2{n2}:cols{cols}:cells{w.ps.n_space}"
+    with forced_plan(tmp_path, w, B, plan):
+        full = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+        for i in range(B):
+            full.admit(i, w.f0[i], w.dt[i], 30)
+        full.run(30)
+        for slot in (3, 200):
+            one = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+            assert one.gemm_plan(0) == full.gemm_plan(0)
+            one.admit(slot, w.f0[slot], w.dt[slot], 30)
+            one.admit(0, w.f0[0], w.dt[0], 5)
+            one.run(30)
+            np.testing.assert_array_equal(one.get_f(slot), full.get_f(slot))
+            assert one.info(0)["steps_done"] == 5
+            one.close()
+        if plan is not None:
+            assert (full.gemm_plan(0)["pair"], full.gemm_plan(0)["bn"]) == (bool(plan[0]), plan[1])
+        full.close()
 
 
 def test_sm_pair_gemm_agrees_with_one_sm_gemm(cuda, tmp_path):
@@ -383,6 +418,32 @@ def test_multicell_slots_match_oracle(cuda, n_space, domain):
     for i in range(6):
         f = f0s[i].copy()
         for _ in range(30):
+            f, _, _ = ops.step(f, dts[i], 0)
+        assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
+    m.close()
+
+
+def test_multicell_slots_on_sm_pairs(cuda, tmp_path):
+    """Multi-cell columns through the SM-pair GEMM (forced): 2 cells x 100 slots = 200 columns
+    of one 256-column tile (224 computed), two m tiles (M = 160); 10 steps against the FP64
+    oracle of the same two-cell grid for three slots."""
+    w = synth.small(p_num=10, u_num=8, seed=66, n_space=2, randomize_vectors=True)
+    w.fluxm.X_Flux = synth.space_flux(w.ps, np.random.default_rng(67), 1.0)
+    B = 100
+    n = w.ps.n_state
+    rng = np.random.default_rng(6)
+    f0s = [w.f0 * rng.uniform(0.7, 1.3, n) for _ in range(B)]
+    dts = rng.uniform(0.5, 1.0, B)
+    with forced_plan(tmp_path, w, B, (1, 256, 37)):
+        m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    assert m.gemm_plan(0)["pair"]
+    for i in range(B):
+        m.admit(i, f0s[i], dts[i], 10)
+    m.run(10)
+    ops = oracle.blocked_from_workload(w)
+    for i in (0, 57, B - 1):
+        f = f0s[i].copy()
+        for _ in range(10):
             f, _, _ = ops.step(f, dts[i], 0)
         assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
     m.close()
