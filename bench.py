@@ -566,6 +566,9 @@ def run_serving(args):
     if rank != 0:
         return 0
     torch.cuda.set_device(local)
+    if args.tune_cache:
+        from dtb.batch import set_tune_cache
+        set_tune_cache(args.tune_cache)
     rng = np.random.default_rng(44)
     n_req = args.requests
     rate = args.rate
