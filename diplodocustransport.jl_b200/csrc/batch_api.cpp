@@ -217,11 +217,24 @@ int tune_group(dtb_ctx* c, MixedGroup& G, int Bcols, int max_pairs, GemmPlan* be
         apply_plan(G, p, Bcols);
         scratch = std::max(scratch, sizeof(float) * (size_t)G.n_splits * G.Bpad * G.M);
     }
-    float* part = nullptr;
-    DTB_CUDA(cudaMalloc(&part, scratch));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    DTB_CUDA(cudaEventCreate(&e0));
-    DTB_CUDA(cudaEventCreate(&e1));
+    // the timing run's scratch partials and events, released on every way out
+    struct Scratch {
+        float* part = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        MixedGroup* G = nullptr;
+        ~Scratch() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (part) cudaFree(part);
+            if (G) G->partial = nullptr;
+        }
+    } sc;
+    sc.G = &G;
+    DTB_CUDA(cudaMalloc(&sc.part, scratch));
+    DTB_CUDA(cudaEventCreate(&sc.e0));
+    DTB_CUDA(cudaEventCreate(&sc.e1));
+    float* const part = sc.part;
+    const cudaEvent_t e0 = sc.e0, e1 = sc.e1;
     const int all = Bcols;
     DTB_CUDA(cudaMemcpyAsync(m->active_hi, &all, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     double best_ms = 1e30;
@@ -254,10 +267,6 @@ int tune_group(dtb_ctx* c, MixedGroup& G, int Bcols, int max_pairs, GemmPlan* be
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     int kerr = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&kerr, c->err, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(part);
-    G.partial = nullptr;
     DTB_CUDA(e);
     if (kerr != 0) {
         set_error("gain GEMM autotuning: a bounded device wait gave up (code " + std::to_string(kerr) + ")");
