@@ -1,7 +1,9 @@
 # B200 backend for DiplodocusTransport.jl's explicit Euler path, over libdtb.so.
 #
 # Not exercised in this repository (no Julia toolchain here); it shows the exact `ccall`
-# bindings of include/dtb.h that the reference would add. Loaded after DiplodocusTransport:
+# bindings of include/dtb.h that the reference would add: the plain method behind the
+# reference's stepping struct and Solve, and batched solves of one grid (B200BatchedEuler).
+# Loaded after DiplodocusTransport:
 #
 #     using DiplodocusTransport
 #     include("DTB200Backend.jl"); using .DTB200Backend
@@ -19,6 +21,7 @@ using SparseArrays
 import DiplodocusTransport: BackendType, PhaseSpaceStruct
 
 export B200Backend, B200ForwardEulerStruct, b200_solve
+export B200BatchedEuler, admit!, run!, run_io!, get_f, batch_moments, gemm_plan, set_tune_cache
 
 const libdtb = get(ENV, "DTB_LIB", joinpath(@__DIR__, "..", "lib", "libdtb.so"))
 
@@ -26,6 +29,9 @@ struct B200Backend <: BackendType end  # next to Backends.jl:3-4
 
 const DTB_F64 = Int32(0)
 const DTB_F32 = Int32(1)
+const DTB_MIXED = Int32(2)
+const DTB_FLAG_NO_AUTOTUNE = Int32(2)
+const DTB_ENOTFOUND = Int32(7)
 
 struct Dims
     n_species::Int32
@@ -85,6 +91,44 @@ function upload_csc!(ctx, A::SparseMatrixCSC)
         ctx, size(A, 1), A.colptr, A.rowval, nz))
 end
 
+# The operators the step reads (SteppingStructs.jl:33-100), uploaded into a fresh context:
+# F = X + P, M_Bin (dense or Bin_sparse), BinM.Domain, M_Emi, Ap, Vol, the initial state and
+# the injection.
+function upload_operators!(ctx::Ptr{Cvoid}, PhaseSpace::PhaseSpaceStruct, Initial::Vector{Float64},
+                           Injection::Vector{Float64}, BinM, EmiM, FluxM)
+    Momentum = PhaseSpace.Momentum
+    sizes = Momentum.px_num_list .* Momentum.py_num_list .* Momentum.pz_num_list
+    upload_csc!(ctx, FluxM.X_Flux)   # F = X + P (SteppingStructs.jl:60)
+    upload_csc!(ctx, FluxM.P_Flux)
+    n_mom = sum(sizes)
+    if !isempty(BinM.Binary_list)
+        if BinM.M_Bin isa SparseMatrixCSC   # Bin_sparse (BuildBinaryMatrices.jl:44-52), 1-based CSC
+            S = SparseMatrixCSC{Float64,Int64}(BinM.M_Bin)
+            GC.@preserve S check(ccall((:dtb_upload_mbin_csc, libdtb), Int32,
+                                       (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}),
+                                       ctx, n_mom, S.colptr, S.rowval, S.nzval))
+        else
+            M = Matrix{Float64}(BinM.M_Bin)
+            GC.@preserve M check(ccall((:dtb_upload_mbin_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
+                                       ctx, M, n_mom))
+        end
+        if !isnothing(BinM.Domain)   # Bin_Domain (SteppingStructs.jl:51, SteppingMethods.jl:369)
+            D = Vector{Int64}(BinM.Domain)
+            GC.@preserve D check(ccall((:dtb_set_bin_domain, libdtb), Int32, (Ptr{Cvoid}, Ptr{Int64}, Int64),
+                                       ctx, D, length(D)))
+        end
+    end
+    if !isempty(EmiM.Emission_list)
+        E = Matrix{Float64}(EmiM.M_Emi)
+        GC.@preserve E check(ccall((:dtb_upload_emi_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
+                                   ctx, E, size(E, 1)))
+    end
+    Ap = Float64.(FluxM.Ap_Flux); Vol = Float64.(FluxM.Vol)
+    GC.@preserve Ap Vol Initial Injection check(ccall((:dtb_upload_vectors, libdtb), Int32,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), ctx, Ap, Vol, Initial, Injection))
+    return nothing
+end
+
 # The stepping struct of the B200 backend. Same constructor arguments as ForwardEulerStruct
 # (SteppingStructs.jl:33) and the fields Solve reads (PhaseSpace, f_init, f).
 mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
@@ -105,34 +149,7 @@ mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
         opts = Opts(Precision == Float32 ? DTB_F32 : DTB_F64, device, C_NULL, 1, 16, PhaseSpace.Time.dt0, 1, 0)
         ctx = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:dtb_create, libdtb), Int32, (Ref{Dims}, Ref{Opts}, Ref{Ptr{Cvoid}}), dims, opts, ctx))
-        upload_csc!(ctx[], FluxM.X_Flux)   # F = X + P (SteppingStructs.jl:60)
-        upload_csc!(ctx[], FluxM.P_Flux)
-        n_mom = sum(sizes)
-        if !isempty(BinM.Binary_list)
-            if BinM.M_Bin isa SparseMatrixCSC   # Bin_sparse (BuildBinaryMatrices.jl:44-52), 1-based CSC
-                S = SparseMatrixCSC{Float64,Int64}(BinM.M_Bin)
-                GC.@preserve S check(ccall((:dtb_upload_mbin_csc, libdtb), Int32,
-                                           (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}),
-                                           ctx[], n_mom, S.colptr, S.rowval, S.nzval))
-            else
-                M = Matrix{Float64}(BinM.M_Bin)
-                GC.@preserve M check(ccall((:dtb_upload_mbin_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
-                                           ctx[], M, n_mom))
-            end
-            if !isnothing(BinM.Domain)   # Bin_Domain (SteppingStructs.jl:51, SteppingMethods.jl:369)
-                D = Vector{Int64}(BinM.Domain)
-                GC.@preserve D check(ccall((:dtb_set_bin_domain, libdtb), Int32, (Ptr{Cvoid}, Ptr{Int64}, Int64),
-                                           ctx[], D, length(D)))
-            end
-        end
-        if !isempty(EmiM.Emission_list)
-            E = Matrix{Float64}(EmiM.M_Emi)
-            GC.@preserve E check(ccall((:dtb_upload_emi_ref, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Int64),
-                                       ctx[], E, size(E, 1)))
-        end
-        Ap = Float64.(FluxM.Ap_Flux); Vol = Float64.(FluxM.Vol)
-        GC.@preserve Ap Vol Initial Injection check(ccall((:dtb_upload_vectors, libdtb), Int32,
-            (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), ctx[], Ap, Vol, Initial, Injection))
+        upload_operators!(ctx[], PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)
         check(ccall((:dtb_commit, libdtb), Int32, (Ptr{Cvoid},), ctx[]))
         self = new(PhaseSpace, PhaseSpace.Time.dt0, copy(Initial), B200State(ctx[], length(Initial)), ctx[])
         finalizer(m -> ccall((:dtb_destroy, libdtb), Int32, (Ptr{Cvoid},), m.ctx), self)
@@ -168,5 +185,90 @@ function b200_solve(method::B200ForwardEulerStruct, dt_initial::Float64, t_save:
         method.ctx, dt_initial, t_save, length(t_save), Verbose, F, nsteps))
     return F, nsteps[]
 end
+
+# ---------------------------------------------------------------- batched solves
+# Many independent solves of one grid (a parameter scan over initial spectra and time steps)
+# in one batched context: the shared G, stored as BF16 hi + lo with per-row scales, is
+# contracted against every slot's f1 (x) f2 by one tensor-core GEMM per step, f is FP32 with an
+# FP32 compensation term and the update is FP64. Slots are 1-based here; states go in and out
+# as n_state x capacity matrices (column s = slot s).
+mutable struct B200BatchedEuler
+    ctx::Ptr{Cvoid}
+    n::Int
+    capacity::Int
+    dt0::Float64
+    n_species::Int
+    n_space::Int
+
+    function B200BatchedEuler(PhaseSpace::PhaseSpaceStruct, Injection::Vector{Float64}, BinM, EmiM, FluxM,
+                              capacity::Integer; device::Integer=0, autotune::Bool=true)
+        Momentum = PhaseSpace.Momentum
+        sizes = Momentum.px_num_list .* Momentum.py_num_list .* Momentum.pz_num_list
+        ns = length(sizes)
+        n_space = PhaseSpace.Space.x_num * PhaseSpace.Space.y_num * PhaseSpace.Space.z_num
+        dims = Dims(ns, n_space, ntuple(i -> i <= ns ? Int64(sizes[i]) : Int64(0), 16))
+        opts = Opts(DTB_MIXED, device, C_NULL, 1, 16, PhaseSpace.Time.dt0, Int32(capacity),
+                    autotune ? Int32(0) : DTB_FLAG_NO_AUTOTUNE)
+        ctx = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:dtb_create, libdtb), Int32, (Ref{Dims}, Ref{Opts}, Ref{Ptr{Cvoid}}), dims, opts, ctx))
+        n = length(Injection)
+        upload_operators!(ctx[], PhaseSpace, zeros(n), Injection, BinM, EmiM, FluxM)
+        check(ccall((:dtb_commit, libdtb), Int32, (Ptr{Cvoid},), ctx[]))  # plans (autotunes) the gain GEMM
+        self = new(ctx[], n, Int(capacity), PhaseSpace.Time.dt0, ns, n_space)
+        finalizer(b -> ccall((:dtb_destroy, libdtb), Int32, (Ptr{Cvoid},), b.ctx), self)
+        return self
+    end
+end
+
+# Starts a solve in `slot`: f = f0, step dt (dt/dt0 is applied as in SteppingMethods.jl:27),
+# n_steps steps from the current batched step.
+admit!(b::B200BatchedEuler, slot::Integer, f0::Vector{Float64}, dt::Float64, n_steps::Integer) =
+    check(ccall((:dtb_batch_admit, libdtb), Int32, (Ptr{Cvoid}, Int32, Ptr{Float64}, Float64, Int64),
+                b.ctx, slot - 1, f0, dt / b.dt0, n_steps))
+
+# nsteps batched steps of every slot with steps left (enqueued; errors surface at the next read).
+run!(b::B200BatchedEuler, nsteps::Integer) =
+    check(ccall((:dtb_batch_run, libdtb), Int32, (Ptr{Cvoid}, Int64), b.ctx, nsteps))
+
+function get_f(b::B200BatchedEuler, slot::Integer)
+    f = Vector{Float64}(undef, b.n)
+    check(ccall((:dtb_batch_get_f, libdtb), Int32, (Ptr{Cvoid}, Int32, Ptr{Float64}), b.ctx, slot - 1, f))
+    return f
+end
+
+# The whole batch in, nsteps steps, the whole batch out, under one wait. F_in === nothing keeps
+# the device state; F_out may be F_in.
+function run_io!(b::B200BatchedEuler, F_in::Union{Nothing,Matrix{Float64}}, nsteps::Integer,
+                 F_out::Matrix{Float64}=Matrix{Float64}(undef, b.n, b.capacity))
+    @assert size(F_out) == (b.n, b.capacity)
+    pin = F_in === nothing ? C_NULL : pointer(F_in)
+    GC.@preserve F_in F_out check(ccall((:dtb_batch_run_io, libdtb), Int32,
+                                        (Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{Float64}), b.ctx, pin, nsteps, F_out))
+    return F_out
+end
+
+# FP64 number and energy of every (species, cell, slot) (DistributionMoments.jl:33,145,162);
+# w: energy weight per momentum state.
+function batch_moments(b::B200BatchedEuler, w::Vector{Float64})
+    number = zeros(b.n_species, b.n_space, b.capacity)
+    energy = zeros(b.n_species, b.n_space, b.capacity)
+    check(ccall((:dtb_batch_moments, libdtb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                b.ctx, w, number, energy))
+    return number, energy
+end
+
+# The gain-GEMM plan of gain group `group` (1-based), or nothing past the last group.
+function gemm_plan(b::B200BatchedEuler, group::Integer=1)
+    pair = Ref{Int32}(0); bn = Ref{Int32}(0); ns = Ref{Int32}(0); us = Ref{Float64}(0)
+    rc = ccall((:dtb_batch_gemm_plan, libdtb), Int32,
+               (Ptr{Cvoid}, Int32, Ref{Int32}, Ref{Int32}, Ref{Int32}, Ref{Float64}), b.ctx, group - 1, pair, bn, ns, us)
+    rc == DTB_ENOTFOUND && return nothing
+    check(rc)
+    return (pair=pair[] != 0, bn=Int(bn[]), n_splits=Int(ns[]), tuned_us=us[])
+end
+
+# Plans measured in earlier runs are reused from `path`, new ones appended (nothing: forget).
+set_tune_cache(path::Union{Nothing,AbstractString}) =
+    check(ccall((:dtb_set_tune_cache, libdtb), Int32, (Cstring,), path === nothing ? C_NULL : path))
 
 end # module
