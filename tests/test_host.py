@@ -179,3 +179,15 @@ def test_julia_binding_calls_only_declared_exported_symbols():
         n_jl = len([a for a in argtypes.split(",") if a.strip()])
         assert n_jl == n_decl, (name, n_jl, n_decl)
         assert hasattr(lib, name), name
+
+
+def test_tune_cache_is_host_only(tmp_path):
+    """dtb_set_tune_cache needs no device: it loads a cache file (recorded lines and a file that
+    does not exist yet alike) and forgets the plans with NULL."""
+    L = _lib.load()
+    cache = tmp_path / "plans.txt"
+    cache.write_text("sm148:M512:N1256:n2256:cols256:cells1 1 256 37 37.267\n")
+    assert L.dtb_set_tune_cache(str(cache).encode()) == _lib.DTB_OK
+    assert L.dtb_set_tune_cache(str(tmp_path / "new.txt").encode()) == _lib.DTB_OK
+    assert L.dtb_set_tune_cache(None) == _lib.DTB_OK
+    assert not (tmp_path / "new.txt").exists()  # written only when a plan is measured
