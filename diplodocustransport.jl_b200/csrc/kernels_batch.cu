@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
 // The even CTA (rank 0) issues the MMAs for the pair. The odd CTA's producer warps arrive on the
 // even CTA's X barrier directly and one odd-CTA thread forwards the landing of each of its G
 // stages; the even CTA commits stage releases and the final accumulator to the barriers of
-// both. TMA multicast is not used.
+// both. Each CTA copies only its own tiles, from this GPU's memory, into its own shared memory.
 struct PairCfg {
     static constexpr int BN = 256;               // X columns of a pair (the MMA's N)
     static constexpr int HN = BN / 2;            // X columns staged by each CTA
