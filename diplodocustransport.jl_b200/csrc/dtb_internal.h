@@ -133,13 +133,23 @@ void set_error(const std::string& msg);
 // Kernel-level gain contraction of one block (gain_op.cu).
 cudaError_t launch_row_sums(const double* partial, int n_rows, int splits, double* out, cudaStream_t s);
 }  // namespace dtb
-#include <vector>
 namespace dtb {
-int gain_op_plan(int64_t n_out, int64_t n1, int64_t n2, int esz, int num_sms, int bps, std::vector<GainUnit>& units,
-                 int& splits);
+// Work split of one kernel-level gain contraction: n_out rows x `splits` b-ranges of `nb`
+// b-rows each, staged `tile_b` b-rows per tile.
+struct GainOpPlan {
+    int64_t n_units;
+    int splits;
+    int64_t nb;
+    int tile_b;
+};
+int gain_op_plan(int64_t n_out, int64_t n1, int64_t n2, int esz, int num_sms, int bps, GainOpPlan& plan);
 int gain_op_run(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2, const void* f1, const void* f2,
-                double* out, const std::vector<GainUnit>& units, int splits, unsigned char* scratch, int* err,
-                cudaStream_t s);
+                double* out, const GainOpPlan& plan, unsigned char* scratch, int* err, cudaStream_t s);
 size_t gain_op_scratch_bytes(int64_t n_units, int64_t n1, int64_t n2, int esz);
+// Common argument checks of the kernel-level entries (null pointers, dtype, alignment).
+int gain_op_check_args(const char* who, int32_t dtype, const void* G, const void* f1, const void* f2,
+                       const double* out);
+// Reads (synchronising `s`) and clears a kernel-level entry's device error flag.
+int gain_op_read_flag(const char* who, int* err, cudaStream_t s);
 
 }  // namespace dtb

@@ -37,18 +37,23 @@ void* g_scratch_dev[64] = {};  // device address of g_noalloc_scratch, per devic
 
 }  // namespace
 
+namespace dtb {
+// The device address of this entry's kernel error flag on `dev`, or nullptr before the entry's
+// set-up on that device (dtb_gain_contract_status reads it).
+int* noalloc_flag(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_scratch_dev[dev] ? reinterpret_cast<int*>(static_cast<unsigned char*>(g_scratch_dev[dev]) + kErrOffset)
+                              : nullptr;
+}
+}  // namespace dtb
+
 using namespace dtb;
 
 extern "C" int32_t dtb_gain_contract_noalloc(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2,
                                              const void* f1, const void* f2, double* out, void* stream) {
-    if (!G || !f1 || !f2 || !out) {
-        set_error("dtb_gain_contract_noalloc: null argument");
-        return DTB_EINVAL;
-    }
-    if (dtype != DTB_DTYPE_F64 && dtype != DTB_DTYPE_F32) {
-        set_error("dtb_gain_contract_noalloc: bad dtype");
-        return DTB_EINVAL;
-    }
+    int rc = gain_op_check_args("dtb_gain_contract_noalloc", dtype, G, f1, f2, out);
+    if (rc != DTB_OK) return rc;
     const int esz = dtype == DTB_DTYPE_F64 ? 8 : 4;
     if (n1 <= 0 || n2 <= 0 || n1 + n2 > kNoallocMaxVec) {
         set_error("dtb_gain_contract_noalloc: n1 + n2 must be at most " + std::to_string(kNoallocMaxVec) +
@@ -61,13 +66,12 @@ extern "C" int32_t dtb_gain_contract_noalloc(int32_t dtype, const void* G, int64
         return DTB_ENODEV;
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    std::vector<GainUnit> units;
-    int splits = 0;
+    GainOpPlan plan;
     const int f_len = (int)((n1 + 7) / 8 * 8 + n2);
-    int rc = gain_op_plan(n_out, n1, n2, esz, sms, gain_stream_blocks_per_sm(esz, f_len), units, splits);
+    rc = gain_op_plan(n_out, n1, n2, esz, sms, gain_stream_blocks_per_sm(esz, f_len), plan);
     if (rc != DTB_OK) return rc;
-    if ((int64_t)units.size() > kNoallocMaxUnits) {
-        set_error("dtb_gain_contract_noalloc: the block needs " + std::to_string(units.size()) +
+    if (plan.n_units > kNoallocMaxUnits) {
+        set_error("dtb_gain_contract_noalloc: the block needs " + std::to_string(plan.n_units) +
                   " work units; the static scratch holds at most " + std::to_string(kNoallocMaxUnits));
         return DTB_EINVAL;
     }
@@ -88,15 +92,10 @@ extern "C" int32_t dtb_gain_contract_noalloc(int32_t dtype, const void* G, int64
         }
         base = static_cast<unsigned char*>(g_scratch_dev[dev]);
     }
-    // the array keeps the previous call's contents: the error flag must start at zero; the
-    // work table, the partials and the staged vectors are fully rewritten by this call
+    // The array keeps the previous call's contents. gain_op_run clears the error flag first
+    // (in stream order) and then rewrites the work table, the partials and the staged vectors;
+    // it places the work table at base, the partials after it (both rounded to 256 bytes) and
+    // the staged f1|f2 after those, all within the regions sized above.
     int* err = reinterpret_cast<int*>(base + kErrOffset);
-    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), s);
-    if (e != cudaSuccess) {
-        set_error(std::string("dtb_gain_contract_noalloc: ") + cudaGetErrorString(e));
-        return DTB_ECUDA;
-    }
-    // gain_op_run places the work table at base, the partials after it (both rounded to 256
-    // bytes) and the staged f1|f2 after those; all three fit in the regions sized above
-    return gain_op_run(dtype, G, n_out, n1, n2, f1, f2, out, units, splits, base, err, s);
+    return gain_op_run(dtype, G, n_out, n1, n2, f1, f2, out, plan, base, err, s);
 }

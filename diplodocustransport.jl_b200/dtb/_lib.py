@@ -107,6 +107,9 @@ SIGNATURES = {
     "dtb_set_profiling": (_i32, [_P, _i32]),
     "dtb_selftest_bounded_wait": (_i32, [_P, _d]),
     "dtb_gain_contract": (_i32, [_i32, _P, _i64, _i64, _i64, _P, _P, _P, _P]),
+    "dtb_gain_contract_status": (_i32, [_P]),
+    "dtb_prepare": (_i32, [_P]),
+    "dtb_selftest_gain_contract_timeout": (_i32, [_i32, _d, _P]),
     "dtb_batch_admit": (_i32, [_P, _i32, _dp, _d, _i64]),
     "dtb_batch_run": (_i32, [_P, _i64]),
     "dtb_batch_get_f": (_i32, [_P, _i32, _dp]),

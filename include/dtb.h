@@ -163,6 +163,13 @@ int32_t dtb_commit(dtb_ctx* ctx);
 int32_t dtb_step(dtb_ctx* ctx, double t_start, double t_stop, double dt, int32_t verbose,
                  double* dt_out, int32_t* save_out, dtb_step_diag* diag_out);
 
+/* Captures, instantiates and uploads the CUDA graphs that dtb_run (Verbose = 0) or, for a
+ * batched context, dtb_batch_run replay, without running a step (commits first if needed).
+ * Optional: without it the first run long enough for a graph captures it. A caller that times
+ * its steps calls it once beforehand so no capture falls inside the timed steps. No
+ * counterpart in the reference (its Julia loop has no graphs). */
+int32_t dtb_prepare(dtb_ctx* ctx);
+
 /* nsteps steps with the given dt/dt0 values, replayed from captured CUDA graphs.
  * diag_hist (nullable) receives one dtb_step_diag per step. */
 int32_t dtb_run(dtb_ctx* ctx, const double* dt_scales, int64_t nsteps, int32_t verbose,
@@ -353,9 +360,27 @@ int32_t dtb_serve_destroy(dtb_server* srv);
  * out (n_out doubles) is a device vector. Runs asynchronously on `stream` (NULL: the legacy
  * default stream) on the current device. Its scratch (work table, per-unit partial sums and a
  * copy of f1|f2) is allocated on the first call on a device, grown when a larger block needs
- * more, and kept until the process exits. Calls on one device are serialised on the host. */
+ * more, and kept until the process exits. Calls on one device are serialised on the host.
+ * DTB_EINVAL when G is not 16-byte aligned, out not 8-byte aligned or f1, f2 not aligned to
+ * their element size. The call only enqueues work: a bounded device wait that gives up leaves
+ * `out` incomplete and is reported by dtb_gain_contract_status. */
 int32_t dtb_gain_contract(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2,
                           const void* f1, const void* f2, double* out, void* stream);
+
+/* Device-side status of the kernel-level entries (no counterpart in the reference, whose
+ * mul! calls report nothing): synchronises `stream`, then reads and clears the kernel error
+ * flags of dtb_gain_contract and dtb_gain_contract_noalloc on the current device. Each call of
+ * those entries clears its flag first, so the status covers the latest call of each entry on
+ * this device. DTB_ETIMEOUT when a bounded wait gave up (that call's `out` is incomplete),
+ * DTB_OK otherwise. */
+int32_t dtb_gain_contract_status(void* stream);
+
+/* Test hook (no counterpart in the reference): runs a kernel whose bounded wait on a flag that
+ * nothing sets gives up after limit_s seconds (0 < limit_s <= 2) and raises the timeout flag of
+ * dtb_gain_contract (noalloc = 0) or dtb_gain_contract_noalloc (noalloc = 1) on the current
+ * device, through the give-up path of the contraction's waits; DTB_ESTATE when that entry has
+ * not run on the device yet. */
+int32_t dtb_selftest_gain_contract_timeout(int32_t noalloc, double limit_s, void* stream);
 
 /* dtb_gain_contract for callers that cannot call cudaMalloc; it has no counterpart in the
  * reference. A host application that gives all device memory to its own pool allocator (a
@@ -369,7 +394,8 @@ int32_t dtb_gain_contract(int32_t dtype, const void* G, int64_t n_out, int64_t n
  * (set-up, once per device, with that device current); make that first call before any
  * stream capture. Every call on a device shares the one array and it keeps the last call's
  * contents (each call clears what must start at zero), so calls that overlap on the GPU
- * (different streams, no ordering between them) race; order them on one stream. */
+ * (different streams, no ordering between them) race; order them on one stream. Alignment
+ * rules and error reporting (dtb_gain_contract_status) are those of dtb_gain_contract. */
 int32_t dtb_gain_contract_noalloc(int32_t dtype, const void* G, int64_t n_out, int64_t n1, int64_t n2,
                                   const void* f1, const void* f2, double* out, void* stream);
 

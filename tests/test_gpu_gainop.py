@@ -51,3 +51,23 @@ def test_gain_contract_rejects_bad_shapes(cuda):
                              ctypes.c_void_p(out.data_ptr()), None)
     assert rc == _lib.DTB_EINVAL  # n2 = 12 is not a multiple of 8
     assert L.dtb_gain_contract(_lib.DTB_DTYPE_F32, None, 4, 4, 16, None, None, None, None) == _lib.DTB_EINVAL
+
+
+def test_gain_contract_status_reports_a_bounded_wait_that_gave_up(cuda):
+    """A timed-out wait of the contraction is reported by dtb_gain_contract_status, once: the
+    flag is raised through the same give-up path by a kernel whose wait runs out after 50 ms."""
+    import torch
+    L = _lib.load()
+    G = torch.rand(16, 8, 8, device="cuda", dtype=torch.float64)
+    f = torch.rand(8, device="cuda", dtype=torch.float64)
+    ref = _contract(G, f, f)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_OK
+    _lib.check(L.dtb_selftest_gain_contract_timeout(0, 0.05, s))
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_ETIMEOUT
+    assert b"gave up" in L.dtb_last_error()
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_OK  # read and cleared
+    # the next contraction starts from a clear flag and is correct
+    _lib.check(L.dtb_selftest_gain_contract_timeout(0, 0.05, s))
+    assert np.array_equal(_contract(G, f, f), ref)
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_OK

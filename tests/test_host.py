@@ -195,3 +195,18 @@ def test_tune_cache_is_host_only(tmp_path):
     assert L.dtb_set_tune_cache(str(tmp_path / "new.txt").encode()) == _lib.DTB_OK
     assert L.dtb_set_tune_cache(None) == _lib.DTB_OK
     assert not (tmp_path / "new.txt").exists()  # written only when a plan is measured
+
+
+def test_gain_contract_entries_refuse_misaligned_pointers_on_the_host():
+    """Both kernel-level entries check alignment before any CUDA call (no device needed): G must
+    be 16-byte aligned (bulk copies), out 8-byte aligned, f1 and f2 aligned to their element."""
+    import ctypes
+    from dtb import _lib
+    L = _lib.load()
+    P = ctypes.c_void_p
+    ok, g_bad, o_bad = P(0x10000), P(0x10008), P(0x10004)
+    for fn in (L.dtb_gain_contract, L.dtb_gain_contract_noalloc):
+        assert fn(_lib.DTB_DTYPE_F32, g_bad, 8, 8, 8, ok, ok, ok, None) == _lib.DTB_EINVAL
+        assert b"16-byte aligned" in L.dtb_last_error()
+        assert fn(_lib.DTB_DTYPE_F32, ok, 8, 8, 8, ok, ok, o_bad, None) == _lib.DTB_EINVAL
+        assert fn(_lib.DTB_DTYPE_F64, ok, 8, 8, 8, o_bad, ok, ok, None) == _lib.DTB_EINVAL

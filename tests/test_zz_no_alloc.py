@@ -76,3 +76,23 @@ def test_noalloc_rejects_blocks_beyond_the_static_limit(cuda):
     # too many work units: 40000 output rows of a 1-tile contraction
     rc = L.dtb_gain_contract_noalloc(_lib.DTB_DTYPE_F32, p, 40000, 8, 8, p, p, ctypes.c_void_p(out.data_ptr()), None)
     assert rc == _lib.DTB_EINVAL and b"work units" in L.dtb_last_error()
+
+
+def test_noalloc_reports_a_bounded_wait_that_gave_up(cuda):
+    """The allocation-free entry reports a timed-out wait through dtb_gain_contract_status like
+    the allocating one; its flag lives in the static array and the next call clears it."""
+    import torch
+    L = _lib.load()
+    G, f1, f2 = _inputs((64, 64, 64), torch.float64, 3)
+    out = torch.zeros(64, dtype=torch.float64, device="cuda")
+    ref = _call(L.dtb_gain_contract_noalloc, G, f1, f2, out)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_OK
+    free0 = torch.cuda.mem_get_info()[0]
+    _lib.check(L.dtb_selftest_gain_contract_timeout(1, 0.05, s))
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_ETIMEOUT
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_OK
+    _lib.check(L.dtb_selftest_gain_contract_timeout(1, 0.05, s))
+    assert np.array_equal(_call(L.dtb_gain_contract_noalloc, G, f1, f2, out), ref)
+    assert L.dtb_gain_contract_status(s) == _lib.DTB_OK
+    assert torch.cuda.mem_get_info()[0] == free0
