@@ -1,12 +1,15 @@
 // Serving loop: continuous batching of solve requests over batched (DTB_MIXED) contexts.
 //
-// Each registered grid is one batched context with its own stream. A library-owned host
-// thread repeatedly (1) admits queued requests into free slots of their grid, (2) launches a
-// chunk of batched steps on every grid that has running slots (the chunks of different grids
-// run concurrently on their streams), (3) waits for the chunks, reads back the f of every slot
-// whose steps are done and frees the slot. Requests that arrive meanwhile join at the next
+// Each registered grid is one batched context with its own stream, and each grid progresses
+// on its own: a library-owned host thread polls the grids and, for every grid whose previous
+// chunk has finished (an event on its stream), (1) reads back the f of every slot whose steps
+// are done and frees the slot, (2) admits queued requests into free slots, (3) launches the
+// next chunk of batched steps if the grid has running slots. Grids never wait for one another:
+// a small grid's requests are admitted and finished at its own chunk boundaries while a large
+// grid's chunk is still on the device. Requests that arrive meanwhile join at their grid's next
 // admission point, so work of different requests and grids overlaps on the device. Device
-// memory of all grids is checked against an HBM budget when a grid is registered.
+// memory of all grids (operators and every slot's state, allocated with the grid's context) is
+// checked against an HBM budget when a grid is registered.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -36,7 +39,6 @@ struct Request {
     int64_t n_steps = 0;
     int state = 0;          // 0 queued, 1 running, 2 done, 3 failed
     int slot = -1;
-    long long stop = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
     double cr_max = 0;
     int finite = 1;
@@ -45,8 +47,14 @@ struct Request {
 struct Grid {
     dtb_ctx* ctx = nullptr;
     int capacity = 0;
-    std::vector<int64_t> slot_req;  // request id per slot, -1 when free
-    std::deque<int64_t> queue;
+    // slot tables, written by the loop thread only (under the lock when they change)
+    std::vector<int64_t> slot_req;     // request id per slot, -1 when free
+    std::vector<long long> slot_stop;  // device step at which the slot's request is done
+    std::deque<int64_t> queue;         // guarded by the server lock
+    cudaEvent_t done_ev = nullptr;     // recorded after the grid's chunk in flight
+    bool in_flight = false;
+    double t_launch = 0;
+    int64_t chunk = 0;
     double ema_step_ms = 0.1;
     int n_running = 0;
 };
@@ -56,7 +64,7 @@ struct Grid {
 struct dtb_server {
     dtb_serve_opts opts{};
     std::vector<Grid> grids;
-    std::map<int64_t, Request> req;
+    std::map<int64_t, Request> req;  // guarded by mu; done requests are erased when collected
     int64_t next_id = 1;
     int64_t bytes = 0;
     std::mutex mu;
@@ -87,112 +95,150 @@ void fail(dtb_server* s, int rc) {
     s->cv_done.notify_all();
 }
 
+// Reads back and frees every slot of `g` whose request is done at the grid's current step.
+int complete_slots(dtb_server* s, Grid& g) {
+    const long long st = batch_step(g.ctx);
+    bool any = false;
+    for (int sl = 0; sl < g.capacity; ++sl) {
+        const int64_t id = g.slot_req[(size_t)sl];
+        if (id < 0 || st < g.slot_stop[(size_t)sl]) continue;
+        Request* r;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r = &s->req.at(id);  // not erased before it is done
+        }
+        int64_t done = 0, left = 0;
+        double cr = 0;
+        int32_t fin = 1;
+        int rc = dtb_batch_get_f(g.ctx, sl, r->f.data());
+        if (rc == DTB_OK) rc = dtb_batch_slot_info(g.ctx, sl, &done, &left, &cr, &fin);
+        if (rc == DTB_OK) rc = dtb_batch_release(g.ctx, sl);
+        if (rc != DTB_OK) return rc;
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->cr_max = cr;
+        r->finite = fin;
+        r->t_done = s->now();
+        r->state = 2;
+        g.slot_req[(size_t)sl] = -1;
+        g.n_running--;
+        s->steps_done += r->n_steps;
+        s->completed++;
+        any = true;
+    }
+    if (any) s->cv_done.notify_all();
+    return DTB_OK;
+}
+
+// Admits queued requests of `g` into its free slots (the grid has no chunk in flight).
+int admit_slots(dtb_server* s, Grid& g) {
+    std::vector<std::pair<int, Request*>> a;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (int sl = 0; sl < g.capacity && !g.queue.empty(); ++sl) {
+            if (g.slot_req[(size_t)sl] >= 0) continue;
+            const int64_t id = g.queue.front();
+            g.queue.pop_front();
+            Request& r = s->req.at(id);
+            r.slot = sl;
+            r.state = 1;
+            g.slot_req[(size_t)sl] = id;
+            g.n_running++;
+            a.push_back({sl, &r});
+        }
+    }
+    // uploads outside the lock: a running request is neither erased nor written by others, and
+    // its f0 and dt are fixed at submission
+    for (auto& sr : a) {
+        Request& r = *sr.second;
+        const long long stop = batch_step(g.ctx) + r.n_steps;
+        int rc = dtb_batch_admit(g.ctx, sr.first, r.f.data(), r.dt_scale, r.n_steps);
+        if (rc != DTB_OK) return rc;
+        g.slot_stop[(size_t)sr.first] = stop;
+        std::lock_guard<std::mutex> lk(s->mu);
+        r.t_admit = s->now();
+    }
+    return DTB_OK;
+}
+
+// Launches the next chunk of `g`: up to the earliest finishing request, capped at the target
+// device time per chunk so that arrivals are admitted promptly.
+int launch_chunk(dtb_server* s, Grid& g, int max_chunk, double target_ms) {
+    const long long st = batch_step(g.ctx);
+    long long left = (long long)1 << 60;
+    for (int sl = 0; sl < g.capacity; ++sl)
+        if (g.slot_req[(size_t)sl] >= 0) left = std::min(left, g.slot_stop[(size_t)sl] - st);
+    const int cap = std::max(1, std::min(max_chunk, (int)(target_ms / std::max(1e-3, g.ema_step_ms))));
+    g.chunk = std::max<long long>(1, std::min<long long>(left, cap));
+    DTB_TRY(batch_launch(g.ctx, g.chunk));
+    {
+        DeviceGuard dg(g.ctx->device);
+        DTB_CUDA(cudaEventRecord(g.done_ev, g.ctx->stream));
+    }
+    g.in_flight = true;
+    g.t_launch = s->now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->batched_steps += g.chunk;
+    return DTB_OK;
+}
+
 void loop(dtb_server* s) {
     const int max_chunk = s->opts.max_chunk_steps > 0 ? s->opts.max_chunk_steps : 256;
     const double target_ms = s->opts.chunk_ms > 0 ? s->opts.chunk_ms : 20.0;
+    double t_prev = s->now();
+    bool busy_prev = false;
     while (true) {
-        std::vector<std::pair<int, std::vector<std::pair<int, Request*>>>> admits;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             bool any = false;
-            for (auto& g : s->grids) any = any || g.n_running > 0 || !g.queue.empty();
+            for (auto& g : s->grids) any = any || g.in_flight || g.n_running > 0 || !g.queue.empty();
             if (!any && !s->stop) s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
             if (s->stop) return;
-            // (1) admission: queued requests into free slots
-            for (size_t gi = 0; gi < s->grids.size(); ++gi) {
-                Grid& g = s->grids[gi];
-                std::vector<std::pair<int, Request*>> a;
-                for (int sl = 0; sl < g.capacity && !g.queue.empty(); ++sl) {
-                    if (g.slot_req[(size_t)sl] >= 0) continue;
-                    const int64_t id = g.queue.front();
-                    g.queue.pop_front();
-                    Request& r = s->req[id];
-                    r.slot = sl;
-                    r.state = 1;
-                    g.slot_req[(size_t)sl] = id;
-                    g.n_running++;
-                    a.push_back({sl, &r});
-                }
-                if (!a.empty()) admits.push_back({(int)gi, std::move(a)});
-            }
         }
-        // admission uploads outside the lock (requests stay valid: the map only grows, entries
-        // are erased by nobody while the server runs)
-        for (auto& ga : admits) {
-            Grid& g = s->grids[(size_t)ga.first];
-            for (auto& sr : ga.second) {
-                Request& r = *sr.second;
-                int rc = dtb_batch_admit(g.ctx, sr.first, r.f.data(), r.dt_scale, r.n_steps);
-                if (rc != DTB_OK) return fail(s, rc);
-                r.t_admit = s->now();
-                r.stop = batch_step(g.ctx) + r.n_steps;
-            }
-        }
-        // (2) a chunk of batched steps on every grid with running slots
-        std::vector<int> launched;
-        std::vector<int64_t> chunks;
-        const double t_start = s->now();
-        for (size_t gi = 0; gi < s->grids.size(); ++gi) {
-            Grid& g = s->grids[gi];
-            if (g.n_running == 0) continue;
-            long long left = (long long)1 << 60;
-            const long long st = batch_step(g.ctx);
-            for (int sl = 0; sl < g.capacity; ++sl) {
-                const int64_t id = g.slot_req[(size_t)sl];
-                if (id >= 0) left = std::min(left, s->req[id].stop - st);
-            }
-            const int cap = std::max(1, std::min(max_chunk, (int)(target_ms / std::max(1e-3, g.ema_step_ms))));
-            const int64_t chunk = std::max<long long>(1, std::min<long long>(left, cap));
-            int rc = batch_launch(g.ctx, chunk);
-            if (rc != DTB_OK) return fail(s, rc);
-            launched.push_back((int)gi);
-            chunks.push_back(chunk);
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->batched_steps += chunk;
-        }
-        // (3) completions
-        for (size_t li = 0; li < launched.size(); ++li) {
-            Grid& g = s->grids[(size_t)launched[li]];
-            int rc = batch_finish(g.ctx);
-            if (rc != DTB_OK) return fail(s, rc);
-            const double t_end = s->now();
-            // device time per batched step of this grid (an upper bound while grids overlap)
-            g.ema_step_ms = 0.7 * g.ema_step_ms + 0.3 * (1e3 * (t_end - t_start) / (double)chunks[li]);
-            const long long st = batch_step(g.ctx);
-            for (int sl = 0; sl < g.capacity; ++sl) {
-                const int64_t id = g.slot_req[(size_t)sl];
-                if (id < 0) continue;
-                Request* r;
+        bool progressed = false;
+        for (auto& g : s->grids) {
+            if (g.in_flight) {
+                cudaError_t q;
                 {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    r = &s->req[id];
+                    DeviceGuard dg(g.ctx->device);
+                    q = cudaEventQuery(g.done_ev);
                 }
-                if (st < r->stop) continue;
-                int64_t done = 0, left = 0;
-                double cr = 0;
-                int32_t fin = 1;
-                rc = dtb_batch_get_f(g.ctx, sl, r->f.data());
-                if (rc == DTB_OK) rc = dtb_batch_slot_info(g.ctx, sl, &done, &left, &cr, &fin);
-                if (rc == DTB_OK) rc = dtb_batch_release(g.ctx, sl);
+                if (q == cudaErrorNotReady) continue;
+                g.in_flight = false;
+                int rc = batch_finish(g.ctx);  // the chunk is done: reads its error flag
                 if (rc != DTB_OK) return fail(s, rc);
-                std::lock_guard<std::mutex> lk(s->mu);
-                r->cr_max = cr;
-                r->finite = fin;
-                r->t_done = s->now();
-                r->state = 2;
-                g.slot_req[(size_t)sl] = -1;
-                g.n_running--;
-                s->steps_done += r->n_steps;
-                s->completed++;
-                (void)t_end;
+                // device time per batched step of this grid (an upper bound while grids overlap)
+                g.ema_step_ms = 0.7 * g.ema_step_ms + 0.3 * (1e3 * (s->now() - g.t_launch) / (double)g.chunk);
+                rc = complete_slots(s, g);
+                if (rc != DTB_OK) return fail(s, rc);
+                progressed = true;
             }
-            s->cv_done.notify_all();
+            bool queued;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                queued = !g.queue.empty();
+            }
+            if (queued && g.n_running < g.capacity) {
+                int rc = admit_slots(s, g);
+                if (rc != DTB_OK) return fail(s, rc);
+            }
+            if (g.n_running > 0) {
+                int rc = launch_chunk(s, g, max_chunk, target_ms);
+                if (rc != DTB_OK) return fail(s, rc);
+                progressed = true;
+            }
         }
-        if (!launched.empty()) {
-            const double dt = s->now() - t_start;
+        // busy time: intervals during which some grid had a chunk on the device
+        bool busy = false;
+        for (auto& g : s->grids) busy = busy || g.in_flight;
+        const double t = s->now();
+        if (busy_prev) {
             std::lock_guard<std::mutex> lk(s->mu);
-            s->busy_s += dt;
+            s->busy_s += t - t_prev;
         }
+        t_prev = t;
+        busy_prev = busy;
+        // nothing finished: give the device a moment before polling the events again
+        if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
 }
 
@@ -220,11 +266,16 @@ int32_t dtb_serve_add_grid(dtb_server* s, dtb_ctx* ctx, int32_t* grid_id) {
                   std::to_string(s->opts.hbm_budget_bytes - s->bytes) + " of the HBM budget are left");
         return DTB_ENOMEM;
     }
-    s->bytes += b;
     Grid g;
     g.ctx = ctx;
     g.capacity = batch_capacity(ctx);
     g.slot_req.assign((size_t)g.capacity, -1);
+    g.slot_stop.assign((size_t)g.capacity, 0);
+    {
+        DeviceGuard dg(ctx->device);
+        DTB_CUDA(cudaEventCreateWithFlags(&g.done_ev, cudaEventDisableTiming));
+    }
+    s->bytes += b;
     s->grids.push_back(std::move(g));
     *grid_id = (int32_t)s->grids.size() - 1;
     return DTB_OK;
@@ -290,6 +341,7 @@ int32_t dtb_serve_wait(dtb_server* s, int64_t request_id, double timeout_s, doub
         st->finite = r.finite;
         st->grid = r.grid;
     }
+    s->req.erase(it);  // collected: the id is unknown from now on
     return DTB_OK;
 }
 
@@ -320,6 +372,12 @@ int32_t dtb_serve_destroy(dtb_server* s) {
         s->cv_work.notify_all();
     }
     if (s->th.joinable()) s->th.join();
+    for (auto& g : s->grids) {
+        if (!g.done_ev) continue;
+        DeviceGuard dg(g.ctx->device);
+        if (g.in_flight) cudaEventSynchronize(g.done_ev);  // the caller may destroy the context next
+        cudaEventDestroy(g.done_ev);
+    }
     delete s;
     return DTB_OK;
 }
