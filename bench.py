@@ -1,6 +1,6 @@
 """Benchmark of the explicit Euler step on B200 (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K (2000)] [--warmup W (5; at least 32 are run)] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K (2000)] [--warmup W (5)] [--impl ours|reference]
                     [--config 2|3|0|1|4]
 
 Workload (default, --config 2): batching, 256 independent instances on one grid of two
@@ -22,6 +22,14 @@ call and one wait per step).
 roofline: the gain GEMM (dominant), algorithmic FLOPs = 3 MMAs x 2 x M x K x instances per
 step (tensor-bound; config 3: operator bytes, HBM-bound), duration from CUDA events around
 every GEMM launch over a second run of the same steps.
+plain_fp64: one instance of the same grid on the plain FP64 path (graphs prepared, the same
+W warm-up and K timed steps), with its gain kernel's HBM roofline.
+accuracy: every instance re-run over the configuration's run length (10,000 steps for config
+2, 5,000 for config 3); three instances compared with the plain FP64 path over the same steps,
+with FP64 number and energy moments (drift of both paths, and the mixed path's error against
+FP64); also a W-step comparison with the FP64 oracle itself.
+serving (default run): 200 requests per GPU of config 4's grids and request mix at 0.7 of the
+full-occupancy capacity, routed across GPUs; p50/p99 time to solution (tts_p50_s, tts_p99_s).
 cpu_baseline / --impl reference: the FP64 oracle port timed on the host cores with OpenMP on
 one instance for a few steps, scaled to instance-steps/s.
 """
@@ -40,7 +48,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "diplodocustransport.jl_b200"))
 
 METRIC = "steps/s & p99 latency, batched BF16-split vs plain FP64, at ≤1e-5 rel err"
-GRAPH_WARMUP = 32  # two captured graphs of 16 steps
 
 
 def _env_rank():
@@ -232,7 +239,8 @@ def run_reference(args):
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "instance-steps/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": _config_dict(args.config, w),
+                "data": "synthetic (seeded; no collision data files)", "config": _config_dict(args.config, w, world),
+                "precision": "FP64 oracle port (C, OpenMP): FP64 operators and state",
                 "cpu_baseline": {"value": value, "unit": "instance-steps/s", "cores": cores, "kind": "port",
                                  "sample": desc},
                 "e2e": {"value": value, "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
@@ -245,8 +253,9 @@ def run_reference(args):
     value = v
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": _config_dict(args.config, w),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no collision data files)",
+            "config": _config_dict(args.config, w, world),
+            "precision": "FP64 oracle port (C, OpenMP): FP64 operators and state",
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -261,28 +270,31 @@ def _has_cuda():
         return False
 
 
-def _config_dict(config: int, w):
+def _config_dict(config: int, w, world: int = 1):
+    """The workload description; both arms (--impl ours / reference) print the same object."""
     sizes = w.ps.species_sizes
     if config == 2:
         return {"workload": "batching (config 2): 256 independent instances, 2 species x 256 states "
-                            "(32 log p x 8 u), shared G 2 x 256 x 65536 as BF16 hi+lo, per-instance f0 and dt",
-                "species_states": sizes, "batch": 256, "precision": "BF16x3 gain GEMM, FP32 f, FP64 update",
-                "l2": "G hi+lo 134 MB per step, larger than L2"}
+                            "(32 log p x 8 u), shared G 2 x 256 x 65536, per-instance f0 and dt",
+                "species_states": sizes, "batch": 256, "run_length_steps": 10000,
+                "l2": "G hi+lo 134 MB per step, larger than L2", "parallelism": f"batch replicas x{world}"}
     if config == 3:
         return {"workload": "mixed precision (config 3): 64 instances, e-, e+, gamma x 576 states "
-                            "(48 log p x 12 u), 6 gain tensors 576 x 331776 as BF16 hi+lo, synchrotron-like emission",
-                "species_states": sizes, "batch": 64, "precision": "BF16x3 gain GEMM, FP32 f, FP64 update",
-                "l2": "G hi+lo 4.6 GB per step, larger than L2"}
+                            "(48 log p x 12 u), 6 gain tensors 576 x 331776, synchrotron-like emission",
+                "species_states": sizes, "batch": 64, "run_length_steps": 5000,
+                "l2": "G hi+lo 4.6 GB per step, larger than L2", "parallelism": f"batch replicas x{world}"}
     if config == 1 and sizes != [1024, 1024]:
-        return {"workload": f"config-1 recipe on a smaller grid: 2 species x {sizes[0]} states, FP32",
-                "species_states": sizes, "precision": "FP32"}
+        return {"workload": f"config-1 recipe on a smaller grid: 2 species x {sizes[0]} states",
+                "species_states": sizes, "parallelism": f"replicas x{world}"}
     if config == 1:
         return {"workload": "plain single instance (config 1): 2 species x 1024 states (64 log p x 16 u), "
-                            "FP32 gain 2 x 1024 x 1048576, 2000-step run shape",
-                "species_states": sizes, "precision": "FP32", "l2": "inputs larger than L2 (8.6 GB gain)"}
-    return {"workload": "plain single instance (config 0): 2 species x 128 states (16 log p x 8 u), FP64",
-            "species_states": sizes, "precision": "FP64",
-            "l2": "operators (34 MB) fit in L2; no flush between steps (launch/L2-bound case)"}
+                            "gain 2 x 1024 x 1048576, 2000-step run shape",
+                "species_states": sizes, "l2": "inputs larger than L2 (8.6 GB gain)",
+                "parallelism": f"replicas x{world}"}
+    return {"workload": "plain single instance (config 0): 2 species x 128 states (16 log p x 8 u)",
+            "species_states": sizes,
+            "l2": "operators (34 MB) fit in L2; no flush between steps (launch/L2-bound case)",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_ours(args):
@@ -308,10 +320,10 @@ def run_ours(args):
     w.binm.gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, None) for g in w.binm.gains]
     torch.cuda.empty_cache()
     L = m.L
-    # warm-up: at least two graphs' worth of steps, so the 16-step graph is captured and
-    # instantiated before the timed region
-    K, W = args.steps, max(args.warmup, GRAPH_WARMUP)
+    # graphs captured and uploaded first, then exactly W warm-up steps
+    K, W = args.steps, args.warmup
     scales = np.ones(K)
+    m.prepare()
     m.run(np.ones(W))
     lps = _lib.ctypes.c_int32()
     L.dtb_launches_per_step(m.ctx, _lib.ctypes.byref(lps))
@@ -365,7 +377,8 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": dtype, "data": "synthetic (seeded; no collision data files)",
-            "config": dict(_config_dict(args.config, w), parallelism=f"replicas x{world}"),
+            "config": _config_dict(args.config, w, world),
+            "precision": "FP32 operators and state" if dtype == "f32" else "FP64 operators and state",
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": n * esz,
                     "d2h_bytes_per_step": n * esz, "wall_s": t_wall},
             "gpu_launches": int(lps.value) * K,
@@ -387,6 +400,89 @@ def run_ours(args):
     return 0
 
 
+def _plain_leg(plain, stream, dt: float, K: int, W: int, hbm: float):
+    """Plain FP64 single instance on the batched grid: graphs prepared, W warm-up steps, K timed
+    steps (CUDA events on the library's stream), then K steps with the gain kernel timed per
+    launch for its HBM roofline. Returns the plain leg's JSON object."""
+    import numpy as np
+    import torch
+    from dtb import _lib
+    plain.prepare()
+    plain.run(np.full(W, dt))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain.run(np.full(K, dt))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    L = plain.L
+    L.dtb_set_profiling(plain.ctx, 1)
+    plain.run(np.full(K, dt))
+    avg_ms, bpl = _lib.ctypes.c_double(), _lib.ctypes.c_double()
+    L.dtb_gain_kernel_stats(plain.ctx, _lib.ctypes.byref(avg_ms), _lib.ctypes.byref(bpl))
+    L.dtb_set_profiling(plain.ctx, 0)
+    step_ms = ms / K
+    gbs_kernel = bpl.value / (avg_ms.value / 1e3) / 1e9 if avg_ms.value > 0 else None
+    gbs_step = bpl.value / (step_ms / 1e3) / 1e9
+    return {"value": 1e3 / step_ms, "unit": "steps/s", "ms_per_step": step_ms, "steps": K, "warmup": W,
+            "workload": "same grid, one instance, FP64 (gain_stream + euler_rows per step)",
+            "roofline": {"bound": "hbm", "kernel": "gain_stream<double>", "unit": "GB/s",
+                         "algorithmic_bytes_per_step": bpl.value, "avg_launch_ms": avg_ms.value,
+                         "achieved": gbs_kernel, "frac": gbs_kernel / hbm if gbs_kernel else None,
+                         "step_achieved": gbs_step, "step_frac": gbs_step / hbm, "peak": hbm}}
+
+
+def _accuracy_leg(m, w, plain, n_steps: int, inst, oracle_ops=None):
+    """Full-length accuracy of the batched mixed path: every slot re-admitted with its f0 and
+    run n_steps; the instances `inst` compared with the plain FP64 GPU path over the same steps
+    (relative L-inf), and FP64 device moments (number, energy per species) before and after for
+    both, giving each path's drift |S(T) - S(0)| / S(0) and the mixed path's conservation error
+    |S_mixed(T) - S_fp64(T)| / S(0). With oracle_ops, instance inst[0] is also run on the FP64
+    oracle (host) over the same steps."""
+    import numpy as np
+    from dtb.structs import energy_weights
+    B = w.f0.shape[0]
+    for i in range(B):
+        m.admit(i, w.f0[i], float(w.dt[i]), n_steps)
+    wts = energy_weights(w.ps)
+    num0, en0 = m.moments(wts)
+    m.run(n_steps)
+    num1, en1 = m.moments(wts)
+    errs, drift = {}, []
+    for i in inst:
+        plain.f = w.f0[i]
+        plain.run(np.full(n_steps, float(w.dt[i])))
+        ref = plain.f
+        got = m.get_f(i)
+        errs[str(i)] = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+        pn, pe = plain.moments(wts)
+        pn, pe = np.asarray(pn)[0], np.asarray(pe)[0]
+        drift.append({
+            "instance": i,
+            "number_drift_mixed": (np.abs(num1[i] - num0[i]) / num0[i]).tolist(),
+            "number_drift_fp64": (np.abs(pn - num0[i]) / num0[i]).tolist(),
+            "energy_drift_mixed": (np.abs(en1[i] - en0[i]) / en0[i]).tolist(),
+            "energy_drift_fp64": (np.abs(pe - en0[i]) / en0[i]).tolist(),
+            "number_error_mixed_vs_fp64": (np.abs(num1[i] - pn) / num0[i]).tolist(),
+            "energy_error_mixed_vs_fp64": (np.abs(en1[i] - pe) / en0[i]).tolist()})
+    out = {"steps": n_steps, "instances": list(inst), "rel_linf_vs_fp64": max(errs.values()),
+           "rel_linf_per_instance": errs,
+           "reference": "plain FP64 GPU path, same f0 and dt (FP64 oracle parity <= 1e-12 in tests)",
+           "tolerance": 1e-5, "moments": drift,
+           "max_number_error_mixed_vs_fp64": max(max(d["number_error_mixed_vs_fp64"]) for d in drift),
+           "max_energy_error_mixed_vs_fp64": max(max(d["energy_error_mixed_vs_fp64"]) for d in drift)}
+    if oracle_ops is not None:
+        i = inst[0]
+        f = np.array(w.f0[i])
+        for _ in range(n_steps):
+            f, _, _ = oracle_ops.step(f, float(w.dt[i]), 0)
+        got = m.get_f(i)
+        out["oracle"] = {"instance": i, "steps": n_steps,
+                         "rel_linf_mixed_vs_oracle": float(np.max(np.abs(got - f)) / np.max(np.abs(f)))}
+    return out
+
+
 def run_batched(args):
     import numpy as np
     import torch
@@ -405,9 +501,7 @@ def run_batched(args):
     w = build_batched(args.config, dev)
     B = w.f0.shape[0]
     n = w.ps.n_state
-    # warm-up: at least two graphs' worth of steps (the 16-step graph is captured and instantiated
-    # before the timed region)
-    K, W = args.steps, max(args.warmup, GRAPH_WARMUP)
+    K, W = args.steps, args.warmup
     stream = torch.cuda.Stream()
     m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B, device=local, stream=stream.cuda_stream)
     for i in range(B):
@@ -415,13 +509,13 @@ def run_batched(args):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_sample_batched(w, budget_s=15.0)
-    # accuracy against the FP64 oracle: W warm-up steps of two instances
-    acc = None
+    ops = None
     if rank == 0 and not args.no_check:
         import oracle
         gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, g.G.double().cpu().numpy()) for g in w.binm.gains]
         ops = oracle.BlockedOperands(w.ps.species_sizes, 1, gains, w.binm.losses, w.emim.blocks, w.fluxm.F_Flux,
                                      1.0 / np.asarray(w.fluxm.Ap_Flux), w.fluxm.Vol, w.inj)
+        del gains
     # plain FP64 path on the same grid (one instance), for the batched-vs-plain comparison
     gains64 = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, g.G.double()) for g in w.binm.gains]
     from dtb.structs import BinaryMatrices
@@ -431,8 +525,11 @@ def run_batched(args):
     del gains64, binm64
     w.binm.gains = [type(g)(g.out_sp, g.in1_sp, g.in2_sp, None) for g in w.binm.gains]
     torch.cuda.empty_cache()
-    m.run(W)  # warm-up (captures and instantiates the graphs)
-    if rank == 0 and not args.no_check:
+    # graphs captured and uploaded before any step, then exactly W warm-up steps
+    m.prepare()
+    m.run(W)
+    acc_short = None
+    if ops is not None:
         errs = []
         for i in (0, B - 1):
             f = np.array(w.f0[i])
@@ -440,8 +537,7 @@ def run_batched(args):
                 f, _, _ = ops.step(f, float(w.dt[i]), 0)
             g = m.get_f(i)
             errs.append(float(np.max(np.abs(g - f)) / np.max(np.abs(f))))
-        acc = {"rel_linf_vs_fp64_oracle": max(errs), "steps": W, "instances": [0, B - 1]}
-        del ops
+        acc_short = {"rel_linf_vs_fp64_oracle": max(errs), "steps": W, "instances": [0, B - 1]}
     # ---- timed region: graph replay, device resident
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
@@ -466,38 +562,41 @@ def run_batched(args):
     while (pl := m.gemm_plan(len(plans))) is not None:
         plans.append(pl)
     m.set_profiling(False)
-    # ---- e2e: the whole batch state from pinned host memory in and out every step
+    # ---- e2e: the whole batch state from pinned host memory in and out every step, K steps
     Fh = torch.empty((B, n), dtype=torch.float64).pin_memory().numpy()
     m.get_f_all(Fh)
-    K2 = max(1, K // 4)
+    m.run_io(Fh, 1, Fh)  # the 1-step graphs of both state buffers are warm
+    m.run_io(Fh, 1, Fh)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
-    for _ in range(K2):
+    for _ in range(K):
         m.run_io(Fh, 1, Fh)  # upload, one batched step, download: one call, one wait
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
+    pj = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = float(pj.get("hbm_gbs", 6650.0))
     # ---- plain FP64 single instance on the same grid
-    K3 = max(16, K // 4)
-    plain.run(np.ones(4))
-    e6, e7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e6.record(stream)
-    plain.run(np.full(K3, float(w.dt[0])))
-    e7.record(stream)
-    torch.cuda.synchronize()
-    ms_plain = e6.elapsed_time(e7)
+    plain_line = _plain_leg(plain, stream, float(w.dt[0]), K, W, hbm)
+    ms_plain = plain_line["ms_per_step"] * K
+    # ---- accuracy and drift over the configuration's full run length
+    acc = None
+    if rank == 0 and not args.no_check:
+        L_run = args.check_steps if args.check_steps is not None else int(w.n_steps)
+        acc = _accuracy_leg(m, w, plain, L_run, [0, B // 2, B - 1], ops if args.oracle_long else None)
+        acc["short_run_vs_oracle"] = acc_short
     plain.close()
     if world > 1:
         t = torch.tensor([ms, ms_e2e, ms_plain], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e, ms_plain = float(t[0]), float(t[1]), float(t[2])
     value = world * B * K / (ms / 1e3)
-    plain_sps = world * K3 / (ms_plain / 1e3)
-    pj = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    plain_sps = world * K / (ms_plain / 1e3)
+    plain_line["value"] = plain_sps
     peak = float(pj.get("bf16_tflops", 1590.0))
     peak_s = float(pj.get("bf16_tflops_sustained", 1400.0))
     achieved = st["flops_per_step"] / (st["avg_ms"] / 1e3) / 1e12 if st["avg_ms"] > 0 else None
@@ -506,7 +605,6 @@ def run_batched(args):
     GEMM_LABEL = ("gain_gemm_pair (tcgen05.mma.cta_group::2, BF16 hi+lo x3)" if all(p["pair"] for p in plans)
                   else "gain_gemm (tcgen05, BF16 hi+lo x3)")
     # the GEMM's bound: the slower of its tensor time and its operator-streaming time
-    hbm = float(pj.get("hbm_gbs", 6650.0))
     hbm_bound = st["bytes_per_step"] / (hbm * 1e9) > st["flops_per_step"] / (peak * 1e12)
     if hbm_bound:
         gbs = st["bytes_per_step"] / (st["avg_ms"] / 1e3) / 1e9 if st["avg_ms"] > 0 else None
@@ -524,12 +622,13 @@ def run_batched(args):
     line = {"metric": METRIC, "value": value, "unit": "instance-steps/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16x3 (gain GEMM), f32 state, f64 update", "data": "synthetic (seeded; no collision data files)",
-            "config": dict(_config_dict(args.config, w), parallelism=f"batch replicas x{world}"),
-            "e2e": {"value": world * B * K2 / (ms_e2e / 1e3), "unit": "instance-steps/s",
-                    "h2d_bytes_per_step": B * n * 8, "d2h_bytes_per_step": B * n * 8},
+            "config": _config_dict(args.config, w, world),
+            "precision": "BF16 hi+lo gain (3 MMAs, FP32 accumulation), FP32 f, FP64 compensated update",
+            "e2e": {"value": world * B * K / (ms_e2e / 1e3), "unit": "instance-steps/s",
+                    "h2d_bytes_per_step": B * n * 8, "d2h_bytes_per_step": B * n * 8, "steps": K},
             "gpu_launches": int(st["launches_per_step"]) * K + (K + 15) // 16,  # + one step-counter advance per graph
             "roofline": roof,
-            "plain_fp64": {"value": plain_sps, "unit": "steps/s", "workload": "same grid, one instance, FP64"},
+            "plain_fp64": plain_line,
             "speedup_vs_plain_fp64": value / plain_sps,
             "clocks": cs.summary()}
     if acc is not None:
@@ -539,6 +638,15 @@ def run_batched(args):
         line["cpu_baseline"] = {"value": v, "unit": "instance-steps/s", "cores": cores, "kind": "port",
                                 "sample": desc}
     m.close()
+    torch.cuda.empty_cache()
+    if args.config == 2 and args.serve_requests > 0:
+        # the metric's p99: a served stream (config 4's grids and request mix) at 0.7 of capacity
+        setup = _serving_grids(local, args.capacity)
+        sv = _serving_leg(rank, world, local, args.serve_requests, 0.7, args.capacity, 45, setup)
+        for b in setup[1]:
+            b.close()
+        line["tts_p50_s"], line["tts_p99_s"] = sv["tts_p50_s"], sv["tts_p99_s"]
+        line["serving"] = sv
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -550,106 +658,182 @@ def run_batched(args):
 SERVE_GRIDS = [(16, 8), (32, 8), (32, 16), (64, 16)]
 
 
-def run_serving(args):
-    """Config 4: a Poisson stream of solve requests over four grids, served with continuous
-    batching; p50/p99 time-to-solution and aggregate instance-steps/s, beside the same stream
-    one at a time on the plain FP64 path (FIFO single server with per-grid FP64 step times
-    measured here)."""
+def _serving_grids(local: int, capacity: int):
+    """The four served grids (2 species each, seeded operators): one batched context per grid
+    with `capacity` slots, the batched step time of each grid with every slot running, and the
+    plain FP64 step time of one instance (the one-at-a-time comparison)."""
     import numpy as np
     import torch
     from dtb import synth
     from dtb.batch import BatchedEuler
-    from dtb.serve import Server
     from dtb.stepping import ForwardEulerStruct
     from dtb.structs import BinaryMatrices
-    rank, local, world = _env_rank()
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local)
-    if args.tune_cache:
-        from dtb.batch import set_tune_cache
-        set_tune_cache(args.tune_cache)
-    rng = np.random.default_rng(44)
-    n_req = args.requests
-    rate = args.rate
-    grids, batched, step_ms_fp64 = [], [], []
-    srv = Server(hbm_budget_bytes=150 * 10**9)
-    gids = []
+    grids, batched, t_full_ms, step_ms_fp64 = [], [], [], []
     for g, (p, u) in enumerate(SERVE_GRIDS):
         w = synth.two_species(p, 1e-2, 1e2, u, seed=100 + g, gain_on_device=True, device=f"cuda:{local}")
-        b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, args.capacity, device=local)
-        gids.append(srv.add_grid(b))
-        # plain FP64 step time of this grid (one instance), for the one-at-a-time comparison
+        stream = torch.cuda.Stream()
         gains64 = [type(x)(x.out_sp, x.in1_sp, x.in2_sp, x.G.double()) for x in w.binm.gains]
-        ps_stream = torch.cuda.Stream()
         pl = ForwardEulerStruct(w.ps, w.f0, w.inj, BinaryMatrices(gains=gains64, losses=w.binm.losses), w.emim,
-                                w.fluxm, Precision=np.float64, device=local, stream=ps_stream.cuda_stream)
+                                w.fluxm, Precision=np.float64, device=local, stream=stream.cuda_stream)
         del gains64
-        pl.run(np.ones(8))
-        K = 200 if p * u <= 256 else 50
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(ps_stream)
+        pl.prepare()
+        pl.run(np.ones(4))
+        K = 200 if p * u <= 256 else 48
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
         pl.run(np.ones(K))
-        t1.record(ps_stream)
+        t1.record(stream)
         torch.cuda.synchronize()
         step_ms_fp64.append(t0.elapsed_time(t1) / K)
         pl.close()
+        torch.cuda.empty_cache()
+        b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, capacity, device=local, stream=stream.cuda_stream)
         w.binm.gains = []
         torch.cuda.empty_cache()
+        # full occupancy: every slot running
+        for sl in range(capacity):
+            b.admit(sl, w.f0, 1.0, 1 << 40)
+        b.prepare()
+        b.run(3)
+        Kb = 48 if p * u >= 1024 else 160
+        t0.record(stream)
+        b.run(Kb)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        t_full_ms.append(t0.elapsed_time(t1) / Kb)
+        for sl in range(capacity):
+            b.release(sl)
         grids.append(w)
         batched.append(b)
-    # the request stream
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
-    gsel = rng.integers(0, len(SERVE_GRIDS), size=n_req)
-    steps = rng.integers(500, 20001, size=n_req)
-    mus = rng.uniform(-1, 1, size=n_req)
-    dts = rng.uniform(0.5, 1.0, size=n_req)
-    f0s = [synth.lognormal_f0(grids[g].ps, [mu, mu], 1.0) for g, mu in zip(gsel, mus)]
+    return grids, batched, t_full_ms, step_ms_fp64
+
+
+def _request_stream(n: int, rate: float, seed: int, rng_grids: int):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return {"arrivals": np.cumsum(rng.exponential(1.0 / rate, size=n)),
+            "grid": rng.integers(0, rng_grids, size=n), "steps": rng.integers(500, 20001, size=n),
+            "mu": rng.uniform(-1, 1, size=n), "dt": rng.uniform(0.5, 1.0, size=n)}
+
+
+def _serve_share(batched, grids, stream, mine, budget):
+    """Serves the requests `mine` (global indices into `stream`) on this GPU with continuous
+    batching, submitting each at its arrival time; one record per request."""
+    import numpy as np
+    from dtb import synth
+    from dtb.serve import Server
+    srv = Server(hbm_budget_bytes=budget)
+    gids = [srv.add_grid(b) for b in batched]
+    f0s = {k: synth.lognormal_f0(grids[stream["grid"][k]].ps, [stream["mu"][k]] * 2, 1.0) for k in mine}
     srv.start()
     t_start = time.perf_counter()
     rids = []
-    for k in range(n_req):
-        delay = arrivals[k] - (time.perf_counter() - t_start)
+    for k in mine:
+        delay = stream["arrivals"][k] - (time.perf_counter() - t_start)
         if delay > 0:
             time.sleep(delay)
-        rids.append(srv.submit(gids[gsel[k]], f0s[k], float(dts[k]), int(steps[k])))
+        rids.append(srv.submit(gids[stream["grid"][k]], f0s[k], float(stream["dt"][k]), int(stream["steps"][k])))
     infos = [srv.wait(r, timeout_s=3600, with_f=False)[1] for r in rids]
     st = srv.stats()
     srv.close()
-    for b in batched:
-        b.close()
-    tts = np.array([i["t_done"] - i["t_submit"] for i in infos])
-    t_first = min(i["t_submit"] for i in infos)
-    t_last = max(i["t_done"] for i in infos)
-    total = int(steps.sum())
-    agg = total / (t_last - t_first)
-    # one at a time on the plain FP64 path: FIFO single server over the same arrivals
-    svc = np.array([steps[k] * step_ms_fp64[gsel[k]] / 1e3 for k in range(n_req)])
-    free_at, tts_plain, done_plain = 0.0, [], []
-    for k in range(n_req):
-        start = max(free_at, arrivals[k])
-        free_at = start + svc[k]
-        tts_plain.append(free_at - arrivals[k])
-    agg_plain = total / (free_at - arrivals[0])
-    line = {"metric": METRIC, "value": agg, "unit": "instance-steps/s", "n_gpus": 1, "steps": total,
-            "warmup": 0, "ms_per_step": 1e3 / agg, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16x3 (gain GEMM), f32 state, f64 update",
-            "data": "synthetic (seeded Poisson stream, seeded operators and spectra)",
-            "config": {"workload": f"serving (config 4): {n_req} requests, Poisson rate {rate}/s, grids "
-                                   "p16xu8, p32xu8, p32xu16, p64xu16 (2 species), 500-20000 steps each",
-                       "capacity_per_grid": args.capacity, "hbm_budget_bytes": 150 * 10**9,
-                       "device_bytes": st["device_bytes"]},
+    recs = [{"tts": i["t_done"] - i["t_submit"], "t_submit": i["t_submit"], "t_done": i["t_done"],
+             "queue_s": i["t_admit"] - i["t_submit"], "steps": int(i["steps"]), "finite": bool(i["finite"])}
+            for i in infos]
+    if recs:
+        recs[0]["serve_stats"] = st
+    return recs
+
+
+def _serving_leg(rank: int, world: int, local: int, n_req: int, load: float, capacity: int, seed: int,
+                 setup=None, rate=None):
+    """One served stream: n_req requests per GPU (weak scaling), Poisson arrivals at `load` times
+    the capacity of the four grids at full occupancy (or at `rate` requests/s per GPU), routed
+    across ranks; p50/p99 time to solution and aggregate instance-steps/s, beside the same requests
+    served one at a time on the plain FP64 path (FIFO per GPU)."""
+    import numpy as np
+    from dtb.shard import route, serve_sharded
+    grids, batched, t_full_ms, step_ms_fp64 = setup
+    mean_steps = (500 + 20000) / 2.0
+    # at full occupancy every grid is stepping; one step of every grid moves 4 x capacity instances
+    lam_max = len(SERVE_GRIDS) * capacity / (mean_steps * sum(t_full_ms) / 1e3)
+    lam = rate if rate is not None else load * lam_max
+    stream = _request_stream(n_req * world, lam * world, seed, len(SERVE_GRIDS))
+    budget = 150 * 10**9
+    recs = serve_sharded([float(x) for x in stream["steps"]], rank, world,
+                         lambda mine: _serve_share(batched, grids, stream, mine, budget))
+    tts = np.array([r["tts"] for r in recs])
+    total = int(stream["steps"].sum())
+    span = max(max(r["t_done"] for r in recs if r["rank"] == q) - min(r["t_submit"] for r in recs if r["rank"] == q)
+               for q in set(r["rank"] for r in recs))
+    # one at a time on the plain FP64 path: a FIFO single server per GPU over the same arrivals
+    ranks = route([float(x) for x in stream["steps"]], world)
+    tts_plain, span_plain = [], 0.0
+    for q in range(world):
+        free_at, first = 0.0, None
+        for k in (k for k in range(len(ranks)) if ranks[k] == q):
+            a = float(stream["arrivals"][k])
+            first = a if first is None else first
+            free_at = max(free_at, a) + stream["steps"][k] * step_ms_fp64[stream["grid"][k]] / 1e3
+            tts_plain.append(free_at - a)
+        if first is not None:
+            span_plain = max(span_plain, free_at - first)
+    stats = [r["serve_stats"] for r in recs if "serve_stats" in r]
+    return {"requests": n_req * world, "load": None if rate is not None else load,
+            "rate_per_s": lam * world, "capacity_rate_per_s": lam_max * world,
             "tts_p50_s": float(np.percentile(tts, 50)), "tts_p99_s": float(np.percentile(tts, 99)),
-            "plain_fp64_one_at_a_time": {"value": agg_plain, "unit": "instance-steps/s",
+            "queue_p99_s": float(np.percentile([r["queue_s"] for r in recs], 99)),
+            "instance_steps_per_s": total / span, "all_finite": all(r["finite"] for r in recs),
+            "full_occupancy_step_ms": t_full_ms, "capacity_per_grid": capacity,
+            "plain_fp64_one_at_a_time": {"instance_steps_per_s": total / span_plain,
                                          "tts_p50_s": float(np.percentile(tts_plain, 50)),
                                          "tts_p99_s": float(np.percentile(tts_plain, 99)),
                                          "step_ms_per_grid": step_ms_fp64,
-                                         "method": "FIFO single server over the same arrivals, service time = "
-                                                   "steps x FP64 step time measured per grid"},
-            "speedup_vs_plain_fp64": agg / agg_plain,
-            "serve_stats": st}
-    print(json.dumps(line), flush=True)
+                                         "method": "FIFO single server per GPU over the same arrivals, service "
+                                                   "time = steps x FP64 step time measured per grid"},
+            "device_bytes": sum(s["device_bytes"] for s in stats) // max(1, len(stats)),
+            "busy_s": max((s["busy_s"] for s in stats), default=None)}
+
+
+def run_serving(args):
+    """Config 4: Poisson streams of solve requests over four grids served with continuous
+    batching at each requested load (fraction of the full-occupancy capacity), or one stream at
+    --rate; p50/p99 time to solution and aggregate instance-steps/s, beside the same stream one
+    at a time on the plain FP64 path."""
+    import torch
+    import torch.distributed as dist
+    rank, local, world = _env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    if args.tune_cache:
+        from dtb.batch import set_tune_cache
+        set_tune_cache(args.tune_cache)
+    setup = _serving_grids(local, args.capacity)
+    points = []
+    if args.rate is not None:
+        points.append(_serving_leg(rank, world, local, args.requests, 0.0, args.capacity, 44, setup, rate=args.rate))
+    else:
+        for ld in args.loads:
+            points.append(_serving_leg(rank, world, local, args.requests, ld, args.capacity, 44, setup))
+    for b in setup[1]:
+        b.close()
+    head = points[0]
+    line = {"metric": METRIC, "value": head["instance_steps_per_s"], "unit": "instance-steps/s", "n_gpus": world,
+            "steps": int(args.requests * world), "warmup": 0, "ms_per_step": 1e3 / head["instance_steps_per_s"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 (gain GEMM), f32 state, f64 update",
+            "data": "synthetic (seeded Poisson stream, seeded operators and spectra)",
+            "config": {"workload": f"serving (config 4): {args.requests} requests per GPU, grids p16xu8, p32xu8, "
+                                   "p32xu16, p64xu16 (2 species), 500-20000 steps each",
+                       "capacity_per_grid": args.capacity, "hbm_budget_bytes": 150 * 10**9,
+                       "parallelism": f"requests routed over {world} GPU(s)"},
+            "tts_p50_s": head["tts_p50_s"], "tts_p99_s": head["tts_p99_s"], "serving": points}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -662,12 +846,22 @@ def main():
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="p_bins x u_bins override of the config-1 grid, e.g. 32x16")
-    ap.add_argument("--no-check", action="store_true", help="skip the FP64 accuracy check of the batched run")
+    ap.add_argument("--no-check", action="store_true", help="skip the FP64 accuracy checks of the batched run")
+    ap.add_argument("--check-steps", type=int, default=None,
+                    help="length of the batched accuracy run (default: the configuration's run length, "
+                         "10000 steps for --config 2, 5000 for --config 3)")
+    ap.add_argument("--oracle-long", action="store_true",
+                    help="also run one instance of the accuracy run on the FP64 oracle (host cores)")
     ap.add_argument("--tune-cache", default=None,
                     help="gain-GEMM plan cache file: plans recorded there are reused, new ones are measured and "
                          "appended (a profiling run can replay the plan a plain run chose)")
-    ap.add_argument("--requests", type=int, default=2000, help="serving stream length (--config 4)")
-    ap.add_argument("--rate", type=float, default=20.0, help="mean request arrival rate per second (--config 4)")
+    ap.add_argument("--requests", type=int, default=200, help="serving stream length per GPU (--config 4)")
+    ap.add_argument("--rate", type=float, default=None,
+                    help="mean request arrival rate per second per GPU (--config 4; default: --loads)")
+    ap.add_argument("--loads", type=lambda x: [float(v) for v in x.split(",")], default=[0.5, 0.7, 0.9],
+                    help="serving loads as fractions of the four grids' full-occupancy capacity (--config 4)")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests per GPU of the default run's serving leg (0: skip it)")
     ap.add_argument("--capacity", type=int, default=256, help="slots per grid (--config 4)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -932,6 +932,26 @@ int batch_finish(dtb_ctx* c) {
     return mixed_check_err(c);
 }
 
+// Captures, instantiates and uploads every graph dtb_batch_run replays (the graph of
+// graph_steps steps, which starts on state buffer 0, and the 1-step graph of each buffer);
+// capture enqueues nothing, so the state and the step counter are unchanged.
+int batch_prepare(dtb_ctx* c) {
+    MixedState* m = c->mixed;
+    const int cur = m->cur;
+    m->cur = 0;
+    int rc = ensure_mixed_graph(c);
+    for (int k = 0; k < 2 && rc == DTB_OK; ++k) {
+        m->cur = k;
+        rc = ensure_mixed_graph1(c);
+    }
+    m->cur = cur;
+    if (rc != DTB_OK) return rc;
+    DTB_CUDA(cudaGraphUpload(m->graph, c->stream));
+    for (auto& g1 : m->graph1) DTB_CUDA(cudaGraphUpload(g1, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    return DTB_OK;
+}
+
 int batch_capacity(dtb_ctx* c) { return c->mixed ? c->mixed->Buser : 0; }
 long long batch_step(dtb_ctx* c) { return c->mixed ? c->mixed->host_step : 0; }
 

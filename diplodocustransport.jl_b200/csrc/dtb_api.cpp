@@ -968,6 +968,8 @@ static int check_kernel_err(dtb_ctx* c) {
     return DTB_OK;
 }
 
+int batch_prepare(dtb_ctx* c);  // batch_api.cpp
+
 static int ensure_graph(dtb_ctx* c, int verbose) {
     if (c->graph && c->graph_verbose == verbose) return DTB_OK;
     if (c->graph) {
@@ -1059,6 +1061,18 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
         DTB_TRY(check_kernel_err(c));
         if (diag_out) std::memcpy(diag_out, c->pin_hist, sizeof(StepDiagDev));
     }
+    return DTB_OK;
+}
+
+int32_t dtb_prepare(dtb_ctx* c) {
+    DTB_CHECK(c, DTB_EINVAL, "dtb_prepare: null context");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    if (c->prec == DTB_MIXED) return batch_prepare(c);
+    if (c->profiling) return DTB_OK;  // profiled runs launch step by step
+    DTB_TRY(ensure_graph(c, 0));
+    DTB_CUDA(cudaGraphUpload(c->graph, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
     return DTB_OK;
 }
 

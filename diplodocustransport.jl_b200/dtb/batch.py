@@ -87,6 +87,10 @@ class BatchedEuler:
         f = np.ascontiguousarray(f0, dtype=np.float64)
         check(self.L.dtb_batch_admit(self.ctx, int(slot), dptr(f), float(dt) / self.dt0, int(n_steps)))
 
+    def prepare(self) -> None:
+        """Captures and uploads the batched step graphs now (dtb_prepare), so no later run pays for it."""
+        check(self.L.dtb_prepare(self.ctx))
+
     def run(self, nsteps: int) -> None:
         check(self.L.dtb_batch_run(self.ctx, int(nsteps)))
 

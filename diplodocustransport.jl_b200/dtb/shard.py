@@ -8,7 +8,7 @@ per-request statistics at the end.
 """
 from __future__ import annotations
 
-from typing import List, Optional, Sequence, Tuple
+from typing import Callable, List, Optional, Sequence, Tuple
 
 
 def shard_range(n: int, rank: int, world: int) -> Tuple[int, int]:
@@ -49,3 +49,29 @@ def gather(obj, group=None) -> Optional[list]:
     out = [None] * dist.get_world_size(group)
     dist.all_gather_object(out, obj, group=group)
     return out
+
+
+def serve_sharded(costs: Sequence[float], rank: int, world: int, serve_share: Callable[[List[int]], list],
+                  policy: str = "least_work") -> list:
+    """Runs one request stream across ranks with no data-path collective.
+
+    ``costs`` is the stream in arrival order (identical on every rank, e.g. the request step
+    counts). Each request is routed to a rank (``route``); this rank passes the global indices
+    of its share to ``serve_share``, which serves them (on this rank's GPU) and returns one
+    record per index, in the order given. The records of all ranks are then gathered once and
+    returned on every rank in arrival order, each with its ``rank`` and ``index`` added. A rank
+    that fails raises before the gather; the other ranks' gather then ends with the process
+    group's timeout error instead of waiting for good.
+    """
+    ranks = route(costs, world, policy)
+    mine = [k for k, r in enumerate(ranks) if r == rank]
+    recs = serve_share(mine)
+    if len(recs) != len(mine):
+        raise RuntimeError(f"rank {rank}: {len(recs)} records for {len(mine)} requests")
+    local = [dict(rec, rank=rank, index=k) for k, rec in zip(mine, recs)]
+    allv = gather(local) or [local]
+    merged = [rec for part in allv for rec in part]
+    merged.sort(key=lambda r: r["index"])
+    if [r["index"] for r in merged] != list(range(len(costs))):
+        raise RuntimeError("gathered records do not cover the stream exactly once")
+    return merged

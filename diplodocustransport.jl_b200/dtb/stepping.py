@@ -183,6 +183,10 @@ class ForwardEulerStruct:
     def reset(self) -> None:
         check(self.L.dtb_reset(self.ctx))
 
+    def prepare(self) -> None:
+        """Captures and uploads the step graphs now (dtb_prepare), so no later run pays for it."""
+        check(self.L.dtb_prepare(self.ctx))
+
     def run(self, dt_scales: Sequence[float], Verbose: int = 0, diag: bool = False):
         s = np.ascontiguousarray(dt_scales, dtype=np.float64)
         hist = (_lib.StepDiag * len(s))() if diag else None
