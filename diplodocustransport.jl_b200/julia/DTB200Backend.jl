@@ -8,7 +8,8 @@
 #     using DiplodocusTransport
 #     include("DTB200Backend.jl"); using .DTB200Backend
 #     Backend = B200Backend()            # instead of CPUBackend() / CUDABackend()
-#     method = B200ForwardEulerStruct(PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)
+#     method = ForwardEulerStruct(PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)  # patched reference
+#     method = B200ForwardEulerStruct(PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)  # unpatched
 #     output = Solve(method, dt, t_save)  # the reference's Solve, unchanged
 #
 # B200ForwardEulerStruct takes the same arguments as ForwardEulerStruct and carries the
@@ -25,7 +26,14 @@ export B200BatchedEuler, admit!, run!, run_io!, get_f, batch_moments, gemm_plan,
 
 const libdtb = get(ENV, "DTB_LIB", joinpath(@__DIR__, "..", "lib", "libdtb.so"))
 
-struct B200Backend <: BackendType end  # next to Backends.jl:3-4
+# With the reference patched (Backends.jl defines B200Backend and b200_stepping_struct), the
+# reference's own ForwardEulerStruct(...) returns the B200 stepping struct under
+# Backend = B200Backend(); against an unpatched reference the type is defined here.
+if isdefined(DiplodocusTransport, :b200_stepping_struct)
+    import DiplodocusTransport: B200Backend
+else
+    struct B200Backend <: BackendType end  # next to Backends.jl:3-4
+end
 
 const DTB_F64 = Int32(0)
 const DTB_F32 = Int32(1)
@@ -157,6 +165,10 @@ mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
     end
 end
 
+if isdefined(DiplodocusTransport, :b200_stepping_struct)
+    DiplodocusTransport.b200_stepping_struct(args...; kw...) = B200ForwardEulerStruct(args...; kw...)
+end
+
 # The functor (SteppingMethods.jl:12-107): one ccall per step; dt truncation happens in the
 # library exactly as in :18-23 and the diagnostics are printed like :87-93.
 function (method::B200ForwardEulerStruct)(t_start, t_stop, dt, Verbose::Int64)
@@ -225,6 +237,10 @@ end
 admit!(b::B200BatchedEuler, slot::Integer, f0::Vector{Float64}, dt::Float64, n_steps::Integer) =
     check(ccall((:dtb_batch_admit, libdtb), Int32, (Ptr{Cvoid}, Int32, Ptr{Float64}, Float64, Int64),
                 b.ctx, slot - 1, f0, dt / b.dt0, n_steps))
+
+# Captures and uploads the step graphs now, so the first run!/b200_solve pays no capture.
+prepare!(b::B200BatchedEuler) = check(ccall((:dtb_prepare, libdtb), Int32, (Ptr{Cvoid},), b.ctx))
+prepare!(m::B200ForwardEulerStruct) = check(ccall((:dtb_prepare, libdtb), Int32, (Ptr{Cvoid},), m.ctx))
 
 # nsteps batched steps of every slot with steps left (enqueued; errors surface at the next read).
 run!(b::B200BatchedEuler, nsteps::Integer) =
