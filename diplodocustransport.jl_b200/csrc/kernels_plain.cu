@@ -335,8 +335,11 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
     __shared__ double s_red[kRowsWarps][kRedFields];
     __shared__ double s_fin[6][kRowsWarps * 32];
     __shared__ int s_last;
-    pdl_wait();  // this step's inputs (gain partials, momentum pass) and the previous step's state and counter
-    if (threadIdx.x == 0) pdl_trigger();
+    // The previous step's state and step counter were final before this grid could launch: the
+    // gain kernel it depends on let it launch only after that kernel's own wait for the previous
+    // row kernel. So the flux, emission and loss products, which read only the state and static
+    // operands, run before the wait for this step's gain partials (on SMs beside the gain kernel
+    // where it leaves room); everything this grid writes is written after the wait.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
     const double dt_scale = dt_arr ? dt_arr[step] : dt_imm;
@@ -344,15 +347,17 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
 
     double m_cr = CUDART_INF, m_bin = CUDART_INF, m_emi = CUDART_INF, m_flux = CUDART_INF;
     double s_df = 0.0, s_f = 0.0;
+    const int cell = i < ops.n_state ? i / ops.n_mom : 0;
+    const int a = i - cell * ops.n_mom;
+    const T* fc = f_in + (size_t)cell * ops.n_mom;
+    int s = 0;
+    double flux = 0.0, emi = 0.0, loss = 0.0, gain = 0.0;
+    // binary term of this cell (SteppingMethods.jl:369): outside BinM.Domain it is zero
+    const bool bin_here = i < ops.n_state && ops.has_bin && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
     if (i < ops.n_state) {
-        const int cell = i / ops.n_mom;
-        const int a = i - cell * ops.n_mom;
-        const T* fc = f_in + (size_t)cell * ops.n_mom;
-        int s = 0;
         while (s + 1 < ops.n_species && a >= ops.sp_off[s + 1]) ++s;
 
         // (a) banded flux row: ELL slots of width ell_w, 128-bit loads of 4 slots per lane
-        double flux = 0.0;
         {
             const T* vrow = ops.ell_val + (size_t)i * ops.ell_w;
             const int* crow = ops.ell_col + (size_t)i * ops.ell_w;
@@ -375,7 +380,6 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
             }
         }
         // (c) emission row pieces
-        double emi = 0.0;
         if (ops.has_emi) {
             for (int p = ops.emi_rptr[i]; p < ops.emi_rptr[i + 1]; ++p) {
                 const int pc = ops.emi_piece[p];
@@ -385,10 +389,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
                 for (int c = lane; c < nc; c += 32) emi += (double)row[c] * (double)fx[c];
             }
         }
-        // loss bilinear term and gain partials
-        double loss = 0.0, gain = 0.0;
-        // binary term of this cell (SteppingMethods.jl:369): outside BinM.Domain it is zero
-        const bool bin_here = ops.has_bin && (ops.bin_on == nullptr || ops.bin_on[cell] != 0);
+        // loss bilinear term
         if (bin_here) {
             const int la = a - ops.sp_off[s];
             for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
@@ -397,12 +398,18 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
                 const int nc = ops.loss_ncols[b];
                 for (int c = lane; c < nc; c += 32) loss += (double)row[c] * (double)fx[c];
             }
-            const double* pr = ops.partial + (size_t)cell * ops.n_units;
-            for (int u = ops.unit_ptr[a] + lane; u < ops.unit_ptr[a + 1]; u += 32) gain += pr[u];
         }
         flux = warp_sum(flux);
         emi = warp_sum(emi);
         loss = warp_sum(loss);
+    }
+    pdl_wait();  // this step's gain partials (and, in the space pass, the momentum pass) are complete
+    if (threadIdx.x == 0) pdl_trigger();
+    if (i < ops.n_state) {
+        if (bin_here) {
+            const double* pr = ops.partial + (size_t)cell * ops.n_units;
+            for (int u = ops.unit_ptr[a] + lane; u < ops.unit_ptr[a + 1]; u += 32) gain += pr[u];
+        }
         gain = warp_sum(gain);
 
         if (lane == 0 && ops.mode == 1) {

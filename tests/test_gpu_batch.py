@@ -533,3 +533,74 @@ def test_batched_cr_and_finite_flags_match_oracle(cuda):
         assert info["finite"]
         assert info["cr_max"] == pytest.approx(max(crs), rel=1e-4), i
     m.close()
+
+
+def _moments_oracle(ps, f):
+    from dtb.structs import energy_weights
+    wts = energy_weights(ps)
+    off = ps.momentum_species_offset
+    sizes = ps.species_sizes
+    return (np.array([f[off[s]:off[s] + sizes[s]].sum() for s in range(len(sizes))]),
+            np.array([(f[off[s]:off[s] + sizes[s]] * wts[off[s]:off[s] + sizes[s]]).sum() for s in range(len(sizes))]))
+
+
+@pytest.mark.parametrize("n_steps", [5000, 10000])
+def test_long_run_matches_oracle_with_drift(cuda, n_steps):
+    """Mixed precision over a configuration's full run length (5,000 steps as config 3, 10,000
+    as config 2) on a reduced grid (2 species x 32 states, 16 instances, every operator, per-
+    instance dt, injection): every instance within relative L-inf 1e-5 of the FP64 oracle run;
+    the FP64 device moments of the mixed run within 1e-5 (relative to the initial moment) of the
+    oracle's number and energy per species, i.e. the mixed path adds at most 1e-5 of number or
+    energy drift over the oracle's own."""
+    from dtb.structs import energy_weights
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, 16, seed=31)
+    rng = np.random.default_rng(2)
+    w.inj = rng.uniform(0, 1e-4, w.ps.n_state)
+    m = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 16)
+    for i in range(16):
+        m.admit(i, w.f0[i], w.dt[i], n_steps)
+    wts = energy_weights(w.ps)
+    num0, en0 = m.moments(wts)
+    m.run(n_steps)
+    num1, en1 = m.moments(wts)
+    ops = oracle.blocked_from_workload(w)
+    for i in range(16):
+        f = w.f0[i].copy()
+        for _ in range(n_steps):
+            f, _, _ = ops.step(f, w.dt[i], 0)
+        assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
+        on, oe = _moments_oracle(w.ps, f)
+        assert np.all(np.abs(num1[i] - on) / num0[i] <= 1e-5), i
+        assert np.all(np.abs(en1[i] - oe) / en0[i] <= 1e-5), i
+    m.close()
+
+
+def test_long_run_number_conservation(cuda):
+    """Known answer over 5,000 steps: gain and loss built to conserve number per species (flux
+    and emission off); the mixed path's FP64 device number moments stay within 1e-5 of the
+    initial number (the FP64 oracle conserves it to rounding)."""
+    from dtb.structs import FluxMatrices
+    w = synth.small(p_num=8, u_num=4, seed=8, with_emission=False)
+    ns = w.ps.species_sizes[0]
+    n = w.ps.n_state
+    Ge = np.asarray(w.binm.gains[0].G)
+    Gg = np.asarray(w.binm.gains[1].G)
+    w.binm.losses = [LossBlock(0, 1, Ge.sum(axis=0)), LossBlock(1, 0, Gg.sum(axis=0).T)]
+    w.fluxm = FluxMatrices(Ap_Flux=np.ones(n), Am_Flux=-np.ones(n), X_Flux=sp.csc_matrix((n, n)),
+                           P_Flux=sp.csc_matrix((n, n)), Vol=np.ones(1))
+    w.inj = np.zeros(n)
+    n0 = np.array([w.f0[:ns].sum(), w.f0[ns:].sum()])
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 4)
+    for i in range(4):
+        b.admit(i, w.f0 * (1.0 + 0.1 * i), 0.5 + 0.1 * i, 5000)
+    b.run(5000)
+    num, _ = b.moments(np.ones(w.ps.n_momentum))
+    for i in range(4):
+        ref = n0 * (1.0 + 0.1 * i)
+        assert np.all(np.abs(num[i] - ref) / ref < 1e-5), (i, num[i], ref)
+    ops = oracle.blocked_from_workload(w)
+    f = w.f0.copy()
+    for _ in range(5000):
+        f, _, _ = ops.step(f, 0.5, 0)
+    assert abs(f[:ns].sum() - n0[0]) / n0[0] < 1e-12 and abs(f[ns:].sum() - n0[1]) / n0[1] < 1e-12
+    b.close()
