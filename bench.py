@@ -499,6 +499,11 @@ def run_batched(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     dev = f"cuda:{local}"
     w = build_batched(args.config, dev)
+    if args.shard and world > 1:
+        # strong scaling: the configuration's instances partitioned across the ranks
+        from dtb.shard import shard_range
+        lo, hi = shard_range(w.f0.shape[0], rank, world)
+        w.f0, w.dt = w.f0[lo:hi], w.dt[lo:hi]
     B = w.f0.shape[0]
     n = w.ps.n_state
     K, W = args.steps, args.warmup
@@ -594,7 +599,9 @@ def run_batched(args):
         t = torch.tensor([ms, ms_e2e, ms_plain], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e, ms_plain = float(t[0]), float(t[1]), float(t[2])
-    value = world * B * K / (ms / 1e3)
+    # every rank steps B instances (its share when sharded); the whole job is the sum
+    B_all = sum(_gather_ints([B])) if world > 1 else B
+    value = B_all * K / (ms / 1e3)
     plain_sps = world * K / (ms_plain / 1e3)
     plain_line["value"] = plain_sps
     peak = float(pj.get("bf16_tflops", 1590.0))
@@ -619,12 +626,16 @@ def run_batched(args):
     roof.update({"gemm_plans": [dict(p, tuned_us=round(p["tuned_us"], 2)) for p in plans], "traffic": traffic, "algorithmic_flops_per_step": st["flops_per_step"],
                  "operator_bytes_per_step": st["bytes_per_step"], "avg_gemm_ms_per_step": st["avg_ms"],
                  "profiled_ms_per_step": ms_prof / K})
+    cfg = _config_dict(args.config, w, world)
+    if args.shard and world > 1:
+        cfg["parallelism"] = f"instances sharded over {world} GPUs"
     line = {"metric": METRIC, "value": value, "unit": "instance-steps/s", "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "strong" if (args.shard and world > 1) else "weak", "vs_baseline": None,
             "dtype": "bf16x3 (gain GEMM), f32 state, f64 update", "data": "synthetic (seeded; no collision data files)",
-            "config": _config_dict(args.config, w, world),
+            "config": cfg,
             "precision": "BF16 hi+lo gain (3 MMAs, FP32 accumulation), FP32 f, FP64 compensated update",
-            "e2e": {"value": world * B * K / (ms_e2e / 1e3), "unit": "instance-steps/s",
+            "e2e": {"value": B_all * K / (ms_e2e / 1e3), "unit": "instance-steps/s",
                     "h2d_bytes_per_step": B * n * 8, "d2h_bytes_per_step": B * n * 8, "steps": K},
             "gpu_launches": int(st["launches_per_step"]) * K + (K + 15) // 16,  # + one step-counter advance per graph
             "roofline": roof,
@@ -656,6 +667,14 @@ def run_batched(args):
 
 
 SERVE_GRIDS = [(16, 8), (32, 8), (32, 16), (64, 16)]
+
+
+def _gather_ints(vals):
+    """Every rank's list of ints, concatenated in rank order (torch.distributed)."""
+    import torch.distributed as dist
+    out = [None] * dist.get_world_size()
+    dist.all_gather_object(out, list(vals))
+    return [v for part in out for v in part]
 
 
 def _serving_grids(local: int, capacity: int):
@@ -860,6 +879,9 @@ def main():
                     help="mean request arrival rate per second per GPU (--config 4; default: --loads)")
     ap.add_argument("--loads", type=lambda x: [float(v) for v in x.split(",")], default=[0.5, 0.7, 0.9],
                     help="serving loads as fractions of the four grids' full-occupancy capacity (--config 4)")
+    ap.add_argument("--shard", action="store_true",
+                    help="batched configs under torchrun: partition the instances across the GPUs (strong "
+                         "scaling) instead of a full batch per GPU (weak scaling)")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests per GPU of the default run's serving leg (0: skip it)")
     ap.add_argument("--capacity", type=int, default=256, help="slots per grid (--config 4)")
