@@ -907,8 +907,10 @@ int mixed_ready(dtb_ctx* c) {
 // Launch / finish halves of dtb_batch_run for the serving loop (contexts of different grids
 // run their chunks concurrently on their own streams).
 int batch_launch(dtb_ctx* c, int64_t nsteps) {
+    DTB_RANGE("dtb serve chunk");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
+    c->steps_run += nsteps;
     DTB_TRY(refresh_active_hi(c));
     int64_t done = 0;
     if (nsteps >= m->graph_steps) {
@@ -936,6 +938,7 @@ int batch_finish(dtb_ctx* c) {
 // graph_steps steps, which starts on state buffer 0, and the 1-step graph of each buffer);
 // capture enqueues nothing, so the state and the step counter are unchanged.
 int batch_prepare(dtb_ctx* c) {
+    DTB_RANGE("dtb_prepare (batched graphs)");
     MixedState* m = c->mixed;
     const int cur = m->cur;
     m->cur = 0;
@@ -953,11 +956,34 @@ int batch_prepare(dtb_ctx* c) {
 }
 
 int batch_capacity(dtb_ctx* c) { return c->mixed ? c->mixed->Buser : 0; }
+
+namespace dtb {
+std::string batch_profile_json(const dtb_ctx* c) {
+    const MixedState* m = c->mixed;
+    if (!m) return "\"batch\": 0";
+    std::string js = "\"batch\": " + std::to_string(m->Buser) + ", \"batched_steps\": " + std::to_string(m->host_step);
+    if (m->prof_n > 0) {
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.6g", m->prof_ms / (double)m->prof_n);
+        js += std::string(", \"gemm_avg_ms_per_step\": ") + b;
+    }
+    js += ", \"gemm_plans\": [";
+    for (size_t i = 0; i < m->groups.size(); ++i) {
+        const MixedGroup& G = m->groups[i];
+        char b[160];
+        std::snprintf(b, sizeof(b), "%s{\"M\": %d, \"pair\": %d, \"bn\": %d, \"n_splits\": %d, \"tuned_us\": %.4g}",
+                      i ? ", " : "", G.M, G.pair ? 1 : 0, G.bn, G.n_splits, G.tuned_us);
+        js += b;
+    }
+    return js + "]";
+}
+}  // namespace dtb
 long long batch_step(dtb_ctx* c) { return c->mixed ? c->mixed->host_step : 0; }
 
 extern "C" {
 
 int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_scale, int64_t n_steps) {
+    DTB_RANGE("dtb_batch_admit");
     DTB_TRY(mixed_ready(c));
     MixedState* m = c->mixed;
     DTB_CHECK(slot >= 0 && slot < m->Buser, DTB_ENOTFOUND, "dtb_batch_admit: slot out of range");
@@ -1007,10 +1033,12 @@ int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_sc
 }
 
 int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
+    DTB_RANGE("dtb_batch_run");
     DTB_TRY(mixed_ready(c));
     DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_batch_run: nsteps < 0");
     MixedState* m = c->mixed;
     DeviceGuard g(c->device);
+    c->steps_run += nsteps;
     DTB_TRY(refresh_active_hi(c));
     int64_t done = 0;
     if (!m->profiling && nsteps >= m->graph_steps) {
@@ -1067,6 +1095,7 @@ int download_all(dtb_ctx* c, double* f) {
 }  // namespace
 
 int32_t dtb_batch_run_io(dtb_ctx* c, const double* f_in, int64_t nsteps, double* f_out) {
+    DTB_RANGE("dtb_batch_run_io");
     DTB_TRY(mixed_ready(c));
     DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_batch_run_io: nsteps < 0");
     DeviceGuard g(c->device);

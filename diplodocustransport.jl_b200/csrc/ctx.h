@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -37,6 +38,23 @@ namespace dtb {
 
 constexpr int kProfRing = 256;
 constexpr int64_t kMaxScheduleSteps = 100000000;
+
+// An NVTX range over a host entry point (upload, commit, steps, graph replays, serving chunks):
+// visible on a profiler timeline, a no-op without one.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define DTB_RANGE_CAT2(a, b) a##b
+#define DTB_RANGE_CAT(a, b) DTB_RANGE_CAT2(a, b)
+#define DTB_RANGE(name) ::dtb::NvtxRange DTB_RANGE_CAT(dtb_range_, __LINE__)(name)
+
+// Path of the run summary each context appends at dtb_destroy (environment DTB_PROFILE), or null.
+const char* profile_path();
+// The batched context's part of that summary (batch_api.cpp): JSON members without braces.
+std::string batch_profile_json(const dtb_ctx* c);
 
 struct DeviceGuard {
     int prev = -1;
@@ -75,6 +93,7 @@ struct MixedState;
 }  // namespace dtb
 
 struct dtb_ctx {
+    long long steps_run = 0;  // steps launched over the context's life (the DTB_PROFILE summary)
     dtb_dims dims{};
     dtb_opts opts{};
     int ns = 0;

@@ -9,9 +9,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -46,6 +48,43 @@ int32_t dtb_device_count(int32_t* n) {
     *n = c;
     return DTB_OK;
 }
+
+}  // extern "C"
+
+namespace dtb {
+const char* profile_path() {
+    static const char* p = [] {
+        const char* e = std::getenv("DTB_PROFILE");
+        return (e && *e) ? e : nullptr;
+    }();
+    return p;
+}
+}  // namespace dtb
+
+// One JSON line per context: its shape, the steps it launched, its device bytes and, when
+// per-launch timing was on, the gain kernel's average launch time.
+static void write_profile(const dtb_ctx* c, const char* path) {
+    static std::mutex mu;
+    std::string js = "{\"precision\": " + std::to_string(c->prec) + ", \"n_state\": " + std::to_string(c->n_state) +
+                     ", \"n_space\": " + std::to_string(c->n_space) + ", \"device\": " + std::to_string(c->device) +
+                     ", \"steps_run\": " + std::to_string(c->steps_run) + ", \"device_bytes\": " +
+                     std::to_string(c->dev_bytes) + ", \"gain_bytes_per_step\": " + std::to_string(c->gain_bytes);
+    if (c->prec == DTB_MIXED) {
+        js += ", " + batch_profile_json(c);
+    } else if (c->prof_n > 0) {
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.6g", c->prof_ms / (double)c->prof_n);
+        js += std::string(", \"gain_kernel_avg_ms\": ") + b + ", \"gain_kernel_launches\": " + std::to_string(c->prof_n);
+    }
+    js += "}\n";
+    std::lock_guard<std::mutex> lk(mu);
+    if (FILE* f = std::fopen(path, "a")) {
+        std::fputs(js.c_str(), f);
+        std::fclose(f);
+    }
+}
+
+extern "C" {
 
 int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out) {
     DTB_CHECK(dims && opts && out, DTB_EINVAL, "dtb_create: null argument");
@@ -108,6 +147,7 @@ int32_t dtb_destroy(dtb_ctx* c) {
     if (!c) return DTB_OK;
     DeviceGuard g(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (const char* path = profile_path()) write_profile(c, path);
     destroy_mixed(c);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
@@ -839,6 +879,7 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
 extern "C" int32_t dtb_commit(dtb_ctx* c) {
     DTB_CHECK(c, DTB_EINVAL, "dtb_commit: null context");
     if (c->committed) return DTB_OK;
+    DTB_RANGE("dtb_commit");
     DTB_CHECK(c->have_vectors, DTB_ESTATE, "dtb_commit: dtb_upload_vectors was not called");
     DeviceGuard g(c->device);
     if (c->prec == DTB_MIXED) {
@@ -1037,6 +1078,7 @@ extern "C" {
 
 int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t verbose, double* dt_out,
                  int32_t* save_out, dtb_step_diag* diag_out) {
+    DTB_RANGE("dtb_step");
     DTB_CHECK(c, DTB_EINVAL, "dtb_step: null context");
     DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_step: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
@@ -1054,6 +1096,7 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
     }
     const unsigned long long idx = c->host_ctr;
     DTB_TRY(do_step(c, dt_scale, false, verbose, false));
+    c->steps_run++;
     if (dt_out) *dt_out = dt;
     if (save_out) *save_out = save;
     if (verbose == 1 || verbose == 2 || verbose == 3 || diag_out) {
@@ -1065,6 +1108,7 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
 }
 
 int32_t dtb_prepare(dtb_ctx* c) {
+    DTB_RANGE("dtb_prepare");
     DTB_CHECK(c, DTB_EINVAL, "dtb_prepare: null context");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
@@ -1077,6 +1121,7 @@ int32_t dtb_prepare(dtb_ctx* c) {
 }
 
 int32_t dtb_run(dtb_ctx* c, const double* dt_scales, int64_t nsteps, int32_t verbose, dtb_step_diag* diag_hist) {
+    DTB_RANGE("dtb_run");
     DTB_CHECK(c && (dt_scales || nsteps == 0), DTB_EINVAL, "dtb_run: null argument");
     DTB_CHECK(nsteps >= 0, DTB_EINVAL, "dtb_run: nsteps < 0");
     DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_run: batched contexts use the dtb_batch_* entry points");
@@ -1087,6 +1132,7 @@ int32_t dtb_run(dtb_ctx* c, const double* dt_scales, int64_t nsteps, int32_t ver
         DTB_CUDA(cudaStreamSynchronize(c->stream));  // pinned staging is reused
         std::memcpy(c->pin_dt, dt_scales + s0, sizeof(double) * (size_t)n);
         DTB_TRY(run_chunk(c, n, verbose, true));
+        c->steps_run += n;
         if (diag_hist) {
             DTB_CUDA(cudaMemcpyAsync(c->pin_hist, c->hist, sizeof(StepDiagDev) * (size_t)n, cudaMemcpyDeviceToHost,
                                      c->stream));
@@ -1234,6 +1280,7 @@ struct StepInfo {
 extern "C" int32_t dtb_solve_ex(dtb_ctx* c, double dt_initial, const double* t_save, int64_t n_save, int32_t verbose,
                                 double* f_out, const double* w, double* number, double* energy,
                                 int64_t* n_steps_out) {
+    DTB_RANGE("dtb_solve");
     DTB_CHECK(c && t_save && n_save >= 1, DTB_EINVAL, "dtb_solve_ex: null argument");
     DTB_CHECK(!w || (number && energy), DTB_EINVAL, "dtb_solve_ex: moments need number and energy outputs");
     DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_solve: batched contexts use the dtb_batch_* entry points");
@@ -1404,6 +1451,7 @@ extern "C" int32_t dtb_solve_ex(dtb_ctx* c, double dt_initial, const double* t_s
     }
     if (rc != DTB_OK) return rc;
     DTB_TRY(check_kernel_err(c));
+    c->steps_run += total;
     if (n_steps_out) *n_steps_out = total;
     return DTB_OK;
 }
