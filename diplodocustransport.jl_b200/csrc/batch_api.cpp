@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -71,6 +72,44 @@ struct MixedState {
 };
 
 }  // namespace dtb
+
+namespace {
+
+// BF16 bits of x rounded to nearest, ties to even (NaN kept a NaN).
+uint16_t bf16_bits_rn(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);
+    return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+double bf16_value(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+// 2^floor(log2(m)) for a finite m > 0, else 1: a row scale that brings the row's largest
+// magnitude into [1, 2) without rounding anything
+double pow2_scale(double m) { return (m > 0 && std::isfinite(m)) ? std::ldexp(1.0, std::ilogb(m)) : 1.0; }
+
+// Operand rows for the batched epilogue: values v = x / scale(row) stored as BF16 hi = bf16(v)
+// and lo = bf16(v - hi) (together about 16 significant bits), hi halves first, then the lo
+// halves, in one device allocation.
+int upload_hi_lo(dtb_ctx* c, const std::vector<double>& scaled, __nv_bfloat16** dst) {
+    const size_t n = scaled.size();
+    std::vector<uint16_t> h(2 * std::max<size_t>(1, n), 0);
+    for (size_t k = 0; k < n; ++k) {
+        const uint16_t hi = bf16_bits_rn((float)scaled[k]);
+        h[k] = hi;
+        h[n + k] = bf16_bits_rn((float)(scaled[k] - bf16_value(hi)));
+    }
+    DTB_TRY(c->alloc(dst, sizeof(uint16_t) * h.size()));
+    DTB_CUDA(cudaMemcpyAsync(*dst, h.data(), sizeof(uint16_t) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    return DTB_OK;
+}
+
+}  // namespace
 
 namespace {
 
@@ -441,18 +480,31 @@ int commit_mixed(dtb_ctx* c) {
         }
         ops.gain_ptr[c->ns] = e;
     }
-    // ---------------- loss (FP32), grouped by row species
+    // ---------------- loss, grouped by row species: BF16 hi + lo of the rows divided by a
+    // power-of-two scale per momentum row (common to the row's loss blocks, so the products of
+    // all its blocks share one accumulator)
     {
         std::vector<long long> doff;
         std::vector<int> ld, coff, ncols;
         std::vector<double> data;
+        std::vector<double> rmax((size_t)n_mom, 0.0);
+        for (auto& kv : c->losses) {
+            const int sp = kv.first.first;
+            const int64_t nr = c->sz[sp], nc = c->sz[kv.first.second];
+            for (int64_t r = 0; r < nr; ++r)
+                for (int64_t k = 0; k < nc; ++k)
+                    rmax[(size_t)(c->off[sp] + r)] = std::max(rmax[(size_t)(c->off[sp] + r)],
+                                                               std::fabs(kv.second[(size_t)(r * nc + k)]));
+        }
+        std::vector<double> rscale((size_t)n_mom);
+        for (int64_t a = 0; a < n_mom; ++a) rscale[(size_t)a] = pow2_scale(rmax[(size_t)a]);
         for (int sp = 0; sp < c->ns; ++sp) {
             ops.loss_ptr[sp] = (int)doff.size();
             for (auto& kv : c->losses) {
                 if (kv.first.first != sp) continue;
                 const int oth = kv.first.second;
-                const int64_t nr = c->sz[sp], nc = c->sz[oth], l = round_up(nc, 4);
-                // rows padded with zeros to a multiple of 4 (16-byte rows for the epilogue's async copies)
+                const int64_t nr = c->sz[sp], nc = c->sz[oth], l = round_up(nc, 8);
+                // rows padded with zeros to a multiple of 8 (16-byte rows for the epilogue's async copies)
                 doff.push_back((long long)data.size());
                 ld.push_back((int)l);
                 coff.push_back((int)c->off[oth]);
@@ -460,34 +512,47 @@ int commit_mixed(dtb_ctx* c) {
                 const size_t base = data.size();
                 data.resize(base + (size_t)(nr * l), 0.0);
                 for (int64_t r = 0; r < nr; ++r)
-                    for (int64_t k = 0; k < nc; ++k) data[base + (size_t)(r * l + k)] = kv.second[(size_t)(r * nc + k)];
+                    for (int64_t k = 0; k < nc; ++k)
+                        data[base + (size_t)(r * l + k)] = kv.second[(size_t)(r * nc + k)] / rscale[(size_t)(c->off[sp] + r)];
             }
         }
         ops.loss_ptr[c->ns] = (int)doff.size();
         long long* d_doff;
         int *d_ld, *d_coff, *d_nc;
-        float* d_data;
+        __nv_bfloat16* d_data;
+        float* d_rs;
         DTB_TRY(copy_host_ints(c, &d_doff, doff));
         DTB_TRY(copy_host_ints(c, &d_ld, ld));
         DTB_TRY(copy_host_ints(c, &d_coff, coff));
         DTB_TRY(copy_host_ints(c, &d_nc, ncols));
-        DTB_TRY(copy_host_vec(c, &d_data, data));
+        DTB_TRY(upload_hi_lo(c, data, &d_data));
+        DTB_TRY(copy_host_vec(c, &d_rs, rscale));
         ops.loss_data_off = d_doff;
         ops.loss_ld = d_ld;
         ops.loss_col_off = d_coff;
         ops.loss_ncols = d_nc;
         ops.loss_data = d_data;
+        ops.loss_lo = (long long)std::max<size_t>(1, data.size());
+        ops.loss_rscale = d_rs;
     }
-    // ---------------- emission pieces: FP32 rows padded with zeros to a multiple of 4
+    // ---------------- emission pieces: BF16 hi + lo of the rows divided by a power-of-two scale
+    // per state row (common to the pieces over that row), rows padded with zeros to a multiple of 8
     {
         c->has_emi = !c->emis.empty();
         std::vector<long long> doff;
         std::vector<int> ld, r0v, c0v, ncv;
         std::vector<std::vector<int>> rows((size_t)n_st);
         std::vector<double> data;
+        std::vector<double> rmax((size_t)n_st, 0.0);
+        for (const EmiPiece& e : c->emis)
+            for (int64_t r = 0; r < e.nrows; ++r)
+                for (int64_t k = 0; k < e.ncols; ++k)
+                    rmax[(size_t)(e.row0 + r)] = std::max(rmax[(size_t)(e.row0 + r)], std::fabs(e.data[(size_t)(r * e.ncols + k)]));
+        std::vector<double> rscale((size_t)n_st);
+        for (int64_t a = 0; a < n_st; ++a) rscale[(size_t)a] = pow2_scale(rmax[(size_t)a]);
         for (size_t p = 0; p < c->emis.size(); ++p) {
             const EmiPiece& e = c->emis[p];
-            const int64_t l = round_up(e.ncols, 4);
+            const int64_t l = round_up(e.ncols, 8);
             doff.push_back((long long)data.size());
             ld.push_back((int)l);
             r0v.push_back((int)e.row0);
@@ -496,12 +561,17 @@ int commit_mixed(dtb_ctx* c) {
             const size_t base = data.size();
             data.resize(base + (size_t)(e.nrows * l), 0.0);
             for (int64_t r = 0; r < e.nrows; ++r) {
-                for (int64_t k = 0; k < e.ncols; ++k) data[base + (size_t)(r * l + k)] = e.data[(size_t)(r * e.ncols + k)];
+                for (int64_t k = 0; k < e.ncols; ++k)
+                    data[base + (size_t)(r * l + k)] = e.data[(size_t)(r * e.ncols + k)] / rscale[(size_t)(e.row0 + r)];
                 rows[(size_t)(e.row0 + r)].push_back((int)p);
             }
         }
-        float* d_data = nullptr;
-        DTB_TRY(copy_host_vec(c, &d_data, data));
+        __nv_bfloat16* d_data = nullptr;
+        float* d_rs = nullptr;
+        DTB_TRY(upload_hi_lo(c, data, &d_data));
+        DTB_TRY(copy_host_vec(c, &d_rs, rscale));
+        ops.emi_lo = (long long)std::max<size_t>(1, data.size());
+        ops.emi_rscale = d_rs;
         std::vector<int> rptr((size_t)n_st + 1, 0), piece;
         for (int i = 0; i < n_st; ++i) {
             rptr[(size_t)i] = (int)piece.size();
@@ -675,7 +745,7 @@ int commit_mixed(dtb_ctx* c) {
         std::vector<RowJob> jobs((size_t)n_tiles_r * kRowsMaxJobs);
         std::vector<int> njobs((size_t)n_tiles_r, 0);
         struct Opnd {
-            const float* T;  // row 0 of the operand block, column 0
+            const __nv_bfloat16* T;  // hi half of row 0 of the operand block, column 0
             int ld, col0, nc;
         };
         std::vector<std::vector<Opnd>> loss_of((size_t)c->ns);  // per species
@@ -684,7 +754,7 @@ int commit_mixed(dtb_ctx* c) {
             for (int sp = 0; sp < c->ns; ++sp)
                 for (auto& kv : c->losses) {
                     if (kv.first.first != sp) continue;
-                    const int64_t nr = c->sz[sp], nc = c->sz[kv.first.second], l = round_up(nc, 4);
+                    const int64_t nr = c->sz[sp], nc = c->sz[kv.first.second], l = round_up(nc, 8);
                     loss_of[(size_t)sp].push_back({ops.loss_data + off, (int)l, (int)c->off[kv.first.second], (int)nc});
                     off += nr * l;
                 }
@@ -694,7 +764,7 @@ int commit_mixed(dtb_ctx* c) {
             long long off = 0;
             for (size_t p = 0; p < c->emis.size(); ++p) {
                 emi_off[p] = off;
-                off += c->emis[p].nrows * round_up(c->emis[p].ncols, 4);
+                off += c->emis[p].nrows * round_up(c->emis[p].ncols, 8);
             }
         }
         for (int t = 0; t < n_tiles_r; ++t) {
@@ -709,7 +779,7 @@ int commit_mixed(dtb_ctx* c) {
                     L.push_back({o.T + (size_t)(a0 - cell * n_mom - c->off[s0]) * o.ld, o.ld, o.col0 + cell * n_mom, o.nc});
             for (int p : emi_rows[(size_t)a0]) {
                 const EmiPiece& e = c->emis[(size_t)p];
-                const int l = (int)round_up(e.ncols, 4);
+                const int l = (int)round_up(e.ncols, 8);
                 E.push_back({ops.emi_data + emi_off[(size_t)p] + (size_t)(a0 - e.row0) * l, l, (int)e.col0, (int)e.ncols});
             }
             RowJob* J = jobs.data() + (size_t)t * kRowsMaxJobs;

@@ -54,14 +54,16 @@ cudaError_t prepare_gain_gemm(int bn);
 constexpr int kRowsMaxJobs = 32;
 constexpr int kRowsChunk = 128;
 
-// One K chunk of an epilogue tile product: kRowsChunk columns of a row-major FP32 operand
-// (loss or emission rows) against the same state rows of the tile's instances. Built on the
-// host per 32-row tile.
+// One K chunk of an epilogue tile product: kRowsChunk columns of a row-major operand (loss or
+// emission rows, stored as BF16 hi and lo halves of the row-scaled values) against the same state
+// rows of the tile's instances. Built on the host per 32-row tile.
 struct RowJob {
-    const float* TL;  // loss operand row of the tile's first row at column 0, or null
-    const float* TE;  // emission operand row likewise, or null (loss and emission over the
-                      // same state rows share one job and one staged state chunk)
-    int ldl, lde;     // operand row pitches (multiples of 4)
+    const __nv_bfloat16* TL;  // loss operand (hi half) at the tile's first row, column 0, or null;
+                              // the lo half is ops.loss_lo elements further
+    const __nv_bfloat16* TE;  // emission operand likewise (lo half ops.emi_lo further), or null
+                              // (loss and emission over the same state rows share one job and
+                              // one staged state chunk)
+    int ldl, lde;     // operand row pitches (multiples of 8)
     int col0;         // state row of operand column 0
     int nc;           // operand columns
     int c0;           // first column of the chunk
@@ -85,13 +87,20 @@ struct MixedRowOps {
     const int* emi_row0;
     const int* emi_col0;
     const int* emi_ncols;
-    const float* emi_data;           // E rows, FP32, each row padded with zeros to emi_ld (a multiple of 4)
+    // E rows as BF16 hi halves of E[a][c] / emi_rscale[a], each row padded with zeros to emi_ld
+    // (a multiple of 8); the lo halves (the BF16 rounding of the remainder) emi_lo elements further
+    const __nv_bfloat16* emi_data;
+    long long emi_lo;
+    const float* emi_rscale;         // [n_state] power-of-two scale of each state row's emission
     int loss_ptr[DTB_MAX_SPECIES + 1];
     const long long* loss_data_off;
     const int* loss_ld;
     const int* loss_col_off;
     const int* loss_ncols;
-    const float* loss_data;
+    // loss rows likewise: hi halves of L[a][c] / loss_rscale[a], lo halves loss_lo elements further
+    const __nv_bfloat16* loss_data;
+    long long loss_lo;
+    const float* loss_rscale;        // [n_mom] power-of-two scale of each momentum row's loss blocks
     // gain: for a row of species s, entries [gain_ptr[s], gain_ptr[s+1]) give (group, row offset)
     int gain_ptr[DTB_MAX_SPECIES + 1];
     int gain_grp[64];

@@ -7,9 +7,10 @@
 // Per 16-wide K step three MMAs accumulate hi*hi + hi*lo + lo*hi. One elected thread issues
 // the MMAs and commits them to mbarriers; every wait is bounded.
 //
-// mixed_rows: one (32 rows x 32 instances) tile per block: split-K partial sums of the gain
-// (transposed through shared memory), banded flux, emission (BF16 hi+lo), loss, then the
-// update of SteppingMethods.jl:46-101 with an FP64 compensated (Kahan) accumulation of f.
+// mixed_rows: one (32 rows x 32 instances) tile per block: loss and emission (operands stored
+// as BF16 hi+lo with per-row scales) as tensor-core tile products, split-K partial sums of the
+// gain, banded flux, then the update of SteppingMethods.jl:46-101 with an FP64 compensated
+// (Kahan) accumulation of f.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -862,10 +863,13 @@ __device__ __forceinline__ unsigned long long ord_enc(double x) {
 constexpr int kRT = 32;   // rows per tile
 constexpr int kIT = 32;   // instances per tile
 constexpr int kCK = kRowsChunk;  // K chunk of the loss / emission tile products
-constexpr int kLS = kCK + 4;      // row pitch of a staged operand chunk (16-byte aligned rows)
+constexpr int kOP = kCK + 8;      // BF16 row pitch of a staged operand chunk (272 bytes: 16-byte
+                                  // aligned rows whose 8-row ldmatrix phases hit 32 distinct banks)
+constexpr int kFP = kIT + 4;      // FP32 row pitch of a staged state chunk (conflict-free B loads)
 constexpr int kRowStages = 3;     // cp.async ring depth
-constexpr int kStageFloats = 2 * kRT * kLS + kCK * kIT;  // loss chunk, emission chunk, state chunk
-constexpr int kRowsSmem = kRowStages * kStageFloats * 4;  // dynamic: the operand / state chunk ring
+constexpr int kOpBytes = kRT * kOP * 2;  // one half (hi or lo) of one operand chunk
+constexpr int kStageBytes = 4 * kOpBytes + kCK * kFP * 4;  // loss hi, lo, emission hi, lo, state chunk
+constexpr int kRowsSmem = kRowStages * kStageBytes;  // dynamic: the operand / state chunk ring
 
 
 __device__ __forceinline__ int species_of_row(const MixedRowOps& ops, int a) {
@@ -874,7 +878,9 @@ __device__ __forceinline__ int species_of_row(const MixedRowOps& ops, int a) {
     return s;
 }
 
-// Loss and emission of one (row, instance) pair with direct loads (tiles the fast path cannot take).
+// Loss and emission of one (row, instance) pair with direct loads (tiles the fast path cannot take),
+// from the same BF16 hi + lo operands as the tile products: each operand value hi + lo (exact in
+// FP32) times the state in FP32, the row scale applied to the sum.
 // a: state row (global), am: its momentum index within cell `cell`, s: its species.
 __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict__ F, int a, int am, int cell, int s,
                                  int i, float& loss, float& emi) {
@@ -884,32 +890,45 @@ __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict
     if (ops.has_bin) {
         const int la = am - ops.sp_off[s];
         for (int b = ops.loss_ptr[s]; b < ops.loss_ptr[s + 1]; ++b) {
-            const float* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
+            const __nv_bfloat16* row = ops.loss_data + ops.loss_data_off[b] + (size_t)la * ops.loss_ld[b];
             const int co = ops.loss_col_off[b] + cell * ops.n_mom, nc = ops.loss_ncols[b];
-            for (int c = 0; c < nc; ++c) loss += row[c] * F[(size_t)(co + c) * B + i];
+            for (int c = 0; c < nc; ++c)
+                loss += (__bfloat162float(row[c]) + __bfloat162float(row[c + ops.loss_lo])) * F[(size_t)(co + c) * B + i];
         }
+        loss *= ops.loss_rscale[am];
     }
     if (ops.has_emi) {
         for (int p = ops.emi_rptr[a]; p < ops.emi_rptr[a + 1]; ++p) {
             const int pc = ops.emi_piece[p];
-            const float* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
+            const __nv_bfloat16* row = ops.emi_data + ops.emi_data_off[pc] + (size_t)(a - ops.emi_row0[pc]) * ops.emi_ld[pc];
             const int col0 = ops.emi_col0[pc], nc = ops.emi_ncols[pc];
-            for (int c = 0; c < nc; ++c) emi += row[c] * F[(size_t)(col0 + c) * B + i];
+            for (int c = 0; c < nc; ++c)
+                emi += (__bfloat162float(row[c]) + __bfloat162float(row[c + ops.emi_lo])) * F[(size_t)(col0 + c) * B + i];
         }
+        emi *= ops.emi_rscale[a];
     }
 }
 
-// Two FP32 FMAs in one instruction: acc.{lo, hi} = fma(a, b.{lo, hi}, acc.{lo, hi}), each
-// rounded to nearest like the scalar fma (a pair of floats packed in 64 bits, lo first).
-__device__ __forceinline__ void ffma2(unsigned long long& acc, float a, unsigned long long b) {
-    unsigned long long aa;
-    asm("mov.b64 %0, {%1, %1};" : "=l"(aa) : "f"(a));
-    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(aa), "l"(b));
+// Four 8x8 BF16 matrices from shared memory: the A fragment of one m16n8k16 MMA (rows 0-7 and
+// 8-15 at K 0-7, then the same rows at K 8-15), each lane giving the address of one row.
+__device__ __forceinline__ void ldsm_x4(uint32_t saddr, uint32_t (&r)[4]) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(saddr));
 }
-__device__ __forceinline__ float2 unpack_f32x2(unsigned long long v) {
-    float2 r;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-    return r;
+// d += A (16 x 16, BF16, row-major) * B (16 x 8, BF16, K-major per column), FP32 accumulation.
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// BF16 hi and lo halves of two FP32 values (x0 in the low 16 bits): hi = bf16(x), lo = bf16(x - hi)
+__device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+    hi = pack_bf16x2(x0, x1);
+    const float h0 = __uint_as_float(hi << 16), h1 = __uint_as_float(hi & 0xffff0000u);
+    lo = pack_bf16x2(x0 - h0, x1 - h1);
 }
 
 // 16-byte asynchronous copy global -> shared; src_bytes 0 fills the destination with zeros.
@@ -924,14 +943,18 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // One 32-row x 32-instance tile per block, 512 threads. Loss and emission are tile products
 // when the tile's rows belong to one species and every emission piece touching them covers
 // them all (tile_fast): all their K chunks form one job list streamed through a 3-stage
-// cp.async ring (operand chunk 32 x 128, state chunk 128 x 32); the two halves of the block take
-// the two halves of each chunk with a 2 x 2 (row x instance) micro-tile per thread, and the
-// halves' sums are added in a fixed order. The update then gives each thread one row and two
-// instances, with every load it needs issued before the arithmetic (flux columns and values,
-// state, vectors), so the latency of the L2 round trips overlaps.
+// cp.async ring (operand chunk 32 x 128 as BF16 hi and lo halves, state chunk 128 x 32 FP32).
+// The products run on the tensor cores as m16n8k16 BF16 MMAs with FP32 accumulation: each of
+// the 16 warps owns a 16-row x 8-instance block over one half of every chunk's K range, splits
+// the state into BF16 hi + lo as it builds its B fragments, and accumulates
+// hi*hi + hi*lo + lo*hi (the scheme of the gain GEMM); the two K halves' sums are added in a
+// fixed order and scaled back by the rows' power-of-two scales. The update then gives each
+// thread one row and two instances, with every load it needs issued before the arithmetic
+// (flux columns and values, state, vectors), so the latency of the L2 round trips overlaps.
 constexpr int kRowsThreads = 512;
-constexpr int kKGroups = kRowsThreads / 64;  // K-slices of each product chunk
-static_assert(2 * kKGroups * kRT * (kIT + 1) <= kRowStages * kStageFloats, "partial tiles fit the ring");
+constexpr int kKHalves = 2;  // K halves of each product chunk (8 warps each)
+static_assert(kRowsThreads / 32 == 2 * 4 * kKHalves, "16 warps: 2 row blocks x 4 instance blocks x 2 K halves");
+static_assert(2 * kKHalves * kRT * (kIT + 1) * 4 <= kRowStages * kStageBytes, "partial tiles fit the ring");
 constexpr int kEllFast = 8;  // ELL widths up to this take the hoisted-load flux path
 constexpr int kGatherChunk = 18;  // split partials in flight per instance in the gain gather
 
@@ -943,15 +966,17 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     __shared__ RowJob s_job[kRowsMaxJobs];
     __shared__ int s_njob;
     extern __shared__ __align__(16) float rows_dyn[];
-    // after the products the same memory holds the two halves' loss and emission tiles
+    // after the products the same memory holds the two K halves' loss and emission tiles
     float(*s_pl)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn);
-    float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + kKGroups * kRT * (kIT + 1));
+    float(*s_pe)[kRT][kIT + 1] = reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + kKHalves * kRT * (kIT + 1));
+    unsigned char* ring = reinterpret_cast<unsigned char*>(rows_dyn);
     __shared__ double s_min[kRT][kIT + 1];  // padded: the per-instance reduction reads down columns
     __shared__ int s_nonfin[kIT];
     const int tid = threadIdx.x;
-    // products: 8 groups of 64 threads split each K chunk; a 4 x 4 micro-tile per thread (rows
-    // ty + 8k, instances 4 tx .. 4 tx + 3), so a 16-wide slice of K costs 5 shared loads per 16 FMAs
-    const int kg = tid >> 6, lt = tid & 63, tx = lt & 7, ty = lt >> 3;
+    // products: warp w takes rows 16 (w & 1) .. + 15, instances 8 ((w >> 1) & 3) .. + 7 and the
+    // K half w >> 3 of every chunk
+    const int wp = tid >> 5, ln = tid & 31;
+    const int mblk = wp & 1, nblk = (wp >> 1) & 3, khalf = wp >> 3;
     const int a0 = blockIdx.x * kRT, i0 = blockIdx.y * kIT;
     const int n = ops.n_state, B = ops.Bcap;
     // the device step counter advances once per launch sequence (advance_step); kpos is this
@@ -981,9 +1006,12 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         cols[e] = -1;
         vals[e] = 0.f;
     }
+    float lsc = 1.f, esc = 1.f;
     if (mine) {
         inv_ap = (double)__ldg(ops.invAp + a);
         injv = (double)__ldg(ops.inj + a);
+        if (ops.has_bin) lsc = __ldg(ops.loss_rscale + (a % ops.n_mom));
+        if (ops.has_emi) esc = __ldg(ops.emi_rscale + a);
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const int i = ib + j;
@@ -1012,24 +1040,36 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
     // the next step's GEMM may launch now: it waits for this grid's completion before it reads
     // the new state, so only its set-up (barriers, tensor memory, its first G tile) overlaps
     if (tid == 0) pdl_trigger();
-    // a chunk into ring stage st: 1024 16-byte pieces of each operand and of the state, 2 + 2 + 2
-    // per thread
+    // a chunk into ring stage st: 512 16-byte pieces of each operand half (32 rows x 128 BF16)
+    // and 1024 of the state (128 rows x 32 FP32), 4 + 2 per thread
     auto issue = [&](int k, int st) {
-        float* sL = rows_dyn + st * kStageFloats;
-        float* sE = sL + kRT * kLS;
-        float* sF = sE + kRT * kLS;
+        unsigned char* base = ring + (size_t)st * kStageBytes;
         const RowJob J = s_job[k];
+        {
+            const int rr = tid >> 4, c8 = (tid & 15) * 8;
+            const bool ok = a0 + rr < n && J.c0 + c8 < J.nc;
+            const size_t ol = (size_t)rr * kOP + c8;
+            if (J.TL) {
+                const __nv_bfloat16* src = J.TL + (size_t)rr * J.ldl + J.c0 + c8;
+                cp_async16(base + 2 * ol, ok ? src : J.TL, ok ? 16 : 0);
+                cp_async16(base + kOpBytes + 2 * ol, ok ? src + ops.loss_lo : J.TL, ok ? 16 : 0);
+            }
+            if (J.TE) {
+                const __nv_bfloat16* src = J.TE + (size_t)rr * J.lde + J.c0 + c8;
+                cp_async16(base + 2 * kOpBytes + 2 * ol, ok ? src : J.TE, ok ? 16 : 0);
+                cp_async16(base + 3 * kOpBytes + 2 * ol, ok ? src + ops.emi_lo : J.TE, ok ? 16 : 0);
+            }
+        }
+        float* sF = reinterpret_cast<float*>(base + 4 * kOpBytes);
 #pragma unroll
         for (int q2 = 0; q2 < 2; ++q2) {
             const int q = tid + kRowsThreads * q2;
-            const int rr = q >> 5, c4 = (q & 31) * 4;
-            const bool ok = a0 + rr < n && J.c0 + c4 < J.nc;
-            if (J.TL) cp_async16(sL + rr * kLS + c4, ok ? J.TL + (size_t)rr * J.ldl + J.c0 + c4 : J.TL, ok ? 16 : 0);
-            if (J.TE) cp_async16(sE + rr * kLS + c4, ok ? J.TE + (size_t)rr * J.lde + J.c0 + c4 : J.TE, ok ? 16 : 0);
             const int cr = q >> 3, i4 = (q & 7) * 4;
+            // state rows past the operand's columns are zero: the A operand there is zero too,
+            // and zero times a stale value could be a NaN
             const bool okf = J.c0 + cr < J.nc && i0 + i4 < B;
             const float* srcf = okf ? F + (size_t)(J.col0 + J.c0 + cr) * B + i0 + i4 : F;
-            cp_async16(sF + cr * kIT + i4, srcf, okf ? 16 : 0);
+            cp_async16(sF + cr * kFP + i4, srcf, okf ? 16 : 0);
         }
     };
     // the first chunks are in flight while the update's operands are loaded below
@@ -1053,64 +1093,61 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         fv[e] = (mine && cols[e] >= 0) ? *reinterpret_cast<const float2*>(F + (size_t)cols[e] * B + ib)
                                        : make_float2(0.f, 0.f);
 
-    // accumulators as packed pairs of instances (tx * 4 + {0, 1} and {2, 3}) for the f32x2 FMAs
-    unsigned long long acc_l[4][2], acc_e[4][2];
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            acc_l[k][j] = 0ull;
-            acc_e[k][j] = 0ull;
-        }
+    // MMA accumulators of the warp's 16 x 8 block: rows g and g + 8, instances 2t and 2t + 1
+    // (g = lane / 4, t = lane % 4)
+    float acc_l[4] = {0.f, 0.f, 0.f, 0.f}, acc_e[4] = {0.f, 0.f, 0.f, 0.f};
     if (fast) {
         const int nj = s_njob;
-        const int k0 = kg * (kCK / kKGroups);
+        const int g = ln >> 2, t = ln & 3;
+        // ldmatrix row of this lane: matrices 0/1 take rows 0-7 / 8-15 at K 0-7, 2/3 at K 8-15
+        const int lrow = 16 * mblk + (ln & 7) + ((ln >> 3) & 1) * 8, lcol = (ln >> 4) * 8;
         for (int k = 0; k < nj; ++k) {
             cp_async_wait<kRowStages - 2>();
             __syncthreads();  // chunk k landed for every thread; chunk k - 1's stage is free
             if (k + kRowStages - 1 < nj) issue(k + kRowStages - 1, (k + kRowStages - 1) % kRowStages);
             cp_async_commit();
-            const float* sL = rows_dyn + (k % kRowStages) * kStageFloats;
-            const float* sE = sL + kRT * kLS;
-            const float* sF = sE + kRT * kLS;
+            const unsigned char* base = ring + (size_t)(k % kRowStages) * kStageBytes;
+            const uint32_t sa = smem_addr(base);
+            const float* sF = reinterpret_cast<const float*>(base + 4 * kOpBytes);
             const bool hl = s_job[k].TL != nullptr, he = s_job[k].TE != nullptr;
-            if (hl) {
 #pragma unroll
-                for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
-                    const ulonglong2 f4 = *reinterpret_cast<const ulonglong2*>(sF + cc * kIT + tx * 4);
-#pragma unroll
-                    for (int k2 = 0; k2 < 4; ++k2) {
-                        const float l = sL[(ty + 8 * k2) * kLS + cc];
-                        ffma2(acc_l[k2][0], l, f4.x);
-                        ffma2(acc_l[k2][1], l, f4.y);
-                    }
+            for (int kk = 0; kk < kCK / kKHalves / 16; ++kk) {
+                const int kb = khalf * (kCK / kKHalves) + kk * 16;
+                // B fragment: state rows kb + 2t, +1 and kb + 2t + 8, +9 of instance 8 nblk + g
+                const float* fp = sF + (kb + 2 * t) * kFP + 8 * nblk + g;
+                uint32_t bh0, bl0, bh1, bl1;
+                split_pair(fp[0], fp[kFP], bh0, bl0);
+                split_pair(fp[8 * kFP], fp[9 * kFP], bh1, bl1);
+                const uint32_t ao = (uint32_t)(2 * (lrow * kOP + kb + lcol));
+                if (hl) {
+                    uint32_t ah[4], al[4];
+                    ldsm_x4(sa + ao, ah);
+                    ldsm_x4(sa + kOpBytes + ao, al);
+                    mma_bf16_16816(acc_l, ah, bh0, bh1);
+                    mma_bf16_16816(acc_l, ah, bl0, bl1);
+                    mma_bf16_16816(acc_l, al, bh0, bh1);
                 }
-            }
-            if (he) {
-#pragma unroll
-                for (int cc = k0; cc < k0 + kCK / kKGroups; ++cc) {
-                    const ulonglong2 f4 = *reinterpret_cast<const ulonglong2*>(sF + cc * kIT + tx * 4);
-#pragma unroll
-                    for (int k2 = 0; k2 < 4; ++k2) {
-                        const float e = sE[(ty + 8 * k2) * kLS + cc];
-                        ffma2(acc_e[k2][0], e, f4.x);
-                        ffma2(acc_e[k2][1], e, f4.y);
-                    }
+                if (he) {
+                    uint32_t ah[4], al[4];
+                    ldsm_x4(sa + 2 * kOpBytes + ao, ah);
+                    ldsm_x4(sa + 3 * kOpBytes + ao, al);
+                    mma_bf16_16816(acc_e, ah, bh0, bh1);
+                    mma_bf16_16816(acc_e, ah, bl0, bl1);
+                    mma_bf16_16816(acc_e, al, bh0, bh1);
                 }
             }
         }
         cp_async_wait<0>();
-        __syncthreads();  // the ring is free: park the groups' sums
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const float2 pl = unpack_f32x2(acc_l[k][j]), pe = unpack_f32x2(acc_e[k][j]);
-                s_pl[kg][ty + 8 * k][tx * 4 + 2 * j] = pl.x;
-                s_pl[kg][ty + 8 * k][tx * 4 + 2 * j + 1] = pl.y;
-                s_pe[kg][ty + 8 * k][tx * 4 + 2 * j] = pe.x;
-                s_pe[kg][ty + 8 * k][tx * 4 + 2 * j + 1] = pe.y;
-            }
+        __syncthreads();  // the ring is free: park the K halves' sums
+        const int r0 = 16 * mblk + g, c0 = 8 * nblk + 2 * t;
+        s_pl[khalf][r0][c0] = acc_l[0];
+        s_pl[khalf][r0][c0 + 1] = acc_l[1];
+        s_pl[khalf][r0 + 8][c0] = acc_l[2];
+        s_pl[khalf][r0 + 8][c0 + 1] = acc_l[3];
+        s_pe[khalf][r0][c0] = acc_e[0];
+        s_pe[khalf][r0][c0 + 1] = acc_e[1];
+        s_pe[khalf][r0 + 8][c0] = acc_e[2];
+        s_pe[khalf][r0 + 8][c0 + 1] = acc_e[3];
     }
     pdl_wait();  // this step's gain GEMM has completed: its split partials are visible
     // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
@@ -1205,14 +1242,9 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                 continue;
             }
             float loss, emi;
-            if (fast) {
-                loss = 0.f;
-                emi = 0.f;
-#pragma unroll
-                for (int g = 0; g < kKGroups; ++g) {  // fixed order
-                    loss += s_pl[g][r][jb + j];
-                    emi += s_pe[g][r][jb + j];
-                }
+            if (fast) {  // the K halves in a fixed order, then the rows' scales (powers of two)
+                loss = (s_pl[0][r][jb + j] + s_pl[1][r][jb + j]) * lsc;
+                emi = (s_pe[0][r][jb + j] + s_pe[1][r][jb + j]) * esc;
             } else {
                 row_terms_direct(ops, F, a, am, cell, s, ib + j, loss, emi);
             }

@@ -35,8 +35,9 @@ extern "C" {
 /* state precision (Main.Precision, SteppingStructs.jl:36-38) */
 #define DTB_F64 0       /* Float64 state and operators */
 #define DTB_F32 1       /* Float32 state and operators (the reference's CUDA precision, Backends.jl:12) */
-#define DTB_MIXED 2     /* batched: G and E as BF16 hi+lo with per-row FP32 scale, f in FP32,
-                           FP64 compensated update and moments */
+#define DTB_MIXED 2     /* batched: G, the loss rows and E as BF16 hi+lo with per-row scales (FP32
+                           accumulation on the tensor cores), f in FP32, FP64 compensated update
+                           and moments */
 
 /* dtb_opts.flags */
 #define DTB_FLAG_SYMPLECTIC 1  /* ForwardSymplecticEulerStruct (SteppingStructs.jl:104-229):
