@@ -549,9 +549,9 @@ def test_long_run_matches_oracle_with_drift(cuda, n_steps):
     """Mixed precision over a configuration's full run length (5,000 steps as config 3, 10,000
     as config 2) on a reduced grid (2 species x 32 states, 16 instances, every operator, per-
     instance dt, injection): every instance within relative L-inf 1e-5 of the FP64 oracle run;
-    the FP64 device moments of the mixed run within 1e-5 (relative to the initial moment) of the
-    oracle's number and energy per species, i.e. the mixed path adds at most 1e-5 of number or
-    energy drift over the oracle's own."""
+    the FP64 device moments of the mixed run within relative 1e-5 of the oracle's number and
+    energy per species at the end, i.e. the mixed path's number and energy drift is the oracle's
+    own to 1e-5."""
     from dtb.structs import energy_weights
     w = synth.batched_two_species(8, 1e-2, 1e2, 4, 16, seed=31)
     rng = np.random.default_rng(2)
@@ -570,8 +570,8 @@ def test_long_run_matches_oracle_with_drift(cuda, n_steps):
             f, _, _ = ops.step(f, w.dt[i], 0)
         assert rel_linf(m.get_f(i), f) <= TOL_RUN, i
         on, oe = _moments_oracle(w.ps, f)
-        assert np.all(np.abs(num1[i] - on) / num0[i] <= 1e-5), i
-        assert np.all(np.abs(en1[i] - oe) / en0[i] <= 1e-5), i
+        assert np.all(np.abs(num1[i] - on) / np.abs(on) <= 1e-5), i
+        assert np.all(np.abs(en1[i] - oe) / np.abs(oe) <= 1e-5), i
     m.close()
 
 
