@@ -181,10 +181,21 @@ void apply_plan(MixedGroup& G, const GemmPlan& p, int Bcols) {
 }
 
 // Splits that fill the device once: one CTA per SM, or one pair per co-resident cluster.
+// K splits that fill the device once, or a whole number of times when one fill would leave a
+// hi*hi accumulator more than kMaxTilesPerAcc K tiles. A GEMM kernel spreads a split's hi*hi
+// products over 512 / bn - 1 tensor-memory accumulators (one on SM pairs); each accumulator is
+// FP32, and its error grows with the number of MMAs it sums (about 2e-5 relative after 3,328 K
+// values in one accumulator), so this bounds the error of the gain term to a few 1e-6.
+constexpr int kMaxTilesPerAcc = 32;
 int fill_splits(const dtb_ctx* c, const MixedGroup& G, int pair, int bn, int Bcols, int max_pairs) {
     const int n_tiles = (Bcols + bn - 1) / bn;
     const double units = pair ? (double)(G.m_tiles / 2 * n_tiles) : (double)(G.m_tiles * n_tiles);
-    return std::max(1, (int)std::lround((pair ? max_pairs : c->num_sms) / units));
+    const int fill = std::max(1, (int)std::lround((pair ? max_pairs : c->num_sms) / units));
+    const int n_hh = pair ? 1 : 512 / bn - 1;
+    const int T = G.n_cb * G.N1;
+    const int need = (T + kMaxTilesPerAcc * n_hh - 1) / (kMaxTilesPerAcc * n_hh);
+    const int waves = std::max(1, (need + fill - 1) / fill);
+    return fill * waves;
 }
 
 // Without timing: the widest tile the columns fill, on SM pairs when the rows pair up.

@@ -121,6 +121,11 @@ struct GemmCfg {
     static constexpr int DATA = SA * 2 * A_BYTES + SB * 2 * B_BYTES;
     static constexpr int BARS = (2 * SA + 2 * SB + 3) * 8;
     static constexpr int SMEM = 1024 + DATA + BARS + 16;   // 1024: alignment slack
+    // tensor memory: all 512 columns as 512 / BN accumulators of BN columns; the hi*hi products
+    // go round-robin by K tile into the first NHH of them and the hi*lo + lo*hi products into the
+    // last, so no FP32 accumulator sums more than a fraction of the split's K range
+    static constexpr int NACC = 512 / BN;
+    static constexpr int NHH = NACC - 1;
 };
 
 template <int BN>
@@ -181,9 +186,9 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    if (warp == C::NPW + 1) {  // TMEM: BN fp32 columns x 128 lanes
+    if (warp == C::NPW + 1) {  // TMEM: NACC accumulators of BN fp32 columns x 128 lanes
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_holder)),
-                     "r"(BN)
+                     "r"(512)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -246,12 +251,14 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 const uint32_t blo = smem_addr(b_base + (size_t)(sb * 2 + 1) * C::B_BYTES);
                 const uint64_t dahi = umma_desc_sw128(ahi), dalo = umma_desc_sw128(alo);
                 const uint64_t dbhi = umma_desc_sw128(bhi), dblo = umma_desc_sw128(blo);
+                const uint32_t d_hh = tmem + (uint32_t)(BN * (j % C::NHH));
+                const uint32_t d_lo = tmem + (uint32_t)(BN * C::NHH);
 #pragma unroll
                 for (int kk = 0; kk < kMmaK / 16; ++kk) {
                     const uint64_t o = (uint64_t)(kk * 2);  // 16 BF16 = 32 bytes = 2 x 16 B
-                    umma_bf16(tmem, dahi + o, dbhi + o, idesc, (j > 0 || kk > 0) ? 1u : 0u);
-                    umma_bf16(tmem, dahi + o, dblo + o, idesc, 1u);
-                    umma_bf16(tmem, dalo + o, dbhi + o, idesc, 1u);
+                    umma_bf16(d_hh, dahi + o, dbhi + o, idesc, (j >= C::NHH || kk > 0) ? 1u : 0u);
+                    umma_bf16(d_lo, dahi + o, dblo + o, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+                    umma_bf16(d_lo, dalo + o, dbhi + o, idesc, 1u);
                 }
                 umma_commit(smem_addr(&empty_a[sa]));
                 umma_commit(smem_addr(&empty_b[sb]));
@@ -359,22 +366,32 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
         }
         if (ok && !*abort_flag) {
             float* dst = a.partial + (size_t)split * a.Bpad * a.M;
-            // two 16-column loads in flight per wait
-            for (int cc = 0; cc < ncol; cc += 32) {
-                uint32_t r0[16], r1[16];
-                const bool ok0 = nt > 0 && c0 + cc < n_eff, ok1 = nt > 0 && c0 + cc + 16 < n_eff && cc + 16 < ncol;
+            // the hi*hi accumulators that received products (tile j went to j % NHH), then the
+            // lo accumulator, summed in that fixed order in FP32 with round-to-nearest; all loads
+            // of a 16-column chunk in flight before one wait
+            const int n_hh = min(C::NHH, nt);
+            for (int cc = 0; cc < ncol; cc += 16) {
+                uint32_t r[C::NACC][16];
+                const bool live = nt > 0 && c0 + cc < n_eff;
                 const uint32_t ta = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(c0 + cc);
-                if (ok0) tmem_ld16_issue(ta, r0);
-                if (ok1) tmem_ld16_issue(ta + 16, r1);
-                if (ok0 || ok1) tmem_ld_wait();
+                if (live) {
+#pragma unroll
+                    for (int h = 0; h < C::NACC; ++h)
+                        if (h < n_hh || h == C::NHH) tmem_ld16_issue(ta + (uint32_t)(BN * h), r[h]);
+                    tmem_ld_wait();
+                }
                 if (row < a.M) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k)
-                        dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = ok0 ? __uint_as_float(r0[k]) : 0.f;
-                    if (cc + 16 < ncol) {
+                    for (int k = 0; k < 16; ++k) {
+                        float v = 0.f;
+                        if (live) {
+                            v = __uint_as_float(r[0][k]);
 #pragma unroll
-                        for (int k = 0; k < 16; ++k)
-                            dst[(size_t)(n0 + c0 + cc + 16 + k) * a.M + row] = ok1 ? __uint_as_float(r1[k]) : 0.f;
+                            for (int h = 1; h < C::NHH; ++h)
+                                if (h < n_hh) v += __uint_as_float(r[h][k]);
+                            v += __uint_as_float(r[C::NHH][k]);
+                        }
+                        dst[(size_t)(n0 + c0 + cc + k) * a.M + row] = v;
                     }
                 }
             }
@@ -384,7 +401,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
     __syncthreads();
     if (warp == C::NPW + 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
     }
 }
 
@@ -507,9 +524,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    if (warp == C::NPW + 1) {  // same warp in both CTAs: BN fp32 columns x 128 lanes in each
+    if (warp == C::NPW + 1) {  // same warp in both CTAs: two accumulators of BN fp32 columns x 128 lanes
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_holder)),
-                     "r"(C::BN)
+                     "r"(2 * C::BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
     }
@@ -573,12 +590,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
                 const uint32_t blo = smem_addr(b_base + (size_t)(sb * 2 + 1) * C::B_BYTES);
                 const uint64_t dahi = umma_desc_sw128(ahi), dalo = umma_desc_sw128(alo);
                 const uint64_t dbhi = umma_desc_sw128(bhi), dblo = umma_desc_sw128(blo);
+                // hi*hi into the first accumulator, hi*lo + lo*hi into the second
 #pragma unroll
                 for (int kk = 0; kk < kMmaK / 16; ++kk) {
                     const uint64_t o = (uint64_t)(kk * 2);
                     umma2_bf16(tmem, dahi + o, dbhi + o, idesc, (j > 0 || kk > 0) ? 1u : 0u);
-                    umma2_bf16(tmem, dahi + o, dblo + o, idesc, 1u);
-                    umma2_bf16(tmem, dalo + o, dbhi + o, idesc, 1u);
+                    umma2_bf16(tmem + C::BN, dahi + o, dblo + o, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+                    umma2_bf16(tmem + C::BN, dalo + o, dbhi + o, idesc, 1u);
                 }
                 umma2_commit(smem_addr(&empty_a[sa]));
                 umma2_commit(peer_addr(smem_addr(&empty_a[sa]), 1u));
@@ -696,22 +714,31 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
             tc_fence_after();
         }
         if (ok && !*abort_flag) {
-            // the warp's 128 columns: every tensor-memory load in flight before one wait
+            // the warp's 128 columns, 64 at a time: both accumulators' loads in flight before one
+            // wait, then hi*hi + (hi*lo + lo*hi) in FP32 with round-to-nearest
             static_assert(C::BN / (C::NPW / 4) == 128, "epilogue covers 128 columns per warp");
             float* dst = a.partial + (size_t)split * a.Bpad * a.M + (size_t)(n0 + c0) * a.M + row;
-            uint32_t rv[8][16];
             const uint32_t ta = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)c0;
-            if (nt > 0 && c0 < n_eff) {
 #pragma unroll
-                for (int q = 0; q < 8; ++q) tmem_ld16_issue(ta + 16 * q, rv[q]);
-                tmem_ld_wait();
-            }
-            if (row < a.M) {
+            for (int hf = 0; hf < 2; ++hf) {
+                uint32_t rv[4][16], rl[4][16];
+                if (nt > 0 && c0 + 64 * hf < n_eff) {
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const bool live = nt > 0 && c0 + 16 * q < n_eff;
+                    for (int q = 0; q < 4; ++q) {
+                        tmem_ld16_issue(ta + 64 * hf + 16 * q, rv[q]);
+                        tmem_ld16_issue(ta + C::BN + 64 * hf + 16 * q, rl[q]);
+                    }
+                    tmem_ld_wait();
+                }
+                if (row < a.M) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) dst[(size_t)(16 * q + k) * a.M] = live ? __uint_as_float(rv[q][k]) : 0.f;
+                    for (int q = 0; q < 4; ++q) {
+                        const bool live = nt > 0 && c0 + 64 * hf + 16 * q < n_eff;
+#pragma unroll
+                        for (int k = 0; k < 16; ++k)
+                            dst[(size_t)(64 * hf + 16 * q + k) * a.M] =
+                                live ? __uint_as_float(rv[q][k]) + __uint_as_float(rl[q][k]) : 0.f;
+                    }
                 }
             }
         }
@@ -723,7 +750,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
     cluster_sync_all();
     if (warp == C::NPW + 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * C::BN) : "memory");
     }
 }
 
@@ -1095,7 +1122,9 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
 
     // MMA accumulators of the warp's 16 x 8 block: rows g and g + 8, instances 2t and 2t + 1
     // (g = lane / 4, t = lane % 4)
+    // (hi*hi and the hi*lo + lo*hi corrections in separate accumulators, as in the gain GEMM)
     float acc_l[4] = {0.f, 0.f, 0.f, 0.f}, acc_e[4] = {0.f, 0.f, 0.f, 0.f};
+    float cor_l[4] = {0.f, 0.f, 0.f, 0.f}, cor_e[4] = {0.f, 0.f, 0.f, 0.f};
     if (fast) {
         const int nj = s_njob;
         const int g = ln >> 2, t = ln & 3;
@@ -1124,22 +1153,27 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
                     ldsm_x4(sa + ao, ah);
                     ldsm_x4(sa + kOpBytes + ao, al);
                     mma_bf16_16816(acc_l, ah, bh0, bh1);
-                    mma_bf16_16816(acc_l, ah, bl0, bl1);
-                    mma_bf16_16816(acc_l, al, bh0, bh1);
+                    mma_bf16_16816(cor_l, ah, bl0, bl1);
+                    mma_bf16_16816(cor_l, al, bh0, bh1);
                 }
                 if (he) {
                     uint32_t ah[4], al[4];
                     ldsm_x4(sa + 2 * kOpBytes + ao, ah);
                     ldsm_x4(sa + 3 * kOpBytes + ao, al);
                     mma_bf16_16816(acc_e, ah, bh0, bh1);
-                    mma_bf16_16816(acc_e, ah, bl0, bl1);
-                    mma_bf16_16816(acc_e, al, bh0, bh1);
+                    mma_bf16_16816(cor_e, ah, bl0, bl1);
+                    mma_bf16_16816(cor_e, al, bh0, bh1);
                 }
             }
         }
         cp_async_wait<0>();
         __syncthreads();  // the ring is free: park the K halves' sums
         const int r0 = 16 * mblk + g, c0 = 8 * nblk + 2 * t;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            acc_l[q] += cor_l[q];
+            acc_e[q] += cor_e[q];
+        }
         s_pl[khalf][r0][c0] = acc_l[0];
         s_pl[khalf][r0][c0 + 1] = acc_l[1];
         s_pl[khalf][r0 + 8][c0] = acc_l[2];
