@@ -181,20 +181,25 @@ void apply_plan(MixedGroup& G, const GemmPlan& p, int Bcols) {
 }
 
 // Splits that fill the device once: one CTA per SM, or one pair per co-resident cluster.
-// K splits that fill the device once, or a whole number of times when one fill would leave a
-// hi*hi accumulator more than kMaxTilesPerAcc K tiles. A GEMM kernel spreads a split's hi*hi
-// products over 512 / bn - 1 tensor-memory accumulators (one on SM pairs); each accumulator is
-// FP32, and its error grows with the number of MMAs it sums (about 2e-5 relative after 3,328 K
-// values in one accumulator), so this bounds the error of the gain term to a few 1e-6.
-constexpr int kMaxTilesPerAcc = 32;
+// K splits that fill the device once, or a whole number of times (at most kMaxWaves) when one
+// fill would leave a hi*hi accumulator more K tiles than its bound. A GEMM kernel spreads a
+// split's hi*hi products over 512 / bn - 1 tensor-memory accumulators (one on SM pairs). Each is
+// FP32 and its error grows with the number of MMAs it sums (measured: about 2e-5 relative after
+// 3,328 K values in one accumulator; config 3 reached 3e-4 in its state after 5,000 steps with
+// 20,736 K values per accumulator), so the bound keeps the gain term's error at a few 1e-6:
+// 16 K tiles per accumulator on one SM, 32 on SM pairs (where a second fill would double the
+// tensor-bound step's partial traffic).
+constexpr int kMaxTilesPerAccSm = 16;
+constexpr int kMaxTilesPerAccPair = 32;
+constexpr int kMaxWaves = 4;
 int fill_splits(const dtb_ctx* c, const MixedGroup& G, int pair, int bn, int Bcols, int max_pairs) {
     const int n_tiles = (Bcols + bn - 1) / bn;
     const double units = pair ? (double)(G.m_tiles / 2 * n_tiles) : (double)(G.m_tiles * n_tiles);
     const int fill = std::max(1, (int)std::lround((pair ? max_pairs : c->num_sms) / units));
-    const int n_hh = pair ? 1 : 512 / bn - 1;
+    const int per_split = pair ? kMaxTilesPerAccPair : kMaxTilesPerAccSm * (512 / bn - 1);
     const int T = G.n_cb * G.N1;
-    const int need = (T + kMaxTilesPerAcc * n_hh - 1) / (kMaxTilesPerAcc * n_hh);
-    const int waves = std::max(1, (need + fill - 1) / fill);
+    const int need = (T + per_split - 1) / per_split;
+    const int waves = std::min(kMaxWaves, std::max(1, (need + fill - 1) / fill));
     return fill * waves;
 }
 
