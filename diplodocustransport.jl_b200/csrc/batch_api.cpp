@@ -37,6 +37,8 @@ struct MixedGroup {
     double bytes = 0;  // hi + lo bytes of G
 };
 
+constexpr int kAdmitRing = 8;
+
 struct MixedState {
     int Bcap = 0;   // slots in the state matrix: the requested capacity rounded up to 4 (row stride)
     int Buser = 0;  // slots the caller may use
@@ -59,7 +61,13 @@ struct MixedState {
     cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step from state buffer 0 / 1
     int graph_steps = 16;
     std::vector<long long> h_stop, h_start;
-    float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation
+    float* pin_col = nullptr;  // [2][n_mom] staging of one slot's f and compensation (reads)
+    // admission records: a ring of kAdmitRing pinned host records, their device copies and an
+    // event per entry (an entry is rewritten only after its previous scatter has run)
+    unsigned char* adm_pin = nullptr;
+    unsigned char* adm_dev = nullptr;
+    cudaEvent_t adm_ev[8] = {};
+    int adm_next = 0;
     double* io_all = nullptr;  // device staging of the whole batch, f64 [Buser][n_mom]
     int* sp_off = nullptr;     // device species offsets
     double* mom_w = nullptr;   // device energy weights (n_mom)
@@ -710,6 +718,12 @@ int commit_mixed(dtb_ctx* c) {
         DTB_TRY(c->alloc(&m->mom_out, sizeof(double) * 2 * (size_t)c->ns * B * nsp));
     }
     DTB_CUDA(cudaMallocHost(&m->pin_col, sizeof(float) * 2 * (size_t)n_st));
+    {
+        const size_t rb = admit_record(n_st, c->ns).bytes;
+        DTB_CUDA(cudaMallocHost(&m->adm_pin, rb * kAdmitRing));
+        DTB_TRY(c->alloc(&m->adm_dev, rb * kAdmitRing));
+        for (int k = 0; k < kAdmitRing; ++k) DTB_CUDA(cudaEventCreateWithFlags(&m->adm_ev[k], cudaEventDisableTiming));
+    }
     DTB_CUDA(cudaMallocHost(&c->pin_err, sizeof(int)));
     m->h_stop.assign((size_t)B, 0);
     m->h_start.assign((size_t)B, 0);
@@ -844,6 +858,9 @@ void destroy_mixed(dtb_ctx* c) {
         if (g1) cudaGraphExecDestroy(g1);
     for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
     if (m->pin_col) cudaFreeHost(m->pin_col);
+    if (m->adm_pin) cudaFreeHost(m->adm_pin);
+    for (cudaEvent_t e : m->adm_ev)
+        if (e) cudaEventDestroy(e);
     delete m;
     c->mixed = nullptr;
 }
@@ -1076,43 +1093,39 @@ int32_t dtb_batch_admit(dtb_ctx* c, int32_t slot, const double* f0, double dt_sc
     DTB_CHECK(f0, DTB_EINVAL, "dtb_batch_admit: null f0");
     DTB_CHECK(n_steps >= 0 && std::isfinite(dt_scale), DTB_EINVAL, "dtb_batch_admit: bad dt_scale or step count");
     DeviceGuard g(c->device);
-    DTB_CUDA(cudaStreamSynchronize(c->stream));
     const int n = (int)c->n_state, B = m->Bcap;
+    // the next staging record of the ring, free once its previous scatter has run
+    const AdmitRecord R = admit_record(n, c->ns);
+    const int k = m->adm_next;
+    m->adm_next = (k + 1) % kAdmitRing;
+    DTB_CUDA(cudaEventSynchronize(m->adm_ev[k]));
+    unsigned char* rec = m->adm_pin + (size_t)k * R.bytes;
+    float* fcol = reinterpret_cast<float*>(rec + R.f);
+    float* ccol = reinterpret_cast<float*>(rec + R.c);
     for (int i = 0; i < n; ++i) {
-        m->pin_col[i] = (float)f0[i];
-        m->pin_col[n + i] = (float)(f0[i] - (double)(float)f0[i]);  // exact remainder as the compensation
+        fcol[i] = (float)f0[i];
+        ccol[i] = (float)(f0[i] - (double)(float)f0[i]);  // exact remainder as the compensation
     }
-    float* Fd = m->F[m->cur] + slot;
-    float* Cd = m->C[m->cur] + slot;
-    DTB_CUDA(cudaMemcpy2DAsync(Fd, sizeof(float) * B, m->pin_col, sizeof(float), sizeof(float), n,
-                               cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaMemcpy2DAsync(Cd, sizeof(float) * B, m->pin_col + n, sizeof(float), sizeof(float), n,
-                               cudaMemcpyHostToDevice, c->stream));
     // power-of-two species scales from the initial spectrum: X uses f * 2^-e
-    std::vector<float> sg((size_t)c->ns), isg((size_t)c->ns);
+    float* sg = reinterpret_cast<float*>(rec + R.sig);
+    float* isg = reinterpret_cast<float*>(rec + R.isig);
     for (int sp = 0; sp < c->ns; ++sp) {
         double mx = 0;
         for (int cl = 0; cl < c->n_space; ++cl)
-            for (int64_t k = c->off[sp]; k < c->off[sp + 1]; ++k) mx = std::max(mx, std::fabs(f0[cl * c->n_mom + k]));
+            for (int64_t q = c->off[sp]; q < c->off[sp + 1]; ++q) mx = std::max(mx, std::fabs(f0[cl * c->n_mom + q]));
         int ex = 0;
         if (mx > 0 && std::isfinite(mx)) std::frexp(mx, &ex);
-        sg[(size_t)sp] = std::ldexp(1.0f, ex);
-        isg[(size_t)sp] = std::ldexp(1.0f, -ex);
-    }
-    for (int sp = 0; sp < c->ns; ++sp) {
-        DTB_CUDA(cudaMemcpyAsync(m->sig + (size_t)sp * B + slot, &sg[(size_t)sp], sizeof(float), cudaMemcpyHostToDevice,
-                                 c->stream));
-        DTB_CUDA(cudaMemcpyAsync(m->isig + (size_t)sp * B + slot, &isg[(size_t)sp], sizeof(float),
-                                 cudaMemcpyHostToDevice, c->stream));
+        sg[sp] = std::ldexp(1.0f, ex);
+        isg[sp] = std::ldexp(1.0f, -ex);
     }
     const long long stop = m->host_step + n_steps;
-    const unsigned long long inf = ord_enc_host(INFINITY);
-    const int zero = 0;
-    DTB_CUDA(cudaMemcpyAsync(m->dt_scale + slot, &dt_scale, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaMemcpyAsync(m->stop_step + slot, &stop, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaMemcpyAsync(m->min_ratio + slot, &inf, sizeof(inf), cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaMemcpyAsync(m->nonfinite + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    DTB_CUDA(cudaStreamSynchronize(c->stream));
+    *reinterpret_cast<double*>(rec + R.dt) = dt_scale;
+    *reinterpret_cast<long long*>(rec + R.stop) = stop;
+    unsigned char* drec = m->adm_dev + (size_t)k * R.bytes;
+    DTB_CUDA(cudaMemcpyAsync(drec, rec, R.bytes, cudaMemcpyHostToDevice, c->stream));
+    DTB_CUDA(launch_admit_slot(drec, n, c->ns, slot, B, m->F[m->cur], m->C[m->cur], m->sig, m->isig, m->dt_scale,
+                               m->stop_step, m->min_ratio, m->nonfinite, ord_enc_host(INFINITY), c->stream));
+    DTB_CUDA(cudaEventRecord(m->adm_ev[k], c->stream));
     m->h_stop[(size_t)slot] = stop;
     m->h_start[(size_t)slot] = m->host_step;
     return DTB_OK;

@@ -130,6 +130,27 @@ struct MixedRowOps {
 cudaError_t launch_mixed_rows(const MixedRowOps& ops, const float* F_in, const float* C_in, float* F_out,
                               float* C_out, const unsigned long long* gstep, int kpos, cudaStream_t s);
 cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s);
+
+// Byte layout of one admission record (n states, ns species): f and compensation columns, the
+// species scales and their reciprocals, dt / dt0 and the stop step; the record is staged in
+// pinned memory, copied in one piece and scattered by admit_slot_kernel.
+struct AdmitRecord {
+    size_t f, c, sig, isig, dt, stop, bytes;
+};
+__host__ __device__ inline AdmitRecord admit_record(int n, int ns) {
+    AdmitRecord r;
+    r.f = 0;
+    r.c = r.f + 4 * (size_t)n;
+    r.sig = r.c + 4 * (size_t)n;
+    r.isig = r.sig + 4 * (size_t)ns;
+    r.dt = (r.isig + 4 * (size_t)ns + 7) / 8 * 8;
+    r.stop = r.dt + 8;
+    r.bytes = (r.stop + 8 + 255) / 256 * 256;
+    return r;
+}
+cudaError_t launch_admit_slot(const unsigned char* rec, int n, int ns, int slot, int Bst, float* F, float* C, float* sig,
+                              float* isig, double* dt_scale, long long* stop, unsigned long long* min_ratio,
+                              int* nonfinite, unsigned long long inf_enc, cudaStream_t s);
 cudaError_t launch_pack_f(const double* io, int Buser, int n, int Bcap, float* F, float* C, cudaStream_t s);
 cudaError_t launch_unpack_f(const float* F, const float* C, int Buser, int n, int Bcap, double* io, cudaStream_t s);
 int mixed_rows_tile_rows();

@@ -17,6 +17,7 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <utility>
 
 #include "batch_internal.h"
@@ -1419,6 +1420,41 @@ cudaError_t launch_batch_moments(const float* F, const float* C, int Bcap, const
 }
 
 __global__ void advance_step_kernel(unsigned long long* gstep, int n) { *gstep += (unsigned long long)n; }
+
+// Admission of one slot from a staged record (f column, compensation column, the species
+// scales and their reciprocals, dt / dt0, stop step): one launch instead of a copy per field.
+__global__ void __launch_bounds__(256) admit_slot_kernel(const unsigned char* __restrict__ rec, int n, int ns, int slot,
+                                                         int Bst, float* __restrict__ F, float* __restrict__ C,
+                                                         float* __restrict__ sig, float* __restrict__ isig,
+                                                         double* __restrict__ dt_scale, long long* __restrict__ stop,
+                                                         unsigned long long* __restrict__ min_ratio,
+                                                         int* __restrict__ nonfinite, unsigned long long inf_enc) {
+    const AdmitRecord R = admit_record(n, ns);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        F[(size_t)i * Bst + slot] = reinterpret_cast<const float*>(rec + R.f)[i];
+        C[(size_t)i * Bst + slot] = reinterpret_cast<const float*>(rec + R.c)[i];
+    }
+    if (i < ns) {
+        sig[(size_t)i * Bst + slot] = reinterpret_cast<const float*>(rec + R.sig)[i];
+        isig[(size_t)i * Bst + slot] = reinterpret_cast<const float*>(rec + R.isig)[i];
+    }
+    if (i == 0) {
+        dt_scale[slot] = *reinterpret_cast<const double*>(rec + R.dt);
+        stop[slot] = *reinterpret_cast<const long long*>(rec + R.stop);
+        min_ratio[slot] = inf_enc;
+        nonfinite[slot] = 0;
+    }
+}
+
+cudaError_t launch_admit_slot(const unsigned char* rec, int n, int ns, int slot, int Bst, float* F, float* C, float* sig,
+                              float* isig, double* dt_scale, long long* stop, unsigned long long* min_ratio,
+                              int* nonfinite, unsigned long long inf_enc, cudaStream_t s) {
+    const int th = std::max(n, ns);
+    admit_slot_kernel<<<(th + 255) / 256, 256, 0, s>>>(rec, n, ns, slot, Bst, F, C, sig, isig, dt_scale, stop,
+                                                       min_ratio, nonfinite, inf_enc);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_advance_step(unsigned long long* gstep, int n, cudaStream_t s) {
     advance_step_kernel<<<1, 1, 0, s>>>(gstep, n);
