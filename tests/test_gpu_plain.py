@@ -139,6 +139,21 @@ def test_f32_path_against_f64_oracle(cuda):
     m.close()
 
 
+def test_config1_recipe_full_run_length_f32(cuda):
+    """Config 1's recipe (p over 1e-3..1e3, FP32 operators and state, the reference's CUDA
+    precision) on a reduced grid (2 x 128 states) over the configuration's 2,000 steps: within
+    the FP32 tolerance of the FP64 oracle run of the same inputs."""
+    w = synth.two_species(16, 1e-3, 1e3, 8, seed=1)
+    m = make_method(w, precision=np.float32)
+    ops = oracle.blocked_from_workload(w)
+    f = w.f0.copy()
+    m.run(np.ones(2000))
+    for _ in range(2000):
+        f, _, _ = ops.step(f, 1.0, 0)
+    assert rel_linf(m.f, f) <= TOL32
+    m.close()
+
+
 def test_clamp_semantics_on_device(cuda):
     """Negative, tiny, NaN and Inf states go through SteppingMethods.jl:97-101 exactly."""
     w = synth.small(p_num=4, u_num=2, seed=14, with_emission=False)
