@@ -40,7 +40,8 @@ def _precision_code(Precision) -> int:
     raise ValueError("Precision must be Float32 or Float64 (SteppingStructs.jl:38)")
 
 
-def _upload_csc(L, ctx, M) -> None:
+def _upload_csc(L, ctx, M, part=None) -> None:
+    """A flux matrix as 0-based CSC: summed into F (part None) or kept as X_Flux / P_Flux."""
     if M is None or M.nnz == 0:
         return
     M = M.tocsc()
@@ -48,7 +49,10 @@ def _upload_csc(L, ctx, M) -> None:
     colptr = np.ascontiguousarray(M.indptr, dtype=np.int64)
     rowval = np.ascontiguousarray(M.indices, dtype=np.int64)
     nzval = np.ascontiguousarray(M.data, dtype=np.float64)
-    check(L.dtb_add_flux_csc(ctx, M.shape[0], iptr(colptr), iptr(rowval), dptr(nzval)))
+    if part is None:
+        check(L.dtb_add_flux_csc(ctx, M.shape[0], iptr(colptr), iptr(rowval), dptr(nzval)))
+    else:
+        check(L.dtb_add_flux_csc_part(ctx, part, M.shape[0], iptr(colptr), iptr(rowval), dptr(nzval)))
 
 
 def _upload_gain(L, ctx, g) -> None:
@@ -69,17 +73,6 @@ def _upload_gain(L, ctx, g) -> None:
         A = np.ascontiguousarray(A, dtype=np.float64)
         dtype = _lib.DTB_DTYPE_F64
     check(L.dtb_add_gain_block(ctx, g.out_sp, g.in1_sp, g.in2_sp, ctypes.c_void_p(A.ctypes.data), dtype, 0))
-
-
-def _upload_csc_part(L, ctx, M, part) -> None:
-    if M is None or M.nnz == 0:
-        return
-    M = M.tocsc()
-    M.sort_indices()
-    colptr = np.ascontiguousarray(M.indptr, dtype=np.int64)
-    rowval = np.ascontiguousarray(M.indices, dtype=np.int64)
-    nzval = np.ascontiguousarray(M.data, dtype=np.float64)
-    check(L.dtb_add_flux_csc_part(ctx, part, M.shape[0], iptr(colptr), iptr(rowval), dptr(nzval)))
 
 
 class ForwardEulerStruct:
@@ -115,8 +108,8 @@ class ForwardEulerStruct:
         self.ctx = ctx
         try:
             L = self.L
-            _upload_csc_part(L, ctx, FluxM.X_Flux, _lib.DTB_FLUX_X)
-            _upload_csc_part(L, ctx, FluxM.P_Flux, _lib.DTB_FLUX_P)
+            _upload_csc(L, ctx, FluxM.X_Flux, _lib.DTB_FLUX_X)
+            _upload_csc(L, ctx, FluxM.P_Flux, _lib.DTB_FLUX_P)
             if BinM.M_Bin is not None and sp.issparse(BinM.M_Bin):  # Bin_sparse (BuildBinaryMatrices.jl:44-52)
                 M = sp.csc_matrix(BinM.M_Bin)
                 colptr = np.ascontiguousarray(M.indptr, dtype=np.int64)
