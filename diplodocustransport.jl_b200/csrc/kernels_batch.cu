@@ -507,6 +507,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
     const int n_eff = max(0, min(C::BN, (hi_cols - n0 + 31) / 32 * 32));
     const int hn = n_eff / 2;
     const int nt = (n_eff > 0 && t1 > t0) ? t1 - t0 : 0;
+    // X producers (warps 0 .. NPW-1): row c of this CTA's half (column n0 + rank * hn + c), two
+    // threads per row, each converting one 32-wide half of the 64-wide K tile. Their wait for the
+    // previous step and their first state loads overlap the pair's set-up: they arrive on the
+    // cluster barrier first and wait on it after the loads.
+    const bool producer = warp < C::NPW;
+    const int c = tid & (C::HN - 1), kh = tid / C::HN;
+    bool valid = false;
+    const float* Fc = a.F;
+    float s1 = 0.f, s2 = 0.f, x1_next = 0.f;
+    int inst = 0, cur_cb = -1;
+    float f2r[kMmaK / 2];
 
     if (tid == 0) {
         for (int s = 0; s < C::SA; ++s) {
@@ -533,7 +544,38 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
     }
     // both CTAs' barriers are initialised before either CTA signals the other
     tc_fence_before();
-    cluster_sync_all();
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    if (producer) {
+        pdl_wait();  // F is the previous step's output, and the previous epilogue reads the partials
+        if (tid == 0) pdl_trigger();
+        if (nt > 0) {
+            const int col = n0 + (int)rank * hn + c;
+            const int cell = col / a.Bst;
+            inst = col - cell * a.Bst;
+            valid = c < hn && cell < a.n_space && inst < a.Bcap;
+            Fc = a.F + (size_t)(valid ? cell : 0) * a.n_mom * a.Bst;
+            s1 = valid ? a.isig1[inst] : 0.f;
+            s2 = valid ? a.isig2[inst] : 0.f;
+            if (valid) {
+                const int b0 = t0 - (t0 / a.N1) * a.N1;
+                x1_next = __ldg(Fc + (size_t)(a.off1 + b0) * a.Bst + inst);
+            }
+            // the first tile's 32 input-2 values (clamped in bounds, padding zeroed after)
+            const int cb0 = t0 / a.N1;
+            const float* fb = Fc + (valid ? inst : 0);
+            const int cbase = cb0 * kMmaK + kh * (kMmaK / 2);
+#pragma unroll
+            for (int e = 0; e < kMmaK / 2; ++e) {
+                const int cc = min(cbase + e, a.n2 - 1);
+                f2r[e] = __ldg(fb + (size_t)(a.off2 + cc) * a.Bst);
+            }
+#pragma unroll
+            for (int e = 0; e < kMmaK / 2; ++e)
+                if (!valid || cbase + e >= a.n2) f2r[e] = 0.f;
+            cur_cb = cb0;
+        }
+    }
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
     tc_fence_after();
     const uint32_t tmem = *tmem_holder;
 
@@ -627,27 +669,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
             }
         }
     } else {
-        // ---------------- X producers: row c of this CTA's half (column n0 + rank * hn + c),
-        // two threads per row, each converting one 32-wide half of the 64-wide K tile
-        const int p = tid;
-        const int c = p & (C::HN - 1), kh = p / C::HN;
-        pdl_wait();  // F is the previous step's output
-        if (tid == 0) pdl_trigger();
+        // ---------------- X producers (their first state loads were issued during the set-up)
         if (nt > 0) {
-            const int col = n0 + (int)rank * hn + c;
-            const int cell = col / a.Bst;
-            const int inst = col - cell * a.Bst;
-            const bool valid = c < hn && cell < a.n_space && inst < a.Bcap;
-            const float* Fc = a.F + (size_t)(valid ? cell : 0) * a.n_mom * a.Bst;
-            const float s1 = valid ? a.isig1[inst] : 0.f;
-            const float s2 = valid ? a.isig2[inst] : 0.f;
-            float f2r[kMmaK / 2];
-            int cur_cb = -1;
-            float x1_next = 0.f;
-            if (valid) {
-                const int b0 = t0 - (t0 / a.N1) * a.N1;
-                x1_next = __ldg(Fc + (size_t)(a.off1 + b0) * a.Bst + inst);
-            }
             for (int j = 0; j < nt; ++j) {
                 const int t = t0 + j, cb = t / a.N1;
                 const int sb = j % C::SB;
