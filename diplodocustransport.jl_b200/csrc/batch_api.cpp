@@ -212,12 +212,15 @@ constexpr int kMaxWaves = 4;
 int fill_splits(const dtb_ctx* c, const MixedGroup& G, int pair, int bn, int Bcols, int max_pairs) {
     const int n_tiles = (Bcols + bn - 1) / bn;
     const double units = pair ? (double)(G.m_tiles / 2 * n_tiles) : (double)(G.m_tiles * n_tiles);
-    const int fill = std::max(1, (int)std::lround((pair ? max_pairs : c->num_sms) / units));
+    const double cap = pair ? max_pairs : c->num_sms;  // CTAs (pairs) the device runs at once
+    const int fill = std::max(1, (int)std::lround(cap / units));
     const int per_split = pair ? kMaxTilesPerAccPair : kMaxTilesPerAccSm * (512 / bn - 1);
     const int T = G.n_cb * G.N1;
     const int need = (T + per_split - 1) / per_split;
     const int waves = std::min(kMaxWaves, std::max(1, (need + fill - 1) / fill));
-    return fill * waves;
+    if (waves == 1) return fill;
+    // several waves: as many splits as whole waves hold (the last wave then runs nearly full)
+    return std::max(fill * waves, (int)(waves * cap / units));
 }
 
 // Without timing: the widest tile the columns fill, on SM pairs when the rows pair up.
