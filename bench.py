@@ -501,7 +501,7 @@ def run_batched(args):
         set_tune_cache(args.tune_cache)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     dev = f"cuda:{local}"
     w = build_batched(args.config, dev)
     if args.shard and world > 1:
