@@ -199,8 +199,13 @@ def cpu_sample(w, dtype: str, budget_s: float = 15.0):
     return 1.0 / t_step, oracle.num_threads(), desc
 
 
-def build_batched(config: int, device: str, host: bool = False):
+def build_batched(config: int, device: str, host: bool = False, grid=None):
     from dtb import synth
+    if config == 3 and grid:  # the config-3 recipe on another grid, e.g. "24x12" (small profiling case)
+        p, u = (int(x) for x in grid.split("x"))
+        w = synth.three_species(p, 1e-3, 1e3, u, 64, seed=3, gain_on_device=not host, device=device)
+        w.n_steps = 5000
+        return w
     if config == 2:
         return synth.config2(seed=2, gain_on_device=not host, device=device)
     if config == 3:
@@ -279,6 +284,9 @@ def _config_dict(config: int, w, world: int = 1):
                             "(32 log p x 8 u), shared G 2 x 256 x 65536, per-instance f0 and dt",
                 "species_states": sizes, "batch": 256, "run_length_steps": 10000,
                 "l2": "G hi+lo 134 MB per step, larger than L2", "parallelism": f"batch replicas x{world}"}
+    if config == 3 and sizes != [576, 576, 576]:
+        return {"workload": f"config-3 recipe on a smaller grid: 64 instances, 3 species x {sizes[0]} states",
+                "species_states": sizes, "batch": 64, "parallelism": f"batch replicas x{world}"}
     if config == 3:
         return {"workload": "mixed precision (config 3): 64 instances, e-, e+, gamma x 576 states "
                             "(48 log p x 12 u), 6 gain tensors 576 x 331776, synchrotron-like emission",
@@ -503,7 +511,7 @@ def run_batched(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     dev = f"cuda:{local}"
-    w = build_batched(args.config, dev)
+    w = build_batched(args.config, dev, grid=args.grid)
     if args.shard and world > 1:
         # strong scaling: the configuration's instances partitioned across the ranks
         from dtb.shard import shard_range
@@ -869,7 +877,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--grid", default=None, help="p_bins x u_bins override of the config-1 grid, e.g. 32x16")
+    ap.add_argument("--grid", default=None,
+                    help="p_bins x u_bins override of the config-1 or config-3 grid, e.g. 32x16 (profiling cases)")
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 accuracy checks of the batched run")
     ap.add_argument("--check-steps", type=int, default=None,
                     help="length of the batched accuracy run (default: the configuration's run length, "
