@@ -260,6 +260,9 @@ GemmArgs gemm_args(const dtb_ctx* c, const MixedGroup& G, const float* Fin) {
     a.partial = G.partial;
     a.err = c->err;
     a.active_hi = m->active_hi;
+    // tensor-bound when the MMAs take longer than streaming G at the copy rate (ridge of about
+    // 250 FLOP per byte on a B200): config 2's group (384 FLOP/B) is, config 3's (96) is not
+    a.ring_after_x0 = G.flops > 250.0 * G.bytes ? 1 : 0;
     return a;
 }
 

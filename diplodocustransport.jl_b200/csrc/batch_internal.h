@@ -36,6 +36,9 @@ struct GemmArgs {
     float* partial;      // [n_splits][Bpad][M]
     int* err;
     const int* active_hi;  // device: 1 + the highest slot that still steps (columns past it are skipped)
+    int ring_after_x0;     // 1: the G ring past its first tiles waits for the first X tile (tensor-bound
+                           // groups, whose state loads must not queue behind the G stream); 0: the whole
+                           // ring streams at once (HBM-bound groups)
 };
 
 cudaError_t launch_gain_gemm(int bn, const GemmArgs& a, cudaStream_t s);

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                           smem_addr(&full_a[sa]));
                 // the producers' state loads come first: the rest of the G ring waits for the first
                 // X tile, so those loads do not queue behind every CTA's full ring of G traffic
-                if (j == 0 && nt > 1 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
+                if (j == 0 && nt > 1 && a.ring_after_x0 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
                     if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
                     *abort_flag = 1;
                     ++j;
@@ -599,7 +599,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
                           smem_addr(&full_a[sa]));
                 // the first two G tiles go out at once, the rest after the first X tile (so the
                 // producers' state loads do not queue behind the whole ring of G traffic)
-                if (j == 1 && nt > 2 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
+                if (j == 1 && nt > 2 && a.ring_after_x0 && !mb_wait(smem_addr(x0_bar), 0u, abort_flag)) {
                     if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_FULL);
                     *abort_flag = 1;
                     ++j;
