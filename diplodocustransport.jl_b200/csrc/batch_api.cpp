@@ -213,7 +213,8 @@ int fill_splits(const dtb_ctx* c, const MixedGroup& G, int pair, int bn, int Bco
     const int n_tiles = (Bcols + bn - 1) / bn;
     const double units = pair ? (double)(G.m_tiles / 2 * n_tiles) : (double)(G.m_tiles * n_tiles);
     const double cap = pair ? max_pairs : c->num_sms;  // CTAs (pairs) the device runs at once
-    const int fill = std::max(1, (int)std::lround(cap / units));
+    // rounded down: one CTA more than the device holds would run in a second wave on its own
+    const int fill = std::max(1, (int)(cap / units));
     const int per_split = pair ? kMaxTilesPerAccPair : kMaxTilesPerAccSm * (512 / bn - 1);
     const int T = G.n_cb * G.N1;
     const int need = (T + per_split - 1) / per_split;
