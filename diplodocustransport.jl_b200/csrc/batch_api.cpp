@@ -58,7 +58,8 @@ struct MixedState {
     long long host_step = 0;
     MixedRowOps ops{};
     cudaGraphExec_t graph = nullptr;
-    cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step from state buffer 0 / 1
+    // graphs[p][n]: n consecutive batched steps (1 <= n <= graph_steps) starting on state buffer p
+    std::vector<cudaGraphExec_t> graphs[2];
     // host round trip of one step as one graph per state buffer (dtb_batch_run_io with
     // page-locked host arrays): upload and pack, the step, unpack and download, error flag
     struct IoGraph {
@@ -417,6 +418,7 @@ int commit_mixed(dtb_ctx* c) {
     m->Buser = c->opts.batch;
     m->Bcap = (int)round_up(c->opts.batch, 4);
     if (c->opts.graph_steps > 0) m->graph_steps = (c->opts.graph_steps + 1) / 2 * 2;
+    for (auto& gp : m->graphs) gp.assign((size_t)m->graph_steps + 1, nullptr);
     MixedRowOps& ops = m->ops;
     const int B = m->Bcap;
     const int n_mom = (int)c->n_mom;
@@ -869,9 +871,9 @@ int commit_mixed(dtb_ctx* c) {
 void destroy_mixed(dtb_ctx* c) {
     MixedState* m = c->mixed;
     if (!m) return;
-    if (m->graph) cudaGraphExecDestroy(m->graph);
-    for (auto& g1 : m->graph1)
-        if (g1) cudaGraphExecDestroy(g1);
+    for (auto& gp : m->graphs)
+        for (cudaGraphExec_t x : gp)
+            if (x) cudaGraphExecDestroy(x);
     for (auto& io : m->io_graph) {
         if (io.x) cudaGraphExecDestroy(io.x);
         if (io.g) cudaGraphDestroy(io.g);
@@ -930,43 +932,40 @@ int mixed_step(dtb_ctx* c, bool profile, int kpos, int advance) {
     return DTB_OK;
 }
 
-int ensure_mixed_graph(dtb_ctx* c) {
+// n consecutive batched steps from the current state buffer as one graph (captured once per
+// buffer and length); the last step advances the device step counter by n.
+int ensure_mixed_graph(dtb_ctx* c, int n) {
     MixedState* m = c->mixed;
-    if (m->graph) return DTB_OK;
+    const int cur = m->cur;
+    if (m->graphs[cur][(size_t)n]) return DTB_OK;
     const long long hs = m->host_step;
     cudaGraph_t gr;
     DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = DTB_OK;
-    for (int k = 0; k < m->graph_steps && rc == DTB_OK; ++k)
-        rc = mixed_step(c, false, k, k == m->graph_steps - 1 ? m->graph_steps : 0);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
-    m->host_step = hs;
-    m->cur = 0;
-    if (rc != DTB_OK) return rc;
-    DTB_CUDA(e);
-    e = cudaGraphInstantiate(&m->graph, gr, 0);
-    cudaGraphDestroy(gr);
-    DTB_CUDA(e);
-    return DTB_OK;
-}
-
-// One batched step as a graph (one per state buffer), for runs shorter than a full graph.
-int ensure_mixed_graph1(dtb_ctx* c) {
-    MixedState* m = c->mixed;
-    const int cur = m->cur;
-    if (m->graph1[cur]) return DTB_OK;
-    const long long hs = m->host_step;
-    cudaGraph_t gr;
-    DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = mixed_step(c, false, 0, 1);
+    for (int k = 0; k < n && rc == DTB_OK; ++k) rc = mixed_step(c, false, k, k == n - 1 ? n : 0);
     cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
     m->host_step = hs;
     m->cur = cur;
     if (rc != DTB_OK) return rc;
     DTB_CUDA(e);
-    e = cudaGraphInstantiate(&m->graph1[cur], gr, 0);
+    e = cudaGraphInstantiate(&m->graphs[cur][(size_t)n], gr, 0);
     cudaGraphDestroy(gr);
     DTB_CUDA(e);
+    return DTB_OK;
+}
+
+// nsteps batched steps as graph replays: whole graphs of graph_steps steps, then one graph of
+// the remainder, from whichever state buffer is current.
+int run_mixed_graphs(dtb_ctx* c, int64_t nsteps) {
+    MixedState* m = c->mixed;
+    for (int64_t done = 0; done < nsteps;) {
+        const int n = (int)std::min<int64_t>(m->graph_steps, nsteps - done);
+        DTB_TRY(ensure_mixed_graph(c, n));
+        DTB_CUDA(cudaGraphLaunch(m->graphs[m->cur][(size_t)n], c->stream));
+        m->cur ^= n & 1;
+        m->host_step += n;
+        done += n;
+    }
     return DTB_OK;
 }
 
@@ -1035,21 +1034,8 @@ int batch_launch(dtb_ctx* c, int64_t nsteps) {
     DeviceGuard g(c->device);
     c->steps_run += nsteps;
     DTB_TRY(refresh_active_hi(c));
-    int64_t done = 0;
-    if (nsteps >= m->graph_steps) {
-        if (m->cur != 0) {
-            DTB_TRY(mixed_step(c, false, 0, 1));
-            done++;
-        }
-        DTB_TRY(ensure_mixed_graph(c));
-        while (nsteps - done >= m->graph_steps) {
-            DTB_CUDA(cudaGraphLaunch(m->graph, c->stream));
-            done += m->graph_steps;
-            m->host_step += m->graph_steps;
-        }
-    }
-    for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, false, 0, 1));
-    return DTB_OK;
+    (void)m;
+    return run_mixed_graphs(c, nsteps);
 }
 
 int batch_finish(dtb_ctx* c) {
@@ -1057,23 +1043,23 @@ int batch_finish(dtb_ctx* c) {
     return mixed_check_err(c);
 }
 
-// Captures, instantiates and uploads every graph dtb_batch_run replays (the graph of
-// graph_steps steps, which starts on state buffer 0, and the 1-step graph of each buffer);
-// capture enqueues nothing, so the state and the step counter are unchanged.
+// Captures, instantiates and uploads every graph dtb_batch_run replays (1 to graph_steps steps
+// from either state buffer); capture enqueues nothing, so the state and the step counter are
+// unchanged.
 int batch_prepare(dtb_ctx* c) {
     DTB_RANGE("dtb_prepare (batched graphs)");
     MixedState* m = c->mixed;
     const int cur = m->cur;
-    m->cur = 0;
-    int rc = ensure_mixed_graph(c);
-    for (int k = 0; k < 2 && rc == DTB_OK; ++k) {
-        m->cur = k;
-        rc = ensure_mixed_graph1(c);
+    int rc = DTB_OK;
+    for (int p = 0; p < 2 && rc == DTB_OK; ++p) {
+        m->cur = p;
+        for (int n = 1; n <= m->graph_steps && rc == DTB_OK; ++n) rc = ensure_mixed_graph(c, n);
     }
     m->cur = cur;
     if (rc != DTB_OK) return rc;
-    DTB_CUDA(cudaGraphUpload(m->graph, c->stream));
-    for (auto& g1 : m->graph1) DTB_CUDA(cudaGraphUpload(g1, c->stream));
+    for (auto& gp : m->graphs)
+        for (cudaGraphExec_t x : gp)
+            if (x) DTB_CUDA(cudaGraphUpload(x, c->stream));
     DTB_CUDA(cudaStreamSynchronize(c->stream));
     return DTB_OK;
 }
@@ -1159,32 +1145,13 @@ int32_t dtb_batch_run(dtb_ctx* c, int64_t nsteps) {
     DeviceGuard g(c->device);
     c->steps_run += nsteps;
     DTB_TRY(refresh_active_hi(c));
-    int64_t done = 0;
-    if (!m->profiling && nsteps >= m->graph_steps) {
-        if (m->cur != 0) {
-            DTB_TRY(mixed_step(c, false, 0, 1));
-            done++;
-        }
-        DTB_TRY(ensure_mixed_graph(c));
-        while (nsteps - done >= m->graph_steps) {
-            DTB_CUDA(cudaGraphLaunch(m->graph, c->stream));
-            done += m->graph_steps;
-            m->host_step += m->graph_steps;
-        }
-    }
     if (m->profiling) {
-        for (; done < nsteps; ++done) DTB_TRY(mixed_step(c, true, 0, 1));
+        for (int64_t done = 0; done < nsteps; ++done) DTB_TRY(mixed_step(c, true, 0, 1));
         DTB_TRY(mixed_flush_profile(m));
         return mixed_check_err(c);
     }
-    for (; done < nsteps; ++done) {
-        DTB_TRY(ensure_mixed_graph1(c));
-        DTB_CUDA(cudaGraphLaunch(m->graph1[m->cur], c->stream));
-        m->cur ^= 1;
-        m->host_step++;
-    }
     // enqueued only: a device error surfaces at the next call that reads results
-    return DTB_OK;
+    return run_mixed_graphs(c, nsteps);
 }
 
 namespace {
