@@ -37,7 +37,8 @@ struct Request {
     std::vector<double> f;  // f0 on submission, the result when done
     double dt_scale = 1.0;
     int64_t n_steps = 0;
-    int state = 0;          // 0 queued, 1 running, 2 done, 3 failed
+    int state = 0;          // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
+    bool cancel = false;    // cancellation asked while running: the slot is freed at its grid's next chunk boundary
     int slot = -1;
     double t_submit = 0, t_admit = 0, t_done = 0;
     double cr_max = 0;
@@ -57,6 +58,7 @@ struct Grid {
     int64_t chunk = 0;
     double ema_step_ms = 0.1;
     int n_running = 0;
+    int n_cancel = 0;                  // running requests cancelled since the last pass (server lock)
 };
 
 }  // namespace
@@ -95,18 +97,33 @@ void fail(dtb_server* s, int rc) {
     s->cv_done.notify_all();
 }
 
-// Reads back and frees every slot of `g` whose request is done at the grid's current step.
+// Reads back and frees every slot of `g` whose request is done at the grid's current step, and
+// frees the slots of running requests that were cancelled.
 int complete_slots(dtb_server* s, Grid& g) {
     const long long st = batch_step(g.ctx);
     bool any = false;
     for (int sl = 0; sl < g.capacity; ++sl) {
         const int64_t id = g.slot_req[(size_t)sl];
-        if (id < 0 || st < g.slot_stop[(size_t)sl]) continue;
+        if (id < 0) continue;
         Request* r;
+        bool cancelled;
         {
             std::lock_guard<std::mutex> lk(s->mu);
             r = &s->req.at(id);  // not erased before it is done
+            cancelled = r->cancel;
         }
+        if (cancelled) {
+            int rc = dtb_batch_release(g.ctx, sl);
+            if (rc != DTB_OK) return rc;
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->state = 4;
+            r->t_done = s->now();
+            g.slot_req[(size_t)sl] = -1;
+            g.n_running--;
+            any = true;
+            continue;
+        }
+        if (st < g.slot_stop[(size_t)sl]) continue;
         int64_t done = 0, left = 0;
         double cr = 0;
         int32_t fin = 1;
@@ -212,10 +229,16 @@ void loop(dtb_server* s) {
                 if (rc != DTB_OK) return fail(s, rc);
                 progressed = true;
             }
-            bool queued;
+            bool queued, cancels;
             {
                 std::lock_guard<std::mutex> lk(s->mu);
                 queued = !g.queue.empty();
+                cancels = g.n_cancel > 0;
+                g.n_cancel = 0;
+            }
+            if (cancels) {  // running requests of this grid were cancelled: free their slots now
+                int rc = complete_slots(s, g);
+                if (rc != DTB_OK) return fail(s, rc);
             }
             if (queued && g.n_running < g.capacity) {
                 int rc = admit_slots(s, g);
@@ -327,6 +350,11 @@ int32_t dtb_serve_wait(dtb_server* s, int64_t request_id, double timeout_s, doub
         }
     }
     Request& r = it->second;
+    if (r.state == 4) {
+        s->req.erase(it);
+        set_error("dtb_serve_wait: request " + std::to_string(request_id) + " was cancelled");
+        return DTB_ESTATE;
+    }
     if (r.state == 3) {
         set_error("dtb_serve_wait: the server stopped after an error: " + s->error_msg);
         return s->error != DTB_OK ? s->error : DTB_ECUDA;
@@ -343,6 +371,26 @@ int32_t dtb_serve_wait(dtb_server* s, int64_t request_id, double timeout_s, doub
     }
     s->req.erase(it);  // collected: the id is unknown from now on
     return DTB_OK;
+}
+
+int32_t dtb_serve_cancel(dtb_server* s, int64_t request_id) {
+    DTB_CHECK(s, DTB_EINVAL, "dtb_serve_cancel: null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->req.find(request_id);
+    DTB_CHECK(it != s->req.end(), DTB_ENOTFOUND, "dtb_serve_cancel: unknown request");
+    Request& r = it->second;
+    if (r.state == 0) {  // queued: leaves the queue at once
+        auto& q = s->grids[(size_t)r.grid].queue;
+        q.erase(std::remove(q.begin(), q.end(), request_id), q.end());
+        r.state = 4;
+        r.t_done = s->now();
+        s->cv_done.notify_all();
+    } else if (r.state == 1 && !r.cancel) {  // running: its slot is freed at the grid's next chunk boundary
+        r.cancel = true;
+        s->grids[(size_t)r.grid].n_cancel++;
+        s->cv_work.notify_all();
+    }
+    return DTB_OK;  // a request already done or failed is left as it is
 }
 
 int32_t dtb_serve_get_stats(dtb_server* s, dtb_serve_stats* st) {

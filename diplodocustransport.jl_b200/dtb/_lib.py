@@ -123,6 +123,7 @@ SIGNATURES = {
     "dtb_serve_start": (_i32, [_P]),
     "dtb_serve_submit": (_i32, [_P, _i32, _dp, _d, _i64, _ip]),
     "dtb_serve_wait": (_i32, [_P, _i64, _d, _dp, ctypes.POINTER(RequestStats)]),
+    "dtb_serve_cancel": (_i32, [_P, _i64]),
     "dtb_serve_get_stats": (_i32, [_P, ctypes.POINTER(ServeStats)]),
     "dtb_serve_destroy": (_i32, [_P]),
     "dtb_batch_capacity": (_i32, [_P, _i32p, _ip]),

@@ -61,6 +61,10 @@ class Server:
             out = out[:self.grids[st.grid].n].copy()
         return out, info
 
+    def cancel(self, request_id: int) -> None:
+        """Cancels a queued or running request; wait() then raises DtbError with DTB_ESTATE."""
+        check(self.L.dtb_serve_cancel(self.srv, int(request_id)))
+
     def stats(self) -> dict:
         st = _lib.ServeStats()
         check(self.L.dtb_serve_get_stats(self.srv, ctypes.byref(st)))

@@ -348,6 +348,11 @@ int32_t dtb_serve_submit(dtb_server* srv, int32_t grid_id, const double* f0, dou
  * copies its final f and timings. */
 int32_t dtb_serve_wait(dtb_server* srv, int64_t request_id, double timeout_s, double* f_out,
                        dtb_request_stats* stats);
+/* Cancels a request (no counterpart in the reference, whose Solve runs one request to its end):
+ * a queued request leaves the queue at once, a running one frees its slot at its grid's next chunk
+ * boundary; dtb_serve_wait then returns DTB_ESTATE for it. Thread-safe; a request already done is
+ * left as it is. */
+int32_t dtb_serve_cancel(dtb_server* srv, int64_t request_id);
 int32_t dtb_serve_get_stats(dtb_server* srv, dtb_serve_stats* stats);
 /* Stops the loop thread (running requests are abandoned) and frees the server. */
 int32_t dtb_serve_destroy(dtb_server* srv);

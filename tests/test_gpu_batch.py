@@ -632,3 +632,28 @@ def test_long_run_number_conservation(cuda):
         f, _, _ = ops.step(f, 0.5, 0)
     assert abs(f[:ns].sum() - n0[0]) / n0[0] < 1e-12 and abs(f[ns:].sum() - n0[1]) / n0[1] < 1e-12
     b.close()
+
+
+def test_nan_seeded_slot_is_flagged_and_leaves_the_others_alone(cuda):
+    """Host-side fault injection on the batched numeric path: one slot's f0 carries a NaN. That
+    slot's finite flag drops and its state clamps to zeros (x * (x >= thr), Julia's strong
+    zero); every other slot is bit-identical to the same batch without the NaN."""
+    B = 8
+    w = synth.batched_two_species(8, 1e-2, 1e2, 4, B, seed=27)
+    a = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, B)
+    for i in range(B):
+        f = w.f0[i].copy()
+        if i == 3:
+            f[7] = np.nan
+        a.admit(i, f, w.dt[i], 5)
+        b.admit(i, w.f0[i], w.dt[i], 5)
+    a.run(5)
+    b.run(5)
+    assert not a.info(3)["finite"] and np.all(a.get_f(3) == 0)
+    for i in range(B):
+        if i != 3:
+            assert a.info(i)["finite"]
+            np.testing.assert_array_equal(a.get_f(i), b.get_f(i))
+    a.close()
+    b.close()

@@ -442,3 +442,65 @@ def test_sparse_mbin_duplicates_and_empty_columns(cuda):
     assert L.dtb_upload_mbin_csc(ctx2, N, cp_.ctypes.data_as(_lib._ip), bad.ctypes.data_as(_lib._ip),
                                  nz.ctypes.data_as(_lib._dp)) == _lib.DTB_EINVAL
     L.dtb_destroy(ctx2)
+
+
+def test_nan_in_state_is_flagged_and_clamped_like_the_reference(cuda):
+    """Host-side fault injection on the numeric path: a NaN seeded into f. The step reports a
+    non-finite df (SteppingMethods.jl:48-50) and the clamp of :99-101 (x * (x >= thr), Julia's
+    strong zero) turns every NaN into 0, exactly as the FP64 oracle does; the next step is finite."""
+    w = synth.small(p_num=8, u_num=4, seed=17)
+    m = make_method(w)
+    f0 = w.f0.copy()
+    f0[5] = np.nan
+    m.f = f0
+    m(0.0, 1e9, 1.0, 1)
+    assert m.last_diag.finite == 0
+    ops = oracle.blocked_from_workload(w)
+    f, _, _ = ops.step(f0, 1.0, 0)
+    got = m.f
+    # the NaN reaches every row through the gain term, so both give all zeros here
+    assert np.all(np.isfinite(got)) and np.array_equal(got == 0, f == 0)
+    assert np.max(np.abs(got - f)) <= TOL64 * np.max(np.abs(w.f0))
+    m.f = w.f0
+    m(0.0, 1e9, 1.0, 1)
+    assert m.last_diag.finite == 1
+    m.close()
+
+
+def test_malformed_flux_csc_is_refused_and_the_context_stays_usable(cuda):
+    """Host-side fault injection: a flux CSC with a row index out of range, and one whose colptr
+    is not monotone, are refused with DTB_EINVAL before anything reaches the device; the same
+    context then takes the valid matrices and steps as the oracle."""
+    import ctypes
+    from dtb.stepping import _upload_gain
+    L = _lib.load()
+    w = synth.small(p_num=4, u_num=2, seed=19)
+    n = w.ps.n_state
+    dims = _lib.Dims()
+    dims.n_species = 2
+    dims.n_space = 1
+    for i, s_ in enumerate(w.ps.species_sizes):
+        dims.species_size[i] = s_
+    opts = _lib.Opts(precision=_lib.DTB_F64, device=0, index_base=0, graph_steps=16, dt0=1.0, batch=1)
+    ctx = ctypes.c_void_p()
+    _lib.check(L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)))
+    colptr = np.arange(n + 1, dtype=np.int64)
+    rowval = np.zeros(n, dtype=np.int64)
+    rowval[3] = n  # out of range
+    vals = np.ones(n)
+    ip = lambda a: a.ctypes.data_as(_lib._ip)  # noqa: E731
+    assert L.dtb_add_flux_csc(ctx, n, ip(colptr), ip(rowval), _lib.dptr(vals)) == _lib.DTB_EINVAL
+    assert b"out of range" in L.dtb_last_error()
+    bad = colptr.copy()
+    bad[4], bad[5] = bad[5], bad[4]
+    rowval[3] = 0
+    assert L.dtb_add_flux_csc(ctx, n, ip(bad), ip(rowval), _lib.dptr(vals)) == _lib.DTB_EINVAL
+    assert b"monotone" in L.dtb_last_error()
+    L.dtb_destroy(ctx)
+    # the valid workload on a fresh context of the same library state steps as the oracle
+    m = make_method(w)
+    m(0.0, 1e9, 1.0, 0)
+    ops = oracle.blocked_from_workload(w)
+    f, _, _ = ops.step(w.f0.copy(), 1.0, 0)
+    assert rel_linf(m.f, f) <= TOL64
+    m.close()

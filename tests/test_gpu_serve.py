@@ -85,3 +85,36 @@ def test_wait_times_out_and_unknown_ids(cuda):
     assert e.value.code == _lib.DTB_ETIMEOUT
     srv.close()
     b.close()
+
+
+def test_cancelled_requests_free_their_slots(cuda):
+    """Host-side fault injection: a running request and a queued one are cancelled. The queued
+    one leaves the queue at once, the running one frees its slot at the next chunk boundary;
+    waiting on either reports DTB_ESTATE, and later requests run in the freed slot and match the
+    same request run alone."""
+    w = _grids()[0]
+    b = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 1)
+    srv = Server(max_chunk_steps=16)
+    gid = srv.add_grid(b)
+    srv.start()
+    long_id = srv.submit(gid, w.f0[0], float(w.dt[0]), 10_000_000)
+    queued_id = srv.submit(gid, w.f0[1], float(w.dt[1]), 50)
+    srv.cancel(queued_id)
+    with pytest.raises(_lib.DtbError) as e:
+        srv.wait(queued_id, timeout_s=30)
+    assert e.value.code == _lib.DTB_ESTATE
+    srv.cancel(long_id)
+    with pytest.raises(_lib.DtbError) as e:
+        srv.wait(long_id, timeout_s=30)
+    assert e.value.code == _lib.DTB_ESTATE
+    rid = srv.submit(gid, w.f0[2], float(w.dt[2]), 40)
+    f_srv, info = srv.wait(rid, timeout_s=60)
+    st = srv.stats()
+    srv.close()
+    assert info["finite"] and st["completed"] == 1 and st["instance_steps"] == 40
+    alone = BatchedEuler(w.ps, w.inj, w.binm, w.emim, w.fluxm, 1)
+    alone.admit(0, w.f0[2], float(w.dt[2]), 40)
+    alone.run(40)
+    assert rel_linf(f_srv, alone.get_f(0)) <= 1e-12
+    alone.close()
+    b.close()
