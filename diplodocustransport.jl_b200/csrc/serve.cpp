@@ -12,6 +12,7 @@
 // checked against an HBM budget when a grid is registered.
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -81,6 +82,7 @@ struct dtb_server {
     int64_t batched_steps = 0;   // batched steps launched, summed over grids
     int64_t completed = 0;
     double busy_s = 0;
+    std::vector<double> tts;     // time to solution of every completed request (DTB_PROFILE summary)
 
     double now() const { return std::chrono::duration<double>(clk::now() - t0).count(); }
 };
@@ -140,6 +142,7 @@ int complete_slots(dtb_server* s, Grid& g) {
         g.n_running--;
         s->steps_done += r->n_steps;
         s->completed++;
+        s->tts.push_back(r->t_done - r->t_submit);
         any = true;
     }
     if (any) s->cv_done.notify_all();
@@ -420,6 +423,24 @@ int32_t dtb_serve_destroy(dtb_server* s) {
         s->cv_work.notify_all();
     }
     if (s->th.joinable()) s->th.join();
+    if (const char* path = profile_path()) {
+        // one JSON line per server: requests served, instance-steps/s, busy time, p50/p99 time to solution
+        std::vector<double> t = s->tts;
+        std::sort(t.begin(), t.end());
+        auto pct = [&](double q) { return t.empty() ? 0.0 : t[(size_t)std::min<double>(t.size() - 1, q * (t.size() - 1) + 0.5)]; };
+        const double el = s->now();
+        char b[512];
+        std::snprintf(b, sizeof(b),
+                      "{\"server\": 1, \"grids\": %zu, \"completed\": %lld, \"instance_steps\": %lld, "
+                      "\"elapsed_s\": %.6g, \"busy_s\": %.6g, \"instance_steps_per_s\": %.6g, \"tts_p50_s\": %.6g, "
+                      "\"tts_p99_s\": %.6g, \"device_bytes\": %lld}\n",
+                      s->grids.size(), (long long)s->completed, (long long)s->steps_done, el, s->busy_s,
+                      el > 0 ? (double)s->steps_done / el : 0.0, pct(0.5), pct(0.99), (long long)s->bytes);
+        if (FILE* f = std::fopen(path, "a")) {
+            std::fputs(b, f);
+            std::fclose(f);
+        }
+    }
     for (auto& g : s->grids) {
         if (!g.done_ev) continue;
         DeviceGuard dg(g.ctx->device);
