@@ -115,10 +115,16 @@ template <int BN>
 struct GemmCfg {
     static constexpr int NPW = BN / 32 < 4 ? 4 : BN / 32;  // producer / epilogue warps
     static constexpr int THREADS = (NPW + 2) * 32;
+    // threads forming one X row, each KW of its 64 K columns: with BN = 64 all four producer
+    // warps form X (the X tile is on the critical path of an HBM-bound group: a G stage stays
+    // held until the MMAs that read it complete, and they wait for X)
+    static constexpr int KS = NPW * 32 / BN;
+    static constexpr int KW = kMmaK / KS;
     static constexpr int A_BYTES = kMmaM * 128;             // one half (hi or lo) of an A stage
     static constexpr int B_BYTES = BN * 128;                // one half of a B stage
-    static constexpr int SB = 2;
-    static constexpr int SA = BN == 256 ? 3 : (BN == 128 ? 4 : 6);
+    // BN = 64: a 4-stage G ring and a 6-stage X ring, so the producers run ahead of the MMAs
+    static constexpr int SB = BN == 64 ? 6 : 2;
+    static constexpr int SA = BN == 256 ? 3 : 4;
     static constexpr int DATA = SA * 2 * A_BYTES + SB * 2 * B_BYTES;
     static constexpr int BARS = (2 * SA + 2 * SB + 3) * 8;
     static constexpr int SMEM = 1024 + DATA + BARS + 16;   // 1024: alignment slack
@@ -127,6 +133,8 @@ struct GemmCfg {
     // last, so no FP32 accumulator sums more than a fraction of the split's K range
     static constexpr int NACC = 512 / BN;
     static constexpr int NHH = NACC - 1;
+    static_assert(KS >= 1 && KS * BN == NPW * 32 && KW % 8 == 0, "producer threads cover whole 16-byte chunks");
+    static_assert(SMEM <= 232448, "gain GEMM shared memory");
 };
 
 template <int BN>
@@ -177,12 +185,12 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             mb_init(smem_addr(&empty_a[s]), 1);
         }
         for (int s = 0; s < C::SB; ++s) {
-            mb_init(smem_addr(&full_b[s]), BN / 32);  // one arrive per producing warp
+            mb_init(smem_addr(&full_b[s]), BN / 32 * C::KS);  // one arrive per producing warp
             mb_init(smem_addr(&empty_b[s]), 1);
         }
         mb_init(smem_addr(acc_bar), 1);
         mb_init(smem_addr(drain_bar), 1);
-        mb_init(smem_addr(x0_bar), BN / 32);
+        mb_init(smem_addr(x0_bar), BN / 32 * C::KS);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -275,11 +283,13 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             }
         }
     } else {
-        // ---------------- X producers (one instance row per thread), then the epilogue
-        const int p = tid;  // row of the B tile
+        // ---------------- X producers (KS threads per instance row, KW of its K columns each),
+        // then the epilogue
+        const int p = tid % BN;   // row of the B tile
+        const int kh = tid / BN;  // K part of the row
         pdl_wait();  // F is the previous step's output
         if (tid == 0) pdl_trigger();
-        if (p < BN && nt > 0) {
+        if (kh < C::KS && nt > 0) {
             // column n0 + p: cell (n0 + p) / Bst of slot (n0 + p) % Bst; the cell's states start at
             // row cell * n_mom of F
             const int col = n0 + p;
@@ -289,7 +299,7 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
             const float* Fc = a.F + (size_t)(valid ? cell : 0) * a.n_mom * a.Bst;
             const float s1 = valid ? a.isig1[inst] : 0.f;
             const float s2 = valid ? a.isig2[inst] : 0.f;
-            float f2r[kMmaK];
+            float f2r[C::KW];
             int cur_cb = -1;
             // f1[b] of the next tile is loaded one tile ahead so its latency hides behind the
             // current tile's conversion
@@ -299,37 +309,37 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                 x1_next = __ldg(Fc + (size_t)(a.off1 + b0) * a.Bst + inst);
             }
             for (int j = 0; j < nt; ++j) {
-                const int t = t0 + j, cb = t / a.N1, b = t - cb * a.N1;
+                const int t = t0 + j, cb = t / a.N1;
                 const int sb = j % C::SB;
                 const float x1 = (x1_next * s1) * s2;  // both scales are powers of two: exact
                 if (valid && j + 1 < nt) {
                     const int tn = t + 1, bn = tn - (tn / a.N1) * a.N1;
                     x1_next = __ldg(Fc + (size_t)(a.off1 + bn) * a.Bst + inst);
                 }
-                (void)b;
                 if (!mb_wait(smem_addr(&empty_b[sb]), ((j / C::SB) & 1u) ^ 1u, abort_flag)) {
                     if (!*abort_flag) atomicOr(a.err, KERR_TIMEOUT_EMPTY);
                     *abort_flag = 1;
                     break;
                 }
                 if (cb != cur_cb) {
-                    // 64 unconditional loads (clamped in bounds) issued back to back, the padding
+                    // KW unconditional loads (clamped in bounds) issued back to back, the padding
                     // zeroed afterwards: one round trip instead of a load-use chain
                     const float* fb = Fc + (valid ? inst : 0);
+                    const int cbase = cb * kMmaK + kh * C::KW;
 #pragma unroll
-                    for (int c = 0; c < kMmaK; ++c) {
-                        const int cc = min(cb * kMmaK + c, a.n2 - 1);
+                    for (int c = 0; c < C::KW; ++c) {
+                        const int cc = min(cbase + c, a.n2 - 1);
                         f2r[c] = __ldg(fb + (size_t)(a.off2 + cc) * a.Bst);
                     }
 #pragma unroll
-                    for (int c = 0; c < kMmaK; ++c)
-                        if (!valid || cb * kMmaK + c >= a.n2) f2r[c] = 0.f;
+                    for (int c = 0; c < C::KW; ++c)
+                        if (!valid || cbase + c >= a.n2) f2r[c] = 0.f;
                     cur_cb = cb;
                 }
                 unsigned char* rhi = b_base + (size_t)(sb * 2) * C::B_BYTES + (size_t)p * 128;
                 unsigned char* rlo = b_base + (size_t)(sb * 2 + 1) * C::B_BYTES + (size_t)p * 128;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
+                for (int q = 0; q < C::KW / 8; ++q) {
                     uint32_t h[4], l[4];
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
@@ -340,7 +350,8 @@ __global__ void __launch_bounds__(GemmCfg<BN>::THREADS, 1)
                         h[e] = *reinterpret_cast<const uint32_t*>(&hh);
                         l[e] = pack_bf16x2(v0 - hf.x, v1 - hf.y);
                     }
-                    const int phys = ((q ^ (p & 7)) << 4);
+                    // 16-byte chunk kh * KW / 8 + q of the row, at its 128-byte-swizzled place
+                    const int phys = (((kh * (C::KW / 8) + q) ^ (p & 7)) << 4);
                     *reinterpret_cast<uint4*>(rhi + phys) = make_uint4(h[0], h[1], h[2], h[3]);
                     *reinterpret_cast<uint4*>(rlo + phys) = make_uint4(l[0], l[1], l[2], l[3]);
                 }
