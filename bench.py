@@ -383,7 +383,7 @@ def run_ours(args):
     esz = 4 if dtype == "f32" else 8
     peak, peak_kind = _peaks()
     achieved = bpl.value / (avg_ms.value / 1e3) / 1e9 if avg_ms.value > 0 else None
-    traffic = _profile_traffic("gain_stream_f32_config1.md") if args.config == 1 else None
+    traffic = _profile_traffic("gain_stream_f32_config1.md") if args.config == 1 and not args.grid else None
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": dtype, "data": "synthetic (seeded; no collision data files)",
@@ -620,7 +620,8 @@ def run_batched(args):
     peak = float(pj.get("bf16_tflops", 1590.0))
     peak_s = float(pj.get("bf16_tflops_sustained", 1400.0))
     achieved = st["flops_per_step"] / (st["avg_ms"] / 1e3) / 1e12 if st["avg_ms"] > 0 else None
-    traffic = _profile_traffic(f"gain_gemm_config{args.config}.md")
+    # per step of the configuration's own grid (a --grid case has other operator bytes)
+    traffic = _profile_traffic(f"gain_gemm_config{args.config}.md") if not args.grid else None
     # 256-column tiles over an even number of 128-row m tiles run on SM pairs (cta_group::2)
     GEMM_LABEL = ("gain_gemm_pair (tcgen05.mma.cta_group::2, BF16 hi+lo x3)" if all(p["pair"] for p in plans)
                   else "gain_gemm (tcgen05, BF16 hi+lo x3)")
