@@ -22,94 +22,12 @@
 
 #include "batch_internal.h"
 #include "pdl.cuh"
+#include "umma.cuh"
 
 namespace dtb {
 
 namespace {
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ unsigned long long gtimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ void mb_init(uint32_t bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mb_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mb_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mb_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mb_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-    if (mb_try(bar, parity)) return true;
-    const unsigned long long t0 = gtimer();
-    while (true) {
-        if (mb_try(bar, parity)) return true;
-        if (abort_flag && *abort_flag) return false;
-        if (gtimer() - t0 > kWaitLimitNs) return false;
-    }
-}
-// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16) of a stream
-// read once per step (the G tiles, larger than L2): the lines are marked evict-first, so the
-// step's small working set (state, split partials, loss and emission operands) stays in L2
-// across the stream.
-__device__ __forceinline__ void bulk_load_stream(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
-            dst),
-        "l"(src), "r"(bytes), "r"(bar), "l"(pol)
-        : "memory");
-}
-// K-major operand tile in the canonical 128-byte swizzle layout: rows of 128 bytes, 8-row
-// groups 1024 bytes apart (stride byte offset 64 x 16 B), descriptor version 1.
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) | ((uint64_t)1 << 46) |
-           ((uint64_t)2 << 61);
-}
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-
-
-// 16 columns of this warp's 32 TMEM lanes without waiting (tcgen05.wait::ld before using r).
-__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
-    __nv_bfloat162 h = __floats2bfloat162_rn(lo_elem, hi_elem);
-    return *reinterpret_cast<uint32_t*>(&h);
-}
 
 template <int BN>
 struct GemmCfg {
@@ -442,38 +360,6 @@ struct PairCfg {
 };
 static_assert(PairCfg::SMEM <= 232448, "pair GEMM shared memory");
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-// shared::cluster address of the same shared-memory location in CTA `rank` of the cluster
-__device__ __forceinline__ uint32_t peer_addr(uint32_t saddr, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
-    return r;
-}
-__device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// arrive on a barrier of the other CTA of the pair (shared::cluster address)
-__device__ __forceinline__ void mb_arrive_remote(uint32_t cluster_bar) {
-    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
-}
-__device__ __forceinline__ void umma2_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                           uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-// arrive on one barrier (this CTA's or the peer's, by shared::cluster address) once the pair
-// MMAs issued so far by this thread have completed
-__device__ __forceinline__ void umma2_commit(uint32_t cluster_bar) {
-    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(cluster_bar)
-                 : "memory");
-}
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg::THREADS, 1)
     gain_gemm_pair_kernel(GemmArgs a) {
@@ -915,12 +801,6 @@ cudaError_t launch_split_rows(const float* src, long long rows, int row0, int n1
 // ------------------------------------------------------------------ batched Euler epilogue
 namespace {
 
-// Order-preserving map of doubles to unsigned integers (NaN is mapped to +Inf before):
-// x < y (with -0.0 < +0.0) <=> enc(x) < enc(y).
-__device__ __forceinline__ unsigned long long ord_enc(double x) {
-    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
-    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
-}
 
 constexpr int kRT = 32;   // rows per tile
 constexpr int kIT = 32;   // instances per tile
@@ -971,27 +851,6 @@ __device__ void row_terms_direct(const MixedRowOps& ops, const float* __restrict
     }
 }
 
-// Four 8x8 BF16 matrices from shared memory: the A fragment of one m16n8k16 MMA (rows 0-7 and
-// 8-15 at K 0-7, then the same rows at K 8-15), each lane giving the address of one row.
-__device__ __forceinline__ void ldsm_x4(uint32_t saddr, uint32_t (&r)[4]) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(saddr));
-}
-// d += A (16 x 16, BF16, row-major) * B (16 x 8, BF16, K-major per column), FP32 accumulation.
-__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-// BF16 hi and lo halves of two FP32 values (x0 in the low 16 bits): hi = bf16(x), lo = bf16(x - hi)
-__device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo) {
-    hi = pack_bf16x2(x0, x1);
-    const float h0 = __uint_as_float(hi << 16), h1 = __uint_as_float(hi & 0xffff0000u);
-    lo = pack_bf16x2(x0 - h0, x1 - h1);
-}
 
 // 16-byte asynchronous copy global -> shared; src_bytes 0 fills the destination with zeros.
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
