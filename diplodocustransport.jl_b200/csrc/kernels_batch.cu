@@ -875,9 +875,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 constexpr int kRowsThreads = 512;
 constexpr int kKHalves = 2;  // K halves of each product chunk (8 warps each)
 static_assert(kRowsThreads / 32 == 2 * 4 * kKHalves, "16 warps: 2 row blocks x 4 instance blocks x 2 K halves");
-static_assert(2 * kKHalves * kRT * (kIT + 1) * 4 <= kRowStages * kStageBytes, "partial tiles fit the ring");
+static_assert((2 * kKHalves + 2) * kRT * (kIT + 1) * 4 <= kRowStages * kStageBytes,
+              "the K halves' loss and emission tiles and the gather's half sums fit the ring");
 constexpr int kEllFast = 8;  // ELL widths up to this take the hoisted-load flux path
 constexpr int kGatherChunk = 18;  // split partials in flight per instance in the gain gather
+constexpr int kGatherVec = 18;    // 16-byte split partials in flight per thread in the vector gather
 
 __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps ops, const float* __restrict__ F,
                                                                   const float* __restrict__ Cc,
@@ -1078,8 +1080,74 @@ __global__ void __launch_bounds__(kRowsThreads) mixed_rows_kernel(MixedRowOps op
         s_pe[khalf][r0 + 8][c0 + 1] = acc_e[3];
     }
     pdl_wait();  // this step's gain GEMM has completed: its split partials are visible
-    // ---- gain of the tile from the reduced group sums (lanes along rows: coalesced)
-    if (ops.has_bin) {
+    // ---- gain of the tile from the reduced group sums
+    // Vector gather (tiles of one cell and species whose group rows start on a multiple of 4,
+    // in groups of M a multiple of 4): the two halves of the block take the two halves of the
+    // split range, each thread 4 consecutive rows of one instance with 16-byte loads, all of a
+    // half's loads in flight at once (the scalar gather below needs two L2 round trips); each
+    // half sums its splits in order, and the two half sums are added in a fixed order.
+    bool vec_gain = false;
+    if (ops.has_bin && fast) {
+        const int cell = a0 / ops.n_mom, am0 = a0 - cell * ops.n_mom;
+        const int s = species_of_row(ops, am0);
+        vec_gain = a0 + kRT <= n;
+        for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1] && vec_gain; ++e) {
+            const int gi = ops.gain_grp[e];
+            vec_gain = ((ops.gain_roff[e] + am0 - ops.sp_off[s]) % 4 == 0) && (ops.grp_M[gi] % 4 == 0);
+        }
+    }
+    if (vec_gain) {
+        float(*s_half)[kRT][kIT + 1] =
+            reinterpret_cast<float(*)[kRT][kIT + 1]>(rows_dyn + 2 * kKHalves * kRT * (kIT + 1));
+        const int cell = a0 / ops.n_mom, am0 = a0 - cell * ops.n_mom;
+        const int s = species_of_row(ops, am0);
+        const bool on = ops.bin_on == nullptr || ops.bin_on[cell] != 0;
+        const int h = tid >> 8, q = tid & 255, rg = q & 7, il = q >> 3;  // rows 4 rg .. + 3, instance il
+        const bool okv = on && i0 + il < B;
+        // the combine below: thread (row r, instances il0 and il0 + 16)
+        const int r = tid & (kRT - 1), il0 = tid >> 5;
+        float g0 = 0.f, g1 = 0.f;
+        for (int e = ops.gain_ptr[s]; e < ops.gain_ptr[s + 1]; ++e) {
+            const int gi = ops.gain_grp[e];
+            const int row0 = ops.gain_roff[e] + (am0 - ops.sp_off[s]);
+            const int Mg = ops.grp_M[gi];
+            const int nsp = ops.grp_nsplit[gi];
+            const int sp_lo = h == 0 ? 0 : (nsp + 1) / 2, sp_hi = h == 0 ? (nsp + 1) / 2 : nsp;
+            const float* pp = ops.grp_partial[gi] + ((size_t)cell * B + i0 + il) * Mg + row0 + 4 * rg;
+            const size_t st = (size_t)ops.grp_stride[gi];
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int c0 = sp_lo; c0 < sp_hi; c0 += kGatherVec) {
+                float4 v[kGatherVec];
+#pragma unroll
+                for (int k = 0; k < kGatherVec; ++k)
+                    v[k] = (okv && c0 + k < sp_hi) ? *reinterpret_cast<const float4*>(pp + (size_t)(c0 + k) * st)
+                                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < kGatherVec; ++k) {
+                    if (c0 + k < sp_hi) {
+                        acc.x += v[k].x;
+                        acc.y += v[k].y;
+                        acc.z += v[k].z;
+                        acc.w += v[k].w;
+                    }
+                }
+            }
+            s_half[h][4 * rg][il] = acc.x;
+            s_half[h][4 * rg + 1][il] = acc.y;
+            s_half[h][4 * rg + 2][il] = acc.z;
+            s_half[h][4 * rg + 3][il] = acc.w;
+            __syncthreads();
+            const float rs = ops.grp_rscale[gi][row0 + r];
+            if (on && i0 + il0 < B)
+                g0 += (s_half[0][r][il0] + s_half[1][r][il0]) * rs * ops.grp_sig1[gi][i0 + il0] * ops.grp_sig2[gi][i0 + il0];
+            if (on && i0 + il0 + 16 < B)
+                g1 += (s_half[0][r][il0 + 16] + s_half[1][r][il0 + 16]) * rs * ops.grp_sig1[gi][i0 + il0 + 16] *
+                      ops.grp_sig2[gi][i0 + il0 + 16];
+            __syncthreads();  // s_half is reused by the next group
+        }
+        s_gain[r][il0] = g0;
+        s_gain[r][il0 + 16] = g1;
+    } else if (ops.has_bin) {
         const int r = tid & (kRT - 1);
         const int a = a0 + r;
         const int cell = a / ops.n_mom, am = a - cell * ops.n_mom;
