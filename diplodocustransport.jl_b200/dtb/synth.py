@@ -202,6 +202,40 @@ def two_species(p_num: int, p_lo: float, p_hi: float, u_num: int, seed: int, dt:
                               g_range=g_range))
 
 
+def uneven_two_species(p_e: int, u_e: int, p_g: int, u_g: int, seed: int, batch: Optional[int] = None,
+                       dt_max: float = 1.0, g_range=(-6.0, 0.0), p_lo: float = 1e-2, p_hi: float = 1e2) -> Workload:
+    """Electron + photon workload on grids of different sizes (p_e x u_e electron states, p_g x u_g
+    photon states; the same p range): gain blocks n_out x n_e x n_g, loss blocks of both sides,
+    photon emission from electrons. With ``batch``, per-instance f0 and dt as batched_two_species."""
+    pe = np.logspace(math.log10(p_lo), math.log10(p_hi), p_e + 1)
+    pg = np.logspace(math.log10(p_lo), math.log10(p_hi), p_g + 1)
+    hr = np.array([0.0, 2.0])
+    ps = PhaseSpace(name_list=["Ele", "Pho"], px_num_list=[p_e, p_g], py_num_list=[u_e, u_g], pz_num_list=[1, 1],
+                    pxr_list=[pe, pg], pyr_list=[np.linspace(-1.0, 1.0, u_e + 1), np.linspace(-1.0, 1.0, u_g + 1)],
+                    pzr_list=[hr.copy(), hr.copy()], mass_list=[1.0, 0.0], x_num=1, dt0=1.0)
+    rng = np.random.default_rng(seed)
+    fluxm = upwind_flux(ps, rng, dt_max)
+    ne, ng = ps.species_sizes
+    lo, hi = g_range
+    gains = [GainBlock(out, 0, 1, _log_uniform(rng, (n_out, ne, ng), lo, hi) * gain_kappa(lo, hi, n_out, dt_max))
+             for out, n_out in ((0, ne), (1, ng))]
+    kl = loss_kappa(lo, hi, dt_max)
+    losses = [LossBlock(0, 1, _log_uniform(rng, (ne, ng), lo, hi) * kl),
+              LossBlock(1, 0, _log_uniform(rng, (ng, ne), lo, hi) * kl)]
+    emim = EmissionMatrices()
+    emim.blocks.append(EmiBlock(row0=ps.momentum_species_offset[1], col0=0,
+                                E=_log_uniform(rng, (ng, ne), lo, hi) * emi_kappa(lo, hi, ng, dt_max)))
+    w = Workload(ps=ps, binm=BinaryMatrices(gains=gains, losses=losses), emim=emim, fluxm=fluxm,
+                 f0=lognormal_f0(ps, [0.0, 0.0], 1.0), inj=np.zeros(ps.n_state), dt=dt_max, n_steps=0,
+                 meta=dict(seed=seed))
+    if batch is not None:
+        r2 = np.random.default_rng(seed + 7)
+        mus = r2.uniform(-1.0, 1.0, size=batch)
+        w.f0 = np.stack([lognormal_f0(ps, [mu, mu], 1.0) for mu in mus])
+        w.dt = r2.uniform(0.5, 1.0, size=batch) * dt_max
+    return w
+
+
 def device_log_uniform(shape, lo: float, hi: float, kappa: float, seed: int, dtype=None,
                        device: str = "cuda"):
     """10**U[lo, hi] * kappa generated on a CUDA device with a seeded torch generator."""
