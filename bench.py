@@ -347,9 +347,12 @@ def run_ours(args):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    # ---- the same K steps with CUDA events around every gain-kernel launch (direct launches)
+    # ---- CUDA events around every gain-kernel launch (direct launches): 8 discarded, then
+    # max(K, 400) timed
     L.dtb_set_profiling(m.ctx, 1)
-    m.run(scales)
+    m.run(scales[:PROF_WARM] if len(scales) >= PROF_WARM else np.full(PROF_WARM, scales[0]))
+    L.dtb_set_profiling(m.ctx, 1)
+    m.run(np.resize(scales, max(len(scales), PROF_MIN)))
     avg_ms = _lib.ctypes.c_double()
     bpl = _lib.ctypes.c_double()
     L.dtb_gain_kernel_stats(m.ctx, _lib.ctypes.byref(avg_ms), _lib.ctypes.byref(bpl))
@@ -412,10 +415,14 @@ def run_ours(args):
     return 0
 
 
+PROF_WARM = 8    # discarded direct launches before a kernel's per-launch timing
+PROF_MIN = 400   # at least this many timed launches
+
+
 def _plain_leg(plain, stream, dt: float, K: int, W: int, hbm: float):
     """Plain FP64 single instance on the batched grid: graphs prepared, W warm-up steps, K timed
-    steps (CUDA events on the library's stream), then K steps with the gain kernel timed per
-    launch for its HBM roofline. Returns the plain leg's JSON object."""
+    steps (CUDA events on the library's stream), then the gain kernel timed per launch for its
+    HBM roofline (8 discarded launches, then max(K, 400)). Returns the plain leg's JSON object."""
     import numpy as np
     import torch
     from dtb import _lib
@@ -430,7 +437,9 @@ def _plain_leg(plain, stream, dt: float, K: int, W: int, hbm: float):
     ms = e0.elapsed_time(e1)
     L = plain.L
     L.dtb_set_profiling(plain.ctx, 1)
-    plain.run(np.full(K, dt))
+    plain.run(np.full(PROF_WARM, dt))  # discarded
+    L.dtb_set_profiling(plain.ctx, 1)  # restarts the average
+    plain.run(np.full(max(K, PROF_MIN), dt))
     avg_ms, bpl = _lib.ctypes.c_double(), _lib.ctypes.c_double()
     L.dtb_gain_kernel_stats(plain.ctx, _lib.ctypes.byref(avg_ms), _lib.ctypes.byref(bpl))
     L.dtb_set_profiling(plain.ctx, 0)
@@ -567,14 +576,19 @@ def run_batched(args):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    # ---- the same K steps with CUDA events around every gain-GEMM launch (direct launches)
+    # ---- CUDA events around every gain-GEMM launch (direct launches): a few launches to warm the
+    # direct-launch path (discarded), then max(K, 400) timed launches, so a short timed region
+    # (the 20-step default of a driver run) still gives a steady per-launch average
     m.set_profiling(True)
+    m.run(PROF_WARM)
+    m.set_profiling(True)  # restarts the averages
+    K_prof = max(K, PROF_MIN)
     e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e4.record(stream)
-    m.run(K)
+    m.run(K_prof)
     e5.record(stream)
     torch.cuda.synchronize()
-    ms_prof = e4.elapsed_time(e5)
+    ms_prof = e4.elapsed_time(e5) * K / K_prof
     st = m.gemm_stats()
     plans = []
     while (pl := m.gemm_plan(len(plans))) is not None:
