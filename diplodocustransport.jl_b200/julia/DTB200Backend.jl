@@ -23,6 +23,7 @@ import DiplodocusTransport: BackendType, PhaseSpaceStruct
 
 export B200Backend, B200ForwardEulerStruct, b200_solve
 export B200BatchedEuler, admit!, run!, run_io!, get_f, batch_moments, gemm_plan, set_tune_cache
+export B200Server, add_grid!, start!, submit!, wait_request, cancel!, serve_stats
 
 const libdtb = get(ENV, "DTB_LIB", joinpath(@__DIR__, "..", "lib", "libdtb.so"))
 
@@ -198,6 +199,25 @@ function b200_solve(method::B200ForwardEulerStruct, dt_initial::Float64, t_save:
     return F, nsteps[]
 end
 
+# Solve with the OutputStruct's FP64 number and energy moments (DistributionMoments.jl:33,145,162)
+# of every saved state computed on the device; w: energy weight per momentum state. Returns the
+# saved states, number and energy as [species, cell, save] arrays, and the step count.
+function b200_solve(method::B200ForwardEulerStruct, dt_initial::Float64, t_save::Vector{Float64},
+                    w::Vector{Float64}; Verbose::Int64=1)
+    n = length(method.f_init)
+    ns = length(method.PhaseSpace.Momentum.px_num_list)
+    Sp = method.PhaseSpace.Space
+    nsp = Sp.x_num * Sp.y_num * Sp.z_num
+    F = Matrix{Float64}(undef, n, length(t_save))
+    number = zeros(ns, nsp, length(t_save))
+    energy = zeros(ns, nsp, length(t_save))
+    nsteps = Ref{Int64}(0)
+    check(ccall((:dtb_solve_ex, libdtb), Int32,
+        (Ptr{Cvoid}, Float64, Ptr{Float64}, Int64, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ref{Int64}),
+        method.ctx, dt_initial, t_save, length(t_save), Verbose, F, w, number, energy, nsteps))
+    return F, number, energy, nsteps[]
+end
+
 # ---------------------------------------------------------------- batched solves
 # Many independent solves of one grid (a parameter scan over initial spectra and time steps)
 # in one batched context: the shared G, stored as BF16 hi + lo with per-row scales, is
@@ -286,5 +306,97 @@ end
 # Plans measured in earlier runs are reused from `path`, new ones appended (nothing: forget).
 set_tune_cache(path::Union{Nothing,AbstractString}) =
     check(ccall((:dtb_set_tune_cache, libdtb), Int32, (Cstring,), path === nothing ? C_NULL : path))
+
+# ---------------------------------------------------------------- serving
+# Continuous batching of solve requests (each a Solve of n_steps steps from its own f0 and dt):
+# a library-owned host thread admits queued requests into free slots of their grid's batched
+# context as slots free up, runs every grid on its own stream and reads finished requests back.
+# Grids are batched contexts (B200BatchedEuler) registered against an HBM budget; the server
+# drives them until it is closed, and the caller closes them afterwards.
+struct ServeOpts
+    hbm_budget_bytes::Int64
+    max_chunk_steps::Int32
+    flags::Int32
+    chunk_ms::Float64
+end
+
+struct RequestStats
+    t_submit::Float64
+    t_admit::Float64
+    t_done::Float64
+    steps::Int64
+    cr_max::Float64
+    finite::Int32
+    grid::Int32
+end
+
+struct ServeStats
+    completed::Int64
+    instance_steps::Int64
+    batched_steps::Int64
+    queued::Int64
+    running::Int64
+    device_bytes::Int64
+    busy_s::Float64
+    elapsed_s::Float64
+end
+
+mutable struct B200Server
+    srv::Ptr{Cvoid}
+    grids::Vector{B200BatchedEuler}
+    function B200Server(; hbm_budget_bytes::Integer=0, max_chunk_steps::Integer=0, chunk_ms::Real=0.0)
+        opts = ServeOpts(Int64(hbm_budget_bytes), Int32(max_chunk_steps), Int32(0), Float64(chunk_ms))
+        out = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:dtb_serve_create, libdtb), Int32, (Ref{ServeOpts}, Ref{Ptr{Cvoid}}), opts, out))
+        self = new(out[], B200BatchedEuler[])
+        finalizer(close, self)
+        return self
+    end
+end
+
+# Registers a committed batched context as a grid; returns its grid id (DTB_ENOMEM past the budget).
+function add_grid!(s::B200Server, b::B200BatchedEuler)
+    id = Ref{Int32}(0)
+    check(ccall((:dtb_serve_add_grid, libdtb), Int32, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Int32}), s.srv, b.ctx, id))
+    push!(s.grids, b)
+    return Int(id[])
+end
+
+start!(s::B200Server) = check(ccall((:dtb_serve_start, libdtb), Int32, (Ptr{Cvoid},), s.srv))
+
+# Queues a solve of n_steps steps from f0 with dt (dt/dt0 applied by the caller, as the
+# functor's dt_scale); returns the request id. Thread-safe.
+function submit!(s::B200Server, grid::Integer, f0::Vector{Float64}, dt_scale::Float64, n_steps::Integer)
+    id = Ref{Int64}(0)
+    GC.@preserve f0 check(ccall((:dtb_serve_submit, libdtb), Int32,
+                                (Ptr{Cvoid}, Int32, Ptr{Float64}, Float64, Int64, Ref{Int64}),
+                                s.srv, grid, f0, dt_scale, n_steps, id))
+    return id[]
+end
+
+# Waits for a request (timeout in seconds, <= 0: no limit) and returns its final f and timings.
+function wait_request(s::B200Server, id::Integer, n_state::Integer; timeout_s::Real=0.0)
+    f = Vector{Float64}(undef, n_state)
+    st = Ref{RequestStats}()
+    check(ccall((:dtb_serve_wait, libdtb), Int32, (Ptr{Cvoid}, Int64, Float64, Ptr{Float64}, Ref{RequestStats}),
+                s.srv, id, timeout_s, f, st))
+    return f, st[]
+end
+
+cancel!(s::B200Server, id::Integer) = check(ccall((:dtb_serve_cancel, libdtb), Int32, (Ptr{Cvoid}, Int64), s.srv, id))
+
+function serve_stats(s::B200Server)
+    st = Ref{ServeStats}()
+    check(ccall((:dtb_serve_get_stats, libdtb), Int32, (Ptr{Cvoid}, Ref{ServeStats}), s.srv, st))
+    return st[]
+end
+
+function Base.close(s::B200Server)
+    if s.srv != C_NULL
+        ccall((:dtb_serve_destroy, libdtb), Int32, (Ptr{Cvoid},), s.srv)
+        s.srv = C_NULL
+    end
+    return nothing
+end
 
 end # module
