@@ -671,8 +671,12 @@ static int commit_typed(dtb_ctx* c, RowOps<T>& ops) {
         std::vector<std::vector<std::pair<const SpBlk*, const SparseRun*>>> srow((size_t)c->n_mom);
         for (auto& sb : sblks)
             for (auto& R : sb.runs) srow[(size_t)(c->off[sb.out] + R.al)].push_back({&sb, &R});
+        // about 8 work units per CTA spread the HBM stream of a large G evenly; an L2-resident G
+        // (64 MB or less) is bound by the per-unit round trip of the tile ring instead, so its
+        // units are about 8 times larger (config 0: 14.8 against 15.6 us per step)
+        const double units_per_cta = tot_bytes <= 64.0 * 1024 * 1024 ? 1.0 : 8.0;
         const double target = std::min(256.0 * 1024, std::max((double)kGainTileBytes,
-                                                               tot_bytes / ((double)c->num_sms * bps * 8)));
+                                                               tot_bytes / ((double)c->num_sms * bps * units_per_cta)));
         for (int64_t a = 0; a < c->n_mom; ++a) {
             unit_ptr[(size_t)a] = (int)units.size();
             const int sa = species_of(c, a);
