@@ -578,7 +578,7 @@ def run_batched(args):
     ms = e0.elapsed_time(e1)
     # ---- CUDA events around every gain-GEMM launch (direct launches): a few launches to warm the
     # direct-launch path (discarded), then max(K, 400) timed launches, so a short timed region
-    # (the 20-step default of a driver run) still gives a steady per-launch average
+    # (20 steps) still gives a steady per-launch average
     m.set_profiling(True)
     m.run(PROF_WARM)
     m.set_profiling(True)  # restarts the averages

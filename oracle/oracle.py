@@ -6,7 +6,7 @@ dt truncation of src/SteppingMethods.jl:18-27) in Python floats, which are IEEE 
 like Julia's Float64, so the step schedule is reproduced exactly.
 
 Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py use this module,
-and only as the checker. Parity is pinned against hand-derived known-answer vectors and a
+and only to check results. Parity is pinned against hand-derived known-answer vectors and a
 literal transliteration of the Julia lines (tests/golden/); it is unpinned against a run of
 the reference itself, which needs Julia.
 """

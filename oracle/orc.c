@@ -3,10 +3,10 @@
  *
  * TEST INFRASTRUCTURE ONLY. This file is a plain-C FP64 restatement of the
  * reference's algorithm, used by the tests, by the smoke check and by the
- * CPU-baseline leg of bench.py as the checker. Nothing in the product library
+ * CPU-baseline leg of bench.py to check results. Nothing in the product library
  * links, calls or falls back to it.
  *
- * Parity status: the reference (Julia) cannot run in this container and its
+ * Parity status: the reference (Julia) cannot run without a Julia toolchain and its
  * own test suite is empty (test/runtests.jl:4-6), so no reference-produced
  * vectors exist. This restatement is pinned instead against hand-derived
  * known-answer vectors and a literal pure-Python transliteration of the cited
