@@ -99,6 +99,22 @@ def test_blocked_equals_reference_layout():
     np.testing.assert_allclose(d1[:4], d2[:4], rtol=1e-12)
 
 
+def test_blocked_equals_reference_layout_uneven_species():
+    """Species of different sizes (electrons 4 x 3 = 12 states, photons 5 x 2 = 10): the blocked
+    operands (gain blocks n_out x n_e x n_g, both loss sides, emission) and the reference-layout
+    M_Bin and M_Emi they expand to step alike."""
+    w = synth.uneven_two_species(4, 3, 5, 2, seed=9)
+    assert w.ps.species_sizes == [12, 10]
+    b = oracle.blocked_from_workload(w)
+    r = oracle.ref_from_workload(w)
+    f, g = w.f0.copy(), w.f0.copy()
+    for _ in range(10):
+        f, d1, _ = b.step(f, 0.9, 3)
+        g, d2, _ = r.step(g, 0.9, 3)
+    assert np.max(np.abs(f - g)) / np.max(np.abs(g)) < 1e-14
+    np.testing.assert_allclose(d1[:4], d2[:4], rtol=1e-12)
+
+
 def test_conserving_gain_loss_preserves_number():
     """KAT 3: gain/loss built to conserve number per species (flux and emission off)."""
     w = synth.small(p_num=4, u_num=2, seed=8, with_emission=False)
