@@ -42,6 +42,23 @@ def test_plain_uneven_species_match_oracle(cuda, precision, tol, grid):
     m.close()
 
 
+def test_reference_layout_upload_uneven_species(cuda):
+    """The reference's dense M_Bin (N^2 x N) and M_Emi of an uneven grid (15 + 14 states),
+    decomposed by the library into blocks, step like the blocked upload (1e-13) and like the
+    oracle (1e-12)."""
+    from dtb.structs import BinaryMatrices, EmissionMatrices, blocked_to_ref, emission_to_dense
+    w = synth.uneven_two_species(5, 3, 7, 2, seed=25)
+    a = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm)
+    b = ForwardEulerStruct(w.ps, w.f0, w.inj, BinaryMatrices(M_Bin=blocked_to_ref(w.ps, w.binm)),
+                           EmissionMatrices(M_Emi=emission_to_dense(w.ps, w.emim)), w.fluxm)
+    a.run(np.full(24, 0.9))
+    b.run(np.full(24, 0.9))
+    assert rel_linf(b.f, a.f) <= 1e-13
+    assert rel_linf(b.f, _oracle_run(w, w.f0, 0.9, 24)) <= TOL64
+    a.close()
+    b.close()
+
+
 def test_plain_zero_length_run_leaves_the_state(cuda):
     w = synth.small(p_num=6, u_num=2, seed=4)
     m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm)
