@@ -185,6 +185,30 @@ def test_julia_binding_calls_only_declared_exported_symbols(path):
         assert hasattr(lib, name), name
 
 
+def test_reference_arm_prints_one_contract_line():
+    """bench.py --impl reference runs the FP64 oracle port on the host cores (no device) and
+    prints exactly one JSON line with the keys of the measurement contract, the same config
+    object as the GPU arm, and e2e copies of zero bytes."""
+    import json
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                          "--warmup", "3"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2 and d["warmup"] == 3
+    assert d["unit"] == "instance-steps/s" and d["higher_is_better"] is True
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["config"]["workload"].startswith("batching (config 2)") and d["config"]["batch"] == 256
+
+
 def test_tune_cache_is_host_only(tmp_path):
     """dtb_set_tune_cache needs no device: it loads a cache file (recorded lines and a file that
     does not exist yet alike) and forgets the plans with NULL."""
