@@ -149,8 +149,13 @@ struct dtb_ctx {
     unsigned long long* ctr = nullptr;
     unsigned long long host_ctr = 0;
     StepDiagDev* hist = nullptr;
+    // row-block diagnostics records: [graph_steps][rows_grid][kStepRecFields], slot k for step k
+    // of a sequence (the symplectic space pass uses the first 2 * rows_grid)
     double* blk_red = nullptr;
+    int rows_grid = 0;
     unsigned* ticket = nullptr;
+    long long launches = 0;      // kernels the step functions have launched (graph replays count their nodes)
+    long long graph_launches = 0;  // kernel nodes of the step graph
     int* err = nullptr;
     int* sp_off_dev = nullptr;
     double* mom_w = nullptr;

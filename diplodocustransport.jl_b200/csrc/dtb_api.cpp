@@ -910,8 +910,8 @@ extern "C" int32_t dtb_commit(dtb_ctx* c) {
     DTB_TRY(c->alloc(&c->dt_arr, sizeof(double) * (size_t)c->hist_cap));
     DTB_TRY(c->alloc(&c->ctr, sizeof(unsigned long long)));
     DTB_TRY(c->alloc(&c->hist, sizeof(StepDiagDev) * (size_t)c->hist_cap));
-    const int rows_grid = (int)((c->n_state + kRowsWarps - 1) / kRowsWarps);
-    DTB_TRY(c->alloc(&c->blk_red, sizeof(double) * 7 * (size_t)rows_grid));
+    c->rows_grid = euler_rows_blocks((int)c->n_state);
+    DTB_TRY(c->alloc(&c->blk_red, sizeof(double) * kStepRecFields * (size_t)c->rows_grid * c->graph_steps));
     DTB_TRY(c->alloc(&c->ticket, sizeof(unsigned)));
     DTB_TRY(c->alloc(&c->err, sizeof(int)));
     std::vector<int> spo(c->off, c->off + c->ns + 1);
@@ -951,11 +951,16 @@ static int flush_profile(dtb_ctx* c) {
     return DTB_OK;
 }
 
+// One step. Outside the symplectic method the step is number *ctr + kpos of the dt sequence and
+// writes record slot kpos; finish_seq reduces a sequence's records and advances the counter. The
+// symplectic space pass reduces its step's diagnostics and advances the counter itself (kpos 0).
 template <typename T>
-static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, int verbose, bool profile) {
+static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, int verbose, bool profile,
+                       int kpos) {
     T* fin = reinterpret_cast<T*>(c->f_buf[c->cur]);
     T* fout = reinterpret_cast<T*>(c->f_buf[c->cur ^ 1]);
-    if (c->n_units > 0 && c->n_bin_cells > 0) {
+    const bool gain = c->n_units > 0 && c->n_bin_cells > 0;
+    if (gain) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile) {
             const size_t k = (size_t)c->prof_pending * 2;
@@ -971,33 +976,58 @@ static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, 
         DTB_CUDA(launch_gain_stream<T>(reinterpret_cast<const T*>(c->G_all), c->units, c->n_units, fin, (int)c->n_mom,
                                        c->sp_off_host, c->ns, c->f_smem_len, c->partial, c->n_bin_cells,
                                        c->gain_grid, c->err, c->stream, c->bin_cells, true));
+        c->launches++;
         if (profile) {
             DTB_CUDA(cudaEventRecord(e1, c->stream));
             c->prof_n++;
             if (++c->prof_pending == kProfRing) DTB_TRY(flush_profile(c));
         }
     }
+    const double* dta = use_arr ? c->dt_arr : nullptr;
     if (c->symplectic) {
         RowOps<T> mom = ops;
         mom.mode = 1;
         T* fm = reinterpret_cast<T*>(c->fm_buf);
         T* dfm = reinterpret_cast<T*>(c->dfm_buf);
-        DTB_CUDA(launch_euler_rows<T>(mom, fin, fm, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist,
-                                      c->hist_cap, verbose, c->blk_red, c->ticket, c->stream));
-        DTB_CUDA(launch_sympl_space<T>(ops, fin, fm, dfm, fout, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist,
-                                       c->hist_cap, verbose, c->blk_red, c->ticket, c->stream));
+        DTB_CUDA(launch_euler_rows<T>(mom, fin, fm, dt_imm, dta, c->ctr, 0, verbose, nullptr, gain, c->stream));
+        DTB_CUDA(launch_sympl_space<T>(ops, fin, fm, dfm, fout, dt_imm, dta, c->ctr, c->hist, c->hist_cap, verbose,
+                                       c->blk_red, c->ticket, c->stream));
+        c->launches += 2;
     } else {
-        DTB_CUDA(launch_euler_rows<T>(ops, fin, fout, dt_imm, use_arr ? c->dt_arr : nullptr, c->ctr, c->hist,
-                                      c->hist_cap, verbose, c->blk_red, c->ticket, c->stream));
+        double* rec = c->blk_red + (size_t)kpos * c->rows_grid * kStepRecFields;
+        DTB_CUDA(launch_euler_rows<T>(ops, fin, fout, dt_imm, dta, c->ctr, kpos, verbose, rec, gain, c->stream));
+        c->launches++;
     }
     c->cur ^= 1;
     c->host_ctr++;
     return DTB_OK;
 }
 
-static int do_step(dtb_ctx* c, double dt_imm, bool use_arr, int verbose, bool profile) {
-    return c->prec == DTB_F64 ? launch_step<double>(c, c->ops_d, dt_imm, use_arr, verbose, profile)
-                              : launch_step<float>(c, c->ops_f, dt_imm, use_arr, verbose, profile);
+static int do_step(dtb_ctx* c, double dt_imm, bool use_arr, int verbose, bool profile, int kpos) {
+    return c->prec == DTB_F64 ? launch_step<double>(c, c->ops_d, dt_imm, use_arr, verbose, profile, kpos)
+                              : launch_step<float>(c, c->ops_f, dt_imm, use_arr, verbose, profile, kpos);
+}
+
+// The diagnostics of the last n steps (a sequence of record slots 0..n-1) and the counter advance.
+static int finish_seq(dtb_ctx* c, int n, int verbose) {
+    if (c->symplectic || n <= 0) return DTB_OK;
+    const int hb = c->prec == DTB_F64 ? c->ops_d.has_bin : c->ops_f.has_bin;
+    const int he = c->prec == DTB_F64 ? c->ops_d.has_emi : c->ops_f.has_emi;
+    DTB_CUDA(launch_step_diag(c->blk_red, c->rows_grid, n, c->ctr, c->hist, c->hist_cap, verbose, hb, he, c->ticket,
+                              c->stream));
+    c->launches++;
+    return DTB_OK;
+}
+
+// n steps outside a graph, in sequences of at most graph_steps (the record slots).
+static int run_loose(dtb_ctx* c, int64_t n, int verbose, bool profile) {
+    for (int64_t done = 0; done < n;) {
+        const int m = (int)std::min<int64_t>(c->graph_steps, n - done);
+        for (int k = 0; k < m; ++k) DTB_TRY(do_step(c, 0.0, true, verbose, profile, k));
+        DTB_TRY(finish_seq(c, m, verbose));
+        done += m;
+    }
+    return DTB_OK;
 }
 
 static int check_kernel_err(dtb_ctx* c) {
@@ -1023,14 +1053,18 @@ static int ensure_graph(dtb_ctx* c, int verbose) {
     }
     const int saved_cur = c->cur;
     const unsigned long long saved_ctr = c->host_ctr;
+    const long long saved_launches = c->launches;
     c->cur = 0;
     cudaGraph_t g;
     DTB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = DTB_OK;
-    for (int k = 0; k < c->graph_steps && rc == DTB_OK; ++k) rc = do_step(c, 0.0, true, verbose, false);
+    for (int k = 0; k < c->graph_steps && rc == DTB_OK; ++k) rc = do_step(c, 0.0, true, verbose, false, k);
+    if (rc == DTB_OK) rc = finish_seq(c, c->graph_steps, verbose);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->graph_launches = c->launches - saved_launches;
     c->cur = saved_cur;
     c->host_ctr = saved_ctr;
+    c->launches = saved_launches;
     if (rc != DTB_OK) return rc;
     DTB_CUDA(e);
     e = cudaGraphInstantiate(&c->graph, g, 0);
@@ -1049,7 +1083,7 @@ static int run_chunk(dtb_ctx* c, int64_t n, int verbose, bool use_graph) {
     int64_t done = 0;
     if (use_graph && !c->profiling && n >= c->graph_steps) {
         if (c->cur != 0) {
-            DTB_TRY(do_step(c, 0.0, true, verbose, false));
+            DTB_TRY(run_loose(c, 1, verbose, false));
             done++;
         }
         DTB_TRY(ensure_graph(c, verbose));
@@ -1057,10 +1091,10 @@ static int run_chunk(dtb_ctx* c, int64_t n, int verbose, bool use_graph) {
             DTB_CUDA(cudaGraphLaunch(c->graph, c->stream));
             done += c->graph_steps;
             c->host_ctr += c->graph_steps;
+            c->launches += c->graph_launches;
         }
     }
-    for (; done < n; ++done) DTB_TRY(do_step(c, 0.0, true, verbose, c->profiling));
-    return DTB_OK;
+    return run_loose(c, n - done, verbose, c->profiling);
 }
 
 static void print_cr(int verbose, const StepDiagDev& d, double t, double t_stop, double dt) {
@@ -1099,7 +1133,8 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
         c->host_ctr = 0;
     }
     const unsigned long long idx = c->host_ctr;
-    DTB_TRY(do_step(c, dt_scale, false, verbose, false));
+    DTB_TRY(do_step(c, dt_scale, false, verbose, false, 0));
+    DTB_TRY(finish_seq(c, 1, verbose));
     c->steps_run++;
     if (dt_out) *dt_out = dt;
     if (save_out) *save_out = save;
@@ -1262,17 +1297,17 @@ static int run_steps(dtb_ctx* c, int64_t n, int verbose) {
     int64_t done = 0;
     if (!c->profiling && n >= c->graph_steps) {
         if (c->cur != 0) {
-            DTB_TRY(do_step(c, 0.0, true, verbose, false));
+            DTB_TRY(run_loose(c, 1, verbose, false));
             done++;
         }
         while (n - done >= c->graph_steps) {
             DTB_CUDA(cudaGraphLaunch(c->graph, c->stream));
             done += c->graph_steps;
             c->host_ctr += c->graph_steps;
+            c->launches += c->graph_launches;
         }
     }
-    for (; done < n; ++done) DTB_TRY(do_step(c, 0.0, true, verbose, c->profiling));
-    return DTB_OK;
+    return run_loose(c, n - done, verbose, c->profiling);
 }
 
 namespace {
@@ -1508,6 +1543,12 @@ int32_t dtb_launches_per_step(dtb_ctx* c, int32_t* n) {
     DTB_CHECK(c && n, DTB_EINVAL, "dtb_launches_per_step: null argument");
     DTB_TRY(dtb_commit(c));
     *n = (c->n_units > 0 ? 2 : 1) + (c->symplectic ? 1 : 0);
+    return DTB_OK;
+}
+
+int32_t dtb_launch_count(dtb_ctx* c, int64_t* n) {
+    DTB_CHECK(c && n, DTB_EINVAL, "dtb_launch_count: null argument");
+    *n = c->launches;
     return DTB_OK;
 }
 

@@ -100,11 +100,26 @@ cudaError_t launch_gain_stream(const T* G, const GainUnit* units, int n_units, c
                                double* partial, int n_space, int grid_x, int* err, cudaStream_t s,
                                const int* cell_list = nullptr, bool pdl = false);
 
+// Fields of one row block's diagnostics record: min cr, cr_bin, cr_emi, cr_flux, sum df, sum f.
+constexpr int kStepRecFields = 6;
+
+// One step's rows. The step is number *ctr + kpos of the dt sequence (the counter advances
+// only in launch_step_diag); each row block writes its diagnostics record to
+// rec[blockIdx][kStepRecFields] (rec: the step's slot of the record buffer). pdl: launch as a
+// programmatic dependent of the previous kernel, which must then be the step's gain kernel (the
+// rows read the state before their dependency wait).
 template <typename T>
 cudaError_t launch_euler_rows(const RowOps<T>& ops, const T* f_in, T* f_out, double dt_imm,
-                              const double* dt_arr, unsigned long long* ctr, StepDiagDev* hist,
-                              long long hist_cap, int verbose, double* blk_red, unsigned* ticket,
-                              cudaStream_t s);
+                              const double* dt_arr, const unsigned long long* ctr, int kpos, int verbose,
+                              double* rec, bool pdl, cudaStream_t s);
+int euler_rows_blocks(int n_state);
+
+// The diagnostics of steps *ctr .. *ctr + n_steps - 1: block k reduces step k's row-block
+// records (slot k of blk_red, n_blocks records of kStepRecFields each) into
+// hist[(*ctr + k) % hist_cap]; the last block to finish advances *ctr by n_steps.
+cudaError_t launch_step_diag(const double* blk_red, int n_blocks, int n_steps, unsigned long long* ctr,
+                             StepDiagDev* hist, long long hist_cap, int verbose, int has_bin, int has_emi,
+                             unsigned* ticket, cudaStream_t s);
 
 template <typename T>
 cudaError_t launch_sympl_space(const RowOps<T>& ops, const T* f_old, const T* fm, const T* dfm, T* f_out,

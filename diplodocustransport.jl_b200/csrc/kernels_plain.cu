@@ -1,13 +1,16 @@
 // Kernels of the plain (single-instance) explicit Euler step, FP64 or FP32.
 //
-// One step is two launches:
+// One step is two launches,
 //   gain_stream  - streams the gain blocks G[a][b][c] from HBM through a bulk-copy (TMA)
 //                  pipeline in shared memory and contracts each tile against f_b f_c formed
 //                  on the fly; writes one FP64 partial per (row, b-range) work unit.
 //   euler_rows   - one warp per state row: banded flux row (ELL, 128-bit loads), emission
 //                  row pieces, loss bilinear term, sum of the row's gain partials, then the
-//                  Euler update and clamp of SteppingMethods.jl:46-101, with the CFL
-//                  diagnostics reduced across the grid by the last block to finish.
+//                  Euler update and clamp of SteppingMethods.jl:46-101; each block writes a
+//                  record of its rows' CFL diagnostics.
+// and, once per sequence of steps (a graph of them, or the steps run outside one),
+//   step_diag    - one block per step reduces the step's block records (SteppingMethods.jl:48-94)
+//                  and advances the step counter, off the steps' critical path.
 // The state is double-buffered (f_in -> f_out) because a row reads other rows' f.
 #include <cuda_runtime.h>
 #include <math_constants.h>
@@ -323,25 +326,22 @@ template cudaError_t launch_gain_stream<float>(const float*, const GainUnit*, in
                                                const int*, bool);
 
 // ------------------------------------------------------------------ euler_rows
-constexpr int kRedFields = 7;  // min cr, cr_bin, cr_emi, cr_flux, sum_df, sum_f, nonfinite count
-
 template <typename T>
 __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> ops, const T* __restrict__ f_in,
                                                                      T* __restrict__ f_out, double dt_imm,
                                                                      const double* __restrict__ dt_arr,
-                                                                     unsigned long long* ctr, StepDiagDev* hist,
-                                                                     long long hist_cap, int verbose,
-                                                                     double* blk_red, unsigned* ticket) {
-    __shared__ double s_red[kRowsWarps][kRedFields];
-    __shared__ double s_fin[6][kRowsWarps * 32];
-    __shared__ int s_last;
-    // The previous step's state and step counter were final before this grid could launch: the
-    // gain kernel it depends on let it launch only after that kernel's own wait for the previous
-    // row kernel. So the flux, emission and loss products, which read only the state and static
-    // operands, run before the wait for this step's gain partials (on SMs beside the gain kernel
-    // where it leaves room); everything this grid writes is written after the wait.
+                                                                     const unsigned long long* ctr, int kpos,
+                                                                     int verbose, double* rec) {
+    __shared__ double s_red[kRowsWarps][kStepRecFields];
+    // The previous step's state and the step counter (which advances only between step
+    // sequences) were final before this grid could launch: as a programmatic dependent it
+    // follows this step's gain kernel, which lets it launch only after that kernel's own wait for
+    // the kernels before it; without a gain kernel it launches in plain stream order. So the
+    // flux, emission and loss products, which read only the state and static operands, run
+    // before the wait for this step's gain partials (on SMs beside the gain kernel where it
+    // leaves room); everything this grid writes is written after the wait.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
+    const unsigned long long step = *reinterpret_cast<const volatile unsigned long long*>(ctr) + (unsigned)kpos;
     const double dt_scale = dt_arr ? dt_arr[step] : dt_imm;
     const int i = blockIdx.x * kRowsWarps + warp;
 
@@ -453,6 +453,8 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         }
     }
     if (ops.mode == 1) return;  // the space pass reduces the step's diagnostics
+    // this block's record; the step's records are reduced by step_diag_kernel, so no row
+    // block waits for the others
     if (lane == 0) {
         s_red[warp][0] = m_cr;
         s_red[warp][1] = m_bin;
@@ -460,80 +462,102 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         s_red[warp][3] = m_flux;
         s_red[warp][4] = s_df;
         s_red[warp][5] = s_f;
-        s_red[warp][6] = 0.0;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double r[kRedFields];
-        for (int k = 0; k < kRedFields; ++k) r[k] = s_red[0][k];
+        double r[kStepRecFields];
+        for (int k = 0; k < kStepRecFields; ++k) r[k] = s_red[0][k];
         for (int w = 1; w < kRowsWarps; ++w) {
             for (int k = 0; k < 4; ++k) r[k] = jl_min(r[k], s_red[w][k]);
             r[4] += s_red[w][4];
             r[5] += s_red[w][5];
         }
-        double* dst = blk_red + (size_t)blockIdx.x * kRedFields;
-        for (int k = 0; k < kRedFields; ++k) dst[k] = r[k];
+        double* dst = rec + (size_t)blockIdx.x * kStepRecFields;
+        for (int k = 0; k < kStepRecFields; ++k) dst[k] = r[k];
+    }
+}
+
+int euler_rows_blocks(int n_state) { return (n_state + kRowsWarps - 1) / kRowsWarps; }
+
+// Block k reduces the row-block records of step *ctr + k with a fixed assignment (record b to
+// thread b mod 256, in order) and a fixed tree, so a step's record does not depend on block
+// completion order or on how the steps were grouped into launches.
+__global__ void __launch_bounds__(kRowsWarps * 32) step_diag_kernel(const double* __restrict__ blk_red,
+                                                                    int n_blocks, int n_steps,
+                                                                    unsigned long long* ctr, StepDiagDev* hist,
+                                                                    long long hist_cap, int verbose,
+                                                                    int has_bin, int has_emi,
+                                                                    unsigned* ticket) {
+    __shared__ double s_fin[kStepRecFields][kRowsWarps * 32];
+    pdl_wait();  // the last step's row blocks have written their records
+    // a gain kernel that follows may start streaming its (static) blocks; it reads the state and
+    // the row kernel after it reads the counter only after this grid has finished
+    if (threadIdx.x == 0) pdl_trigger();
+    const unsigned long long step0 = *reinterpret_cast<volatile unsigned long long*>(ctr);
+    const double* recs = blk_red + (size_t)blockIdx.x * n_blocks * kStepRecFields;
+    double r[kStepRecFields] = {CUDART_INF, CUDART_INF, CUDART_INF, CUDART_INF, 0.0, 0.0};
+    for (int b = threadIdx.x; b < n_blocks; b += blockDim.x) {
+        const double* src = recs + (size_t)b * kStepRecFields;
+        for (int k = 0; k < 4; ++k) r[k] = jl_min(r[k], __ldcg(src + k));
+        r[4] += __ldcg(src + 4);
+        r[5] += __ldcg(src + 5);
+    }
+    for (int k = 0; k < kStepRecFields; ++k) s_fin[k][threadIdx.x] = r[k];
+    __syncthreads();
+    for (int o = kRowsWarps * 16; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            for (int k = 0; k < 4; ++k) s_fin[k][threadIdx.x] = jl_min(s_fin[k][threadIdx.x], s_fin[k][threadIdx.x + o]);
+            s_fin[4][threadIdx.x] += s_fin[4][threadIdx.x + o];
+            s_fin[5][threadIdx.x] += s_fin[5][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kStepRecFields; ++k) r[k] = s_fin[k][0];
+        StepDiagDev d;
+        const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && r[5] != 0.0;
+        d.cr[0] = on ? -r[0] : 0.0;
+        d.cr[1] = (on && verbose == 3 && has_bin) ? -r[1] : 0.0;
+        d.cr[2] = (on && verbose == 3 && has_emi) ? -r[2] : 0.0;
+        d.cr[3] = (on && verbose == 3) ? -r[3] : 0.0;
+        d.sum_df = r[4];
+        d.sum_f = r[5];
+        d.finite = isfinite(r[4]) ? 1 : 0;
+        d.pad = 0;
+        hist[(step0 + blockIdx.x) % (unsigned long long)hist_cap] = d;
+        // every block has read the counter before it takes its ticket; the last one advances it
         __threadfence();
         const unsigned t = atomicAdd(ticket, 1u);
-        s_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        // last block: reduce the per-block records in parallel (fixed assignment and a fixed
-        // tree, so the result does not depend on block completion order)
-        __threadfence();
-        double r[6] = {CUDART_INF, CUDART_INF, CUDART_INF, CUDART_INF, 0.0, 0.0};
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-            const double* src = blk_red + (size_t)b * kRedFields;
-            for (int k = 0; k < 4; ++k) r[k] = jl_min(r[k], __ldcg(src + k));
-            r[4] += __ldcg(src + 4);
-            r[5] += __ldcg(src + 5);
-        }
-        for (int k = 0; k < 6; ++k) s_fin[k][threadIdx.x] = r[k];
-        __syncthreads();
-        for (int o = kRowsWarps * 16; o > 0; o >>= 1) {
-            if (threadIdx.x < o) {
-                for (int k = 0; k < 4; ++k) s_fin[k][threadIdx.x] = jl_min(s_fin[k][threadIdx.x], s_fin[k][threadIdx.x + o]);
-                s_fin[4][threadIdx.x] += s_fin[4][threadIdx.x + o];
-                s_fin[5][threadIdx.x] += s_fin[5][threadIdx.x + o];
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < 6; ++k) r[k] = s_fin[k][0];
-            StepDiagDev d;
-            const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && r[5] != 0.0;
-            d.cr[0] = on ? -r[0] : 0.0;
-            d.cr[1] = (on && verbose == 3 && ops.has_bin) ? -r[1] : 0.0;
-            d.cr[2] = (on && verbose == 3 && ops.has_emi) ? -r[2] : 0.0;
-            d.cr[3] = (on && verbose == 3) ? -r[3] : 0.0;
-            d.sum_df = r[4];
-            d.sum_f = r[5];
-            d.finite = isfinite(r[4]) ? 1 : 0;
-            d.pad = 0;
-            hist[step % (unsigned long long)hist_cap] = d;
+        if (t == gridDim.x - 1) {
             *ticket = 0u;
-            __threadfence();
-            *reinterpret_cast<volatile unsigned long long*>(ctr) = step + 1ull;
+            *reinterpret_cast<volatile unsigned long long*>(ctr) = step0 + (unsigned long long)n_steps;
         }
     }
+}
+
+cudaError_t launch_step_diag(const double* blk_red, int n_blocks, int n_steps, unsigned long long* ctr,
+                             StepDiagDev* hist, long long hist_cap, int verbose, int has_bin, int has_emi,
+                             unsigned* ticket, cudaStream_t s) {
+    return launch_pdl(step_diag_kernel, dim3(n_steps), dim3(kRowsWarps * 32), 0, s, blk_red, n_blocks, n_steps, ctr,
+                      hist, hist_cap, verbose, has_bin, has_emi, ticket);
 }
 
 template <typename T>
 cudaError_t launch_euler_rows(const RowOps<T>& ops, const T* f_in, T* f_out, double dt_imm, const double* dt_arr,
-                              unsigned long long* ctr, StepDiagDev* hist, long long hist_cap, int verbose,
-                              double* blk_red, unsigned* ticket, cudaStream_t s) {
-    const int grid = (ops.n_state + kRowsWarps - 1) / kRowsWarps;
-    return launch_pdl(euler_rows_kernel<T>, grid, dim3(kRowsWarps * 32), 0, s, ops, f_in, f_out, dt_imm, dt_arr, ctr,
-                      hist, hist_cap, verbose, blk_red, ticket);
+                              const unsigned long long* ctr, int kpos, int verbose, double* rec, bool pdl,
+                              cudaStream_t s) {
+    const int grid = euler_rows_blocks(ops.n_state);
+    if (pdl)
+        return launch_pdl(euler_rows_kernel<T>, grid, dim3(kRowsWarps * 32), 0, s, ops, f_in, f_out, dt_imm, dt_arr,
+                          ctr, kpos, verbose, rec);
+    euler_rows_kernel<T><<<grid, kRowsWarps * 32, 0, s>>>(ops, f_in, f_out, dt_imm, dt_arr, ctr, kpos, verbose, rec);
+    return cudaGetLastError();
 }
 
 template cudaError_t launch_euler_rows<double>(const RowOps<double>&, const double*, double*, double, const double*,
-                                               unsigned long long*, StepDiagDev*, long long, int, double*,
-                                               unsigned*, cudaStream_t);
+                                               const unsigned long long*, int, int, double*, bool, cudaStream_t);
 template cudaError_t launch_euler_rows<float>(const RowOps<float>&, const float*, float*, double, const double*,
-                                              unsigned long long*, StepDiagDev*, long long, int, double*,
-                                              unsigned*, cudaStream_t);
+                                              const unsigned long long*, int, int, double*, bool, cudaStream_t);
 
 // ------------------------------------------------------------------ sympl_space
 // ForwardSymplecticEuler space pass (SteppingMethods.jl:165-237): one warp per row,

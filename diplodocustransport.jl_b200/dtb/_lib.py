@@ -103,6 +103,7 @@ SIGNATURES = {
     "dtb_get_stream": (_i32, [_P, ctypes.POINTER(_P)]),
     "dtb_sync": (_i32, [_P]),
     "dtb_launches_per_step": (_i32, [_P, _i32p]),
+    "dtb_launch_count": (_i32, [_P, _ip]),
     "dtb_gain_kernel_stats": (_i32, [_P, _dp, _dp]),
     "dtb_set_profiling": (_i32, [_P, _i32]),
     "dtb_selftest_bounded_wait": (_i32, [_P, _d]),

@@ -215,8 +215,13 @@ int32_t dtb_device_bytes(dtb_ctx* ctx, int64_t* bytes);
 int32_t dtb_get_stream(dtb_ctx* ctx, void** stream);
 int32_t dtb_sync(dtb_ctx* ctx);
 
-/* Kernel launches issued per step by dtb_run (for launch accounting). */
+/* Kernel launches issued per step by dtb_run (for launch accounting); the diagnostics
+ * reduction adds one launch per sequence of steps (a graph replay, or up to 16 steps run
+ * outside one). */
 int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
+/* Kernel launches the context's step functions (dtb_step, dtb_run, dtb_solve) have issued so
+ * far, kernels replayed in graphs included. */
+int32_t dtb_launch_count(dtb_ctx* ctx, int64_t* n);
 
 /* Failure-detection self-test: launches one block that waits, with a limit of limit_s
  * seconds (at most 2), on an mbarrier phase nothing completes, i.e. the give-up path of every

@@ -59,6 +59,60 @@ def test_reference_layout_upload_uneven_species(cuda):
     b.close()
 
 
+@pytest.mark.parametrize("case", ["no_binary", "empty_domain"])
+def test_plain_without_gain_kernel_runs_in_graphs(cuda, case):
+    """Steps with no gain kernel (no binary term, or a binary domain with no cell): each row
+    kernel follows the previous one in plain stream order. 45 steps through dtb_run (a loose
+    step, two graphs of 16, 12 loose steps) against the FP64 oracle."""
+    from dtb.structs import BinaryMatrices
+    w = synth.small(p_num=8, u_num=4, seed=31, n_space=2, randomize_vectors=True)
+    if case == "no_binary":
+        w.binm = BinaryMatrices()
+    else:
+        w.binm.Domain = []
+    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm)
+    m.run(np.full(45, 0.9))
+    assert rel_linf(m.f, _oracle_run(w, w.f0, 0.9, 45)) <= TOL64
+    m.close()
+
+
+def _diag_tuple(d):
+    return (d.cr, d.cr_bin, d.cr_emi, d.cr_flux, d.sum_df, d.sum_f, d.finite)
+
+
+@pytest.mark.parametrize("graph_steps", [4, 16])
+def test_step_records_do_not_depend_on_launch_grouping(cuda, graph_steps):
+    """The per-step diagnostics (Cr, Cr_Bin, Cr_Emi, Cr_Flux, sum df, sum f, finite) of 37 steps
+    run as graph replays and loose sequences equal, bit for bit, those of 37 single dtb_step
+    calls, and match the oracle's (rtol 1e-10). dtb_launch_count counts the gain and row kernel
+    of every step plus one diagnostics reduction per sequence."""
+    import ctypes
+    from dtb import _lib
+    w = synth.small(p_num=10, u_num=4, seed=32, n_space=2, randomize_vectors=True)
+    n = 37
+    a = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=graph_steps)
+    b = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=graph_steps)
+    c0, c1 = ctypes.c_int64(), ctypes.c_int64()
+    a.L.dtb_launch_count(a.ctx, ctypes.byref(c0))
+    sc = (0.9 * a.dt0) / a.dt0  # the dt / dt0 dtb_step forms from dt = 0.9 dt0
+    hist = a.run(np.full(n, sc), Verbose=3, diag=True)
+    a.L.dtb_launch_count(a.ctx, ctypes.byref(c1))
+    graphs, loose = n // graph_steps, n % graph_steps
+    assert c1.value - c0.value == 2 * n + graphs + (1 if loose else 0)
+    ops = oracle.blocked_from_workload(w)
+    f = np.array(w.f0, dtype=np.float64)
+    for k in range(n):
+        b(0.0, 1e9, 0.9 * b.dt0, 3)
+        assert _diag_tuple(hist[k]) == _diag_tuple(b.last_diag), k
+        f, diag, _ = ops.step(f, sc, 3)
+        for got, exp in zip(_diag_tuple(hist[k])[:4], diag[:4]):
+            assert got == pytest.approx(exp, rel=1e-10), k
+        assert bool(hist[k].finite) == bool(diag[4])
+    np.testing.assert_array_equal(a.f, b.f)
+    a.close()
+    b.close()
+
+
 def test_plain_zero_length_run_leaves_the_state(cuda):
     w = synth.small(p_num=6, u_num=2, seed=4)
     m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm)
