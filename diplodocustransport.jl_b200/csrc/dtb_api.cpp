@@ -1112,6 +1112,27 @@ static double dt0_eff(const dtb_ctx* c) {
     return c->prec == DTB_F32 ? (double)(float)c->opts.dt0 : c->opts.dt0;
 }
 
+// The step of dtb_step, enqueued: dt truncated at t_stop (SteppingMethods.jl:18-27), the step's
+// kernels and its diagnostics reduction; *idx gets the step's slot in the step history.
+static int enqueue_step(dtb_ctx* c, double t_start, double t_stop, double* dt, int* save, int verbose,
+                        unsigned long long* idx) {
+    *save = 0;
+    if (t_start + *dt >= t_stop) {
+        *dt = t_stop - t_start;
+        *save = 1;
+    }
+    const double dt_scale = *dt / dt0_eff(c);
+    if (c->host_ctr >= (unsigned long long)c->hist_cap) {
+        DTB_CUDA(cudaMemsetAsync(c->ctr, 0, sizeof(unsigned long long), c->stream));
+        c->host_ctr = 0;
+    }
+    *idx = c->host_ctr;
+    DTB_TRY(do_step(c, dt_scale, false, verbose, false, 0));
+    DTB_TRY(finish_seq(c, 1, verbose));
+    c->steps_run++;
+    return DTB_OK;
+}
+
 extern "C" {
 
 int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t verbose, double* dt_out,
@@ -1121,21 +1142,9 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
     DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_step: batched contexts use the dtb_batch_* entry points");
     DTB_TRY(dtb_commit(c));
     DeviceGuard g(c->device);
-    // SteppingMethods.jl:18-27
     int save = 0;
-    if (t_start + dt >= t_stop) {
-        dt = t_stop - t_start;
-        save = 1;
-    }
-    const double dt_scale = dt / dt0_eff(c);
-    if (c->host_ctr >= (unsigned long long)c->hist_cap) {
-        DTB_CUDA(cudaMemsetAsync(c->ctr, 0, sizeof(unsigned long long), c->stream));
-        c->host_ctr = 0;
-    }
-    const unsigned long long idx = c->host_ctr;
-    DTB_TRY(do_step(c, dt_scale, false, verbose, false, 0));
-    DTB_TRY(finish_seq(c, 1, verbose));
-    c->steps_run++;
+    unsigned long long idx = 0;
+    DTB_TRY(enqueue_step(c, t_start, t_stop, &dt, &save, verbose, &idx));
     if (dt_out) *dt_out = dt;
     if (save_out) *save_out = save;
     if (verbose == 1 || verbose == 2 || verbose == 3 || diag_out) {
@@ -1143,6 +1152,43 @@ int32_t dtb_step(dtb_ctx* c, double t_start, double t_stop, double dt, int32_t v
         DTB_TRY(check_kernel_err(c));
         if (diag_out) std::memcpy(diag_out, c->pin_hist, sizeof(StepDiagDev));
     }
+    return DTB_OK;
+}
+
+int32_t dtb_step_io(dtb_ctx* c, const double* f_in, double* f_out, double t_start, double t_stop, double dt,
+                    int32_t verbose, double* dt_out, int32_t* save_out, dtb_step_diag* diag_out) {
+    DTB_RANGE("dtb_step_io");
+    DTB_CHECK(c && f_out, DTB_EINVAL, "dtb_step_io: null argument");
+    DTB_CHECK(c->prec != DTB_MIXED, DTB_ESTATE, "dtb_step_io: batched contexts use dtb_batch_run_io");
+    DTB_TRY(dtb_commit(c));
+    DeviceGuard g(c->device);
+    const size_t n = (size_t)c->n_state;
+    // the FP32 staging buffer is idle here: every call that fills or drains it waits for its copy
+    if (f_in) {
+        if (c->prec == DTB_F64) {
+            DTB_CUDA(cudaMemcpyAsync(c->f_buf[c->cur], f_in, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        } else {
+            for (size_t k = 0; k < n; ++k) c->pin_f32[k] = (float)f_in[k];
+            DTB_CUDA(cudaMemcpyAsync(c->f_buf[c->cur], c->pin_f32, sizeof(float) * n, cudaMemcpyHostToDevice,
+                                     c->stream));
+        }
+    }
+    int save = 0;
+    unsigned long long idx = 0;
+    DTB_TRY(enqueue_step(c, t_start, t_stop, &dt, &save, verbose, &idx));
+    if (c->prec == DTB_F64)
+        DTB_CUDA(cudaMemcpyAsync(f_out, c->f_buf[c->cur], sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    else
+        DTB_CUDA(cudaMemcpyAsync(c->pin_f32, c->f_buf[c->cur], sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    const bool want_diag = verbose == 1 || verbose == 2 || verbose == 3 || diag_out;
+    if (want_diag)
+        DTB_CUDA(cudaMemcpyAsync(c->pin_hist, c->hist + idx, sizeof(StepDiagDev), cudaMemcpyDeviceToHost, c->stream));
+    DTB_TRY(check_kernel_err(c));  // the one wait of the round trip
+    if (c->prec == DTB_F32)
+        for (size_t k = 0; k < n; ++k) f_out[k] = c->pin_f32[k];
+    if (dt_out) *dt_out = dt;
+    if (save_out) *save_out = save;
+    if (diag_out) std::memcpy(diag_out, c->pin_hist, sizeof(StepDiagDev));
     return DTB_OK;
 }
 

@@ -91,6 +91,7 @@ SIGNATURES = {
     "dtb_upload_mbin_csc": (_i32, [_P, _i64, _ip, _ip, _dp]),
     "dtb_commit": (_i32, [_P]),
     "dtb_step": (_i32, [_P, _d, _d, _d, _i32, _dp, _i32p, ctypes.POINTER(StepDiag)]),
+    "dtb_step_io": (_i32, [_P, _dp, _dp, _d, _d, _d, _i32, _dp, _i32p, ctypes.POINTER(StepDiag)]),
     "dtb_run": (_i32, [_P, _dp, _i64, _i32, ctypes.POINTER(StepDiag)]),
     "dtb_solve": (_i32, [_P, _d, _dp, _i64, _i32, _dp, _ip]),
     "dtb_solve_ex": (_i32, [_P, _d, _dp, _i64, _i32, _dp, _dp, _dp, _dp, _ip]),

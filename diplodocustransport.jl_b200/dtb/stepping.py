@@ -150,16 +150,39 @@ class ForwardEulerStruct:
         d = self.last_diag
         check(self.L.dtb_step(self.ctx, float(t_start), float(t_stop), float(dt), int(Verbose),
                               ctypes.byref(dt_out), ctypes.byref(save), ctypes.byref(d)))
+        self._report(d, Verbose, t_start, t_stop, dt_out.value)
+        return dt_out.value, bool(save.value)
+
+    def step_io(self, f_in, t_start: float, t_stop: float, dt: float, Verbose: int = 0,
+                out: Optional[np.ndarray] = None):
+        """The functor with the state in host memory: f_in (None keeps the device state) is
+        uploaded, one step runs and the new state is returned in `out` (allocated when None; may
+        be f_in itself), all in one library call with one wait (dtb_step_io). Returns
+        (f, dt, save)."""
+        A = None if f_in is None else np.ascontiguousarray(f_in, dtype=np.float64)
+        if out is None:
+            out = np.empty(self.n)
+        dt_out = ctypes.c_double()
+        save = ctypes.c_int32()
+        d = self.last_diag
+        check(self.L.dtb_step_io(self.ctx, None if A is None else dptr(A), dptr(out), float(t_start),
+                                 float(t_stop), float(dt), int(Verbose), ctypes.byref(dt_out),
+                                 ctypes.byref(save), ctypes.byref(d)))
+        self._report(d, Verbose, t_start, t_stop, dt_out.value)
+        return out, dt_out.value, bool(save.value)
+
+    @staticmethod
+    def _report(d, Verbose: int, t_start: float, t_stop: float, dt: float) -> None:
+        # SteppingMethods.jl:87-93
         if not d.finite:
             print("non-finite value in df calculation")
         if Verbose == 1 and d.cr > 1.0:
-            print(f"Cr = {d.cr}, t={t_start}, dt={dt_out.value}, system may be unstable")
+            print(f"Cr = {d.cr}, t={t_start}, dt={dt}, system may be unstable")
         elif Verbose == 2:
-            print(f"\rCr = {d.cr}, t={t_start}, dt={dt_out.value}")
+            print(f"\rCr = {d.cr}, t={t_start}, dt={dt}")
         elif Verbose == 3:
             print(f"Cr = {d.cr},Cr_Bin = {d.cr_bin}, Cr_Emi = {d.cr_emi}, Cr_Flux = {d.cr_flux}, "
-                  f"t={t_start}, t_save ={t_stop}, dt={dt_out.value}")
-        return dt_out.value, bool(save.value)
+                  f"t={t_start}, t_save ={t_stop}, dt={dt}")
 
     # ---- state access
     @property

@@ -21,7 +21,7 @@ using SparseArrays
 
 import DiplodocusTransport: BackendType, PhaseSpaceStruct
 
-export B200Backend, B200ForwardEulerStruct, b200_solve
+export B200Backend, B200ForwardEulerStruct, b200_solve, b200_step_io!
 export B200BatchedEuler, admit!, run!, run_io!, get_f, batch_moments, gemm_plan, set_tune_cache
 export B200Server, add_grid!, start!, submit!, wait_request, cancel!, serve_stats
 
@@ -177,15 +177,32 @@ function (method::B200ForwardEulerStruct)(t_start, t_stop, dt, Verbose::Int64)
     check(ccall((:dtb_step, libdtb), Int32,
         (Ptr{Cvoid}, Float64, Float64, Float64, Int32, Ref{Float64}, Ref{Int32}, Ref{StepDiag}),
         method.ctx, t_start, t_stop, dt, Verbose, dt_out, save, d))
-    d[].finite == 0 && println("non-finite value in df calculation")
-    if Verbose == 1 && d[].cr > 1.0
-        println("Cr = $(d[].cr), t=$t_start, dt=$(dt_out[]), system may be unstable")
-    elseif Verbose == 2
-        println("\rCr = $(d[].cr), t=$t_start, dt=$(dt_out[])")
-    elseif Verbose == 3
-        println("Cr = $(d[].cr),Cr_Bin = $(d[].cr_bin), Cr_Emi = $(d[].cr_emi), Cr_Flux = $(d[].cr_flux), t=$t_start, t_save =$t_stop, dt=$(dt_out[])")
-    end
+    report_step(d[], Verbose, t_start, t_stop, dt_out[])
     return dt_out[], save[] != 0
+end
+
+# The functor with the state in a host vector: f is uploaded, stepped and overwritten with the
+# new state, with one wait for the round trip (dtb_step_io).
+function b200_step_io!(method::B200ForwardEulerStruct, f::Vector{Float64}, t_start, t_stop, dt, Verbose::Int64=0)
+    dt_out = Ref{Float64}(0.0); save = Ref{Int32}(0); d = Ref(StepDiag())
+    check(ccall((:dtb_step_io, libdtb), Int32,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Float64, Int32, Ref{Float64}, Ref{Int32},
+         Ref{StepDiag}),
+        method.ctx, f, f, t_start, t_stop, dt, Verbose, dt_out, save, d))
+    report_step(d[], Verbose, t_start, t_stop, dt_out[])
+    return dt_out[], save[] != 0
+end
+
+# SteppingMethods.jl:87-93
+function report_step(d::StepDiag, Verbose, t_start, t_stop, dt)
+    d.finite == 0 && println("non-finite value in df calculation")
+    if Verbose == 1 && d.cr > 1.0
+        println("Cr = $(d.cr), t=$t_start, dt=$dt, system may be unstable")
+    elseif Verbose == 2
+        println("\rCr = $(d.cr), t=$t_start, dt=$dt")
+    elseif Verbose == 3
+        println("Cr = $(d.cr),Cr_Bin = $(d.cr_bin), Cr_Emi = $(d.cr_emi), Cr_Flux = $(d.cr_flux), t=$t_start, t_save =$t_stop, dt=$dt")
+    end
 end
 
 # Solve (Solver.jl:1-64) with each save interval replayed from CUDA graphs on the device.

@@ -164,6 +164,15 @@ int32_t dtb_commit(dtb_ctx* ctx);
 int32_t dtb_step(dtb_ctx* ctx, double t_start, double t_stop, double dt, int32_t verbose,
                  double* dt_out, int32_t* save_out, dtb_step_diag* diag_out);
 
+/* dtb_step with the state in host memory: f_in (n_state values; NULL keeps the device state)
+ * is uploaded, the step runs, and the new state is written to f_out (may equal f_in), all with
+ * one wait for the whole round trip (dtb_set_f + dtb_step + dtb_get_f make three). Page-locked
+ * arrays avoid the driver's staging copies. The diagnostics are written to diag_out when it is
+ * not NULL. */
+int32_t dtb_step_io(dtb_ctx* ctx, const double* f_in, double* f_out, double t_start, double t_stop,
+                    double dt, int32_t verbose, double* dt_out, int32_t* save_out,
+                    dtb_step_diag* diag_out);
+
 /* Captures, instantiates and uploads the CUDA graphs that dtb_run (Verbose = 0) or, for a
  * batched context, dtb_batch_run replay, without running a step (commits first if needed).
  * Optional: without it the first run long enough for a graph captures it. A caller that times

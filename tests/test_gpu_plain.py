@@ -111,6 +111,38 @@ def test_functor_run_and_solve_agree_bitwise(cuda):
     m1.close()
 
 
+@pytest.mark.parametrize("precision", [np.float64, np.float32])
+def test_step_io_equals_set_step_get(cuda, precision):
+    """dtb_step_io (upload, step, download with one wait) gives, bit for bit, the state, dt, save
+    flag and diagnostics of dtb_set_f + dtb_step + dtb_get_f: with a fresh host state every step,
+    with f_out aliasing f_in, with f_in None (the device state is kept), and at a truncated last
+    step."""
+    import torch
+    w = synth.small(p_num=8, u_num=4, seed=33, randomize_vectors=True)
+    a = make_method(w, precision=precision)
+    b = make_method(w, precision=precision)
+    rng = np.random.default_rng(5)
+    f_pin = torch.empty(w.ps.n_state, dtype=torch.float64).pin_memory().numpy()
+    for k in range(6):
+        f_host = np.abs(w.f0 * (1.0 + 0.1 * rng.standard_normal(w.ps.n_state)))
+        f_pin[:] = f_host
+        t_stop = 5.0 if k < 5 else 0.3  # the last step is truncated at t_stop
+        out, dt_a, sv_a = a.step_io(f_pin, 0.0, t_stop, 0.9 * a.dt0, 3, out=f_pin)
+        assert out is f_pin
+        b.f = f_host
+        dt_b, sv_b = b(0.0, t_stop, 0.9 * b.dt0, 3)
+        np.testing.assert_array_equal(f_pin, b.f)
+        assert (dt_a, sv_a) == (dt_b, sv_b)
+        for fld in ("cr", "cr_bin", "cr_emi", "cr_flux", "sum_df", "sum_f", "finite"):
+            assert getattr(a.last_diag, fld) == getattr(b.last_diag, fld), fld
+    got, _, _ = a.step_io(None, 0.0, 5.0, a.dt0, 0)  # pageable output, device state kept
+    b(0.0, 5.0, b.dt0, 0)
+    np.testing.assert_array_equal(got, b.f)
+    np.testing.assert_array_equal(a.f, b.f)
+    a.close()
+    b.close()
+
+
 def test_config0_full_run(cuda):
     """Config 0: N_s = 128, two species, FP64, 1000 steps at fixed dt."""
     w = synth.config0(0)
