@@ -70,6 +70,11 @@ def test_bad_arguments_are_rejected():
     opts.precision = 7
     assert L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)) == _lib.DTB_EINVAL
     assert L.dtb_create(None, None, None) == _lib.DTB_EINVAL
+    # entry points on a null context refuse before touching a device
+    n = ctypes.c_int64()
+    assert L.dtb_launch_count(None, ctypes.byref(n)) == _lib.DTB_EINVAL
+    f = np.zeros(4)
+    assert L.dtb_step_io(None, _lib.dptr(f), _lib.dptr(f), 0.0, 1.0, 0.5, 0, None, None, None) == _lib.DTB_EINVAL
 
 
 @pytest.mark.parametrize("dt,t_save", [(0.4, [0.0, 1.0, 2.5, 2.6]), (0.3, [0.0, 1.0, 2.0, 3.0]),
