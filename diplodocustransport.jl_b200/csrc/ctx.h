@@ -150,7 +150,7 @@ struct dtb_ctx {
     unsigned long long host_ctr = 0;
     StepDiagDev* hist = nullptr;
     // row-block diagnostics records: [graph_steps][rows_grid][kStepRecFields], slot k for step k
-    // of a sequence (the symplectic space pass uses the first 2 * rows_grid)
+    // of a sequence
     double* blk_red = nullptr;
     int rows_grid = 0;
     unsigned* ticket = nullptr;

@@ -951,9 +951,8 @@ static int flush_profile(dtb_ctx* c) {
     return DTB_OK;
 }
 
-// One step. Outside the symplectic method the step is number *ctr + kpos of the dt sequence and
-// writes record slot kpos; finish_seq reduces a sequence's records and advances the counter. The
-// symplectic space pass reduces its step's diagnostics and advances the counter itself (kpos 0).
+// One step: number *ctr + kpos of the dt sequence, whose row blocks write record slot kpos;
+// finish_seq reduces a sequence's records and advances the counter.
 template <typename T>
 static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, int verbose, bool profile,
                        int kpos) {
@@ -984,17 +983,16 @@ static int launch_step(dtb_ctx* c, RowOps<T>& ops, double dt_imm, bool use_arr, 
         }
     }
     const double* dta = use_arr ? c->dt_arr : nullptr;
+    double* rec = c->blk_red + (size_t)kpos * c->rows_grid * kStepRecFields;
     if (c->symplectic) {
         RowOps<T> mom = ops;
         mom.mode = 1;
         T* fm = reinterpret_cast<T*>(c->fm_buf);
         T* dfm = reinterpret_cast<T*>(c->dfm_buf);
-        DTB_CUDA(launch_euler_rows<T>(mom, fin, fm, dt_imm, dta, c->ctr, 0, verbose, nullptr, gain, c->stream));
-        DTB_CUDA(launch_sympl_space<T>(ops, fin, fm, dfm, fout, dt_imm, dta, c->ctr, c->hist, c->hist_cap, verbose,
-                                       c->blk_red, c->ticket, c->stream));
+        DTB_CUDA(launch_euler_rows<T>(mom, fin, fm, dt_imm, dta, c->ctr, kpos, verbose, nullptr, gain, c->stream));
+        DTB_CUDA(launch_sympl_space<T>(ops, fin, fm, dfm, fout, dt_imm, dta, c->ctr, kpos, rec, c->stream));
         c->launches += 2;
     } else {
-        double* rec = c->blk_red + (size_t)kpos * c->rows_grid * kStepRecFields;
         DTB_CUDA(launch_euler_rows<T>(ops, fin, fout, dt_imm, dta, c->ctr, kpos, verbose, rec, gain, c->stream));
         c->launches++;
     }
@@ -1010,11 +1008,11 @@ static int do_step(dtb_ctx* c, double dt_imm, bool use_arr, int verbose, bool pr
 
 // The diagnostics of the last n steps (a sequence of record slots 0..n-1) and the counter advance.
 static int finish_seq(dtb_ctx* c, int n, int verbose) {
-    if (c->symplectic || n <= 0) return DTB_OK;
+    if (n <= 0) return DTB_OK;
     const int hb = c->prec == DTB_F64 ? c->ops_d.has_bin : c->ops_f.has_bin;
     const int he = c->prec == DTB_F64 ? c->ops_d.has_emi : c->ops_f.has_emi;
-    DTB_CUDA(launch_step_diag(c->blk_red, c->rows_grid, n, c->ctr, c->hist, c->hist_cap, verbose, hb, he, c->ticket,
-                              c->stream));
+    DTB_CUDA(launch_step_diag(c->blk_red, c->rows_grid, n, c->ctr, c->hist, c->hist_cap, verbose, hb, he,
+                              c->symplectic ? 1 : 0, c->ticket, c->stream));
     c->launches++;
     return DTB_OK;
 }
@@ -1588,7 +1586,7 @@ int32_t dtb_sync(dtb_ctx* c) {
 int32_t dtb_launches_per_step(dtb_ctx* c, int32_t* n) {
     DTB_CHECK(c && n, DTB_EINVAL, "dtb_launches_per_step: null argument");
     DTB_TRY(dtb_commit(c));
-    *n = (c->n_units > 0 ? 2 : 1) + (c->symplectic ? 1 : 0);
+    *n = (c->n_units > 0 && c->n_bin_cells > 0 ? 2 : 1) + (c->symplectic ? 1 : 0);
     return DTB_OK;
 }
 

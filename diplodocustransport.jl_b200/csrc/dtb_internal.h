@@ -116,15 +116,18 @@ int euler_rows_blocks(int n_state);
 
 // The diagnostics of steps *ctr .. *ctr + n_steps - 1: block k reduces step k's row-block
 // records (slot k of blk_red, n_blocks records of kStepRecFields each) into
-// hist[(*ctr + k) % hist_cap]; the last block to finish advances *ctr by n_steps.
+// hist[(*ctr + k) % hist_cap]; the last block to finish advances *ctr by n_steps. sympl: the
+// records are the symplectic space pass's (no per-term Crs, no finite check).
 cudaError_t launch_step_diag(const double* blk_red, int n_blocks, int n_steps, unsigned long long* ctr,
-                             StepDiagDev* hist, long long hist_cap, int verbose, int has_bin, int has_emi,
+                             StepDiagDev* hist, long long hist_cap, int verbose, int has_bin, int has_emi, int sympl,
                              unsigned* ticket, cudaStream_t s);
 
+// The symplectic space pass of a step numbered like launch_euler_rows'; its row blocks write
+// records in the same layout (the whole-step Cr and the f sum only).
 template <typename T>
 cudaError_t launch_sympl_space(const RowOps<T>& ops, const T* f_old, const T* fm, const T* dfm, T* f_out,
-                               double dt_imm, const double* dt_arr, unsigned long long* ctr, StepDiagDev* hist,
-                               long long hist_cap, int verbose, double* blk_red, unsigned* ticket, cudaStream_t s);
+                               double dt_imm, const double* dt_arr, const unsigned long long* ctr, int kpos,
+                               double* rec, cudaStream_t s);
 
 template <typename Tin, typename Tout>
 cudaError_t launch_pad_rows(const Tin* src, long long rows, int n, Tout* dst, int np, cudaStream_t s);

@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
             s_f = fd;
         }
     }
-    if (ops.mode == 1) return;  // the space pass reduces the step's diagnostics
+    if (ops.mode == 1) return;  // the space pass writes the step's records
     // this block's record; the step's records are reduced by step_diag_kernel, so no row
     // block waits for the others
     if (lane == 0) {
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(kRowsWarps * 32) step_diag_kernel(const double
                                                                     int n_blocks, int n_steps,
                                                                     unsigned long long* ctr, StepDiagDev* hist,
                                                                     long long hist_cap, int verbose,
-                                                                    int has_bin, int has_emi,
+                                                                    int has_bin, int has_emi, int sympl,
                                                                     unsigned* ticket) {
     __shared__ double s_fin[kStepRecFields][kRowsWarps * 32];
     pdl_wait();  // the last step's row blocks have written their records
@@ -517,12 +517,13 @@ __global__ void __launch_bounds__(kRowsWarps * 32) step_diag_kernel(const double
         StepDiagDev d;
         const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && r[5] != 0.0;
         d.cr[0] = on ? -r[0] : 0.0;
-        d.cr[1] = (on && verbose == 3 && has_bin) ? -r[1] : 0.0;
-        d.cr[2] = (on && verbose == 3 && has_emi) ? -r[2] : 0.0;
-        d.cr[3] = (on && verbose == 3) ? -r[3] : 0.0;
+        d.cr[1] = (on && verbose == 3 && has_bin && !sympl) ? -r[1] : 0.0;
+        d.cr[2] = (on && verbose == 3 && has_emi && !sympl) ? -r[2] : 0.0;
+        d.cr[3] = (on && verbose == 3 && !sympl) ? -r[3] : 0.0;
         d.sum_df = r[4];
         d.sum_f = r[5];
-        d.finite = isfinite(r[4]) ? 1 : 0;
+        // the symplectic method has no finite check (SteppingMethods.jl:120-243)
+        d.finite = (sympl || isfinite(r[4])) ? 1 : 0;
         d.pad = 0;
         hist[(step0 + blockIdx.x) % (unsigned long long)hist_cap] = d;
         // every block has read the counter before it takes its ticket; the last one advances it
@@ -536,10 +537,10 @@ __global__ void __launch_bounds__(kRowsWarps * 32) step_diag_kernel(const double
 }
 
 cudaError_t launch_step_diag(const double* blk_red, int n_blocks, int n_steps, unsigned long long* ctr,
-                             StepDiagDev* hist, long long hist_cap, int verbose, int has_bin, int has_emi,
+                             StepDiagDev* hist, long long hist_cap, int verbose, int has_bin, int has_emi, int sympl,
                              unsigned* ticket, cudaStream_t s) {
     return launch_pdl(step_diag_kernel, dim3(n_steps), dim3(kRowsWarps * 32), 0, s, blk_red, n_blocks, n_steps, ctr,
-                      hist, hist_cap, verbose, has_bin, has_emi, ticket);
+                      hist, hist_cap, verbose, has_bin, has_emi, sympl, ticket);
 }
 
 template <typename T>
@@ -563,22 +564,20 @@ template cudaError_t launch_euler_rows<float>(const RowOps<float>&, const float*
 // ForwardSymplecticEuler space pass (SteppingMethods.jl:165-237): one warp per row,
 // df_Space = -(X f_Momentum) invAp dt/dt0, f_Space = clamp(f_Momentum + df_Space, 1f-20), then
 // f = f_Space + inj dt/dt0 clamped with the sign factor of :235 and the Inf fix of :237.
-// Cr = -min((df_Space + df_Momentum) ./ f_old) (:217-218), reduced by the last block.
+// Each block writes a record of its rows' (df_Space + df_Momentum) ./ f_old minimum and f_old
+// sum in euler_rows' layout; step_diag reduces them to Cr = -min(...) (:217-218).
 template <typename T>
 __global__ void __launch_bounds__(kRowsWarps * 32) sympl_space_kernel(RowOps<T> ops, const T* __restrict__ f_old,
                                                                       const T* __restrict__ fm,
                                                                       const T* __restrict__ dfm, T* __restrict__ f_out,
                                                                       double dt_imm, const double* __restrict__ dt_arr,
-                                                                      unsigned long long* ctr, StepDiagDev* hist,
-                                                                      long long hist_cap, int verbose, double* blk_red,
-                                                                      unsigned* ticket) {
+                                                                      const unsigned long long* ctr, int kpos,
+                                                                      double* rec) {
     __shared__ double s_red[kRowsWarps][2];
-    __shared__ double s_fin[2][kRowsWarps * 32];
-    __shared__ int s_last;
-    pdl_wait();  // this step's inputs (gain partials, momentum pass) and the previous step's state and counter
+    pdl_wait();  // this step's inputs (gain partials, momentum pass)
     if (threadIdx.x == 0) pdl_trigger();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned long long step = *reinterpret_cast<volatile unsigned long long*>(ctr);
+    const unsigned long long step = *reinterpret_cast<const volatile unsigned long long*>(ctr) + (unsigned)kpos;
     const double dt_scale = dt_arr ? dt_arr[step] : dt_imm;
     const int i = blockIdx.x * kRowsWarps + warp;
     double m_cr = CUDART_INF, s_f = 0.0;
@@ -614,61 +613,28 @@ __global__ void __launch_bounds__(kRowsWarps * 32) sympl_space_kernel(RowOps<T> 
             r0 = jl_min(r0, s_red[w][0]);
             r1 += s_red[w][1];
         }
-        blk_red[(size_t)blockIdx.x * 2] = r0;
-        blk_red[(size_t)blockIdx.x * 2 + 1] = r1;
-        __threadfence();
-        const unsigned t = atomicAdd(ticket, 1u);
-        s_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        double r0 = CUDART_INF, r1 = 0.0;
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-            r0 = jl_min(r0, __ldcg(blk_red + (size_t)b * 2));
-            r1 += __ldcg(blk_red + (size_t)b * 2 + 1);
-        }
-        s_fin[0][threadIdx.x] = r0;
-        s_fin[1][threadIdx.x] = r1;
-        __syncthreads();
-        for (int o = kRowsWarps * 16; o > 0; o >>= 1) {
-            if (threadIdx.x < o) {
-                s_fin[0][threadIdx.x] = jl_min(s_fin[0][threadIdx.x], s_fin[0][threadIdx.x + o]);
-                s_fin[1][threadIdx.x] += s_fin[1][threadIdx.x + o];
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            StepDiagDev d;
-            const bool on = (verbose == 1 || verbose == 2 || verbose == 3) && s_fin[1][0] != 0.0;
-            d.cr[0] = on ? -s_fin[0][0] : 0.0;
-            d.cr[1] = d.cr[2] = d.cr[3] = 0.0;
-            d.sum_df = 0.0;
-            d.sum_f = s_fin[1][0];
-            d.finite = 1;  // the symplectic method has no finite check (SteppingMethods.jl:120-243)
-            d.pad = 0;
-            hist[step % (unsigned long long)hist_cap] = d;
-            *ticket = 0u;
-            __threadfence();
-            *reinterpret_cast<volatile unsigned long long*>(ctr) = step + 1ull;
-        }
+        double* dst = rec + (size_t)blockIdx.x * kStepRecFields;
+        dst[0] = r0;
+        dst[1] = dst[2] = dst[3] = CUDART_INF;  // no per-term Crs
+        dst[4] = 0.0;
+        dst[5] = r1;
     }
 }
 
 template <typename T>
 cudaError_t launch_sympl_space(const RowOps<T>& ops, const T* f_old, const T* fm, const T* dfm, T* f_out,
-                               double dt_imm, const double* dt_arr, unsigned long long* ctr, StepDiagDev* hist,
-                               long long hist_cap, int verbose, double* blk_red, unsigned* ticket, cudaStream_t s) {
-    const int grid = (ops.n_state + kRowsWarps - 1) / kRowsWarps;
+                               double dt_imm, const double* dt_arr, const unsigned long long* ctr, int kpos,
+                               double* rec, cudaStream_t s) {
+    const int grid = euler_rows_blocks(ops.n_state);
     return launch_pdl(sympl_space_kernel<T>, grid, dim3(kRowsWarps * 32), 0, s, ops, f_old, fm, dfm, f_out, dt_imm,
-                      dt_arr, ctr, hist, hist_cap, verbose, blk_red, ticket);
+                      dt_arr, ctr, kpos, rec);
 }
 template cudaError_t launch_sympl_space<double>(const RowOps<double>&, const double*, const double*, const double*,
-                                                double*, double, const double*, unsigned long long*, StepDiagDev*,
-                                                long long, int, double*, unsigned*, cudaStream_t);
+                                                double*, double, const double*, const unsigned long long*, int,
+                                                double*, cudaStream_t);
 template cudaError_t launch_sympl_space<float>(const RowOps<float>&, const float*, const float*, const float*, float*,
-                                               double, const double*, unsigned long long*, StepDiagDev*, long long,
-                                               int, double*, unsigned*, cudaStream_t);
+                                               double, const double*, const unsigned long long*, int, double*,
+                                               cudaStream_t);
 
 // ------------------------------------------------------------------ bounded-wait self-test
 // One block waits on an mbarrier phase that nothing completes, with a limit of limit_ns, and

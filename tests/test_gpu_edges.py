@@ -81,29 +81,39 @@ def _diag_tuple(d):
 
 
 @pytest.mark.parametrize("graph_steps", [4, 16])
-def test_step_records_do_not_depend_on_launch_grouping(cuda, graph_steps):
+@pytest.mark.parametrize("symplectic", [False, True])
+def test_step_records_do_not_depend_on_launch_grouping(cuda, graph_steps, symplectic):
     """The per-step diagnostics (Cr, Cr_Bin, Cr_Emi, Cr_Flux, sum df, sum f, finite) of 37 steps
     run as graph replays and loose sequences equal, bit for bit, those of 37 single dtb_step
-    calls, and match the oracle's (rtol 1e-10). dtb_launch_count counts the gain and row kernel
-    of every step plus one diagnostics reduction per sequence."""
+    calls, and (forward Euler) match the oracle's (rtol 1e-10); the states agree bit for bit.
+    dtb_launch_count counts the kernels of every step (gain and rows; the symplectic method's
+    two row passes) plus one diagnostics reduction per sequence."""
     import ctypes
-    from dtb import _lib
+    from dtb.stepping import ForwardSymplecticEulerStruct
     w = synth.small(p_num=10, u_num=4, seed=32, n_space=2, randomize_vectors=True)
+    cls = ForwardEulerStruct
+    if symplectic:
+        w.fluxm.X_Flux = synth.space_flux(w.ps, np.random.default_rng(6), 1.0)
+        cls = ForwardSymplecticEulerStruct
     n = 37
-    a = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=graph_steps)
-    b = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=graph_steps)
+    a = cls(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=graph_steps)
+    b = cls(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=graph_steps)
     c0, c1 = ctypes.c_int64(), ctypes.c_int64()
     a.L.dtb_launch_count(a.ctx, ctypes.byref(c0))
     sc = (0.9 * a.dt0) / a.dt0  # the dt / dt0 dtb_step forms from dt = 0.9 dt0
     hist = a.run(np.full(n, sc), Verbose=3, diag=True)
     a.L.dtb_launch_count(a.ctx, ctypes.byref(c1))
     graphs, loose = n // graph_steps, n % graph_steps
-    assert c1.value - c0.value == 2 * n + graphs + (1 if loose else 0)
+    per_step = 3 if symplectic else 2
+    assert c1.value - c0.value == per_step * n + graphs + (1 if loose else 0)
     ops = oracle.blocked_from_workload(w)
     f = np.array(w.f0, dtype=np.float64)
     for k in range(n):
         b(0.0, 1e9, 0.9 * b.dt0, 3)
         assert _diag_tuple(hist[k]) == _diag_tuple(b.last_diag), k
+        if symplectic:
+            assert hist[k].finite == 1 and hist[k].cr_bin == 0.0 and hist[k].sum_df == 0.0
+            continue
         f, diag, _ = ops.step(f, sc, 3)
         for got, exp in zip(_diag_tuple(hist[k])[:4], diag[:4]):
             assert got == pytest.approx(exp, rel=1e-10), k
