@@ -464,16 +464,12 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         s_red[warp][5] = s_f;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double r[kStepRecFields];
-        for (int k = 0; k < kStepRecFields; ++k) r[k] = s_red[0][k];
-        for (int w = 1; w < kRowsWarps; ++w) {
-            for (int k = 0; k < 4; ++k) r[k] = jl_min(r[k], s_red[w][k]);
-            r[4] += s_red[w][4];
-            r[5] += s_red[w][5];
-        }
-        double* dst = rec + (size_t)blockIdx.x * kStepRecFields;
-        for (int k = 0; k < kStepRecFields; ++k) dst[k] = r[k];
+    if (threadIdx.x < kStepRecFields) {
+        // one thread per field, the warps in order: fields 0-3 are minima, 4-5 sums
+        const int k = threadIdx.x;
+        double r = s_red[0][k];
+        for (int w = 1; w < kRowsWarps; ++w) r = k < 4 ? jl_min(r, s_red[w][k]) : r + s_red[w][k];
+        rec[(size_t)blockIdx.x * kStepRecFields + k] = r;
     }
 }
 
@@ -607,17 +603,15 @@ __global__ void __launch_bounds__(kRowsWarps * 32) sympl_space_kernel(RowOps<T> 
         s_red[warp][1] = s_f;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double r0 = s_red[0][0], r1 = s_red[0][1];
-        for (int w = 1; w < kRowsWarps; ++w) {
-            r0 = jl_min(r0, s_red[w][0]);
-            r1 += s_red[w][1];
-        }
-        double* dst = rec + (size_t)blockIdx.x * kStepRecFields;
-        dst[0] = r0;
-        dst[1] = dst[2] = dst[3] = CUDART_INF;  // no per-term Crs
-        dst[4] = 0.0;
-        dst[5] = r1;
+    if (threadIdx.x < kStepRecFields) {
+        // fields 0 (minimum) and 5 (sum) over the warps in order; no per-term Crs, no df sum
+        const int k = threadIdx.x;
+        double r = k == 0 ? s_red[0][0] : (k == 5 ? s_red[0][1] : (k == 4 ? 0.0 : CUDART_INF));
+        if (k == 0)
+            for (int w = 1; w < kRowsWarps; ++w) r = jl_min(r, s_red[w][0]);
+        if (k == 5)
+            for (int w = 1; w < kRowsWarps; ++w) r += s_red[w][1];
+        rec[(size_t)blockIdx.x * kStepRecFields + k] = r;
     }
 }
 
