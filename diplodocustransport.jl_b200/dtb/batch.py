@@ -117,7 +117,10 @@ class BatchedEuler:
         A = None if F_in is None else np.ascontiguousarray(F_in, dtype=np.float64)
         if out is None:
             out = np.empty((self.capacity, self.n))
-        check(self.L.dtb_batch_run_io(self.ctx, None if A is None else dptr(A), int(nsteps), dptr(out)))
+        if not hasattr(self, "_io_ptrs"):
+            self._io_ptrs = (_lib.LastPtr(), _lib.LastPtr())
+        pin, pout = self._io_ptrs
+        check(self.L.dtb_batch_run_io(self.ctx, pin(A), int(nsteps), pout(out)))
         return out
 
     def moments(self, weights) -> tuple:

@@ -165,9 +165,11 @@ class ForwardEulerStruct:
         dt_out = ctypes.c_double()
         save = ctypes.c_int32()
         d = self.last_diag
-        check(self.L.dtb_step_io(self.ctx, None if A is None else dptr(A), dptr(out), float(t_start),
-                                 float(t_stop), float(dt), int(Verbose), ctypes.byref(dt_out),
-                                 ctypes.byref(save), ctypes.byref(d)))
+        if not hasattr(self, "_io_ptrs"):
+            self._io_ptrs = (_lib.LastPtr(), _lib.LastPtr())
+        pin, pout = self._io_ptrs
+        check(self.L.dtb_step_io(self.ctx, pin(A), pout(out), float(t_start), float(t_stop), float(dt),
+                                 int(Verbose), ctypes.byref(dt_out), ctypes.byref(save), ctypes.byref(d)))
         self._report(d, Verbose, t_start, t_stop, dt_out.value)
         return out, dt_out.value, bool(save.value)
 

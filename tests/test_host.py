@@ -239,3 +239,17 @@ def test_gain_contract_entries_refuse_misaligned_pointers_on_the_host():
         assert b"16-byte aligned" in L.dtb_last_error()
         assert fn(_lib.DTB_DTYPE_F32, ok, 8, 8, 8, ok, ok, o_bad, None) == _lib.DTB_EINVAL
         assert fn(_lib.DTB_DTYPE_F64, ok, 8, 8, 8, o_bad, ok, ok, None) == _lib.DTB_EINVAL
+
+
+def test_last_ptr_follows_the_array_object():
+    """The round-trip bindings reuse the ctypes pointer of the array passed last; another array
+    object (or None) is converted afresh."""
+    p = _lib.LastPtr()
+    a, b = np.zeros(8), np.ones(8)
+    pa = p(a)
+    assert ctypes.addressof(pa.contents) == a.ctypes.data
+    assert p(a) is pa
+    pb = p(b)
+    assert pb is not pa and ctypes.addressof(pb.contents) == b.ctypes.data
+    assert p(None) is None
+    assert ctypes.addressof(p(a).contents) == a.ctypes.data
