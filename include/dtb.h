@@ -164,8 +164,9 @@ int32_t dtb_commit(dtb_ctx* ctx);
 int32_t dtb_step(dtb_ctx* ctx, double t_start, double t_stop, double dt, int32_t verbose,
                  double* dt_out, int32_t* save_out, dtb_step_diag* diag_out);
 
-/* dtb_step with the state in host memory: f_in (n_state values; NULL keeps the device state)
- * is uploaded, the step runs, and the new state is written to f_out (may equal f_in), all with
+/* The functor of SteppingMethods.jl:12-107 on a state kept in host memory, as the reference's
+ * CPU backend keeps method.f: f_in (n_state values; NULL keeps the device state) is uploaded,
+ * the step of dtb_step runs, and the new state is written to f_out (may equal f_in), all with
  * one wait for the whole round trip (dtb_set_f + dtb_step + dtb_get_f make three). Page-locked
  * arrays avoid the driver's staging copies. The diagnostics are written to diag_out when it is
  * not NULL. */
@@ -228,8 +229,8 @@ int32_t dtb_sync(dtb_ctx* ctx);
  * reduction adds one launch per sequence of steps (a graph replay, or up to 16 steps run
  * outside one). */
 int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
-/* Kernel launches the context's step functions (dtb_step, dtb_run, dtb_solve) have issued so
- * far, kernels replayed in graphs included. */
+/* Kernel launches the context's step functions (dtb_step, dtb_step_io, dtb_run, dtb_solve) have
+ * issued so far, kernels replayed in graphs included. No counterpart in the reference. */
 int32_t dtb_launch_count(dtb_ctx* ctx, int64_t* n);
 
 /* Failure-detection self-test: launches one block that waits, with a limit of limit_s
