@@ -38,6 +38,7 @@ namespace dtb {
 
 constexpr int kProfRing = 256;
 constexpr int64_t kMaxScheduleSteps = 100000000;
+constexpr int kMaxGraphSteps = 1024;  // steps per captured graph (dtb_opts.graph_steps)
 
 // An NVTX range over a host entry point (upload, commit, steps, graph replays, serving chunks):
 // visible on a profiler timeline, a no-op without one.

@@ -100,6 +100,10 @@ int32_t dtb_create(const dtb_dims* dims, const dtb_opts* opts, dtb_ctx** out) {
     DTB_CHECK(opts->precision != DTB_MIXED || (opts->batch >= 1 && opts->batch <= 65536), DTB_EINVAL,
               "dtb_create: a batched context needs 1 <= batch <= 65536");
     DTB_CHECK(std::isfinite(opts->dt0) && opts->dt0 > 0, DTB_EINVAL, "dtb_create: dt0 must be finite and > 0");
+    // graph_steps also sizes the step-record buffer (graph_steps x rows / 8 x 48 B) and the
+    // batched path's set of captured graphs (one per length 1..graph_steps)
+    DTB_CHECK(opts->graph_steps >= 0 && opts->graph_steps <= kMaxGraphSteps, DTB_EINVAL,
+              "dtb_create: graph_steps must be in [0, " + std::to_string(kMaxGraphSteps) + "]");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         set_error("dtb_create: no CUDA device available");

@@ -70,6 +70,11 @@ def test_bad_arguments_are_rejected():
     opts.precision = 7
     assert L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)) == _lib.DTB_EINVAL
     assert L.dtb_create(None, None, None) == _lib.DTB_EINVAL
+    opts.precision = _lib.DTB_F64
+    for bad in (-1, 1025, 2 ** 31 - 1):  # refused on the host, before any device is touched
+        opts.graph_steps = bad
+        assert L.dtb_create(ctypes.byref(dims), ctypes.byref(opts), ctypes.byref(ctx)) == _lib.DTB_EINVAL
+        assert b"graph_steps" in L.dtb_last_error()
     # entry points on a null context refuse before touching a device
     n = ctypes.c_int64()
     assert L.dtb_launch_count(None, ctypes.byref(n)) == _lib.DTB_EINVAL
