@@ -207,6 +207,9 @@ __global__ void __launch_bounds__(kGainThreads) gain_stream_kernel(const T* __re
     }
 
     // ---------------- consumers: 8 warps
+    // The work table is static: the block's first unit is read before the wait.
+    GainUnit U0{};
+    if ((int)blockIdx.x < n_units) U0 = units[blockIdx.x];
     // f is the previous step's output and the previous step still reads the partials this
     // kernel writes: wait for it (the G tiles already stream in meanwhile)
     pdl_wait();
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(kGainThreads) gain_stream_kernel(const T* __re
     uint32_t it = 0;
     uint32_t lk = 0;  // units done by this block
     for (int u = blockIdx.x; u < n_units; u += gridDim.x, ++lk) {
-        const GainUnit U = units[u];
+        const GainUnit U = u == (int)blockIdx.x ? U0 : units[u];
         if (U.tile_b <= 0 || U.n2p <= 0 || U.tile_b * U.n2p > kTileElems) return;
         const int nt = (U.nb + U.tile_b - 1) / U.tile_b;
         const int nvr = U.n2p / V::n;  // vectors per b-row
@@ -403,39 +406,53 @@ __global__ void __launch_bounds__(kRowsWarps * 32) euler_rows_kernel(RowOps<T> o
         emi = warp_sum(emi);
         loss = warp_sum(loss);
     }
+    // The row's unit range, old state and vectors are static or the previous step's: read them
+    // before the wait too, so only the gain partials' round trip follows it.
+    int u_lo = 0, u_hi = 0;
+    T fa = T(0), iap = T(0), injv = T(0), volc = T(0);
+    if (i < ops.n_state) {
+        if (bin_here) {
+            u_lo = ops.unit_ptr[a];
+            u_hi = ops.unit_ptr[a + 1];
+        }
+        if (lane == 0) {
+            fa = fc[a];
+            iap = ops.invAp[i];
+            if (ops.mode == 0) injv = ops.inj[i];
+            if (bin_here) volc = ops.vol[cell];
+        }
+    }
     pdl_wait();  // this step's gain partials (and, in the space pass, the momentum pass) are complete
     if (threadIdx.x == 0) pdl_trigger();
     if (i < ops.n_state) {
         if (bin_here) {
             const double* pr = ops.partial + (size_t)cell * ops.n_units;
-            for (int u = ops.unit_ptr[a] + lane; u < ops.unit_ptr[a + 1]; u += 32) gain += pr[u];
+            for (int u = u_lo + lane; u < u_hi; u += 32) gain += pr[u];
         }
         gain = warp_sum(gain);
 
         if (lane == 0 && ops.mode == 1) {
             // ForwardSymplecticEuler momentum pass (SteppingMethods.jl:140-160)
-            const T fa = fc[a];
             T df = -(T)flux;
             if (ops.has_emi) df = df + (T)emi;
-            if (ops.has_bin) df = df + (bin_here ? (T)((double)ops.vol[cell] * (gain - (double)fa * loss)) : T(0));
-            df = (T)((double)df * ((double)ops.invAp[i] * dt_scale));
+            if (ops.has_bin) df = df + (bin_here ? (T)((double)volc * (gain - (double)fa * loss)) : T(0));
+            df = (T)((double)df * ((double)iap * dt_scale));
             T fm = fa + df;
             fm = jl_mul_bool(fm, fm >= (T)ops.thr_mom);
             f_out[i] = fm;
             ops.dfm_out[i] = df;
         }
         if (lane == 0 && ops.mode == 0) {
-            const T fa = fc[a];
             const T dflux = (T)flux;
             const T demi = (T)emi;
-            const T dbin = bin_here ? (T)((double)ops.vol[cell] * (gain - (double)fa * loss)) : T(0);
+            const T dbin = bin_here ? (T)((double)volc * (gain - (double)fa * loss)) : T(0);
             // SteppingMethods.jl:31-46
             T df = -dflux;
             if (ops.has_emi) df = df + demi;
             if (ops.has_bin) df = df + dbin;
-            df = (T)((double)df * ((double)ops.invAp[i] * dt_scale));
+            df = (T)((double)df * ((double)iap * dt_scale));
             // :97-101, arithmetic in Float64 like Julia's promotion, one rounding at the store
-            const double fnew = (double)fa + ((double)df + (double)ops.inj[i] * dt_scale);
+            const double fnew = (double)fa + ((double)df + (double)injv * dt_scale);
             T fn = (T)fnew;
             fn = jl_mul_bool(fn, fn >= (T)ops.thr);
             fn = jl_mul_bool(fn, fn != (T)CUDART_INF);
