@@ -185,7 +185,7 @@ struct dtb_ctx {
 
     // graphs
     cudaGraphExec_t graph = nullptr;
-    int graph_steps = 16;
+    int graph_steps = 16;  // set at creation (the plain path's default depends on the grid size)
     int graph_verbose = -1;
 
     // profiling

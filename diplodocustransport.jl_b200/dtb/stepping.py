@@ -83,7 +83,7 @@ class ForwardEulerStruct:
     def __init__(self, PhaseSpace: PhaseSpace, Initial, Injection, BinM: BinaryMatrices,
                  EmiM: EmissionMatrices, FluxM: FluxMatrices, *, Adaptive: bool = False,
                  Precision=np.float64, device: int = 0, stream: Optional[int] = None,
-                 graph_steps: int = 16):
+                 graph_steps: int = 0):
         self.L = _lib.load()
         self.PhaseSpace = PhaseSpace
         self.Precision = Precision

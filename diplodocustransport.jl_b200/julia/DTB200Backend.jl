@@ -155,7 +155,7 @@ mutable struct B200ForwardEulerStruct <: DiplodocusTransport.SteppingMethodType
         ns = length(sizes)
         n_space = PhaseSpace.Space.x_num * PhaseSpace.Space.y_num * PhaseSpace.Space.z_num
         dims = Dims(ns, n_space, ntuple(i -> i <= ns ? Int64(sizes[i]) : Int64(0), 16))
-        opts = Opts(Precision == Float32 ? DTB_F32 : DTB_F64, device, C_NULL, 1, 16, PhaseSpace.Time.dt0, 1, 0)
+        opts = Opts(Precision == Float32 ? DTB_F32 : DTB_F64, device, C_NULL, 1, 0, PhaseSpace.Time.dt0, 1, 0)  # graph_steps 0: the library's default
         ctx = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:dtb_create, libdtb), Int32, (Ref{Dims}, Ref{Opts}, Ref{Ptr{Cvoid}}), dims, opts, ctx))
         upload_operators!(ctx[], PhaseSpace, Initial, Injection, BinM, EmiM, FluxM)

@@ -69,7 +69,9 @@ typedef struct dtb_opts {
     int32_t device;        /* CUDA device ordinal */
     void* stream;          /* cudaStream_t to run on, or NULL for a library-owned stream */
     int32_t index_base;    /* base of sparse indices the caller passes: 1 (Julia) or 0 */
-    int32_t graph_steps;   /* steps per captured CUDA graph in dtb_run (0: default 16; at most 1024) */
+    int32_t graph_steps;   /* steps per captured CUDA graph (at most 1024). 0: the default, for
+                              plain contexts 64 when the step records of 64 steps fit in 8 MB
+                              (grids up to about 175,000 states) and 16 above; 16 for batched ones */
     double dt0;            /* TimeStruct.dt0 (StructsAndDictionaries.jl:55) */
     int32_t batch;         /* instances per context; 1 for the plain method */
     int32_t flags;         /* reserved, 0 */

@@ -36,7 +36,7 @@ def test_plain_uneven_species_match_oracle(cuda, precision, tol, grid):
     n_out x n_e x n_g, loss blocks of both sides and emission, 40 steps (two graphs of 16 and 8
     single steps)."""
     w = synth.uneven_two_species(*grid, seed=21)
-    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, Precision=precision)
+    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, Precision=precision, graph_steps=16)
     m.run(np.full(40, 0.9))
     assert rel_linf(m.f, _oracle_run(w, w.f0, 0.9, 40)) <= tol
     m.close()
@@ -70,7 +70,7 @@ def test_plain_without_gain_kernel_runs_in_graphs(cuda, case):
         w.binm = BinaryMatrices()
     else:
         w.binm.Domain = []
-    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm)
+    m = ForwardEulerStruct(w.ps, w.f0, w.inj, w.binm, w.emim, w.fluxm, graph_steps=16)
     m.run(np.full(45, 0.9))
     assert rel_linf(m.f, _oracle_run(w, w.f0, 0.9, 45)) <= TOL64
     m.close()
@@ -80,7 +80,7 @@ def _diag_tuple(d):
     return (d.cr, d.cr_bin, d.cr_emi, d.cr_flux, d.sum_df, d.sum_f, d.finite)
 
 
-@pytest.mark.parametrize("graph_steps", [4, 16])
+@pytest.mark.parametrize("graph_steps", [4, 16, 0])
 @pytest.mark.parametrize("symplectic", [False, True])
 def test_step_records_do_not_depend_on_launch_grouping(cuda, graph_steps, symplectic):
     """The per-step diagnostics (Cr, Cr_Bin, Cr_Emi, Cr_Flux, sum df, sum f, finite) of 37 steps
@@ -103,7 +103,8 @@ def test_step_records_do_not_depend_on_launch_grouping(cuda, graph_steps, symple
     sc = (0.9 * a.dt0) / a.dt0  # the dt / dt0 dtb_step forms from dt = 0.9 dt0
     hist = a.run(np.full(n, sc), Verbose=3, diag=True)
     a.L.dtb_launch_count(a.ctx, ctypes.byref(c1))
-    graphs, loose = n // graph_steps, n % graph_steps
+    gs = graph_steps or 64  # 0: the default, 64 steps per graph on this grid
+    graphs, loose = n // gs, n % gs
     per_step = 3 if symplectic else 2
     assert c1.value - c0.value == per_step * n + graphs + (1 if loose else 0)
     ops = oracle.blocked_from_workload(w)
