@@ -228,8 +228,8 @@ int32_t dtb_get_stream(dtb_ctx* ctx, void** stream);
 int32_t dtb_sync(dtb_ctx* ctx);
 
 /* Kernel launches issued per step by dtb_run (for launch accounting); the diagnostics
- * reduction adds one launch per sequence of steps (a graph replay, or up to 16 steps run
- * outside one). */
+ * reduction adds one launch per sequence of steps (a graph replay, or up to a graph's length
+ * of steps run outside one). */
 int32_t dtb_launches_per_step(dtb_ctx* ctx, int32_t* n);
 /* Kernel launches the context's step functions (dtb_step, dtb_step_io, dtb_run, dtb_solve) have
  * issued so far, kernels replayed in graphs included. No counterpart in the reference. */
